@@ -1,0 +1,186 @@
+"""ctypes bindings of the CPU checker library (oracle/liboracle.so).
+
+Test infrastructure only: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py, never by the gtfock_b200 package.  Each wrapper
+names the reference function its C counterpart restates (see oracle/oracle.h).
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+def build():
+    """Compile liboracle.so with oracle/Makefile (gcc only, no GPU)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        vp, ip, dp, i, d = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), \
+            ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_double
+        L.CInt_createBasisSet.argtypes = [ctypes.POINTER(vp)]
+        L.CInt_loadBasisSet.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p]
+        L.CInt_destroyBasisSet.argtypes = [vp]
+        for name in ("CInt_getNumShells", "CInt_getNumFuncs", "CInt_getNumAtoms",
+                     "CInt_getNumOccOrb", "CInt_getMaxShellDim"):
+            getattr(L, name).argtypes = [vp]
+            getattr(L, name).restype = i
+        L.CInt_getNucEnergy.argtypes = [vp]
+        L.CInt_getNucEnergy.restype = d
+        L.CInt_getShellDim.argtypes = [vp, i]
+        L.CInt_getFuncStartInd.argtypes = [vp, i]
+        L.CInt_createERD.argtypes = [vp, ctypes.POINTER(vp), i]
+        L.CInt_destroyERD.argtypes = [vp]
+        L.CInt_computeShellQuartet.argtypes = [vp, vp, i, i, i, i, i,
+                                               ctypes.POINTER(dp), ip]
+        L.CInt_createOED.argtypes = [vp, ctypes.POINTER(vp)]
+        L.CInt_destroyOED.argtypes = [vp]
+        for name in ("CInt_computePairOvl", "CInt_computePairKin",
+                     "CInt_computePairPot", "CInt_computePairCoreH"):
+            getattr(L, name).argtypes = [vp, vp, i, i, ctypes.POINTER(dp), ip]
+        L.or_screening.argtypes = [vp, d, i, ctypes.POINTER(ip), ctypes.POINTER(ip),
+                                   ctypes.POINTER(ip), ctypes.POINTER(dp), ip, dp]
+        L.or_fock_build.argtypes = [vp, d, i, ip, ip, ip, dp, dp, dp, dp, dp]
+        L.or_one_electron.argtypes = [vp, dp, dp, dp]
+        L.or_purification.argtypes = [i, i, dp, dp, dp]
+        L.or_scf.argtypes = [vp, d, i, i, dp, dp, dp]
+        L.or_free.argtypes = [vp]
+        L.or_set_blas_threads.argtypes = [i]
+        _LIB = L
+    return _LIB
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+class Basis:
+    """A CInt basis set loaded by the product's parser (basis.c) into the
+    checker library."""
+
+    def __init__(self, gbs, xyz):
+        L = lib()
+        self.h = ctypes.c_void_p()
+        L.CInt_createBasisSet(ctypes.byref(self.h))
+        st = L.CInt_loadBasisSet(self.h, gbs.encode(), xyz.encode())
+        if st != 0:
+            raise RuntimeError("CInt_loadBasisSet failed (%d) for %s / %s" % (st, gbs, xyz))
+        self.nbf = L.CInt_getNumFuncs(self.h)
+        self.nshells = L.CInt_getNumShells(self.h)
+        self.natoms = L.CInt_getNumAtoms(self.h)
+        self.nocc = L.CInt_getNumOccOrb(self.h)
+        self.enuc = L.CInt_getNucEnergy(self.h)
+
+    def __del__(self):
+        try:
+            lib().CInt_destroyBasisSet(self.h)
+        except Exception:
+            pass
+
+    def shell_dim(self, s):
+        return lib().CInt_getShellDim(self.h, s)
+
+    def func_start(self, s):
+        return lib().CInt_getFuncStartInd(self.h, s)
+
+
+def shell_quartet(basis, A, B, C, D):
+    """(AB|CD) block from the oracle engine, shape (dA,dB,dC,dD)."""
+    L = lib()
+    erd = ctypes.c_void_p()
+    L.CInt_createERD(basis.h, ctypes.byref(erd), 1)
+    ptr = ctypes.POINTER(ctypes.c_double)()
+    n = ctypes.c_int()
+    L.CInt_computeShellQuartet(basis.h, erd, 0, A, B, C, D, ctypes.byref(ptr), ctypes.byref(n))
+    dims = [basis.shell_dim(s) for s in (A, B, C, D)]
+    out = np.ctypeslib.as_array(ptr, shape=(n.value,)).copy()
+    L.CInt_destroyERD(erd)
+    # first index fastest -> reshape in Fortran order
+    return out.reshape(dims, order="F")
+
+
+def screening(basis, tol, nthreads=os.cpu_count()):
+    """pfock/screening.c:15-180 -> (shellptr, shellid, shellrid, shellvalue, maxvalue)."""
+    L = lib()
+    sp, si, sr = (ctypes.POINTER(ctypes.c_int)() for _ in range(3))
+    sv = ctypes.POINTER(ctypes.c_double)()
+    nnz = ctypes.c_int()
+    mx = ctypes.c_double()
+    st = L.or_screening(basis.h, tol, nthreads, ctypes.byref(sp), ctypes.byref(si),
+                        ctypes.byref(sr), ctypes.byref(sv), ctypes.byref(nnz), ctypes.byref(mx))
+    if st != 0:
+        raise RuntimeError("or_screening failed")
+    n = nnz.value
+    res = (np.ctypeslib.as_array(sp, shape=(basis.nshells + 1,)).copy(),
+           np.ctypeslib.as_array(si, shape=(max(n, 1),))[:n].copy(),
+           np.ctypeslib.as_array(sr, shape=(max(n, 1),))[:n].copy(),
+           np.ctypeslib.as_array(sv, shape=(max(n, 1),))[:n].copy(),
+           mx.value)
+    for p in (sp, si, sr, sv):
+        L.or_free(ctypes.cast(p, ctypes.c_void_p))
+    return res
+
+
+def fock_build(basis, tol, D, scr=None, nthreads=os.cpu_count()):
+    """PFock_computeFock + getMat(F) restated: returns (F = 2J - K, usq, uitl)."""
+    L = lib()
+    if scr is None:
+        scr = screening(basis, tol, nthreads)
+    shellptr, shellid, shellrid, shellvalue, _ = scr
+    D = np.ascontiguousarray(D, dtype=np.float64)
+    F = np.zeros_like(D)
+    usq = ctypes.c_double()
+    uitl = ctypes.c_double()
+    sid = np.ascontiguousarray(shellid, dtype=np.int32)
+    srid = np.ascontiguousarray(shellrid, dtype=np.int32)
+    sval = np.ascontiguousarray(shellvalue, dtype=np.float64)
+    sptr = np.ascontiguousarray(shellptr, dtype=np.int32)
+    if sid.size == 0:
+        sid = np.zeros(1, np.int32); srid = np.zeros(1, np.int32); sval = np.zeros(1)
+    st = L.or_fock_build(basis.h, tol, nthreads, _ip(sptr), _ip(sid), _ip(srid), _dp(sval),
+                         _dp(D), _dp(F), ctypes.byref(usq), ctypes.byref(uitl))
+    if st != 0:
+        raise RuntimeError("or_fock_build failed")
+    return F, usq.value, uitl.value
+
+
+def one_electron(basis):
+    """(S, H, X) as PFock_createOvlMat / PFock_createCoreHMat produce them."""
+    n = basis.nbf
+    S = np.zeros((n, n)); H = np.zeros((n, n)); X = np.zeros((n, n))
+    lib().or_one_electron(basis.h, _dp(S), _dp(H), _dp(X))
+    return S, H, X
+
+
+def purification(nobtls, X, F_orth):
+    n = X.shape[0]
+    D = np.zeros((n, n))
+    it = lib().or_purification(n, nobtls, _dp(np.ascontiguousarray(X)),
+                               _dp(np.ascontiguousarray(F_orth)), _dp(D))
+    return D, it
+
+
+def scf(basis, tol, niters, nthreads=os.cpu_count()):
+    """pscf/scf.c main loop restated; returns (energies, F_last, D_last)."""
+    n = basis.nbf
+    e = np.zeros(niters)
+    F = np.zeros((n, n))
+    D = np.zeros((n, n))
+    it = lib().or_scf(basis.h, tol, niters, nthreads, _dp(e), _dp(F), _dp(D))
+    if it < 0:
+        raise RuntimeError("or_scf failed")
+    return e[:it], F, D
