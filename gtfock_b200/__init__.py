@@ -1,0 +1,301 @@
+"""gtfock_b200 -- GTFock's Fock-build and purification hot path on one B200.
+
+The product is the C-ABI library gtfock_b200/lib/libgtfock_b200.so (PFock,
+purif and CInt APIs, see include/*.h).  This module binds it with ctypes for
+tests, benchmarks and Python callers; it performs no computation itself and
+fails loudly when the library (or a CUDA device, for compute calls) is
+missing.
+
+    import gtfock_b200 as gb
+    basis = gb.BasisSet(gb.basis_file("cc-pvdz"), "mol.xyz")
+    pf = gb.PFock(basis, tolscr=1e-10)
+    pf.put_density(D); F = pf.compute_fock()
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from .molecules import basis_file  # noqa: F401
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libgtfock_b200.so")
+SCF_BIN = os.path.join(_HERE, "lib", "scf")
+
+MAT_D, MAT_F, MAT_J, MAT_K = 0, 1, 2, 3
+
+_lib = None
+
+_vp = ctypes.c_void_p
+_i = ctypes.c_int
+_d = ctypes.c_double
+_ip = ctypes.POINTER(ctypes.c_int)
+_dp = ctypes.POINTER(ctypes.c_double)
+_cp = ctypes.c_char_p
+
+
+class GtfError(RuntimeError):
+    pass
+
+
+def _sig(L, name, args, res=ctypes.c_int):
+    f = getattr(L, name)
+    f.argtypes = args
+    f.restype = res
+
+
+def load():
+    """Load libgtfock_b200.so (raises GtfError when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise GtfError("libgtfock_b200.so not built (%s); run __graft_entry__.build() "
+                       "or make -C gtfock_b200" % LIB_PATH)
+    L = ctypes.CDLL(LIB_PATH)
+    _sig(L, "CInt_createBasisSet", [ctypes.POINTER(_vp)])
+    _sig(L, "CInt_destroyBasisSet", [_vp])
+    _sig(L, "CInt_loadBasisSet", [_vp, _cp, _cp])
+    for n in ("CInt_getNumShells", "CInt_getNumFuncs", "CInt_getNumAtoms",
+              "CInt_getNumOccOrb", "CInt_getMaxShellDim", "CInt_getTotalCharge",
+              "CInt_getNneutral"):
+        _sig(L, n, [_vp])
+    _sig(L, "CInt_getNucEnergy", [_vp], _d)
+    _sig(L, "CInt_getShellDim", [_vp, _i])
+    _sig(L, "CInt_getFuncStartInd", [_vp, _i])
+    _sig(L, "CInt_packBasisSet", [_vp, ctypes.POINTER(_vp), _ip])
+    _sig(L, "CInt_unpackBasisSet", [_vp, _vp])
+    _sig(L, "PFock_create", [_vp, _i, _i, _i, _d, _i, _i, ctypes.POINTER(_vp)])
+    _sig(L, "PFock_destroy", [_vp])
+    _sig(L, "PFock_setNumDenMat", [_i, _vp])
+    _sig(L, "PFock_putDenMat", [_i, _i, _i, _i, _i, _dp, _i, _vp])
+    _sig(L, "PFock_fillDenMat", [_d, _i, _vp])
+    _sig(L, "PFock_commitDenMats", [_vp])
+    _sig(L, "PFock_sync", [_vp])
+    _sig(L, "PFock_getMat", [_vp, _i, _i, _i, _i, _i, _i, _i, _dp])
+    _sig(L, "PFock_computeFock", [_vp, _vp])
+    _sig(L, "PFock_createOvlMat", [_vp, _vp])
+    _sig(L, "PFock_destroyOvlMat", [_vp])
+    _sig(L, "PFock_getOvlMat", [_vp, _i, _i, _i, _i, _i, _dp])
+    _sig(L, "PFock_getOvlMat2", [_vp, _i, _i, _i, _i, _i, _dp])
+    _sig(L, "PFock_createCoreHMat", [_vp, _vp])
+    _sig(L, "PFock_destroyCoreHMat", [_vp])
+    _sig(L, "PFock_getCoreHMat", [_vp, _i, _i, _i, _i, _i, _dp])
+    _sig(L, "PFock_getMemorySize", [_vp, _dp])
+    _sig(L, "PFock_getStatistics", [_vp])
+    _sig(L, "create_purif", [_vp, _i, _i, _i], _vp)
+    _sig(L, "destroy_purif", [_vp], None)
+    _sig(L, "compute_purification", [_vp, _dp, _dp])
+    _sig(L, "compute_diis", [_vp, _vp, _dp, _dp, _i], None)
+    _sig(L, "gtf_pfock_counts", [_vp, _ip, _dp, _dp, _dp])
+    _sig(L, "gtf_pfock_screening", [_vp, _ip, _ip, _ip, _dp])
+    _sig(L, "gtf_pfock_timing", [_vp, _dp, _dp, _dp])
+    _sig(L, "gtf_pfock_set_precision", [_vp, _i, _d])
+    _sig(L, "gtf_scf_run", [_cp, _cp, _d, _i, _i, _dp, _dp])
+    _sig(L, "gtf_device_info", [_ip, _ip])
+    _lib = L
+    return L
+
+
+def device_info():
+    """(number of CUDA devices, compute capability of device 0 as 10*major+minor)."""
+    L = load()
+    n = ctypes.c_int()
+    cc = ctypes.c_int()
+    L.gtf_device_info(ctypes.byref(n), ctypes.byref(cc))
+    return n.value, cc.value
+
+
+def _dptr(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _iptr(a):
+    return a.ctypes.data_as(_ip)
+
+
+class BasisSet:
+    """CInt_createBasisSet + CInt_loadBasisSet (libcint/include/CInt.h:45-80)."""
+
+    def __init__(self, gbs, xyz):
+        L = load()
+        self.h = _vp()
+        L.CInt_createBasisSet(ctypes.byref(self.h))
+        st = L.CInt_loadBasisSet(self.h, gbs.encode(), xyz.encode())
+        if st != 0:
+            L.CInt_destroyBasisSet(self.h)
+            self.h = None
+            raise GtfError("CInt_loadBasisSet failed (status %d): %s, %s" % (st, gbs, xyz))
+        self.gbs, self.xyz = gbs, xyz
+        self.nbf = L.CInt_getNumFuncs(self.h)
+        self.nshells = L.CInt_getNumShells(self.h)
+        self.natoms = L.CInt_getNumAtoms(self.h)
+        self.nocc = L.CInt_getNumOccOrb(self.h)
+        self.enuc = L.CInt_getNucEnergy(self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None) is not None and _lib is not None:
+            _lib.CInt_destroyBasisSet(self.h)
+            self.h = None
+
+
+class PFock:
+    """The PFock engine (pfock/pfock.h:241-565) on the GPU."""
+
+    def __init__(self, basis, tolscr=1e-10, max_numdmat=1, symm=1, nprow=1, npcol=1, ntasks=4):
+        L = load()
+        self.basis = basis
+        self.h = _vp()
+        st = L.PFock_create(basis.h, nprow, npcol, ntasks, tolscr, max_numdmat, symm,
+                            ctypes.byref(self.h))
+        if st != 0:
+            self.h = None
+            raise GtfError("PFock_create failed (status %d)" % st)
+        self.nbf = basis.nbf
+        L.PFock_setNumDenMat(max_numdmat, self.h)
+
+    def close(self):
+        if getattr(self, "h", None) is not None and _lib is not None:
+            _lib.PFock_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def _check(self, st, what):
+        if st != 0:
+            raise GtfError("%s failed (status %d)" % (what, st))
+
+    def put_density(self, D, index=0):
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        n = self.nbf
+        self._check(load().PFock_putDenMat(0, n - 1, 0, n - 1, n, _dptr(D), index, self.h),
+                    "PFock_putDenMat")
+
+    def commit(self):
+        self._check(load().PFock_commitDenMats(self.h), "PFock_commitDenMats")
+
+    def compute(self):
+        self._check(load().PFock_computeFock(self.basis.h, self.h), "PFock_computeFock")
+
+    def get_mat(self, mtype=MAT_F, index=0):
+        n = self.nbf
+        out = np.zeros((n, n))
+        self._check(load().PFock_getMat(self.h, mtype, index, 0, n - 1, 0, n - 1, n, _dptr(out)),
+                    "PFock_getMat")
+        return out
+
+    def compute_fock(self, D):
+        """putDenMat + commitDenMats + computeFock + getMat(F), as pscf/scf.c:106-127."""
+        self.put_density(D)
+        self.commit()
+        self.compute()
+        return self.get_mat(MAT_F)
+
+    def counts(self):
+        L = load()
+        nnz = ctypes.c_int()
+        mx, usq, uitl = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        L.gtf_pfock_counts(self.h, ctypes.byref(nnz), ctypes.byref(mx), ctypes.byref(usq),
+                           ctypes.byref(uitl))
+        return {"nnz": nnz.value, "maxvalue": mx.value, "usq": usq.value, "uitl": uitl.value}
+
+    def screening(self):
+        c = self.counts()
+        nnz = c["nnz"]
+        sp = np.zeros(self.basis.nshells + 1, np.int32)
+        si = np.zeros(max(nnz, 1), np.int32)
+        sr = np.zeros(max(nnz, 1), np.int32)
+        sv = np.zeros(max(nnz, 1))
+        self._check(load().gtf_pfock_screening(self.h, _iptr(sp), _iptr(si), _iptr(sr), _dptr(sv)),
+                    "gtf_pfock_screening")
+        return sp, si[:nnz], sr[:nnz], sv[:nnz], c["maxvalue"]
+
+    def timing(self):
+        a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        load().gtf_pfock_timing(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+        return {"ms_total": a.value, "ms_eri": b.value, "eri_flops": c.value}
+
+    def set_precision(self, mode, fp32_cutoff=0.0):
+        self._check(load().gtf_pfock_set_precision(self.h, mode, fp32_cutoff),
+                    "gtf_pfock_set_precision")
+
+    def one_electron(self):
+        """(S, X, H) as PFock_createOvlMat/getOvlMat/getOvlMat2/createCoreHMat produce them."""
+        L = load()
+        n = self.nbf
+        S, X, H = np.zeros((n, n)), np.zeros((n, n)), np.zeros((n, n))
+        self._check(L.PFock_createOvlMat(self.h, self.basis.h), "PFock_createOvlMat")
+        L.PFock_getOvlMat(self.h, 0, n - 1, 0, n - 1, n, _dptr(S))
+        L.PFock_getOvlMat2(self.h, 0, n - 1, 0, n - 1, n, _dptr(X))
+        L.PFock_destroyOvlMat(self.h)
+        self._check(L.PFock_createCoreHMat(self.h, self.basis.h), "PFock_createCoreHMat")
+        L.PFock_getCoreHMat(self.h, 0, n - 1, 0, n - 1, n, _dptr(H))
+        L.PFock_destroyCoreHMat(self.h)
+        return S, X, H
+
+
+class Purif:
+    """create_purif / compute_diis / compute_purification (pscf/purif.h:78-86)."""
+
+    def __init__(self, basis):
+        L = load()
+        self.basis = basis
+        self.h = L.create_purif(basis.h, 1, 1, 1)
+        if not self.h:
+            raise GtfError("create_purif failed")
+        self.n = basis.nbf
+        # purif_t field offsets: S_block and X_block pointers (see include/purif.h)
+        self._struct = ctypes.cast(self.h, ctypes.POINTER(_PurifT)).contents
+
+    def close(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.destroy_purif(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def _block(self, name):
+        ptr = getattr(self._struct, name)
+        return np.ctypeslib.as_array(ptr, shape=(self.n, self.n))
+
+    def set_sx(self, S, X):
+        self._block("S_block")[:] = S
+        self._block("X_block")[:] = X
+
+    def diis(self, pfock, D, F, it):
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        F = np.ascontiguousarray(F, dtype=np.float64).copy()
+        load().compute_diis(pfock.h if pfock else None, self.h, _dptr(D), _dptr(F), it)
+        return F
+
+    def purify(self, F_orth):
+        F = np.ascontiguousarray(F_orth, dtype=np.float64).copy()
+        D = np.zeros((self.n, self.n))
+        it = load().compute_purification(self.h, _dptr(F), _dptr(D))
+        if it < 0:
+            raise GtfError("compute_purification failed")
+        return D, it
+
+
+class _PurifT(ctypes.Structure):
+    _fields_ = [("runpurif", ctypes.c_int), ("rundgemm", ctypes.c_int), ("nbf", ctypes.c_int),
+                ("nobtls", ctypes.c_int), ("np_purif", ctypes.c_int), ("nprow_purif", ctypes.c_int),
+                ("npcol_purif", ctypes.c_int), ("npgrd_purif", ctypes.c_int),
+                ("srow_purif", ctypes.c_int), ("scol_purif", ctypes.c_int),
+                ("nrows_purif", ctypes.c_int), ("ncols_purif", ctypes.c_int),
+                ("meshsize", ctypes.c_int), ("ldx", ctypes.c_int),
+                ("H_block", _dp), ("X_block", _dp), ("S_block", _dp), ("F_block", _dp),
+                ("D_block", _dp)]
+
+
+def scf_run(gbs, xyz, tolscr=1e-10, niters=10, device_resident=False):
+    """Native SCF loop of pscf/scf.c on the GPU (gtf_scf_run): returns
+    (energies per iteration, timings dict)."""
+    L = load()
+    e = np.zeros(niters)
+    t = np.zeros(4)
+    it = L.gtf_scf_run(gbs.encode(), xyz.encode(), tolscr, niters, 1 if device_resident else 0,
+                       _dptr(e), _dptr(t))
+    if it < 0:
+        raise GtfError("gtf_scf_run failed (%d)" % it)
+    return e[:it], {"fock_s": t[0], "diis_s": t[1], "purif_s": t[2], "total_s": t[3]}

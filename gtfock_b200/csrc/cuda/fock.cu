@@ -1,0 +1,1132 @@
+// fock.cu -- the PFock engine on one B200.
+//
+// Setup (PFock_create, pfock/pfock.c:801-997):
+//   * device Schwarz screening: one thread per shell pair evaluates the
+//     diagonal quartet (MN|MN) by Rys quadrature and keeps max |(mn|mn)|
+//     (pfock/screening.c:59-90); the global max and eta = tol^2/max follow
+//     pfock/screening.c:100,111;
+//   * the reference's CSR pair list (parity rule and signed values,
+//     pfock/screening.c:118-175) is built on the device by scan + scatter;
+//   * the same pairs, re-oriented so that L(a) >= L(b), are radix-sorted by
+//     angular class and by bound (descending) into the device pair list;
+//   * per class pair (bra class X >= ket class Y) and per bra pair, the
+//     number of ket pairs passing the quartet Schwarz test
+//     |v1 v2| >= tol^2 (pfock/fock_task.c:192) is a prefix of the sorted ket
+//     class (binary search); X == Y keeps ket <= bra so every unique quartet
+//     (pfock/fock_task.c:169-175) is visited once; 32 kets form one unit.
+// Build (PFock_computeFock, pfock/pfock.c:1274-1729):
+//   * D (spherical) -> Cartesian, Fj/Fk zeroed;
+//   * one persistent kernel per class pair: warps claim units from an
+//     atomic counter, each lane evaluates one quartet and the warp digests
+//     into Fj (Coulomb terms) and Fk (exchange terms) with FP64 atomics;
+//   * symmetrise (GA_Symmetrize) and transform back: F = J + K.
+#include <cub/cub.cuh>
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "gtf_cuda.h"
+#include "gtf_dev.cuh"
+
+
+#define NCLS 6
+#define NCLSPAIR 21
+
+static thread_local char g_errbuf[512];
+
+extern "C" const char *gtf_last_error(void) { return g_errbuf; }
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) {                                                          \
+            snprintf(g_errbuf, sizeof(g_errbuf), "%s:%d %s: %s", __FILE__, __LINE__, #call, \
+                     cudaGetErrorString(e_));                                             \
+            return GTF_ERR_CUDA;                                                          \
+        }                                                                                 \
+    } while (0)
+
+// pair class of (La, Lb), La >= Lb: ss=0 ps=1 pp=2 ds=3 dp=4 dd=5
+__host__ __device__ inline int pair_class(int la, int lb)
+{
+    if (la < lb) { int t = la; la = lb; lb = t; }
+    return la * (la + 1) / 2 + lb;
+}
+
+static const int k_cls_la[NCLS] = {0, 1, 1, 2, 2, 2};
+static const int k_cls_lb[NCLS] = {0, 0, 1, 0, 1, 2};
+
+struct ClassPairTask {
+    int X, Y;
+    int bra_start, nbra;
+    int ket_start, nketcls;
+    long long nunits;
+    double nquart;
+    int *d_nket;
+    long long *d_unit_prefix;
+};
+
+struct gtf_fock_dev {
+    int dev;
+    int nsm;
+    cudaStream_t stream;
+    // basis
+    int natoms, nshells, nbf, nbf_cart, nprims, pure, max_numdmat;
+    std::vector<int> h_sh_L, h_f_start, h_fc_start;
+    int *d_sh_L, *d_sh_nprim, *d_sh_pstart, *d_f_start, *d_fc_start, *d_sph2shell, *d_cart2shell, *d_Z;
+    double *d_sh_xyz, *d_alpha, *d_coef, *d_atom_xyz;
+    // screening
+    double tolscr, tolscr2, maxvalue;
+    int nnz;
+    double *d_sq;
+    int *d_shellptr, *d_shellid, *d_shellrid;
+    double *d_shellvalue;
+    // device pair list
+    int npairs;
+    int cls_start[NCLS + 1];
+    PairRec *d_pairs;
+    double *d_pair_v;
+    int nprimpairs;
+    double *d_pp;   // 5 * nprimpairs: p, Px, Py, Pz, K
+    ClassPairTask tasks[NCLSPAIR];
+    unsigned long long *d_counters;
+    double usq, uitl, eri_flops;
+    // matrices
+    double *d_D;     // [max_numdmat][nbf*nbf]
+    double *d_Dc;    // cart scratch
+    double *d_Fj, *d_Fk;  // cart accumulators
+    double *d_F, *d_J, *d_K;  // [max_numdmat][nbf*nbf] results
+    double *d_S, *d_X, *d_H;
+    double *d_host_stage;     // pinned staging for strided copies
+    size_t host_stage_bytes;
+    // timing
+    cudaEvent_t ev0, ev1, ev2, ev3;
+    double ms_total, ms_eri, ms_other;
+    int prec;
+    double fp32_cutoff;
+    size_t dev_bytes;
+};
+
+template <typename T>
+static int dalloc(gtf_fock_dev *f, T **p, size_t n)
+{
+    *p = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+    if (e != cudaSuccess) {
+        snprintf(g_errbuf, sizeof(g_errbuf), "cudaMalloc(%zu bytes): %s", n * sizeof(T),
+                 cudaGetErrorString(e));
+        return GTF_ERR_ALLOC;
+    }
+    f->dev_bytes += n * sizeof(T);
+    return 0;
+}
+
+#define DALLOC(ptr, n)                          \
+    do {                                        \
+        int r_ = dalloc(f, &(ptr), (size_t)(n)); \
+        if (r_) return r_;                      \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// spherical <-> Cartesian transforms (d shells only)
+// rows m = -2..2, cols xx, xy, xz, yy, yz, zz
+// ---------------------------------------------------------------------------
+__constant__ double c_sph_d[5][6] = {
+    {0.0, 1.7320508075688772, 0.0, 0.0, 0.0, 0.0},
+    {0.0, 0.0, 0.0, 0.0, 1.7320508075688772, 0.0},
+    {-0.5, 0.0, 0.0, -0.5, 0.0, 1.0},
+    {0.0, 0.0, 1.7320508075688772, 0.0, 0.0, 0.0},
+    {0.8660254037844386, 0.0, 0.0, -0.8660254037844386, 0.0, 0.0}};
+
+__device__ __forceinline__ double sph_coef(int L, int pure, int m, int c)
+{
+    if (pure && L == 2) return c_sph_d[m][c];
+    return (m == c) ? 1.0 : 0.0;
+}
+
+__device__ __forceinline__ int nsph_of(int L, int pure) { return (pure && L == 2) ? 5 : ncart(L); }
+
+// D_cart[i][j] = sum_{m,n} T[m][i] T[n][j] D[m][n]
+__global__ void k_d_to_cart(const double *__restrict__ D, double *__restrict__ Dc,
+                            const int *__restrict__ cart2shell, const int *__restrict__ sh_L,
+                            const int *__restrict__ f_start, const int *__restrict__ fc_start,
+                            int nbf, int nbfc, int pure)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y;
+    if (j >= nbfc) return;
+    const int si = cart2shell[i], sj = cart2shell[j];
+    const int ci = i - fc_start[si], cj = j - fc_start[sj];
+    const int Li = sh_L[si], Lj = sh_L[sj];
+    const int mi = nsph_of(Li, pure), mj = nsph_of(Lj, pure);
+    const int fi = f_start[si], fj = f_start[sj];
+    double v = 0.0;
+    for (int m = 0; m < mi; m++) {
+        const double tm = sph_coef(Li, pure, m, ci);
+        if (tm == 0.0) continue;
+        for (int n = 0; n < mj; n++) {
+            const double tn = sph_coef(Lj, pure, n, cj);
+            if (tn == 0.0) continue;
+            v += tm * tn * D[(size_t)(fi + m) * nbf + fj + n];
+        }
+    }
+    Dc[(size_t)i * nbfc + j] = v;
+}
+
+// J = T sym(Fj) T^T, K = T sym(Fk) T^T, F = J + K (pfock/pfock.c:1719-1726, 1161-1185)
+__global__ void k_f_to_sph(const double *__restrict__ Fj, const double *__restrict__ Fk,
+                           double *__restrict__ F, double *__restrict__ J, double *__restrict__ K,
+                           const int *__restrict__ sph2shell, const int *__restrict__ sh_L,
+                           const int *__restrict__ f_start, const int *__restrict__ fc_start,
+                           int nbf, int nbfc, int pure)
+{
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = blockIdx.y;
+    if (n >= nbf) return;
+    const int sm = sph2shell[m], sn = sph2shell[n];
+    const int cm = m - f_start[sm], cn = n - f_start[sn];
+    const int Lm = sh_L[sm], Ln = sh_L[sn];
+    const int fm = fc_start[sm], fn = fc_start[sn];
+    const int nm = ncart(Lm), nn = ncart(Ln);
+    double j = 0.0, k = 0.0;
+    for (int a = 0; a < nm; a++) {
+        const double ta = sph_coef(Lm, pure, cm, a);
+        if (ta == 0.0) continue;
+        for (int b = 0; b < nn; b++) {
+            const double tb = sph_coef(Ln, pure, cn, b);
+            if (tb == 0.0) continue;
+            const size_t ab = (size_t)(fm + a) * nbfc + fn + b;
+            const size_t ba = (size_t)(fn + b) * nbfc + fm + a;
+            j += ta * tb * (0.5 * (Fj[ab] + Fj[ba]));
+            k += ta * tb * (0.5 * (Fk[ab] + Fk[ba]));
+        }
+    }
+    const size_t o = (size_t)m * nbf + n;
+    J[o] = j;
+    K[o] = k;
+    F[o] = j + k;
+}
+
+// ---------------------------------------------------------------------------
+// screening
+// ---------------------------------------------------------------------------
+struct BasisDev {
+    const int *sh_L, *sh_nprim, *sh_pstart;
+    const double *sh_xyz, *alpha, *coef;
+    int nshells, pure;
+};
+
+// pair record and primitive-pair data of shell pair (a, b), L(a) >= L(b)
+__device__ __forceinline__ void make_pair(const BasisDev &b, int a, int bb, int off, int fa, int fb,
+                                          PairRec *__restrict__ pr, double *__restrict__ pp, size_t npp)
+{
+    PairRec r;
+    r.Ax = b.sh_xyz[3 * a];
+    r.Ay = b.sh_xyz[3 * a + 1];
+    r.Az = b.sh_xyz[3 * a + 2];
+    const double Bx = b.sh_xyz[3 * bb], By = b.sh_xyz[3 * bb + 1], Bz = b.sh_xyz[3 * bb + 2];
+    r.ABx = r.Ax - Bx;
+    r.ABy = r.Ay - By;
+    r.ABz = r.Az - Bz;
+    r.fa = fa;
+    r.fb = fb;
+    r.off = off;
+    const int na = b.sh_nprim[a], nb = b.sh_nprim[bb];
+    r.n = na * nb;
+    *pr = r;
+    const double r2 = r.ABx * r.ABx + r.ABy * r.ABy + r.ABz * r.ABz;
+    const int pa = b.sh_pstart[a], pb = b.sh_pstart[bb];
+    for (int i = 0; i < na; i++) {
+        for (int j = 0; j < nb; j++) {
+            const double al = b.alpha[pa + i], be = b.alpha[pb + j];
+            const double p = al + be, ip = 1.0 / p;
+            const size_t o = (size_t)off + i * nb + j;
+            pp[o] = p;
+            pp[npp + o] = (al * r.Ax + be * Bx) * ip;
+            pp[2 * npp + o] = (al * r.Ay + be * By) * ip;
+            pp[3 * npp + o] = (al * r.Az + be * Bz) * ip;
+            pp[4 * npp + o] = GTF_PAIR_PREF * b.coef[pa + i] * b.coef[pb + j] * exp(-al * be * ip * r2) * ip;
+        }
+    }
+}
+
+// pair data of every shell pair M >= N of one class (screening pass)
+__global__ void k_screen_prep(BasisDev b, const int2 *__restrict__ mn, const int *__restrict__ off, int n,
+                              PairRec *__restrict__ pairs, double *__restrict__ pp, size_t npp)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int M = mn[t].x, N = mn[t].y;
+    const int a = (b.sh_L[M] >= b.sh_L[N]) ? M : N;
+    const int bb = (a == M) ? N : M;
+    make_pair(b, a, bb, off[t], 0, 0, pairs + t, pp, npp);
+}
+
+// max |(mn|mn)| over the diagonal of (MN|MN) in the basis's own functions
+// (pfock/screening.c:59-90), for the pairs of one class
+template <int LA, int LB>
+__global__ void __launch_bounds__(64) k_screen(const PairRec *__restrict__ pairs, PrimPairs pp,
+                                               const int2 *__restrict__ mn, int n, int ns, int pure,
+                                               double *__restrict__ sq, unsigned long long *__restrict__ gmax)
+{
+    constexpr int NA = ncart(LA), NB = ncart(LB);
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const PairRec pr = pairs[t];
+    PPStored src{pp};
+    double acc[NA * NB * NA * NB];
+#pragma unroll
+    for (int k = 0; k < NA * NB * NA * NB; k++) acc[k] = 0.0;
+    eri_accumulate<LA, LB, LA, LB>(src, pr, src, pr, acc);
+    const int sa = (pure && LA == 2) ? 5 : NA;
+    const int sb = (pure && LB == 2) ? 5 : NB;
+    double mx = 0.0;
+    for (int m = 0; m < sa; m++) {
+        for (int n2 = 0; n2 < sb; n2++) {
+            double s = 0.0;
+            for (int i = 0; i < NA; i++) {
+                const double ti = sph_coef(LA, pure, m, i);
+                if (ti == 0.0) continue;
+                for (int k = 0; k < NA; k++) {
+                    const double tk = sph_coef(LA, pure, m, k);
+                    if (tk == 0.0) continue;
+                    for (int j = 0; j < NB; j++) {
+                        const double tj = sph_coef(LB, pure, n2, j);
+                        if (tj == 0.0) continue;
+                        for (int l = 0; l < NB; l++) {
+                            const double tl = sph_coef(LB, pure, n2, l);
+                            if (tl == 0.0) continue;
+                            s += ti * tj * tk * tl * acc[i + NA * (j + NB * (k + NA * l))];
+                        }
+                    }
+                }
+            }
+            if (fabs(s) > mx) mx = fabs(s);
+        }
+    }
+    const int M = mn[t].x, N = mn[t].y;
+    sq[(size_t)M * ns + N] = mx;
+    sq[(size_t)N * ns + M] = mx;
+    atomicMax(gmax, (unsigned long long)__double_as_longlong(mx));
+}
+
+static int launch_screen(int cls, const PairRec *pairs, PrimPairs pp, const int2 *mn, int n, int ns, int pure,
+                         double *sq, unsigned long long *gmax, cudaStream_t st)
+{
+    const unsigned g = (unsigned)((n + 63) / 64);
+    switch (cls) {
+        case 0: k_screen<0, 0><<<g, 64, 0, st>>>(pairs, pp, mn, n, ns, pure, sq, gmax); break;
+        case 1: k_screen<1, 0><<<g, 64, 0, st>>>(pairs, pp, mn, n, ns, pure, sq, gmax); break;
+        case 2: k_screen<1, 1><<<g, 64, 0, st>>>(pairs, pp, mn, n, ns, pure, sq, gmax); break;
+        case 3: k_screen<2, 0><<<g, 64, 0, st>>>(pairs, pp, mn, n, ns, pure, sq, gmax); break;
+        case 4: k_screen<2, 1><<<g, 64, 0, st>>>(pairs, pp, mn, n, ns, pure, sq, gmax); break;
+        case 5: k_screen<2, 2><<<g, 64, 0, st>>>(pairs, pp, mn, n, ns, pure, sq, gmax); break;
+    }
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+// keep flag per (M, N): value > eta and the parity rule (pfock/screening.c:127-133)
+__global__ void k_csr_flags(const double *__restrict__ sq, int ns, double eta, int *__restrict__ flags)
+{
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (long long)ns * ns) return;
+    const int M = (int)(e / ns), N = (int)(e % ns);
+    int keep = sq[e] > eta;
+    if ((M > N && (M + N) % 2 == 1) || (M < N && (M + N) % 2 == 0)) keep = 0;
+    flags[e] = keep;
+}
+
+__global__ void k_csr_scatter(const double *__restrict__ sq, const int *__restrict__ flags,
+                              const int *__restrict__ pos, int ns, int *__restrict__ shellid,
+                              int *__restrict__ shellrid, double *__restrict__ shellvalue,
+                              int *__restrict__ shellptr)
+{
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n2 = (long long)ns * ns;
+    if (e >= n2) return;
+    const int M = (int)(e / ns), N = (int)(e % ns);
+    if (N == 0) shellptr[M] = pos[e];
+    if (e == n2 - 1) shellptr[ns] = pos[e] + flags[e];
+    if (!flags[e]) return;
+    const int k = pos[e];
+    const double v = sq[e];
+    shellid[k] = N;
+    shellrid[k] = M;
+    shellvalue[k] = (M == N) ? v : -v;
+}
+
+__global__ void k_sort_keys(const double *__restrict__ shellvalue, const int *__restrict__ shellid,
+                            const int *__restrict__ shellrid, const int *__restrict__ sh_L, int nnz,
+                            unsigned long long *__restrict__ kval, int *__restrict__ kcls,
+                            int *__restrict__ idx)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nnz) return;
+    const double v = fabs(shellvalue[k]);
+    kval[k] = ~(unsigned long long)__double_as_longlong(v);  // descending by value
+    kcls[k] = pair_class(sh_L[shellrid[k]], sh_L[shellid[k]]);
+    idx[k] = k;
+}
+
+__global__ void k_gather_cls(const int *__restrict__ idx, const int *__restrict__ shellid,
+                             const int *__restrict__ shellrid, const int *__restrict__ sh_L, int nnz,
+                             int *__restrict__ kcls)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nnz) return;
+    const int k = idx[s];
+    kcls[s] = pair_class(sh_L[shellrid[k]], sh_L[shellid[k]]);
+}
+
+__global__ void k_build_pairs(const int *__restrict__ idx, const int *__restrict__ shellid,
+                              const int *__restrict__ shellrid, const double *__restrict__ shellvalue,
+                              BasisDev b, const int *__restrict__ fc_start, int nnz,
+                              PairRec *__restrict__ pairs, double *__restrict__ pair_v,
+                              int *__restrict__ pair_n)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nnz) return;
+    const int k = idx[s];
+    const int M = shellrid[k], N = shellid[k];
+    const int a = (b.sh_L[M] >= b.sh_L[N]) ? M : N;
+    const int bb = (a == M) ? N : M;
+    PairRec r;
+    r.Ax = b.sh_xyz[3 * a];
+    r.Ay = b.sh_xyz[3 * a + 1];
+    r.Az = b.sh_xyz[3 * a + 2];
+    r.ABx = r.Ax - b.sh_xyz[3 * bb];
+    r.ABy = r.Ay - b.sh_xyz[3 * bb + 1];
+    r.ABz = r.Az - b.sh_xyz[3 * bb + 2];
+    r.fa = fc_start[a];
+    r.fb = fc_start[bb];
+    r.off = 0;
+    r.n = b.sh_nprim[a] * b.sh_nprim[bb];
+    pairs[s] = r;
+    pair_v[s] = fabs(shellvalue[k]);
+    pair_n[s] = r.n;
+}
+
+__global__ void k_fill_primpairs(PairRec *__restrict__ pairs, const int *__restrict__ idx,
+                                 const int *__restrict__ shellid, const int *__restrict__ shellrid,
+                                 const int *__restrict__ pair_off, BasisDev b, int npairs, double *pp,
+                                 int npp)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= npairs) return;
+    const int k = idx[s];
+    const int M = shellrid[k], N = shellid[k];
+    const int a = (b.sh_L[M] >= b.sh_L[N]) ? M : N;
+    const int bb = (a == M) ? N : M;
+    const int off = pair_off[s];
+    pairs[s].off = off;
+    const double Ax = b.sh_xyz[3 * a], Ay = b.sh_xyz[3 * a + 1], Az = b.sh_xyz[3 * a + 2];
+    const double Bx = b.sh_xyz[3 * bb], By = b.sh_xyz[3 * bb + 1], Bz = b.sh_xyz[3 * bb + 2];
+    const double r2 = (Ax - Bx) * (Ax - Bx) + (Ay - By) * (Ay - By) + (Az - Bz) * (Az - Bz);
+    const int na = b.sh_nprim[a], nb = b.sh_nprim[bb];
+    const int pa = b.sh_pstart[a], pb = b.sh_pstart[bb];
+    for (int i = 0; i < na; i++) {
+        for (int j = 0; j < nb; j++) {
+            const double al = b.alpha[pa + i], be = b.alpha[pb + j];
+            const double p = al + be, ip = 1.0 / p;
+            const int o = off + i * nb + j;
+            pp[o] = p;
+            pp[npp + o] = (al * Ax + be * Bx) * ip;
+            pp[2 * npp + o] = (al * Ay + be * By) * ip;
+            pp[3 * npp + o] = (al * Az + be * Bz) * ip;
+            pp[4 * npp + o] = GTF_PAIR_PREF * b.coef[pa + i] * b.coef[pb + j] * exp(-al * be * ip * r2) * ip;
+        }
+    }
+}
+
+// number of ket pairs of the ket class that pass v_bra * v_ket >= tol2
+// (pfock/fock_task.c:192); the ket class is sorted by value, descending
+__global__ void k_count_kets(const double *__restrict__ pair_v, int bra_start, int nbra, int ket_start,
+                             int nketcls, int same, double tol2, int *__restrict__ nket,
+                             long long *__restrict__ units)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > nbra) return;
+    if (i == nbra) {
+        units[nbra] = 0;
+        return;
+    }
+    const double v = pair_v[bra_start + i];
+    int lo = 0, hi = nketcls;  // count = first index failing the test
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (fabs(v * pair_v[ket_start + mid]) >= tol2) lo = mid + 1;
+        else hi = mid;
+    }
+    int c = lo;
+    if (same && c > i + 1) c = i + 1;
+    nket[i] = c;
+    units[i] = (c + 31) / 32;
+}
+
+// the Fock kernels live in fock_kernel.cuh, instantiated across several
+// translation units (fock_cls_*.cu) so that they compile in parallel
+#include "fock_kernel.cuh"
+
+typedef int (*fock_group_launch_t)(int la, int lb, int lc, int ld, const FockLaunch &a, cudaStream_t st);
+extern fock_group_launch_t gtf_fock_groups[];
+extern const int gtf_fock_ngroups;
+
+static int launch_fock(int X, int Y, const FockLaunch &a, cudaStream_t st)
+{
+    for (int g = 0; g < gtf_fock_ngroups; g++) {
+        int r = gtf_fock_groups[g](k_cls_la[X], k_cls_lb[X], k_cls_la[Y], k_cls_lb[Y], a, st);
+        if (r != 1) return r;  // 0 launched, <0 error
+    }
+    return GTF_ERR_INVALID;
+}
+
+// Rys-model FLOPs of one quartet of a class (normalisation used for the roofline):
+// K [30 n_r + 12 n_r (la+lb+1)(lc+ld+1) + 3 n_r Nc] + 2 K Nc + 12 Ns
+static double class_flops_per_prim(int X, int Y, double *contract_part)
+{
+    const int la = k_cls_la[X], lb = k_cls_lb[X], lc = k_cls_la[Y], ld = k_cls_lb[Y];
+    const int nr = (la + lb + lc + ld) / 2 + 1;
+    const double nc = (double)ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
+    *contract_part = 2.0 * nc;
+    return 30.0 * nr + 12.0 * nr * (la + lb + 1) * (lc + ld + 1) + 3.0 * nr * nc;
+}
+
+// ---------------------------------------------------------------------------
+// host API
+// ---------------------------------------------------------------------------
+// device, stream, events and the basis arrays (shared by the Fock engine and
+// the basis-only context of the per-quartet CInt entry points)
+static int upload_basis(gtf_fock_dev *f, const gtf_basis_view_t *b)
+{
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        snprintf(g_errbuf, sizeof(g_errbuf), "no CUDA device visible");
+        return GTF_ERR_NODEVICE;
+    }
+    if (b->nshells <= 0) return GTF_ERR_INVALID;
+    CK(cudaGetDevice(&f->dev));
+    CK(cudaDeviceGetAttribute(&f->nsm, cudaDevAttrMultiProcessorCount, f->dev));
+    CK(cudaStreamCreateWithFlags(&f->stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&f->ev0));
+    CK(cudaEventCreate(&f->ev1));
+    CK(cudaEventCreate(&f->ev2));
+    CK(cudaEventCreate(&f->ev3));
+    f->natoms = b->natoms;
+    f->nshells = b->nshells;
+    f->nbf = b->nbf;
+    f->nbf_cart = b->nbf_cart;
+    f->nprims = b->nprims;
+    f->pure = b->pure;
+    const int ns = b->nshells;
+    cudaStream_t st = f->stream;
+    f->h_sh_L.assign(b->sh_L, b->sh_L + ns);
+    f->h_f_start.assign(b->f_start, b->f_start + ns + 1);
+    f->h_fc_start.assign(b->fc_start, b->fc_start + ns + 1);
+    std::vector<double> sh_xyz(3 * ns);
+    for (int s = 0; s < ns; s++)
+        for (int k = 0; k < 3; k++) sh_xyz[3 * s + k] = b->xyz[3 * b->sh_atom[s] + k];
+    std::vector<int> sph2shell(b->nbf), cart2shell(b->nbf_cart);
+    for (int s = 0; s < ns; s++) {
+        for (int k = b->f_start[s]; k < b->f_start[s + 1]; k++) sph2shell[k] = s;
+        for (int k = b->fc_start[s]; k < b->fc_start[s + 1]; k++) cart2shell[k] = s;
+    }
+    DALLOC(f->d_sh_L, ns);
+    DALLOC(f->d_sh_nprim, ns);
+    DALLOC(f->d_sh_pstart, ns);
+    DALLOC(f->d_f_start, ns + 1);
+    DALLOC(f->d_fc_start, ns + 1);
+    DALLOC(f->d_sph2shell, b->nbf);
+    DALLOC(f->d_cart2shell, b->nbf_cart);
+    DALLOC(f->d_Z, b->natoms);
+    DALLOC(f->d_sh_xyz, 3 * ns);
+    DALLOC(f->d_alpha, b->nprims);
+    DALLOC(f->d_coef, b->nprims);
+    DALLOC(f->d_atom_xyz, 3 * b->natoms);
+    CK(cudaMemcpyAsync(f->d_sh_L, b->sh_L, sizeof(int) * ns, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(f->d_sh_nprim, b->sh_nprim, sizeof(int) * ns, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(f->d_sh_pstart, b->sh_pstart, sizeof(int) * ns, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(f->d_f_start, b->f_start, sizeof(int) * (ns + 1), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(f->d_fc_start, b->fc_start, sizeof(int) * (ns + 1), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(f->d_sph2shell, sph2shell.data(), sizeof(int) * b->nbf, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(f->d_cart2shell, cart2shell.data(), sizeof(int) * b->nbf_cart,
+                       cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(f->d_Z, b->Z, sizeof(int) * b->natoms, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(f->d_sh_xyz, sh_xyz.data(), sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(f->d_alpha, b->alpha, sizeof(double) * b->nprims, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(f->d_coef, b->coef, sizeof(double) * b->nprims, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(f->d_atom_xyz, b->xyz, sizeof(double) * 3 * b->natoms, cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    return GTF_OK;
+}
+
+// basis-only context: no screening, no Fock buffers
+extern "C" int gtf_basis_dev_create(const gtf_basis_view_t *b, gtf_fock_dev_t **out)
+{
+    gtf_fock_dev *f = new gtf_fock_dev();
+    memset(f->tasks, 0, sizeof(f->tasks));
+    f->max_numdmat = 0;
+    *out = f;
+    return upload_basis(f, b);
+}
+
+extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max_numdmat,
+                               gtf_fock_dev_t **out)
+{
+    *out = nullptr;
+    if (b->nshells <= 0 || tolscr < 0.0 || max_numdmat <= 0) return GTF_ERR_INVALID;
+    gtf_fock_dev *f = new gtf_fock_dev();
+    memset(f->tasks, 0, sizeof(f->tasks));
+    *out = f;
+    int r = upload_basis(f, b);
+    if (r) return r;
+    f->max_numdmat = max_numdmat;
+    f->tolscr = tolscr;
+    f->tolscr2 = tolscr * tolscr;
+    f->prec = GTF_PREC_FP64;
+    f->fp32_cutoff = 0.0;
+    const int ns = b->nshells;
+    cudaStream_t st = f->stream;
+    BasisDev bd{f->d_sh_L, f->d_sh_nprim, f->d_sh_pstart, f->d_sh_xyz, f->d_alpha, f->d_coef, ns, b->pure};
+
+    // ---- Schwarz values of every shell pair (M >= N), one class at a time ----
+    const size_t n2 = (size_t)ns * ns;
+    DALLOC(f->d_sq, n2);
+    unsigned long long *d_gmax;
+    DALLOC(d_gmax, 1);
+    CK(cudaMemsetAsync(d_gmax, 0, sizeof(unsigned long long), st));
+    {
+        std::vector<int2> mn[NCLS];
+        std::vector<int> off[NCLS];
+        size_t npp_cls[NCLS] = {0, 0, 0, 0, 0, 0};
+        for (int M = 0; M < ns; M++) {
+            for (int N = 0; N <= M; N++) {
+                const int c = pair_class(b->sh_L[M], b->sh_L[N]);
+                mn[c].push_back(make_int2(M, N));
+                off[c].push_back((int)npp_cls[c]);
+                npp_cls[c] += (size_t)b->sh_nprim[M] * b->sh_nprim[N];
+            }
+        }
+        for (int c = 0; c < NCLS; c++) {
+            const int n = (int)mn[c].size();
+            if (n == 0) continue;
+            int2 *d_mn;
+            int *d_off;
+            PairRec *d_pr;
+            double *d_pp;
+            CK(cudaMalloc(&d_mn, sizeof(int2) * n));
+            CK(cudaMalloc(&d_off, sizeof(int) * n));
+            CK(cudaMalloc(&d_pr, sizeof(PairRec) * n));
+            CK(cudaMalloc(&d_pp, sizeof(double) * 5 * npp_cls[c]));
+            CK(cudaMemcpyAsync(d_mn, mn[c].data(), sizeof(int2) * n, cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(d_off, off[c].data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
+            k_screen_prep<<<(n + 127) / 128, 128, 0, st>>>(bd, d_mn, d_off, n, d_pr, d_pp, npp_cls[c]);
+            CK(cudaGetLastError());
+            const size_t np_ = npp_cls[c];
+            PrimPairs pps{d_pp, d_pp + np_, d_pp + 2 * np_, d_pp + 3 * np_, d_pp + 4 * np_};
+            if (launch_screen(c, d_pr, pps, d_mn, n, ns, b->pure, f->d_sq, d_gmax, st) != 0)
+                CK(cudaGetLastError());
+            CK(cudaStreamSynchronize(st));
+            cudaFree(d_mn);
+            cudaFree(d_off);
+            cudaFree(d_pr);
+            cudaFree(d_pp);
+        }
+    }
+    unsigned long long hmax = 0;
+    CK(cudaMemcpyAsync(&hmax, d_gmax, sizeof(hmax), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    memcpy(&f->maxvalue, &hmax, sizeof(double));
+    cudaFree(d_gmax);
+    f->dev_bytes -= sizeof(unsigned long long);
+    const double eta = f->tolscr2 / f->maxvalue;
+
+    // ---- reference CSR list (row-major scan + scatter) ----
+    int *d_flags, *d_pos;
+    DALLOC(d_flags, n2);
+    DALLOC(d_pos, n2);
+    const unsigned g2 = (unsigned)((n2 + 255) / 256);
+    k_csr_flags<<<g2, 256, 0, st>>>(f->d_sq, ns, eta, d_flags);
+    CK(cudaGetLastError());
+    size_t tmp_bytes = 0;
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, d_flags, d_pos, (int)n2, st));
+    void *d_tmp = nullptr;
+    size_t tmp_cap = tmp_bytes;
+    CK(cudaMalloc(&d_tmp, tmp_cap));
+    CK(cub::DeviceScan::ExclusiveSum(d_tmp, tmp_bytes, d_flags, d_pos, (int)n2, st));
+    int last_pos = 0, last_flag = 0;
+    CK(cudaMemcpyAsync(&last_pos, d_pos + n2 - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&last_flag, d_flags + n2 - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const int nnz = last_pos + last_flag;
+    f->nnz = nnz;
+    DALLOC(f->d_shellptr, ns + 1);
+    DALLOC(f->d_shellid, nnz);
+    DALLOC(f->d_shellrid, nnz);
+    DALLOC(f->d_shellvalue, nnz);
+    k_csr_scatter<<<g2, 256, 0, st>>>(f->d_sq, d_flags, d_pos, ns, f->d_shellid, f->d_shellrid,
+                                      f->d_shellvalue, f->d_shellptr);
+    CK(cudaGetLastError());
+
+    // ---- device pair list: sort by class, then value descending ----
+    f->npairs = nnz;
+    unsigned long long *d_kval, *d_kval2;
+    int *d_kcls, *d_kcls2, *d_idx, *d_idx2, *d_pair_n, *d_pair_off;
+    DALLOC(d_kval, nnz);
+    DALLOC(d_kval2, nnz);
+    DALLOC(d_kcls, nnz);
+    DALLOC(d_kcls2, nnz);
+    DALLOC(d_idx, nnz);
+    DALLOC(d_idx2, nnz);
+    DALLOC(d_pair_n, nnz + 1);
+    DALLOC(d_pair_off, nnz + 1);
+    const unsigned gp = (unsigned)((nnz + 255) / 256 > 0 ? (nnz + 255) / 256 : 1);
+    if (nnz > 0) {
+        k_sort_keys<<<gp, 256, 0, st>>>(f->d_shellvalue, f->d_shellid, f->d_shellrid, f->d_sh_L, nnz,
+                                        d_kval, d_kcls, d_idx);
+        CK(cudaGetLastError());
+        size_t b1 = 0, b2 = 0;
+        CK(cub::DeviceRadixSort::SortPairs(nullptr, b1, d_kval, d_kval2, d_idx, d_idx2, nnz, 0, 64, st));
+        CK(cub::DeviceRadixSort::SortPairs(nullptr, b2, d_kcls, d_kcls2, d_idx2, d_idx, nnz, 0, 3, st));
+        size_t need = b1 > b2 ? b1 : b2;
+        if (need > tmp_cap) {
+            cudaFree(d_tmp);
+            tmp_cap = need;
+            CK(cudaMalloc(&d_tmp, tmp_cap));
+        }
+        b1 = tmp_cap;
+        CK(cub::DeviceRadixSort::SortPairs(d_tmp, b1, d_kval, d_kval2, d_idx, d_idx2, nnz, 0, 64, st));
+        k_gather_cls<<<gp, 256, 0, st>>>(d_idx2, f->d_shellid, f->d_shellrid, f->d_sh_L, nnz, d_kcls);
+        CK(cudaGetLastError());
+        b2 = tmp_cap;
+        CK(cub::DeviceRadixSort::SortPairs(d_tmp, b2, d_kcls, d_kcls2, d_idx2, d_idx, nnz, 0, 3, st));
+    }
+    DALLOC(f->d_pairs, nnz);
+    DALLOC(f->d_pair_v, nnz);
+    if (nnz > 0) {
+        k_build_pairs<<<gp, 256, 0, st>>>(d_idx, f->d_shellid, f->d_shellrid, f->d_shellvalue, bd,
+                                          f->d_fc_start, nnz, f->d_pairs, f->d_pair_v, d_pair_n);
+        CK(cudaGetLastError());
+    }
+    CK(cudaMemsetAsync(d_pair_n + nnz, 0, sizeof(int), st));
+    size_t b3 = 0;
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, b3, d_pair_n, d_pair_off, nnz + 1, st));
+    if (b3 > tmp_cap) {
+        cudaFree(d_tmp);
+        tmp_cap = b3;
+        CK(cudaMalloc(&d_tmp, tmp_cap));
+    }
+    b3 = tmp_cap;
+    CK(cub::DeviceScan::ExclusiveSum(d_tmp, b3, d_pair_n, d_pair_off, nnz + 1, st));
+    int npp = 0;
+    CK(cudaMemcpyAsync(&npp, d_pair_off + nnz, sizeof(int), cudaMemcpyDeviceToHost, st));
+    std::vector<int> cls_sorted(nnz > 0 ? nnz : 1);
+    if (nnz > 0)
+        CK(cudaMemcpyAsync(cls_sorted.data(), d_kcls2, sizeof(int) * nnz, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    f->nprimpairs = npp;
+    DALLOC(f->d_pp, 5 * (size_t)(npp > 0 ? npp : 1));
+    if (nnz > 0) {
+        k_fill_primpairs<<<gp, 256, 0, st>>>(f->d_pairs, d_idx, f->d_shellid, f->d_shellrid, d_pair_off, bd,
+                                             nnz, f->d_pp, npp);
+        CK(cudaGetLastError());
+    }
+    for (int c = 0; c <= NCLS; c++) f->cls_start[c] = nnz;
+    for (int s = nnz - 1; s >= 0; s--) f->cls_start[cls_sorted[s]] = s;
+    for (int c = NCLS - 1; c >= 0; c--)
+        if (f->cls_start[c] > f->cls_start[c + 1]) f->cls_start[c] = f->cls_start[c + 1];
+
+    // ---- task lists per class pair ----
+    f->usq = 0.0;
+    f->uitl = 0.0;
+    f->eri_flops = 0.0;
+    DALLOC(f->d_counters, NCLSPAIR);
+    int cp = 0;
+    for (int X = 0; X < NCLS; X++) {
+        for (int Y = 0; Y <= X; Y++, cp++) {
+            ClassPairTask &t = f->tasks[cp];
+            t.X = X;
+            t.Y = Y;
+            t.bra_start = f->cls_start[X];
+            t.nbra = f->cls_start[X + 1] - f->cls_start[X];
+            t.ket_start = f->cls_start[Y];
+            t.nketcls = f->cls_start[Y + 1] - f->cls_start[Y];
+            t.nunits = 0;
+            t.nquart = 0.0;
+            if (t.nbra == 0 || t.nketcls == 0) continue;
+            DALLOC(t.d_nket, t.nbra);
+            DALLOC(t.d_unit_prefix, t.nbra + 1);
+            long long *d_units;
+            CK(cudaMalloc(&d_units, sizeof(long long) * (t.nbra + 1)));
+            k_count_kets<<<(t.nbra + 1 + 255) / 256, 256, 0, st>>>(f->d_pair_v, t.bra_start, t.nbra,
+                                                                  t.ket_start, t.nketcls, X == Y,
+                                                                  f->tolscr2, t.d_nket, d_units);
+            CK(cudaGetLastError());
+            size_t b4 = 0;
+            CK(cub::DeviceScan::ExclusiveSum(nullptr, b4, d_units, t.d_unit_prefix, t.nbra + 1, st));
+            if (b4 > tmp_cap) {
+                cudaFree(d_tmp);
+                tmp_cap = b4;
+                CK(cudaMalloc(&d_tmp, tmp_cap));
+            }
+            b4 = tmp_cap;
+            CK(cub::DeviceScan::ExclusiveSum(d_tmp, b4, d_units, t.d_unit_prefix, t.nbra + 1, st));
+            std::vector<int> nk(t.nbra);
+            CK(cudaMemcpyAsync(&t.nunits, t.d_unit_prefix + t.nbra, sizeof(long long), cudaMemcpyDeviceToHost,
+                               st));
+            CK(cudaMemcpyAsync(nk.data(), t.d_nket, sizeof(int) * t.nbra, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            cudaFree(d_units);
+            double q = 0.0;
+            for (int i = 0; i < t.nbra; i++) q += nk[i];
+            t.nquart = q;
+            const int la = k_cls_la[X], lb = k_cls_lb[X], lc = k_cls_la[Y], ld = k_cls_lb[Y];
+            const double dims = (double)(b->pure ? (la == 2 ? 5 : ncart(la)) : ncart(la)) *
+                                (b->pure ? (lb == 2 ? 5 : ncart(lb)) : ncart(lb)) *
+                                (b->pure ? (lc == 2 ? 5 : ncart(lc)) : ncart(lc)) *
+                                (b->pure ? (ld == 2 ? 5 : ncart(ld)) : ncart(ld));
+            f->usq += q;
+            f->uitl += q * dims;
+        }
+    }
+    // Rys-model FLOPs per build: needs primitive counts per quartet, summed on the host
+    {
+        std::vector<PairRec> hp(nnz > 0 ? nnz : 1);
+        std::vector<double> hv(nnz > 0 ? nnz : 1);
+        if (nnz > 0) {
+            CK(cudaMemcpyAsync(hp.data(), f->d_pairs, sizeof(PairRec) * nnz, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+        }
+        double flops = 0.0;
+        for (int c2 = 0; c2 < NCLSPAIR; c2++) {
+            ClassPairTask &t = f->tasks[c2];
+            if (t.nunits == 0) continue;
+            std::vector<int> nk(t.nbra);
+            CK(cudaMemcpy(nk.data(), t.d_nket, sizeof(int) * t.nbra, cudaMemcpyDeviceToHost));
+            // prefix sums of ket primitive-pair counts
+            std::vector<double> kpre(t.nketcls + 1, 0.0);
+            for (int j = 0; j < t.nketcls; j++) kpre[j + 1] = kpre[j] + hp[t.ket_start + j].n;
+            double cpart;
+            const double per_prim = class_flops_per_prim(t.X, t.Y, &cpart);
+            const int la = k_cls_la[t.X], lb = k_cls_lb[t.X], lc = k_cls_la[t.Y], ld = k_cls_lb[t.Y];
+            const double ns_ = (double)(b->pure && la == 2 ? 5 : ncart(la)) * (b->pure && lb == 2 ? 5 : ncart(lb)) *
+                               (b->pure && lc == 2 ? 5 : ncart(lc)) * (b->pure && ld == 2 ? 5 : ncart(ld));
+            for (int i = 0; i < t.nbra; i++) {
+                const double kb = hp[t.bra_start + i].n;
+                const double kk = kpre[nk[i]];
+                flops += kb * kk * per_prim + (cpart + 12.0 * ns_) * nk[i];
+            }
+        }
+        f->eri_flops = flops;
+    }
+    cudaFree(d_tmp);
+    cudaFree(d_flags);
+    cudaFree(d_pos);
+    cudaFree(d_kval);
+    cudaFree(d_kval2);
+    cudaFree(d_kcls);
+    cudaFree(d_kcls2);
+    cudaFree(d_idx2);
+    cudaFree(d_pair_n);
+    cudaFree(d_pair_off);
+    cudaFree(d_idx);
+    f->dev_bytes -= n2 * 2 * sizeof(int) + (size_t)nnz * (2 * 8 + 4 * 4) + (size_t)(nnz + 1) * 8;
+
+    // ---- matrices ----
+    const size_t nn = (size_t)b->nbf * b->nbf, nnc = (size_t)b->nbf_cart * b->nbf_cart;
+    DALLOC(f->d_D, nn * max_numdmat);
+    DALLOC(f->d_F, nn * max_numdmat);
+    DALLOC(f->d_J, nn * max_numdmat);
+    DALLOC(f->d_K, nn * max_numdmat);
+    DALLOC(f->d_Dc, nnc);
+    DALLOC(f->d_Fj, nnc);
+    DALLOC(f->d_Fk, nnc);
+    CK(cudaMemsetAsync(f->d_D, 0, sizeof(double) * nn * max_numdmat, st));
+    CK(cudaMemsetAsync(f->d_F, 0, sizeof(double) * nn * max_numdmat, st));
+    CK(cudaMemsetAsync(f->d_J, 0, sizeof(double) * nn * max_numdmat, st));
+    CK(cudaMemsetAsync(f->d_K, 0, sizeof(double) * nn * max_numdmat, st));
+    f->host_stage_bytes = nn * sizeof(double);
+    CK(cudaMallocHost((void **)&f->d_host_stage, f->host_stage_bytes));
+    CK(cudaStreamSynchronize(st));
+    return GTF_OK;
+}
+
+extern "C" void gtf_fock_destroy(gtf_fock_dev_t *f)
+{
+    if (!f) return;
+    cudaStreamSynchronize(f->stream);
+    void *ptrs[] = {f->d_sh_L, f->d_sh_nprim, f->d_sh_pstart, f->d_f_start, f->d_fc_start, f->d_sph2shell,
+                    f->d_cart2shell, f->d_Z, f->d_sh_xyz, f->d_alpha, f->d_coef, f->d_atom_xyz, f->d_sq,
+                    f->d_shellptr, f->d_shellid, f->d_shellrid, f->d_shellvalue, f->d_pairs, f->d_pair_v,
+                    f->d_pp, f->d_counters, f->d_D, f->d_Dc, f->d_Fj, f->d_Fk, f->d_F, f->d_J, f->d_K,
+                    f->d_S, f->d_X, f->d_H};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    for (int c = 0; c < NCLSPAIR; c++) {
+        if (f->tasks[c].d_nket) cudaFree(f->tasks[c].d_nket);
+        if (f->tasks[c].d_unit_prefix) cudaFree(f->tasks[c].d_unit_prefix);
+    }
+    if (f->d_host_stage) cudaFreeHost(f->d_host_stage);
+    cudaEventDestroy(f->ev0);
+    cudaEventDestroy(f->ev1);
+    cudaEventDestroy(f->ev2);
+    cudaEventDestroy(f->ev3);
+    cudaStreamDestroy(f->stream);
+    delete f;
+}
+
+extern "C" int gtf_fock_screening_info(gtf_fock_dev_t *f, int *nnz, double *maxvalue, double *usq,
+                                       double *uitl)
+{
+    if (nnz) *nnz = f->nnz;
+    if (maxvalue) *maxvalue = f->maxvalue;
+    if (usq) *usq = f->usq;
+    if (uitl) *uitl = f->uitl;
+    return GTF_OK;
+}
+
+extern "C" int gtf_fock_get_csr(gtf_fock_dev_t *f, int *shellptr, int *shellid, int *shellrid,
+                                double *shellvalue)
+{
+    cudaStream_t st = f->stream;
+    if (shellptr)
+        CK(cudaMemcpyAsync(shellptr, f->d_shellptr, sizeof(int) * (f->nshells + 1), cudaMemcpyDeviceToHost, st));
+    if (f->nnz > 0) {
+        if (shellid) CK(cudaMemcpyAsync(shellid, f->d_shellid, sizeof(int) * f->nnz, cudaMemcpyDeviceToHost, st));
+        if (shellrid) CK(cudaMemcpyAsync(shellrid, f->d_shellrid, sizeof(int) * f->nnz, cudaMemcpyDeviceToHost, st));
+        if (shellvalue)
+            CK(cudaMemcpyAsync(shellvalue, f->d_shellvalue, sizeof(double) * f->nnz, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    return GTF_OK;
+}
+
+// strided host block <-> device full matrix
+static int put_block(gtf_fock_dev *f, double *dmat, int n, int r0, int r1, int c0, int c1, int stride,
+                     const double *host)
+{
+    if (r0 < 0 || c0 < 0 || r1 >= n || c1 >= n || r1 < r0 || c1 < c0) return GTF_ERR_INVALID;
+    const int nr = r1 - r0 + 1, nc = c1 - c0 + 1;
+    CK(cudaMemcpy2DAsync(dmat + (size_t)r0 * n + c0, sizeof(double) * n, host, sizeof(double) * stride,
+                         sizeof(double) * nc, nr, cudaMemcpyHostToDevice, f->stream));
+    CK(cudaStreamSynchronize(f->stream));
+    return GTF_OK;
+}
+
+static int get_block(gtf_fock_dev *f, const double *dmat, int n, int r0, int r1, int c0, int c1, int stride,
+                     double *host)
+{
+    if (r0 < 0 || c0 < 0 || r1 >= n || c1 >= n || r1 < r0 || c1 < c0) return GTF_ERR_INVALID;
+    const int nr = r1 - r0 + 1, nc = c1 - c0 + 1;
+    CK(cudaMemcpy2DAsync(host, sizeof(double) * stride, dmat + (size_t)r0 * n + c0, sizeof(double) * n,
+                         sizeof(double) * nc, nr, cudaMemcpyDeviceToHost, f->stream));
+    CK(cudaStreamSynchronize(f->stream));
+    return GTF_OK;
+}
+
+__global__ void k_fill(double *p, size_t n, double v)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+extern "C" int gtf_fock_fill_density(gtf_fock_dev_t *f, int index, double value)
+{
+    if (index < 0 || index >= f->max_numdmat) return GTF_ERR_INVALID;
+    const size_t nn = (size_t)f->nbf * f->nbf;
+    k_fill<<<(unsigned)((nn + 255) / 256), 256, 0, f->stream>>>(f->d_D + nn * index, nn, value);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(f->stream));
+    return GTF_OK;
+}
+
+extern "C" int gtf_fock_put_density(gtf_fock_dev_t *f, int index, int r0, int r1, int c0, int c1, int stride,
+                                    const double *host)
+{
+    if (index < 0 || index >= f->max_numdmat) return GTF_ERR_INVALID;
+    const size_t nn = (size_t)f->nbf * f->nbf;
+    return put_block(f, f->d_D + nn * index, f->nbf, r0, r1, c0, c1, stride, host);
+}
+
+extern "C" int gtf_fock_put_density_dev(gtf_fock_dev_t *f, int index, const double *dev)
+{
+    if (index < 0 || index >= f->max_numdmat) return GTF_ERR_INVALID;
+    const size_t nn = (size_t)f->nbf * f->nbf;
+    CK(cudaMemcpyAsync(f->d_D + nn * index, dev, sizeof(double) * nn, cudaMemcpyDeviceToDevice, f->stream));
+    return GTF_OK;
+}
+
+extern "C" int gtf_fock_set_precision(gtf_fock_dev_t *f, int prec, double fp32_cutoff)
+{
+    if (prec != GTF_PREC_FP64 && prec != GTF_PREC_MIXED) return GTF_ERR_INVALID;
+    f->prec = prec;
+    f->fp32_cutoff = fp32_cutoff;
+    return GTF_OK;
+}
+
+extern "C" int gtf_fock_compute(gtf_fock_dev_t *f, int numdmat)
+{
+    if (numdmat <= 0 || numdmat > f->max_numdmat) return GTF_ERR_INVALID;
+    cudaStream_t st = f->stream;
+    const int nbf = f->nbf, nbfc = f->nbf_cart;
+    const size_t nn = (size_t)nbf * nbf, nnc = (size_t)nbfc * nbfc;
+    const bool need_tr = f->pure && nbfc != nbf;
+    PrimPairs pp{f->d_pp, f->d_pp + f->nprimpairs, f->d_pp + 2 * (size_t)f->nprimpairs,
+                 f->d_pp + 3 * (size_t)f->nprimpairs, f->d_pp + 4 * (size_t)f->nprimpairs};
+    CK(cudaEventRecord(f->ev0, st));
+    float eri_ms_total = 0.0f;
+    for (int d = 0; d < numdmat; d++) {
+        const double *D = f->d_D + nn * d;
+        const double *Dc = D;
+        if (need_tr) {
+            dim3 g((nbfc + 127) / 128, nbfc);
+            k_d_to_cart<<<g, 128, 0, st>>>(D, f->d_Dc, f->d_cart2shell, f->d_sh_L, f->d_f_start,
+                                           f->d_fc_start, nbf, nbfc, f->pure);
+            CK(cudaGetLastError());
+            Dc = f->d_Dc;
+        }
+        CK(cudaMemsetAsync(f->d_Fj, 0, sizeof(double) * nnc, st));
+        CK(cudaMemsetAsync(f->d_Fk, 0, sizeof(double) * nnc, st));
+        CK(cudaMemsetAsync(f->d_counters, 0, sizeof(unsigned long long) * NCLSPAIR, st));
+        CK(cudaEventRecord(f->ev1, st));
+        for (int c = 0; c < NCLSPAIR; c++) {
+            ClassPairTask &t = f->tasks[c];
+            if (t.nunits == 0) continue;
+            FockLaunch a;
+            a.pairs = f->d_pairs;
+            a.pp = pp;
+            a.nket = t.d_nket;
+            a.unit_prefix = t.d_unit_prefix;
+            a.nbra = t.nbra;
+            a.nunits = t.nunits;
+            a.bra_start = t.bra_start;
+            a.ket_start = t.ket_start;
+            a.counter = f->d_counters + c;
+            a.D = Dc;
+            a.Fj = f->d_Fj;
+            a.Fk = f->d_Fk;
+            a.ld = nbfc;
+            a.nsm = f->nsm;
+            const int r = launch_fock(t.X, t.Y, a, st);
+            if (r != 0) {
+                snprintf(g_errbuf, sizeof(g_errbuf), "Fock kernel launch for class pair (%d,%d) failed: %d (%s)",
+                         t.X, t.Y, r, cudaGetErrorString(cudaGetLastError()));
+                return GTF_ERR_CUDA;
+            }
+        }
+        CK(cudaEventRecord(f->ev2, st));
+        dim3 g2((nbf + 127) / 128, nbf);
+        k_f_to_sph<<<g2, 128, 0, st>>>(f->d_Fj, f->d_Fk, f->d_F + nn * d, f->d_J + nn * d, f->d_K + nn * d,
+                                       f->d_sph2shell, f->d_sh_L, f->d_f_start, f->d_fc_start, nbf, nbfc,
+                                       f->pure);
+        CK(cudaGetLastError());
+        CK(cudaEventSynchronize(f->ev2));
+        float ms = 0.0f;
+        CK(cudaEventElapsedTime(&ms, f->ev1, f->ev2));
+        eri_ms_total += ms;
+    }
+    CK(cudaEventRecord(f->ev3, st));
+    CK(cudaEventSynchronize(f->ev3));
+    float tot = 0.0f;
+    CK(cudaEventElapsedTime(&tot, f->ev0, f->ev3));
+    f->ms_total = tot;
+    f->ms_eri = eri_ms_total;
+    f->ms_other = tot - eri_ms_total;
+    return GTF_OK;
+}
+
+extern "C" const double *gtf_fock_mat_dev(gtf_fock_dev_t *f, int type, int index)
+{
+    const size_t nn = (size_t)f->nbf * f->nbf;
+    if (index < 0 || index >= f->max_numdmat) return nullptr;
+    switch (type) {
+        case 0: return f->d_D + nn * index;
+        case 1: return f->d_F + nn * index;
+        case 2: return f->d_J + nn * index;
+        case 3: return f->d_K + nn * index;
+    }
+    return nullptr;
+}
+
+extern "C" int gtf_fock_get_mat(gtf_fock_dev_t *f, int type, int index, int r0, int r1, int c0, int c1,
+                                int stride, double *host)
+{
+    const double *m = gtf_fock_mat_dev(f, type, index);
+    if (!m) return GTF_ERR_INVALID;
+    return get_block(f, m, f->nbf, r0, r1, c0, c1, stride, host);
+}
+
+extern "C" int gtf_fock_last_timing(gtf_fock_dev_t *f, double *ms_total, double *ms_eri, double *ms_other)
+{
+    if (ms_total) *ms_total = f->ms_total;
+    if (ms_eri) *ms_eri = f->ms_eri;
+    if (ms_other) *ms_other = f->ms_other;
+    return GTF_OK;
+}
+
+extern "C" int gtf_fock_eri_flops(gtf_fock_dev_t *f, double *flops)
+{
+    *flops = f->eri_flops;
+    return GTF_OK;
+}
+
+extern "C" void *gtf_fock_stream(gtf_fock_dev_t *f) { return (void *)f->stream; }
+extern "C" size_t gtf_fock_device_bytes(gtf_fock_dev_t *f) { return f->dev_bytes; }
+
+// one-electron matrices live in onee.cu; these accessors need the struct
+extern "C" int gtf_onee_compute(gtf_fock_dev_t *f, int want_sx, int want_h, double **S, double **X, double **H);
+
+extern "C" int gtf_fock_one_electron(gtf_fock_dev_t *f, int want_sx, int want_h)
+{
+    return gtf_onee_compute(f, want_sx, want_h, &f->d_S, &f->d_X, &f->d_H);
+}
+
+extern "C" const double *gtf_fock_onee_dev(gtf_fock_dev_t *f, int which)
+{
+    return which == 0 ? f->d_S : which == 1 ? f->d_X : which == 2 ? f->d_H : nullptr;
+}
+
+extern "C" int gtf_fock_get_onee(gtf_fock_dev_t *f, int which, int r0, int r1, int c0, int c1, int stride,
+                                 double *host)
+{
+    const double *m = gtf_fock_onee_dev(f, which);
+    if (!m) return GTF_ERR_INVALID;
+    return get_block(f, m, f->nbf, r0, r1, c0, c1, stride, host);
+}
+
+extern "C" void gtf_fock_release_onee(gtf_fock_dev_t *f, int which)
+{
+    double **p = which == 0 ? &f->d_S : which == 1 ? &f->d_X : &f->d_H;
+    if (*p) {
+        cudaStreamSynchronize(f->stream);
+        cudaFree(*p);
+        *p = nullptr;
+    }
+}
+
+// basis arrays for onee.cu
+extern "C" void gtf_fock_basis_dev(gtf_fock_dev_t *f, const int **sh_L, const int **sh_nprim,
+                                   const int **sh_pstart, const int **f_start, const int **fc_start,
+                                   const double **sh_xyz, const double **alpha, const double **coef,
+                                   const int **Z, const double **atom_xyz, int *nshells, int *natoms, int *nbf,
+                                   int *pure)
+{
+    *sh_L = f->d_sh_L;
+    *sh_nprim = f->d_sh_nprim;
+    *sh_pstart = f->d_sh_pstart;
+    *f_start = f->d_f_start;
+    *fc_start = f->d_fc_start;
+    *sh_xyz = f->d_sh_xyz;
+    *alpha = f->d_alpha;
+    *coef = f->d_coef;
+    *Z = f->d_Z;
+    *atom_xyz = f->d_atom_xyz;
+    *nshells = f->nshells;
+    *natoms = f->natoms;
+    *nbf = f->nbf;
+    *pure = f->pure;
+}

@@ -1,0 +1,18 @@
+// fock_cls_0.cu -- instantiations of the Fock kernel for one group of
+// angular class pairs (split for parallel compilation).
+#include "fock_kernel.cuh"
+
+extern "C" int gtf_fock_group_0(int la, int lb, int lc, int ld, const FockLaunch &a, cudaStream_t st)
+{
+    FOCK_GROUP_CASE(0,0,0,0)
+    FOCK_GROUP_CASE(1,0,0,0)
+    FOCK_GROUP_CASE(1,0,1,0)
+    FOCK_GROUP_CASE(1,1,0,0)
+    FOCK_GROUP_CASE(1,1,1,0)
+    FOCK_GROUP_CASE(1,1,1,1)
+    FOCK_GROUP_CASE(2,0,0,0)
+    FOCK_GROUP_CASE(2,0,1,0)
+    FOCK_GROUP_CASE(2,0,1,1)
+    FOCK_GROUP_CASE(2,0,2,0)
+    return 1;
+}

@@ -1,0 +1,9 @@
+// fock_cls_4.cu -- instantiations of the Fock kernel for one group of
+// angular class pairs (split for parallel compilation).
+#include "fock_kernel.cuh"
+
+extern "C" int gtf_fock_group_4(int la, int lb, int lc, int ld, const FockLaunch &a, cudaStream_t st)
+{
+    FOCK_GROUP_CASE(2,2,2,1)
+    return 1;
+}

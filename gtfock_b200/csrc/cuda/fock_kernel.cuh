@@ -1,0 +1,86 @@
+// fock_kernel.cuh -- the persistent Fock kernel (one instantiation per
+// angular class pair) and its launcher; included by fock.cu and by the
+// fock_cls_*.cu translation units that instantiate it.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "gtf_cuda.h"
+#include "gtf_dev.cuh"
+
+#define FOCK_THREADS 128
+
+struct FockLaunch {
+    const PairRec *pairs;
+    PrimPairs pp;
+    const int *nket;
+    const long long *unit_prefix;
+    int nbra;
+    long long nunits;
+    int bra_start, ket_start;
+    unsigned long long *counter;
+    const double *D;
+    double *Fj, *Fk;
+    int ld;
+    int nsm;
+};
+
+// ---------------------------------------------------------------------------
+// the Fock kernel: persistent warps claim units of 32 quartets
+// ---------------------------------------------------------------------------
+template <int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(FOCK_THREADS)
+    k_fock(const PairRec *__restrict__ pairs, PrimPairs pp, const int *__restrict__ nket,
+           const long long *__restrict__ unit_prefix, int nbra, long long nunits, int bra_start,
+           int ket_start, unsigned long long *__restrict__ counter, const double *__restrict__ D,
+           double *__restrict__ Fj, double *__restrict__ Fk, int ld)
+{
+    constexpr int NQ = ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD);
+    const int lane = threadIdx.x & 31;
+    PPStored src{pp};
+    for (;;) {
+        unsigned long long u = 0;
+        if (lane == 0) u = atomicAdd(counter, 1ULL);
+        u = __shfl_sync(GTF_FULL_MASK, u, 0);
+        if (u >= (unsigned long long)nunits) break;
+        int lo = 0, hi = nbra;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (__ldg(unit_prefix + mid) <= (long long)u) lo = mid;
+            else hi = mid;
+        }
+        const int i = lo;
+        const long long chunk = (long long)u - __ldg(unit_prefix + i);
+        const int j = (int)(chunk * 32) + lane;
+        const bool active = j < __ldg(nket + i);
+        const PairRec pb = pairs[bra_start + i];
+        const PairRec pk = active ? pairs[ket_start + j] : pb;
+        double acc[NQ];
+#pragma unroll
+        for (int k = 0; k < NQ; k++) acc[k] = 0.0;
+        if (active) eri_accumulate<LA, LB, LC, LD>(src, pb, src, pk, acc);
+        const bool same = (bra_start + i) == (ket_start + j);
+        digest<LA, LB, LC, LD, double>(acc, active, pb, pk, same, D, Fj, Fk, ld, lane);
+    }
+}
+
+
+template <int LA, int LB, int LC, int LD>
+int launch_fock_t(const FockLaunch &a, cudaStream_t st)
+{
+    auto k = k_fock<LA, LB, LC, LD>;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k, FOCK_THREADS, 0);
+    if (per_sm < 1) per_sm = 1;
+    long long want = (a.nunits + (FOCK_THREADS / 32) - 1) / (FOCK_THREADS / 32);
+    long long grid = (long long)a.nsm * per_sm;
+    if (want < grid) grid = want;
+    if (grid < 1) grid = 1;
+    k<<<(unsigned)grid, FOCK_THREADS, 0, st>>>(a.pairs, a.pp, a.nket, a.unit_prefix, a.nbra, a.nunits,
+                                               a.bra_start, a.ket_start, a.counter, a.D, a.Fj, a.Fk, a.ld);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+// returns 0 when launched, -1 on a launch error, 1 when the class pair is not in this group
+#define FOCK_GROUP_CASE(A, B, C, D) \
+    if (la == A && lb == B && lc == C && ld == D) return launch_fock_t<A, B, C, D>(a, st);

@@ -1,0 +1,100 @@
+/*
+ * gtf_cuda.h -- C ABI between the host C library (pfock.c, purif.c) and the
+ * CUDA modules (fock.cu, onee.cu, purif.cu).  Plain pointers and sizes only;
+ * every function returns 0 on success or a negative gtf_err_t.
+ */
+#ifndef GTF_CUDA_H
+#define GTF_CUDA_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    GTF_OK = 0,
+    GTF_ERR_CUDA = -1,       /* a CUDA runtime / library call failed */
+    GTF_ERR_ALLOC = -2,      /* device or host allocation failed */
+    GTF_ERR_INVALID = -3,    /* bad argument */
+    GTF_ERR_NODEVICE = -4,   /* no CUDA device visible */
+    GTF_ERR_DEVICE_FLAG = -5 /* a kernel reported an error through its status word */
+} gtf_err_t;
+
+/* read-only view of a loaded basis (gtf_basis.h fields) */
+typedef struct {
+    int natoms, nshells, nbf, nbf_cart, nprims, pure;
+    const int *Z;
+    const double *xyz;       /* [3*natoms] bohr */
+    const int *sh_atom, *sh_L, *sh_nprim, *sh_pstart;
+    const int *f_start;      /* [nshells+1] */
+    const int *fc_start;     /* [nshells+1] */
+    const double *alpha, *coef;
+} gtf_basis_view_t;
+
+typedef struct gtf_fock_dev gtf_fock_dev_t;
+
+/* precision of the electron-repulsion kernels */
+typedef enum {
+    GTF_PREC_FP64 = 0,       /* every quartet in FP64 */
+    GTF_PREC_MIXED = 1       /* quartets with Schwarz bound below a cutoff in FP32 */
+} gtf_prec_t;
+
+int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max_numdmat,
+                    gtf_fock_dev_t **out);
+void gtf_fock_destroy(gtf_fock_dev_t *f);
+const char *gtf_last_error(void);
+
+/* screening results (pfock/screening.c:15-180) */
+int gtf_fock_screening_info(gtf_fock_dev_t *f, int *nnz, double *maxvalue,
+                            double *usq, double *uitl);
+int gtf_fock_get_csr(gtf_fock_dev_t *f, int *shellptr, int *shellid, int *shellrid,
+                     double *shellvalue);
+
+/* density matrices (spherical/AO basis, full nbf x nbf) */
+int gtf_fock_fill_density(gtf_fock_dev_t *f, int index, double value);
+int gtf_fock_put_density(gtf_fock_dev_t *f, int index, int r0, int r1, int c0, int c1,
+                         int stride, const double *host);
+int gtf_fock_put_density_dev(gtf_fock_dev_t *f, int index, const double *dev);
+
+/* J/K build for densities [0, numdmat) */
+int gtf_fock_compute(gtf_fock_dev_t *f, int numdmat);
+/* type: 0 D, 1 F (= J + K), 2 J, 3 K, as PFockMatType_t */
+int gtf_fock_get_mat(gtf_fock_dev_t *f, int type, int index, int r0, int r1, int c0, int c1,
+                     int stride, double *host);
+const double *gtf_fock_mat_dev(gtf_fock_dev_t *f, int type, int index);
+
+/* one-electron matrices on the device: 0 S, 1 X = S^-1/2, 2 H_core */
+int gtf_fock_one_electron(gtf_fock_dev_t *f, int want_sx, int want_h);
+int gtf_fock_get_onee(gtf_fock_dev_t *f, int which, int r0, int r1, int c0, int c1,
+                      int stride, double *host);
+const double *gtf_fock_onee_dev(gtf_fock_dev_t *f, int which);
+void gtf_fock_release_onee(gtf_fock_dev_t *f, int which);
+
+/* precision control and statistics */
+int gtf_fock_set_precision(gtf_fock_dev_t *f, int prec, double fp32_cutoff);
+int gtf_fock_last_timing(gtf_fock_dev_t *f, double *ms_total, double *ms_eri, double *ms_other);
+int gtf_fock_eri_flops(gtf_fock_dev_t *f, double *flops);
+void *gtf_fock_stream(gtf_fock_dev_t *f);
+size_t gtf_fock_device_bytes(gtf_fock_dev_t *f);
+
+/* ---- purification / DIIS on the device (purif.cu) ---- */
+typedef struct gtf_purif_dev gtf_purif_dev_t;
+int gtf_purif_create(int nbf, int nocc, void *stream, gtf_purif_dev_t **out);
+void gtf_purif_destroy(gtf_purif_dev_t *p);
+int gtf_purif_set_sx(gtf_purif_dev_t *p, const double *S_host, const double *X_host);
+int gtf_purif_set_sx_dev(gtf_purif_dev_t *p, const double *S_dev, const double *X_dev);
+/* canonical purification of F (orthogonal basis); D_AO returned; iterations */
+int gtf_purif_run(gtf_purif_dev_t *p, const double *F_host, double *D_host, int *iters);
+int gtf_purif_run_dev(gtf_purif_dev_t *p, const double *F_dev, double *D_dev, int *iters);
+/* one DIIS step: F (AO, host or device) in, extrapolated orthogonal F out */
+int gtf_diis_step(gtf_purif_dev_t *p, const double *D_host, double *F_host, int iter);
+int gtf_diis_step_dev(gtf_purif_dev_t *p, const double *D_dev, double *F_dev, int iter);
+int gtf_purif_stats(gtf_purif_dev_t *p, double *ms_gemm, double *ms_total, double *errnorm,
+                    double *idem_err, double *tr_err);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

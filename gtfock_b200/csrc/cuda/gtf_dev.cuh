@@ -1,0 +1,434 @@
+// gtf_dev.cuh -- device building blocks of the Fock build (sm_100a).
+//
+// Replaces the integral engine behind CInt_computeShellQuartet
+// (libcint/include/CInt.h:159-167, called at pfock/fock_task.c:197-198) and
+// the J/K digestion update_F (pfock/fock_task.c:29-117):
+//   * rys_roots<N>: N-point Rys quadrature for the Boys weight from the
+//     generated Chebyshev-fitted table (rys_table.h), large-T Hermite form;
+//   * eri_accumulate<LA,LB,LC,LD>: contracted Cartesian (ab|cd) by Rys
+//     quadrature -- per primitive quartet and root the 2-D integrals
+//     G(i,k) by the Rys recurrences (C00, C00', B10, B01, B00), horizontal
+//     transfer to (a b | c d) per Cartesian direction, and the product
+//     Ix*Iy*Iz accumulated in registers; integrals never leave the thread;
+//   * digest<...>: the six J/K updates of one unique quartet into F with
+//     the reference's degeneracy factors; the bra block (uniform across a
+//     warp) is warp-reduced before its atomics.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define RYS_QUAL __device__
+#define RYS_QUAL_SMALL __constant__
+#include "rys_table.h"
+
+#define GTF_FULL_MASK 0xffffffffu
+#define GTF_MAXL 2
+
+// sqrt(2) * pi^(5/4): the per-pair share of 2 pi^(5/2) / (p q sqrt(p+q))
+#define GTF_PAIR_PREF 5.9149671727956130
+
+// ---------------------------------------------------------------------------
+// Cartesian component tables (lexicographic: xx, xy, xz, yy, yz, zz)
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int ncart(int L) { return (L + 1) * (L + 2) / 2; }
+
+__host__ __device__ constexpr int cart_x(int L, int c)
+{
+    int x = L;
+    int first = 0;  // index of the first component with this x
+    while (x >= 0) {
+        int cnt = L - x + 1;
+        if (c < first + cnt) return x;
+        first += cnt;
+        x--;
+    }
+    return 0;
+}
+
+__host__ __device__ constexpr int cart_y(int L, int c)
+{
+    int x = L;
+    int first = 0;
+    while (x >= 0) {
+        int cnt = L - x + 1;
+        if (c < first + cnt) return (L - x) - (c - first);
+        first += cnt;
+        x--;
+    }
+    return 0;
+}
+
+__host__ __device__ constexpr int cart_z(int L, int c) { return L - cart_x(L, c) - cart_y(L, c); }
+
+// ---------------------------------------------------------------------------
+// Shell-pair record (64 bytes, coalesced by lane)
+// ---------------------------------------------------------------------------
+struct __align__(16) PairRec {
+    double Ax, Ay, Az;     // centre of shell a
+    double ABx, ABy, ABz;  // A - B
+    int fa, fb;            // first Cartesian function of a and b
+    int off, n;            // primitive-pair offset and count
+};
+
+// primitive-pair data, structure of arrays
+struct PrimPairs {
+    const double *p;   // a + b
+    const double *Px, *Py, *Pz;
+    const double *K;   // GTF_PAIR_PREF * ca * cb * exp(-ab/p |AB|^2) / p
+};
+
+// ---------------------------------------------------------------------------
+// Rys roots and weights
+// ---------------------------------------------------------------------------
+template <int N>
+__device__ __forceinline__ void rys_roots(double T, double (&u)[N], double (&w)[N])
+{
+    if (T >= RYS_TMAX[N]) {
+        const double it = 1.0 / T;
+        const double rs = rsqrt(T);
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            u[i] = RYS_LARGE_X2[N][i] * it;
+            w[i] = RYS_LARGE_W[N][i] * rs;
+        }
+        return;
+    }
+    const int k = (int)(T * RYS_INV_H);
+    const double s = T - ((double)k * RYS_H + 0.5 * RYS_H);
+    const double *c = RYS_TABLE + RYS_OFF[N] + k * (RYS_DEG + 1) * (2 * N);
+    double a[2 * N];
+#pragma unroll
+    for (int f = 0; f < 2 * N; f++) a[f] = __ldg(c + RYS_DEG * 2 * N + f);
+#pragma unroll
+    for (int j = RYS_DEG - 1; j >= 0; j--) {
+#pragma unroll
+        for (int f = 0; f < 2 * N; f++) a[f] = fma(a[f], s, __ldg(c + j * 2 * N + f));
+    }
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        u[i] = a[i];
+        w[i] = a[N + i];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// one-dimensional horizontal transfer:
+// t(a, b+1) = t(a+1, b) + dist * t(a, b); input v[0..L1+L2], output o[a][b]
+// ---------------------------------------------------------------------------
+template <int L1, int L2>
+__device__ __forceinline__ void hrr1d(const double (&v)[L1 + L2 + 1], double (&o)[L1 + 1][L2 + 1],
+                                      double dist)
+{
+    double t[L1 + L2 + 1][L2 + 1];
+#pragma unroll
+    for (int a = 0; a <= L1 + L2; a++) t[a][0] = v[a];
+#pragma unroll
+    for (int b = 0; b < L2; b++) {
+#pragma unroll
+        for (int a = 0; a <= L1 + L2 - b - 1; a++) t[a][b + 1] = fma(dist, t[a][b], t[a + 1][b]);
+    }
+#pragma unroll
+    for (int a = 0; a <= L1; a++) {
+#pragma unroll
+        for (int b = 0; b <= L2; b++) o[a][b] = t[a][b];
+    }
+}
+
+// 2-D Rys integrals G[i][k] (i on centre A, k on centre C) for one direction
+template <int NI, int NK>
+__device__ __forceinline__ void rys_2d(double (&G)[NI][NK], double g00, double C00, double C0p,
+                                      double B10, double B01, double B00)
+{
+    G[0][0] = g00;
+    if (NI > 1) G[1][0] = C00 * g00;
+#pragma unroll
+    for (int i = 1; i < NI - 1; i++) G[i + 1][0] = fma(C00, G[i][0], i * B10 * G[i - 1][0]);
+    if (NK > 1) G[0][1] = C0p * g00;
+#pragma unroll
+    for (int k = 1; k < NK - 1; k++) G[0][k + 1] = fma(C0p, G[0][k], k * B01 * G[0][k - 1]);
+#pragma unroll
+    for (int k = 1; k < NK; k++) {
+#pragma unroll
+        for (int i = 0; i < NI - 1; i++) {
+            double v = fma(C00, G[i][k], k * B00 * G[i][k - 1]);
+            if (i > 0) v = fma(i * B10, G[i - 1][k], v);
+            G[i + 1][k] = v;
+        }
+    }
+}
+
+// full 1-D transfer: G[i][k] -> I[a][b][c][d]
+template <int LA, int LB, int LC, int LD>
+__device__ __forceinline__ void hrr_abcd(const double (&G)[LA + LB + 1][LC + LD + 1],
+                                         double (&I)[LA + 1][LB + 1][LC + 1][LD + 1],
+                                         double ab, double cd)
+{
+    constexpr int NI = LA + LB + 1;
+    double K[NI][LC + 1][LD + 1];
+#pragma unroll
+    for (int i = 0; i < NI; i++) {
+        double v[LC + LD + 1];
+#pragma unroll
+        for (int k = 0; k <= LC + LD; k++) v[k] = G[i][k];
+        double o[LC + 1][LD + 1];
+        hrr1d<LC, LD>(v, o, cd);
+#pragma unroll
+        for (int c = 0; c <= LC; c++)
+#pragma unroll
+            for (int d = 0; d <= LD; d++) K[i][c][d] = o[c][d];
+    }
+#pragma unroll
+    for (int c = 0; c <= LC; c++) {
+#pragma unroll
+        for (int d = 0; d <= LD; d++) {
+            double v[NI];
+#pragma unroll
+            for (int i = 0; i < NI; i++) v[i] = K[i][c][d];
+            double o[LA + 1][LB + 1];
+            hrr1d<LA, LB>(v, o, ab);
+#pragma unroll
+            for (int a = 0; a <= LA; a++)
+#pragma unroll
+                for (int b = 0; b <= LB; b++) I[a][b][c][d] = o[a][b];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// contracted Cartesian (ab|cd), accumulated into acc[ia + NA*(ib + NB*(ic + NC*id))]
+// ---------------------------------------------------------------------------
+template <int LA, int LB, int LC, int LD, class PPB, class PPK>
+__device__ __forceinline__ void eri_accumulate(const PPB &bra, const PairRec &pb, const PPK &ket,
+                                               const PairRec &pk,
+                                               double (&acc)[ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD)])
+{
+    constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
+    constexpr int NI = LA + LB + 1, NK = LC + LD + 1;
+    constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    for (int ib = 0; ib < pb.n; ib++) {
+        double p, Px, Py, Pz, Kab;
+        bra.get(pb, ib, p, Px, Py, Pz, Kab);
+        const double PAx = Px - pb.Ax, PAy = Py - pb.Ay, PAz = Pz - pb.Az;
+        for (int ik = 0; ik < pk.n; ik++) {
+            double q, Qx, Qy, Qz, Kcd;
+            ket.get(pk, ik, q, Qx, Qy, Qz, Kcd);
+            const double rpq = rsqrt(p + q);
+            const double ipq = rpq * rpq;
+            const double PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
+            const double rho = p * q * ipq;
+            const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
+            const double pref = Kab * Kcd * rpq;
+            double u[NR], w[NR];
+            rys_roots<NR>(T, u, w);
+            const double QCx = Qx - pk.Ax, QCy = Qy - pk.Ay, QCz = Qz - pk.Az;
+            const double h2p = 0.5 / p, h2q = 0.5 / q;
+            const double qf = q * ipq, pf = p * ipq;
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                const double ur = u[r];
+                const double B00 = 0.5 * ur * ipq;
+                const double B10 = h2p * (1.0 - qf * ur);
+                const double B01 = h2q * (1.0 - pf * ur);
+                const double cq = qf * ur, cp = pf * ur;
+                double Gx[NI][NK], Gy[NI][NK], Gz[NI][NK];
+                rys_2d<NI, NK>(Gx, 1.0, PAx - cq * PQx, QCx + cp * PQx, B10, B01, B00);
+                rys_2d<NI, NK>(Gy, 1.0, PAy - cq * PQy, QCy + cp * PQy, B10, B01, B00);
+                rys_2d<NI, NK>(Gz, w[r] * pref, PAz - cq * PQz, QCz + cp * PQz, B10, B01, B00);
+                double Ix[LA + 1][LB + 1][LC + 1][LD + 1];
+                double Iy[LA + 1][LB + 1][LC + 1][LD + 1];
+                double Iz[LA + 1][LB + 1][LC + 1][LD + 1];
+                hrr_abcd<LA, LB, LC, LD>(Gx, Ix, pb.ABx, pk.ABx);
+                hrr_abcd<LA, LB, LC, LD>(Gy, Iy, pb.ABy, pk.ABy);
+                hrr_abcd<LA, LB, LC, LD>(Gz, Iz, pb.ABz, pk.ABz);
+#pragma unroll
+                for (int id = 0; id < ND; id++)
+#pragma unroll
+                    for (int ic = 0; ic < NC; ic++)
+#pragma unroll
+                        for (int ibb = 0; ibb < NB; ibb++)
+#pragma unroll
+                            for (int ia = 0; ia < NA; ia++) {
+                                const double xy =
+                                    Ix[cart_x(LA, ia)][cart_x(LB, ibb)][cart_x(LC, ic)][cart_x(LD, id)] *
+                                    Iy[cart_y(LA, ia)][cart_y(LB, ibb)][cart_y(LC, ic)][cart_y(LD, id)];
+                                double &dst = acc[ia + NA * (ibb + NB * (ic + NC * id))];
+                                dst = fma(xy,
+                                          Iz[cart_z(LA, ia)][cart_z(LB, ibb)][cart_z(LC, ic)][cart_z(LD, id)],
+                                          dst);
+                            }
+            }
+        }
+    }
+}
+
+// primitive pairs read from the precomputed pair arrays
+struct PPStored {
+    PrimPairs pp;
+    __device__ __forceinline__ void get(const PairRec &pr, int i, double &p, double &Px, double &Py,
+                                        double &Pz, double &K) const
+    {
+        const int k = pr.off + i;
+        p = __ldg(pp.p + k);
+        Px = __ldg(pp.Px + k);
+        Py = __ldg(pp.Py + k);
+        Pz = __ldg(pp.Pz + k);
+        K = __ldg(pp.K + k);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// J/K digestion of one unique quartet (pfock/fock_task.c:29-117 semantics):
+//   Fj[a][b] += 2(1+f1)(1+f2)         sum_cd D[c][d] I
+//   Fj[c][d] += 2 f3 (1+f1)(1+f2)     sum_ab D[a][b] I
+//   Fk[a][c] -= (1+f3)                sum_bd D[b][d] I
+//   Fk[b][c] -= f1 (1+f3)             sum_ad D[a][d] I
+//   Fk[a][d] -= f2 (1+f3)             sum_bc D[b][c] I
+//   Fk[b][d] -= f1 f2 (1+f3)          sum_ac D[a][c] I
+// f1 = a!=b, f2 = c!=d, f3 = bra pair != ket pair.  The caller symmetrises
+// Fj and Fk afterwards (GA_Symmetrize, pfock/pfock.c:1719-1726).
+// The bra pair is shared by the 32 lanes of the warp; `active` lanes carry a
+// quartet, inactive lanes contribute zeros to the warp reductions.
+// ---------------------------------------------------------------------------
+template <int LA, int LB, int LC, int LD, typename R>
+__device__ __forceinline__ void digest(const R (&I)[ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD)],
+                                       bool active, const PairRec &pb, const PairRec &pk, bool same_pair,
+                                       const double *__restrict__ D, double *__restrict__ Fj,
+                                       double *__restrict__ Fk, int ld, int lane)
+{
+    constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    const int fa = pb.fa, fb = pb.fb, fc = pk.fa, fd = pk.fb;
+    const double f1 = (fa != fb) ? 1.0 : 0.0;
+    const double f2 = (fc != fd) ? 1.0 : 0.0;
+    const double f3 = same_pair ? 0.0 : 1.0;
+    const double sJab = 2.0 * (1.0 + f1) * (1.0 + f2);
+    const double sJcd = f3 * sJab;
+    const double sKac = -(1.0 + f3);
+    const double sKbc = f1 * sKac, sKad = f2 * sKac, sKbd = f1 * f2 * sKac;
+
+    // bra block J: warp-uniform destination
+    {
+        double dcd[NC * ND];
+#pragma unroll
+        for (int ic = 0; ic < NC; ic++)
+#pragma unroll
+            for (int id = 0; id < ND; id++)
+                dcd[ic + NC * id] = active ? __ldg(D + (size_t)(fc + ic) * ld + fd + id) : 0.0;
+#pragma unroll
+        for (int ibb = 0; ibb < NB; ibb++) {
+#pragma unroll
+            for (int ia = 0; ia < NA; ia++) {
+                double v = 0.0;
+#pragma unroll
+                for (int id = 0; id < ND; id++)
+#pragma unroll
+                    for (int ic = 0; ic < NC; ic++)
+                        v = fma((double)I[ia + NA * (ibb + NB * (ic + NC * id))], dcd[ic + NC * id], v);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(GTF_FULL_MASK, v, o);
+                if (lane == 0) atomicAdd(Fj + (size_t)(fa + ia) * ld + fb + ibb, sJab * v);
+            }
+        }
+    }
+    if (!active) return;
+    // ket block J
+    if (f3 != 0.0) {
+        double dab[NA * NB];
+#pragma unroll
+        for (int ia = 0; ia < NA; ia++)
+#pragma unroll
+            for (int ibb = 0; ibb < NB; ibb++) dab[ia + NA * ibb] = __ldg(D + (size_t)(fa + ia) * ld + fb + ibb);
+#pragma unroll
+        for (int id = 0; id < ND; id++)
+#pragma unroll
+            for (int ic = 0; ic < NC; ic++) {
+                double v = 0.0;
+#pragma unroll
+                for (int ibb = 0; ibb < NB; ibb++)
+#pragma unroll
+                    for (int ia = 0; ia < NA; ia++)
+                        v = fma((double)I[ia + NA * (ibb + NB * (ic + NC * id))], dab[ia + NA * ibb], v);
+                atomicAdd(Fj + (size_t)(fc + ic) * ld + fd + id, sJcd * v);
+            }
+    }
+    // K[a][c] -= (1+f3) sum_bd D[b][d] I
+    {
+        double dbd[NB * ND];
+#pragma unroll
+        for (int ibb = 0; ibb < NB; ibb++)
+#pragma unroll
+            for (int id = 0; id < ND; id++) dbd[ibb + NB * id] = __ldg(D + (size_t)(fb + ibb) * ld + fd + id);
+#pragma unroll
+        for (int ic = 0; ic < NC; ic++)
+#pragma unroll
+            for (int ia = 0; ia < NA; ia++) {
+                double v = 0.0;
+#pragma unroll
+                for (int id = 0; id < ND; id++)
+#pragma unroll
+                    for (int ibb = 0; ibb < NB; ibb++)
+                        v = fma((double)I[ia + NA * (ibb + NB * (ic + NC * id))], dbd[ibb + NB * id], v);
+                atomicAdd(Fk + (size_t)(fa + ia) * ld + fc + ic, sKac * v);
+            }
+    }
+    // K[b][c] -= f1 (1+f3) sum_ad D[a][d] I
+    if (f1 != 0.0) {
+        double dad[NA * ND];
+#pragma unroll
+        for (int ia = 0; ia < NA; ia++)
+#pragma unroll
+            for (int id = 0; id < ND; id++) dad[ia + NA * id] = __ldg(D + (size_t)(fa + ia) * ld + fd + id);
+#pragma unroll
+        for (int ic = 0; ic < NC; ic++)
+#pragma unroll
+            for (int ibb = 0; ibb < NB; ibb++) {
+                double v = 0.0;
+#pragma unroll
+                for (int id = 0; id < ND; id++)
+#pragma unroll
+                    for (int ia = 0; ia < NA; ia++)
+                        v = fma((double)I[ia + NA * (ibb + NB * (ic + NC * id))], dad[ia + NA * id], v);
+                atomicAdd(Fk + (size_t)(fb + ibb) * ld + fc + ic, sKbc * v);
+            }
+    }
+    // K[a][d] -= f2 (1+f3) sum_bc D[b][c] I
+    if (f2 != 0.0) {
+        double dbc[NB * NC];
+#pragma unroll
+        for (int ibb = 0; ibb < NB; ibb++)
+#pragma unroll
+            for (int ic = 0; ic < NC; ic++) dbc[ibb + NB * ic] = __ldg(D + (size_t)(fb + ibb) * ld + fc + ic);
+#pragma unroll
+        for (int id = 0; id < ND; id++)
+#pragma unroll
+            for (int ia = 0; ia < NA; ia++) {
+                double v = 0.0;
+#pragma unroll
+                for (int ic = 0; ic < NC; ic++)
+#pragma unroll
+                    for (int ibb = 0; ibb < NB; ibb++)
+                        v = fma((double)I[ia + NA * (ibb + NB * (ic + NC * id))], dbc[ibb + NB * ic], v);
+                atomicAdd(Fk + (size_t)(fa + ia) * ld + fd + id, sKad * v);
+            }
+    }
+    // K[b][d] -= f1 f2 (1+f3) sum_ac D[a][c] I
+    if (f1 != 0.0 && f2 != 0.0) {
+        double dac[NA * NC];
+#pragma unroll
+        for (int ia = 0; ia < NA; ia++)
+#pragma unroll
+            for (int ic = 0; ic < NC; ic++) dac[ia + NA * ic] = __ldg(D + (size_t)(fa + ia) * ld + fc + ic);
+#pragma unroll
+        for (int id = 0; id < ND; id++)
+#pragma unroll
+            for (int ibb = 0; ibb < NB; ibb++) {
+                double v = 0.0;
+#pragma unroll
+                for (int ic = 0; ic < NC; ic++)
+#pragma unroll
+                    for (int ia = 0; ia < NA; ia++)
+                        v = fma((double)I[ia + NA * (ibb + NB * (ic + NC * id))], dac[ia + NA * ic], v);
+                atomicAdd(Fk + (size_t)(fb + ibb) * ld + fd + id, sKbd * v);
+            }
+    }
+}

@@ -1,0 +1,464 @@
+// purif.cu -- canonical density purification and Pulay DIIS on one GPU
+// (pscf/purif.c:257-641; the 3-D pdgemm of pscf/pdgemm.c becomes one DGEMM).
+//
+// Purification (pscf/purif.c:301-476): Gershgorin bounds and tr F give the
+// initial D; each iteration forms D2 = D D^T and D3 = D D2, reduces
+// ||D - D2||_F, tr(D2 - D3) and tr(D - D2) deterministically (fixed block
+// partials summed in order), updates D with the trace-conserving polynomial,
+// and stops once ||D - D2||_F < 1e-11.  D_AO = X D X at the end.
+// DIIS (pscf/purif.c:491-641): error X (F D S - S D F) X, dot products into
+// the bordered B matrix, (m+1)^2 solve on the host, F = sum c_i F_i.
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+#include <float.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "gtf_cuda.h"
+
+#define PUR_MAX_ITERS 200
+#define PUR_MAX_DIIS 10
+#define PUR_LDB 128
+#define RED_BLOCKS 148
+#define RED_THREADS 256
+
+#define CKP(call)                                                                       \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess) {                                                        \
+            fprintf(stderr, "gtfock_b200 %s:%d %s\n", __FILE__, __LINE__, cudaGetErrorString(e_)); \
+            return GTF_ERR_CUDA;                                                        \
+        }                                                                               \
+    } while (0)
+#define CKB(call)                                                       \
+    do {                                                                \
+        if ((call) != CUBLAS_STATUS_SUCCESS) {                          \
+            fprintf(stderr, "gtfock_b200 %s:%d cuBLAS failure\n", __FILE__, __LINE__); \
+            return GTF_ERR_CUDA;                                        \
+        }                                                               \
+    } while (0)
+
+struct gtf_purif_dev {
+    int n, nocc;
+    cudaStream_t st;
+    cublasHandle_t blas;
+    double *S, *X, *D, *D2, *D3, *F, *W, *W2;
+    double *vecs, *Fvecs;
+    double *part;     // [RED_BLOCKS * 16] block partials
+    double *scal;     // device scalars
+    double *h_scal;   // pinned mirror
+    int len_diis, bmax_id;
+    double bmax;
+    double b[PUR_LDB * PUR_LDB];
+    int sx_set;
+    cudaEvent_t e0, e1;
+    double ms_gemm, ms_total, errnorm, idem, trerr;
+};
+
+// row-major C = A B^T (pdgemm3D_2) and C = A B, via column-major cuBLAS
+static int gemm_abt(gtf_purif_dev *p, const double *A, const double *B, double *C)
+{
+    const double one = 1.0, zero = 0.0;
+    CKB(cublasDgemm(p->blas, CUBLAS_OP_T, CUBLAS_OP_N, p->n, p->n, p->n, &one, B, p->n, A, p->n, &zero, C, p->n));
+    return GTF_OK;
+}
+
+static int gemm_ab(gtf_purif_dev *p, const double *A, const double *B, double *C)
+{
+    const double one = 1.0, zero = 0.0;
+    CKB(cublasDgemm(p->blas, CUBLAS_OP_N, CUBLAS_OP_N, p->n, p->n, p->n, &one, B, p->n, A, p->n, &zero, C, p->n));
+    return GTF_OK;
+}
+
+// per column i: Gershgorin interval [diag - off, diag + off], off = sum_j |F[j][i]| - |diag|
+// (pscf/purif.c:309-322); block partials of min, max and the trace
+__global__ void k_gersh(const double *__restrict__ F, int n, double *__restrict__ part)
+{
+    __shared__ double smin[RED_THREADS], smax[RED_THREADS], str[RED_THREADS];
+    double lmin = DBL_MAX, lmax = -DBL_MAX, ltr = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double off = 0.0, dg = 0.0;
+        for (int j = 0; j < n; j++) {
+            const double v = F[(size_t)j * n + i];
+            off += fabs(v);
+            if (j == i) dg = v;
+        }
+        off -= fabs(dg);
+        lmin = fmin(lmin, dg - off);
+        lmax = fmax(lmax, dg + off);
+        ltr += dg;
+    }
+    smin[threadIdx.x] = lmin;
+    smax[threadIdx.x] = lmax;
+    str[threadIdx.x] = ltr;
+    __syncthreads();
+    for (int s = RED_THREADS / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            smin[threadIdx.x] = fmin(smin[threadIdx.x], smin[threadIdx.x + s]);
+            smax[threadIdx.x] = fmax(smax[threadIdx.x], smax[threadIdx.x + s]);
+            str[threadIdx.x] += str[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        part[3 * blockIdx.x] = smin[0];
+        part[3 * blockIdx.x + 1] = smax[0];
+        part[3 * blockIdx.x + 2] = str[0];
+    }
+}
+
+// scal[0] = -lambda/n, scal[1] = lambda mu_bar / n + nocc / n (pscf/purif.c:355-373)
+__global__ void k_purif_init(const double *__restrict__ part, int nblk, int n, int nocc, double *scal)
+{
+    if (threadIdx.x != 0) return;
+    double hmin = DBL_MAX, hmax = -DBL_MAX, trF = 0.0;
+    for (int b = 0; b < nblk; b++) {
+        hmin = fmin(hmin, part[3 * b]);
+        hmax = fmax(hmax, part[3 * b + 1]);
+        trF += part[3 * b + 2];
+    }
+    const double mu_bar = trF / (double)n;
+    const double lambda = fmin((double)nocc / (hmax - mu_bar), (double)(n - nocc) / (mu_bar - hmin));
+    scal[0] = -lambda / n;
+    scal[1] = lambda * mu_bar / (double)n + (double)nocc / n;
+    scal[2] = hmin;
+    scal[3] = hmax;
+    scal[4] = mu_bar;
+    scal[5] = lambda;
+}
+
+__global__ void k_purif_d0(const double *__restrict__ F, double *__restrict__ D, int n, const double *scal)
+{
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= (size_t)n * n) return;
+    double v = F[k] * scal[0];
+    if (k / n == k % n) v += scal[1];
+    D[k] = v;
+}
+
+// block partials of ||D - D2||^2, tr(D2 - D3), tr(D - D2)
+__global__ void k_purif_stats(const double *__restrict__ D, const double *__restrict__ D2,
+                              const double *__restrict__ D3, int n, double *__restrict__ part)
+{
+    __shared__ double s0[RED_THREADS], s1[RED_THREADS], s2[RED_THREADS];
+    const size_t nn = (size_t)n * n;
+    double e = 0.0, t = 0.0, t2 = 0.0;
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += (size_t)gridDim.x * blockDim.x) {
+        const double d = D[k] - D2[k];
+        e += d * d;
+    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const size_t k = (size_t)i * n + i;
+        t += D2[k] - D3[k];
+        t2 += D[k] - D2[k];
+    }
+    s0[threadIdx.x] = e;
+    s1[threadIdx.x] = t;
+    s2[threadIdx.x] = t2;
+    __syncthreads();
+    for (int s = RED_THREADS / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            s0[threadIdx.x] += s0[threadIdx.x + s];
+            s1[threadIdx.x] += s1[threadIdx.x + s];
+            s2[threadIdx.x] += s2[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        part[3 * blockIdx.x] = s0[0];
+        part[3 * blockIdx.x + 1] = s1[0];
+        part[3 * blockIdx.x + 2] = s2[0];
+    }
+}
+
+// scal[6] = errnorm, scal[7] = c = tr(D2-D3)/tr(D-D2) (pscf/purif.c:394-440)
+__global__ void k_purif_finish(const double *__restrict__ part, int nblk, double *scal)
+{
+    if (threadIdx.x != 0) return;
+    double e = 0.0, t = 0.0, t2 = 0.0;
+    for (int b = 0; b < nblk; b++) {
+        e += part[3 * b];
+        t += part[3 * b + 1];
+        t2 += part[3 * b + 2];
+    }
+    scal[6] = sqrt(e);
+    scal[7] = t / t2;
+}
+
+// D update (pscf/purif.c:441-455)
+__global__ void k_purif_update(double *__restrict__ D, const double *__restrict__ D2, const double *__restrict__ D3,
+                               size_t nn, const double *scal)
+{
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nn) return;
+    const double c = scal[7];
+    if (c < 0.5) D[k] = ((1.0 - 2.0 * c) * D[k] + (1.0 + c) * D2[k] - D3[k]) / (1.0 - c);
+    else D[k] = ((1.0 + c) * D2[k] - D3[k]) / c;
+}
+
+// cur = W - W^T (F D S - (F D S)^T, pscf/purif.c:553-558)
+__global__ void k_antisym(const double *__restrict__ W, double *__restrict__ cur, int n)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y;
+    if (j >= n) return;
+    cur[(size_t)i * n + j] = W[(size_t)i * n + j] - W[(size_t)j * n + i];
+}
+
+// block partials of <a, b_k> for k < m
+__global__ void k_dots(const double *__restrict__ a, const double *__restrict__ vecs, size_t nn, int m,
+                       double *__restrict__ part)
+{
+    __shared__ double s[RED_THREADS];
+    for (int k = 0; k < m; k++) {
+        const double *b = vecs + nn * k;
+        double v = 0.0;
+        for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += (size_t)gridDim.x * blockDim.x)
+            v += a[i] * b[i];
+        s[threadIdx.x] = v;
+        __syncthreads();
+        for (int st = RED_THREADS / 2; st > 0; st >>= 1) {
+            if (threadIdx.x < st) s[threadIdx.x] += s[threadIdx.x + st];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) part[blockIdx.x * PUR_MAX_DIIS + k] = s[0];
+        __syncthreads();
+    }
+}
+
+struct Coeffs {
+    double c[PUR_MAX_DIIS];
+};
+
+__global__ void k_combine(double *__restrict__ F, const double *__restrict__ Fvecs, size_t nn, int m, Coeffs co)
+{
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nn) return;
+    double v = 0.0;
+    for (int i = 0; i < m; i++) v += co.c[i] * Fvecs[nn * i + k];
+    F[k] = v;
+}
+
+extern "C" int gtf_purif_create(int nbf, int nocc, void *stream, gtf_purif_dev_t **out)
+{
+    *out = nullptr;
+    if (nbf <= 0 || nocc < 0 || nocc > nbf) return GTF_ERR_INVALID;
+    gtf_purif_dev *p = new gtf_purif_dev();
+    memset(p, 0, sizeof(*p));
+    p->n = nbf;
+    p->nocc = nocc;
+    p->st = (cudaStream_t)stream;
+    if (!p->st) CKP(cudaStreamCreateWithFlags(&p->st, cudaStreamNonBlocking));
+    CKB(cublasCreate(&p->blas));
+    CKB(cublasSetStream(p->blas, p->st));
+    const size_t nn = (size_t)nbf * nbf;
+    double **bufs[] = {&p->S, &p->X, &p->D, &p->D2, &p->D3, &p->F, &p->W, &p->W2};
+    for (double **b : bufs) CKP(cudaMalloc((void **)b, sizeof(double) * nn));
+    CKP(cudaMalloc((void **)&p->vecs, sizeof(double) * nn * PUR_MAX_DIIS));
+    CKP(cudaMalloc((void **)&p->Fvecs, sizeof(double) * nn * PUR_MAX_DIIS));
+    CKP(cudaMalloc((void **)&p->part, sizeof(double) * RED_BLOCKS * 16));
+    CKP(cudaMalloc((void **)&p->scal, sizeof(double) * 16));
+    CKP(cudaMallocHost((void **)&p->h_scal, sizeof(double) * 16));
+    CKP(cudaEventCreate(&p->e0));
+    CKP(cudaEventCreate(&p->e1));
+    p->bmax = DBL_MIN;
+    p->bmax_id = -1;
+    for (int i = 0; i < PUR_LDB; i++)
+        for (int j = 0; j < PUR_LDB; j++) p->b[i * PUR_LDB + j] = (i != j) ? -1.0 : 0.0;
+    *out = p;
+    return GTF_OK;
+}
+
+extern "C" void gtf_purif_destroy(gtf_purif_dev_t *p)
+{
+    if (!p) return;
+    cudaStreamSynchronize(p->st);
+    double *bufs[] = {p->S, p->X, p->D, p->D2, p->D3, p->F, p->W, p->W2, p->vecs, p->Fvecs, p->part, p->scal};
+    for (double *b : bufs)
+        if (b) cudaFree(b);
+    if (p->h_scal) cudaFreeHost(p->h_scal);
+    cublasDestroy(p->blas);
+    cudaEventDestroy(p->e0);
+    cudaEventDestroy(p->e1);
+    delete p;
+}
+
+extern "C" int gtf_purif_set_sx(gtf_purif_dev_t *p, const double *S_host, const double *X_host)
+{
+    const size_t nn = (size_t)p->n * p->n;
+    CKP(cudaMemcpyAsync(p->S, S_host, sizeof(double) * nn, cudaMemcpyHostToDevice, p->st));
+    CKP(cudaMemcpyAsync(p->X, X_host, sizeof(double) * nn, cudaMemcpyHostToDevice, p->st));
+    CKP(cudaStreamSynchronize(p->st));
+    p->sx_set = 1;
+    return GTF_OK;
+}
+
+extern "C" int gtf_purif_set_sx_dev(gtf_purif_dev_t *p, const double *S_dev, const double *X_dev)
+{
+    const size_t nn = (size_t)p->n * p->n;
+    CKP(cudaMemcpyAsync(p->S, S_dev, sizeof(double) * nn, cudaMemcpyDeviceToDevice, p->st));
+    CKP(cudaMemcpyAsync(p->X, X_dev, sizeof(double) * nn, cudaMemcpyDeviceToDevice, p->st));
+    p->sx_set = 1;
+    return GTF_OK;
+}
+
+extern "C" int gtf_purif_run_dev(gtf_purif_dev_t *p, const double *F_dev, double *D_dev, int *iters)
+{
+    const int n = p->n;
+    const size_t nn = (size_t)n * n;
+    const unsigned ge = (unsigned)((nn + 255) / 256);
+    cudaStream_t st = p->st;
+    CKP(cudaEventRecord(p->e0, st));
+    k_gersh<<<RED_BLOCKS, RED_THREADS, 0, st>>>(F_dev, n, p->part);
+    k_purif_init<<<1, 32, 0, st>>>(p->part, RED_BLOCKS, n, p->nocc, p->scal);
+    k_purif_d0<<<ge, 256, 0, st>>>(F_dev, p->D, n, p->scal);
+    CKP(cudaGetLastError());
+    int it;
+    double err = 0.0;
+    for (it = 0; it < PUR_MAX_ITERS; it++) {
+        if (gemm_abt(p, p->D, p->D, p->D2)) return GTF_ERR_CUDA;
+        if (gemm_ab(p, p->D, p->D2, p->D3)) return GTF_ERR_CUDA;
+        k_purif_stats<<<RED_BLOCKS, RED_THREADS, 0, st>>>(p->D, p->D2, p->D3, n, p->part);
+        k_purif_finish<<<1, 32, 0, st>>>(p->part, RED_BLOCKS, p->scal);
+        k_purif_update<<<ge, 256, 0, st>>>(p->D, p->D2, p->D3, nn, p->scal);
+        CKP(cudaGetLastError());
+        CKP(cudaMemcpyAsync(p->h_scal + 6, p->scal + 6, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
+        CKP(cudaStreamSynchronize(st));
+        err = p->h_scal[6];
+        if (err < 1e-11) break;
+    }
+    p->errnorm = err;
+    // D_AO = X D X (pscf/purif.c:469-476)
+    if (gemm_abt(p, p->X, p->D, p->W)) return GTF_ERR_CUDA;
+    if (gemm_abt(p, p->W, p->X, D_dev)) return GTF_ERR_CUDA;
+    CKP(cudaEventRecord(p->e1, st));
+    CKP(cudaEventSynchronize(p->e1));
+    float ms = 0.0f;
+    CKP(cudaEventElapsedTime(&ms, p->e0, p->e1));
+    p->ms_total = ms;
+    if (iters) *iters = (it < PUR_MAX_ITERS) ? it : PUR_MAX_ITERS;
+    return GTF_OK;
+}
+
+extern "C" int gtf_purif_run(gtf_purif_dev_t *p, const double *F_host, double *D_host, int *iters)
+{
+    const size_t nn = (size_t)p->n * p->n;
+    CKP(cudaMemcpyAsync(p->F, F_host, sizeof(double) * nn, cudaMemcpyHostToDevice, p->st));
+    int r = gtf_purif_run_dev(p, p->F, p->D2, iters);
+    if (r) return r;
+    CKP(cudaMemcpyAsync(D_host, p->D2, sizeof(double) * nn, cudaMemcpyDeviceToHost, p->st));
+    CKP(cudaStreamSynchronize(p->st));
+    return GTF_OK;
+}
+
+// inverse of the bordered DIIS matrix (symmetric, order <= 11) by Gauss-Jordan
+// elimination with partial pivoting; returns coeffs[i] = -inv[i][m]
+static void diis_coeffs(const double *b, int m, double *coeffs)
+{
+    const int s = m + 1;
+    double a[PUR_MAX_DIIS + 1][2 * (PUR_MAX_DIIS + 1)];
+    for (int i = 0; i < s; i++)
+        for (int j = 0; j < s; j++) {
+            a[i][j] = b[i * PUR_LDB + j];
+            a[i][s + j] = (i == j) ? 1.0 : 0.0;
+        }
+    for (int c = 0; c < s; c++) {
+        int piv = c;
+        for (int r = c + 1; r < s; r++)
+            if (fabs(a[r][c]) > fabs(a[piv][c])) piv = r;
+        if (piv != c)
+            for (int j = 0; j < 2 * s; j++) {
+                double t = a[c][j];
+                a[c][j] = a[piv][j];
+                a[piv][j] = t;
+            }
+        const double d = a[c][c];
+        for (int j = 0; j < 2 * s; j++) a[c][j] /= d;
+        for (int r = 0; r < s; r++) {
+            if (r == c) continue;
+            const double f = a[r][c];
+            if (f == 0.0) continue;
+            for (int j = 0; j < 2 * s; j++) a[r][j] -= f * a[c][j];
+        }
+    }
+    for (int i = 0; i < s; i++) coeffs[i] = -a[i][s + s - 1];
+}
+
+extern "C" int gtf_diis_step_dev(gtf_purif_dev_t *p, const double *D_dev, double *F_dev, int iter)
+{
+    const int n = p->n;
+    const size_t nn = (size_t)n * n;
+    cudaStream_t st = p->st;
+    double *cur_F = F_dev;
+    if (iter > 1) {
+        int cur_idx;
+        if (p->len_diis < PUR_MAX_DIIS) {
+            cur_idx = p->len_diis;
+            p->len_diis++;
+        } else {
+            cur_idx = p->bmax_id;
+        }
+        double *cur = p->vecs + nn * cur_idx;
+        cur_F = p->Fvecs + nn * cur_idx;
+        if (gemm_abt(p, F_dev, D_dev, p->W)) return GTF_ERR_CUDA;
+        if (gemm_abt(p, p->W, p->S, p->W2)) return GTF_ERR_CUDA;
+        dim3 g((n + 127) / 128, n);
+        k_antisym<<<g, 128, 0, st>>>(p->W2, cur, n);
+        if (gemm_abt(p, p->X, cur, p->W)) return GTF_ERR_CUDA;
+        if (gemm_abt(p, p->W, p->X, cur)) return GTF_ERR_CUDA;
+        k_dots<<<RED_BLOCKS, RED_THREADS, 0, st>>>(cur, p->vecs, nn, p->len_diis, p->part);
+        CKP(cudaGetLastError());
+        static double hpart[RED_BLOCKS * PUR_MAX_DIIS];
+        CKP(cudaMemcpyAsync(hpart, p->part, sizeof(double) * RED_BLOCKS * PUR_MAX_DIIS, cudaMemcpyDeviceToHost, st));
+        CKP(cudaStreamSynchronize(st));
+        for (int i = 0; i < p->len_diis; i++) {
+            double v = 0.0;
+            for (int bk = 0; bk < RED_BLOCKS; bk++) v += hpart[bk * PUR_MAX_DIIS + i];
+            p->b[cur_idx * PUR_LDB + i] = v;
+        }
+        p->bmax = -DBL_MAX;
+        for (int i = 0; i < p->len_diis; i++) {
+            p->b[i * PUR_LDB + cur_idx] = p->b[cur_idx * PUR_LDB + i];
+            if (p->bmax < p->b[i * PUR_LDB + i]) {
+                p->bmax = p->b[i * PUR_LDB + i];
+                p->bmax_id = i;
+            }
+        }
+    }
+    // F = X F X
+    if (gemm_abt(p, p->X, F_dev, p->W)) return GTF_ERR_CUDA;
+    if (gemm_abt(p, p->W, p->X, cur_F)) return GTF_ERR_CUDA;
+    if (iter > 1) {
+        double co[PUR_MAX_DIIS + 1];
+        diis_coeffs(p->b, p->len_diis, co);
+        Coeffs c;
+        for (int i = 0; i < PUR_MAX_DIIS; i++) c.c[i] = (i < p->len_diis) ? co[i] : 0.0;
+        k_combine<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(F_dev, p->Fvecs, nn, p->len_diis, c);
+        CKP(cudaGetLastError());
+    }
+    return GTF_OK;
+}
+
+extern "C" int gtf_diis_step(gtf_purif_dev_t *p, const double *D_host, double *F_host, int iter)
+{
+    const size_t nn = (size_t)p->n * p->n;
+    CKP(cudaMemcpyAsync(p->F, F_host, sizeof(double) * nn, cudaMemcpyHostToDevice, p->st));
+    CKP(cudaMemcpyAsync(p->D3, D_host, sizeof(double) * nn, cudaMemcpyHostToDevice, p->st));
+    int r = gtf_diis_step_dev(p, p->D3, p->F, iter);
+    if (r) return r;
+    CKP(cudaMemcpyAsync(F_host, p->F, sizeof(double) * nn, cudaMemcpyDeviceToHost, p->st));
+    CKP(cudaStreamSynchronize(p->st));
+    return GTF_OK;
+}
+
+extern "C" int gtf_purif_stats(gtf_purif_dev_t *p, double *ms_gemm, double *ms_total, double *errnorm,
+                               double *idem_err, double *tr_err)
+{
+    if (ms_gemm) *ms_gemm = p->ms_gemm;
+    if (ms_total) *ms_total = p->ms_total;
+    if (errnorm) *errnorm = p->errnorm;
+    if (idem_err) *idem_err = p->idem;
+    if (tr_err) *tr_err = p->trerr;
+    return GTF_OK;
+}

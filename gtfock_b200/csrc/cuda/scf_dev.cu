@@ -1,0 +1,84 @@
+// scf_dev.cu -- small device helpers for the device-resident SCF driver
+// (energy of pscf/scf.c:80-102 with F += H fused) and device queries.
+#include <cuda_runtime.h>
+#include <stdio.h>
+
+#include "gtf_cuda.h"
+
+#define EN_BLOCKS 148
+#define EN_THREADS 256
+
+// F += H; block partials of sum D (H + F)
+__global__ void k_energy(double *__restrict__ F, const double *__restrict__ H, const double *__restrict__ D,
+                         size_t nn, double *__restrict__ part)
+{
+    __shared__ double s[EN_THREADS];
+    double e = 0.0;
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += (size_t)gridDim.x * blockDim.x) {
+        const double f = F[k] + H[k];
+        F[k] = f;
+        e += D[k] * (H[k] + f);
+    }
+    s[threadIdx.x] = e;
+    __syncthreads();
+    for (int st = EN_THREADS / 2; st > 0; st >>= 1) {
+        if (threadIdx.x < st) s[threadIdx.x] += s[threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = s[0];
+}
+
+extern "C" int gtf_dev_malloc(void **p, size_t bytes)
+{
+    return cudaMalloc(p, bytes) == cudaSuccess ? GTF_OK : GTF_ERR_ALLOC;
+}
+
+extern "C" void gtf_dev_free(void *p)
+{
+    if (p) cudaFree(p);
+}
+
+extern "C" int gtf_dev_copy(void *dst, const void *src, size_t bytes, int kind, void *stream)
+{
+    cudaMemcpyKind k = kind == 0 ? cudaMemcpyHostToDevice : kind == 1 ? cudaMemcpyDeviceToHost
+                                                                       : cudaMemcpyDeviceToDevice;
+    if (cudaMemcpyAsync(dst, src, bytes, k, (cudaStream_t)stream) != cudaSuccess) return GTF_ERR_CUDA;
+    if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) return GTF_ERR_CUDA;
+    return GTF_OK;
+}
+
+// F (device) += H (device); returns sum D (H + F) (deterministic order)
+extern "C" int gtf_dev_energy(double *F, const double *H, const double *D, int n, void *stream, double *energy)
+{
+    static double *part = nullptr;
+    static double *hpart = nullptr;
+    if (!part) {
+        if (cudaMalloc((void **)&part, sizeof(double) * EN_BLOCKS) != cudaSuccess) return GTF_ERR_ALLOC;
+        if (cudaMallocHost((void **)&hpart, sizeof(double) * EN_BLOCKS) != cudaSuccess) return GTF_ERR_ALLOC;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    k_energy<<<EN_BLOCKS, EN_THREADS, 0, st>>>(F, H, D, (size_t)n * n, part);
+    if (cudaGetLastError() != cudaSuccess) return GTF_ERR_CUDA;
+    if (cudaMemcpyAsync(hpart, part, sizeof(double) * EN_BLOCKS, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return GTF_ERR_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return GTF_ERR_CUDA;
+    double e = 0.0;
+    for (int b = 0; b < EN_BLOCKS; b++) e += hpart[b];
+    *energy = e;
+    return GTF_OK;
+}
+
+extern "C" int gtf_device_info(int *ndev, int *cc)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) n = 0;
+    if (ndev) *ndev = n;
+    if (cc) {
+        *cc = -1;
+        if (n > 0) {
+            cudaDeviceProp pr;
+            if (cudaGetDeviceProperties(&pr, 0) == cudaSuccess) *cc = pr.major * 10 + pr.minor;
+        }
+    }
+    return n > 0 ? 0 : -1;
+}

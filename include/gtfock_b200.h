@@ -1,0 +1,64 @@
+/*
+ * gtfock_b200.h -- entry points of libgtfock_b200 beyond GTFock's own API.
+ *
+ * The drop-in API is pfock.h / purif.h / CInt.h.  The functions below expose
+ * what the reference keeps inside its PFock struct (screening lists,
+ * counters), the device-resident forms used by the benchmark, and the native
+ * SCF driver.  Plain C types only; 0 (or PFOCK_STATUS_SUCCESS) on success.
+ */
+#ifndef GTFOCK_B200_H
+#define GTFOCK_B200_H
+
+#include "CInt.h"
+#include "pfock.h"
+#include "purif.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Screening results of PFock_create: the reference's PFock fields nnz,
+ * maxvalue (pfock/pfock.h:22-29) and the quartet counters usq / uitl that
+ * PFock_getStatistics reports (pfock/fock_task.c:195-196). */
+PFockStatus_t gtf_pfock_counts(PFock_t pfock, int *nnz, double *maxvalue,
+                               double *usq, double *uitl);
+
+/* Copy of the CSR shell-pair list (shellptr[nshells+1], shellid[nnz],
+ * shellrid[nnz], shellvalue[nnz]) built as pfock/screening.c:110-175. */
+PFockStatus_t gtf_pfock_screening(PFock_t pfock, int *shellptr, int *shellid,
+                                  int *shellrid, double *shellvalue);
+
+/* CUDA-event timings (ms) of the last PFock_computeFock: whole build and the
+ * electron-repulsion kernels alone; Rys-model FLOPs of one build. */
+PFockStatus_t gtf_pfock_timing(PFock_t pfock, double *ms_total, double *ms_eri,
+                               double *eri_flops);
+
+/* Precision of the ERI kernels: 0 = FP64 (default), 1 = FP32 for quartets
+ * whose Schwarz bound sqrt(v1 v2) is below fp32_cutoff. */
+PFockStatus_t gtf_pfock_set_precision(PFock_t pfock, int mode, double fp32_cutoff);
+
+/* Device-resident Fock build for callers that keep D on the GPU: dev_D is a
+ * device pointer to the nbf x nbf density; the result stays on the device
+ * (returned through *dev_F, valid until the next build). */
+PFockStatus_t gtf_pfock_compute_dev(PFock_t pfock, const double *dev_D,
+                                    const double **dev_F);
+
+/* Native SCF driver: the loop of pscf/scf.c:329-459 (Fock build, energy,
+ * DIIS, purification) on one GPU for the molecule in xyzfile with basis
+ * bsfile.  energies[k] = total energy (incl. nuclear) of iteration k.
+ * mode 0: host D/F buffers cross the C API every iteration (as scf.c);
+ * mode 1: D and F stay resident on the device.  Returns iterations run, or
+ * a negative value on error.  timings (optional, 4 doubles): seconds in Fock
+ * builds, DIIS, purification, total. */
+int gtf_scf_run(const char *bsfile, const char *xyzfile, double tolscr,
+                int niters, int mode, double *energies, double *timings);
+
+/* Device and library identification for tests: number of CUDA devices seen
+ * and the compute capability of device 0 (major*10+minor); -1 on error. */
+int gtf_device_info(int *ndev, int *cc);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
