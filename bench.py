@@ -1,0 +1,328 @@
+"""Benchmark: SCF solves/s of the Fock-build + purification path on one B200.
+
+Workload (default): C54H18 hexagonal graphene flake (C-C 1.42 A, C-H 1.09 A),
+cc-pVDZ (846 functions), Schwarz threshold 1e-10, 10 SCF iterations from the
+core-Hamiltonian guess, all FP64.  One step = one SCF solve.
+
+  value      SCF solves/s with the engine set up and D/F/S/X/H resident on the
+             device (gtf_scf_solve, mode 1), CUDA-event timed on the engine's
+             stream; max over ranks.
+  e2e        SCF solves/s through the reference-facing C API with host
+             buffers (gtf_scf_run, mode 0: basis load, PFock_create, one-
+             electron set-up, and every iteration's putDenMat / getMat /
+             compute_diis / compute_purification host<->device copies).
+  roofline   the electron-repulsion kernels of one Fock build: Rys-model FLOPs
+             (normalisation of the quartet work) / their CUDA-event time,
+             against this device's FP64 FMA rate measured in-run by a probe
+             kernel (no FP64 figure exists in MEASURED_PEAKS.json).
+  cpu_baseline  the CPU restatement of the reference path (oracle/) on all
+             host cores: a bounded sample of one Fock build (every k-th bra
+             shell pair) scaled by the quartet-count ratio, plus one measured
+             DIIS + purification step, extrapolated to the solve.
+
+--impl reference prints the same metric for the reference's CPU path (the
+oracle port, sampled as above), as the reference arm.
+Multi-GPU: molecules are independent, so N GPUs run N replicas of the solve
+(no collective); value = N solves / max-over-ranks time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+TOL = 1e-10
+NITER = 10
+METRIC = "SCF solves/s (C54H18 cc-pVDZ, 10 iterations, FP64)"
+WORKLOAD = "C54H18 graphene flake / cc-pVDZ (846 bf), Schwarz 1e-10, 10 SCF iterations, FP64"
+
+
+def _dist():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons every 200 ms while running."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 5 + i and r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def make_workload(td):
+    from gtfock_b200 import molecules as mol
+    xyz = mol.write_xyz(mol.graphene_flake(2), os.path.join(td, "c54h18.xyz"), "C54H18")
+    return mol.basis_file("cc-pvdz"), xyz
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def cpu_baseline(gbs, xyz, target_s=15.0):
+    """Sampled CPU restatement of one SCF solve on all host cores."""
+    import numpy as np
+    from oracle import pyoracle as po
+    cores = os.cpu_count()
+    b = po.Basis(gbs, xyz)
+    po.lib().or_set_blas_threads(cores)
+    scr = po.screening(b, TOL, cores)
+    D = np.eye(b.nbf) * 0.3
+    usq_total, _, _ = po.fock_build_sample(b, TOL, D, 1, count_only=True, scr=scr, nthreads=cores)
+    # calibrate the stride on small samples until one takes ~target_s
+    stride = 4096
+    usq_s, _, dt = po.fock_build_sample(b, TOL, D, stride, scr=scr, nthreads=cores)
+    for _ in range(3):
+        if dt >= 0.6 * target_s or stride == 1 or usq_s == 0:
+            break
+        stride = max(1, int(stride * dt / target_s)) if dt > 0.05 else max(1, stride // 8)
+        usq_s, _, dt = po.fock_build_sample(b, TOL, D, stride, scr=scr, nthreads=cores)
+    t_fock = dt * usq_total / usq_s
+    # one DIIS step (iter > 1 form, 6 GEMMs) + one purification, full size
+    S, H, X = po.one_electron(b)
+    F = H.copy()
+    state = None
+    t_diis = 0.0
+    for it in range(3):
+        F2, t, state = po.diis_step_timed(X, S, D, F, it, state)
+        t_diis = t
+    t0 = time.perf_counter()
+    _, pits = po.purification(b.nocc, X, F2)
+    t_pur = time.perf_counter() - t0
+    t_solve = NITER * (t_fock + t_diis + t_pur)
+    return {
+        "value": 1.0 / t_solve, "unit": "solves/s", "cores": cores, "kind": "port",
+        "sample": "every %d-th bra shell pair of one C54H18/cc-pVDZ Fock build (%d of %d quartets, "
+                  "%.1f s) scaled by the quartet ratio; DIIS + purification (%d iterations) timed "
+                  "once at full size; x%d iterations" % (stride, usq_s, usq_total, dt, pits, NITER),
+        "fock_build_s_est": t_fock, "diis_s": t_diis, "purif_s": t_pur,
+    }
+
+
+def run_reference(args):
+    rank, world, _ = _dist()
+    if rank != 0:
+        return
+    with tempfile.TemporaryDirectory() as td:
+        gbs, xyz = make_workload(td)
+        per = []
+        for _ in range(args.warmup + args.steps):
+            per.append(cpu_baseline(gbs, xyz, target_s=8.0))
+        timed = per[args.warmup:]
+        v = statistics.median([p["value"] for p in timed])
+        cb = dict(timed[-1])
+        cb["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "parallelism": "cpu (%d threads)" % cb["cores"]},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run(args):
+    import numpy as np
+    import gtfock_b200 as gb
+    rank, world, local = _dist()
+    pg = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+        pg = dist
+    os.environ.setdefault("CUDA_VISIBLE_DEVICES", os.environ.get("CUDA_VISIBLE_DEVICES", ""))
+    n, cc = gb.device_info()
+    if n < 1:
+        raise SystemExit("no CUDA device")
+    with tempfile.TemporaryDirectory() as td:
+        gbs, xyz = make_workload(td)
+        solver = gb.SCFSolver(gbs, xyz, TOL)
+        nbf = solver.nbf
+        # warm-up solves (device-resident)
+        for _ in range(args.warmup):
+            e_warm, _ = solver.solve(NITER, device_resident=True)
+        # timed region: value (device-resident)
+        if pg:
+            pg.barrier()
+        l0 = gb.launch_count()
+        with ClockSampler(local) as clk:
+            t0 = time.perf_counter()
+            energies = None
+            fock_s = diis_s = pur_s = 0.0
+            for _ in range(args.steps):
+                energies, tm = solver.solve(NITER, device_resident=True)
+                fock_s += tm["fock_s"]
+                diis_s += tm["diis_s"]
+                pur_s += tm["purif_s"]
+            dt = time.perf_counter() - t0
+        launches = gb.launch_count() - l0
+        if pg:
+            import torch
+            t = torch.tensor([dt], device="cuda")
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            dt = float(t.item())
+        clocks = clk.summary()
+        # one Fock build's ERI kernels for the roofline
+        pf_basis = gb.BasisSet(gbs, xyz)
+        pf = gb.PFock(pf_basis, tolscr=TOL)
+        D = np.eye(nbf) * 0.3
+        eri_ms = []
+        for k in range(4):
+            pf.compute_fock(D)
+            if k:
+                eri_ms.append(pf.timing()["ms_eri"])
+        tm = pf.timing()
+        counts = pf.counts()
+        eri_flops = tm["eri_flops"]
+        pf.close()
+        solver.close()
+        # e2e through the C API with host buffers (set-up included)
+        e2e_times = []
+        e2e_bytes = (0, 0)
+        for k in range(1 + max(1, args.steps // 2)):
+            t1 = time.perf_counter()
+            e_e2e, te = gb.scf_run(gbs, xyz, TOL, NITER, device_resident=False)
+            if k:
+                e2e_times.append(time.perf_counter() - t1)
+            e2e_bytes = (te["h2d_bytes"], te["d2h_bytes"])
+        fp64_peak = gb.fp64_peak_gflops()
+    value = world * args.steps / dt
+    eri_s = statistics.median(eri_ms) * 1e-3
+    achieved = eri_flops / eri_s / 1e12
+    peak = fp64_peak / 1e3
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1000.0,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (generated C54H18 geometry)",
+        "config": {"workload": WORKLOAD, "nbf": nbf, "parallelism": "replicas x%d" % world,
+                   "l2": "inputs resident; F/D working set (2 x 5.7 MB) stays in L2 by design",
+                   "usq": counts["usq"], "uitl": counts["uitl"], "nnz_pairs": counts["nnz"]},
+        "energy_last": float(energies[-1]) if energies is not None else None,
+        "phase_s_per_solve": {"fock": fock_s / args.steps, "diis": diis_s / args.steps,
+                              "purification": pur_s / args.steps},
+        "e2e": {"value": 1.0 / statistics.median(e2e_times), "unit": "solves/s",
+                "h2d_bytes_per_step": int(e2e_bytes[0]), "d2h_bytes_per_step": int(e2e_bytes[1])},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "kernel": "k_fock<*> (all class pairs of one Fock build)",
+                     "peak_source": "FP64 FMA probe kernel measured in this run "
+                                    "(MEASURED_PEAKS.json has no FP64 figure)",
+                     "work": "Rys-model FLOPs per build %.4g" % eri_flops,
+                     "eri_ms_per_build": eri_s * 1e3},
+        "clocks": clocks,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        with tempfile.TemporaryDirectory() as td2:
+            g2, x2 = make_workload(td2)
+            cb = cpu_baseline(g2, x2)
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def profile_fock(args):
+    """A few Fock builds of one molecule with per-class-pair kernel times (the
+    small cases profiled with ncu): c12h26 (298 bf) or c54h18 (846 bf)."""
+    import numpy as np
+    import gtfock_b200 as gb
+    from gtfock_b200 import molecules as mol
+    atoms = {"c12h26": mol.alkane(12), "c54h18": mol.graphene_flake(2),
+             "c96h24": mol.graphene_flake(3)}[args.profile_fock]
+    with tempfile.TemporaryDirectory() as td:
+        xyz = mol.write_xyz(atoms, os.path.join(td, args.profile_fock + ".xyz"))
+        b = gb.BasisSet(mol.basis_file("cc-pvdz"), xyz)
+        pf = gb.PFock(b, tolscr=TOL)
+        D = np.eye(b.nbf) * 0.3
+        for _ in range(args.builds):
+            pf.compute_fock(D)
+        tm = pf.timing()
+        out = {"molecule": args.profile_fock, "nbf": b.nbf, "counts": pf.counts(), "timing": tm,
+               "classes": [{"bra": x, "ket": y, "ms": ms, "quartets": q}
+                           for x, y, ms, q in pf.class_stats() if q > 0]}
+        pf.close()
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gtfock_b200", choices=["gtfock_b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-fock", choices=["c12h26", "c54h18", "c96h24"], default=None)
+    ap.add_argument("--builds", type=int, default=2)
+    args = ap.parse_args()
+    if args.profile_fock:
+        profile_fock(args)
+        return
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -91,7 +91,14 @@ def load():
     _sig(L, "gtf_pfock_screening", [_vp, _ip, _ip, _ip, _dp])
     _sig(L, "gtf_pfock_timing", [_vp, _dp, _dp, _dp])
     _sig(L, "gtf_pfock_set_precision", [_vp, _i, _d])
+    _sig(L, "gtf_pfock_class_stats", [_vp, _ip, _ip, _dp, _dp])
     _sig(L, "gtf_scf_run", [_cp, _cp, _d, _i, _i, _dp, _dp])
+    _sig(L, "gtf_scf_create", [_cp, _cp, _d], _vp)
+    _sig(L, "gtf_scf_solve", [_vp, _i, _i, _dp, _dp])
+    _sig(L, "gtf_scf_nbf", [_vp])
+    _sig(L, "gtf_scf_destroy", [_vp], None)
+    _sig(L, "gtf_launch_count", [], ctypes.c_ulonglong)
+    _sig(L, "gtf_fp64_peak", [_dp])
     _sig(L, "gtf_device_info", [_ip, _ip])
     _lib = L
     return L
@@ -215,6 +222,15 @@ class PFock:
         load().gtf_pfock_timing(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
         return {"ms_total": a.value, "ms_eri": b.value, "eri_flops": c.value}
 
+    def class_stats(self):
+        """[(bra class, ket class, ms, quartets)] of the last build."""
+        X = np.zeros(32, np.int32)
+        Y = np.zeros(32, np.int32)
+        ms = np.zeros(32)
+        nq = np.zeros(32)
+        n = load().gtf_pfock_class_stats(self.h, _iptr(X), _iptr(Y), _dptr(ms), _dptr(nq))
+        return [(int(X[i]), int(Y[i]), float(ms[i]), float(nq[i])) for i in range(n)]
+
     def set_precision(self, mode, fp32_cutoff=0.0):
         self._check(load().gtf_pfock_set_precision(self.h, mode, fp32_cutoff),
                     "gtf_pfock_set_precision")
@@ -288,14 +304,56 @@ class _PurifT(ctypes.Structure):
                 ("D_block", _dp)]
 
 
+def _timings(t):
+    return {"fock_s": t[0], "diis_s": t[1], "purif_s": t[2], "total_s": t[3],
+            "h2d_bytes": t[4], "d2h_bytes": t[5], "launches": int(t[6])}
+
+
 def scf_run(gbs, xyz, tolscr=1e-10, niters=10, device_resident=False):
-    """Native SCF loop of pscf/scf.c on the GPU (gtf_scf_run): returns
-    (energies per iteration, timings dict)."""
+    """Native SCF loop of pscf/scf.c on the GPU (gtf_scf_run: set-up, solve,
+    tear-down): returns (energies per iteration, timings dict)."""
     L = load()
     e = np.zeros(niters)
-    t = np.zeros(4)
+    t = np.zeros(8)
     it = L.gtf_scf_run(gbs.encode(), xyz.encode(), tolscr, niters, 1 if device_resident else 0,
                        _dptr(e), _dptr(t))
     if it < 0:
         raise GtfError("gtf_scf_run failed (%d)" % it)
-    return e[:it], {"fock_s": t[0], "diis_s": t[1], "purif_s": t[2], "total_s": t[3]}
+    return e[:it], _timings(t)
+
+
+class SCFSolver:
+    """Set up once (gtf_scf_create), then solve repeatedly (gtf_scf_solve)."""
+
+    def __init__(self, gbs, xyz, tolscr=1e-10):
+        L = load()
+        self.h = L.gtf_scf_create(gbs.encode(), xyz.encode(), tolscr)
+        if not self.h:
+            raise GtfError("gtf_scf_create failed")
+        self.nbf = L.gtf_scf_nbf(self.h)
+
+    def solve(self, niters=10, device_resident=True):
+        e = np.zeros(niters)
+        t = np.zeros(8)
+        it = load().gtf_scf_solve(self.h, niters, 1 if device_resident else 0, _dptr(e), _dptr(t))
+        if it < 0:
+            raise GtfError("gtf_scf_solve failed (%d)" % it)
+        return e[:it], _timings(t)
+
+    def close(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.gtf_scf_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+
+def launch_count():
+    return int(load().gtf_launch_count())
+
+
+def fp64_peak_gflops():
+    g = ctypes.c_double()
+    if load().gtf_fp64_peak(ctypes.byref(g)) != 0:
+        raise GtfError("gtf_fp64_peak failed")
+    return g.value

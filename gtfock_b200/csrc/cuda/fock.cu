@@ -39,6 +39,7 @@
 static thread_local char g_errbuf[512];
 
 extern "C" const char *gtf_last_error(void) { return g_errbuf; }
+extern "C" void gtf_note_launches(int n);
 
 #define CK(call)                                                                          \
     do {                                                                                  \
@@ -105,7 +106,9 @@ struct gtf_fock_dev {
     size_t host_stage_bytes;
     // timing
     cudaEvent_t ev0, ev1, ev2, ev3;
+    cudaEvent_t ev_cls[NCLSPAIR + 1];
     double ms_total, ms_eri, ms_other;
+    double ms_cls[NCLSPAIR];
     int prec;
     double fp32_cutoff;
     size_t dev_bytes;
@@ -516,6 +519,7 @@ static int upload_basis(gtf_fock_dev *f, const gtf_basis_view_t *b)
     CK(cudaEventCreate(&f->ev1));
     CK(cudaEventCreate(&f->ev2));
     CK(cudaEventCreate(&f->ev3));
+    for (int c = 0; c <= NCLSPAIR; c++) CK(cudaEventCreate(&f->ev_cls[c]));
     f->natoms = b->natoms;
     f->nshells = b->nshells;
     f->nbf = b->nbf;
@@ -875,6 +879,8 @@ extern "C" void gtf_fock_destroy(gtf_fock_dev_t *f)
     cudaEventDestroy(f->ev1);
     cudaEventDestroy(f->ev2);
     cudaEventDestroy(f->ev3);
+    for (int c = 0; c <= NCLSPAIR; c++)
+        if (f->ev_cls[c]) cudaEventDestroy(f->ev_cls[c]);
     cudaStreamDestroy(f->stream);
     delete f;
 }
@@ -988,6 +994,7 @@ extern "C" int gtf_fock_compute(gtf_fock_dev_t *f, int numdmat)
                                            f->d_fc_start, nbf, nbfc, f->pure);
             CK(cudaGetLastError());
             Dc = f->d_Dc;
+            gtf_note_launches(1);
         }
         CK(cudaMemsetAsync(f->d_Fj, 0, sizeof(double) * nnc, st));
         CK(cudaMemsetAsync(f->d_Fk, 0, sizeof(double) * nnc, st));
@@ -995,6 +1002,7 @@ extern "C" int gtf_fock_compute(gtf_fock_dev_t *f, int numdmat)
         CK(cudaEventRecord(f->ev1, st));
         for (int c = 0; c < NCLSPAIR; c++) {
             ClassPairTask &t = f->tasks[c];
+            CK(cudaEventRecord(f->ev_cls[c], st));
             if (t.nunits == 0) continue;
             FockLaunch a;
             a.pairs = f->d_pairs;
@@ -1012,22 +1020,30 @@ extern "C" int gtf_fock_compute(gtf_fock_dev_t *f, int numdmat)
             a.ld = nbfc;
             a.nsm = f->nsm;
             const int r = launch_fock(t.X, t.Y, a, st);
+            gtf_note_launches(1);
             if (r != 0) {
                 snprintf(g_errbuf, sizeof(g_errbuf), "Fock kernel launch for class pair (%d,%d) failed: %d (%s)",
                          t.X, t.Y, r, cudaGetErrorString(cudaGetLastError()));
                 return GTF_ERR_CUDA;
             }
         }
+        CK(cudaEventRecord(f->ev_cls[NCLSPAIR], st));
         CK(cudaEventRecord(f->ev2, st));
         dim3 g2((nbf + 127) / 128, nbf);
         k_f_to_sph<<<g2, 128, 0, st>>>(f->d_Fj, f->d_Fk, f->d_F + nn * d, f->d_J + nn * d, f->d_K + nn * d,
                                        f->d_sph2shell, f->d_sh_L, f->d_f_start, f->d_fc_start, nbf, nbfc,
                                        f->pure);
         CK(cudaGetLastError());
+        gtf_note_launches(1);
         CK(cudaEventSynchronize(f->ev2));
         float ms = 0.0f;
         CK(cudaEventElapsedTime(&ms, f->ev1, f->ev2));
         eri_ms_total += ms;
+        for (int c = 0; c < NCLSPAIR; c++) {
+            float mc = 0.0f;
+            CK(cudaEventElapsedTime(&mc, f->ev_cls[c], f->ev_cls[c + 1]));
+            f->ms_cls[c] = (d == 0 ? 0.0 : f->ms_cls[c]) + mc;
+        }
     }
     CK(cudaEventRecord(f->ev3, st));
     CK(cudaEventSynchronize(f->ev3));
@@ -1066,6 +1082,18 @@ extern "C" int gtf_fock_last_timing(gtf_fock_dev_t *f, double *ms_total, double 
     if (ms_eri) *ms_eri = f->ms_eri;
     if (ms_other) *ms_other = f->ms_other;
     return GTF_OK;
+}
+
+// per class pair of the last build: (X, Y) classes, ms, quartets, Rys-model FLOPs
+extern "C" int gtf_fock_class_stats(gtf_fock_dev_t *f, int *X, int *Y, double *ms, double *nquart)
+{
+    for (int c = 0; c < NCLSPAIR; c++) {
+        if (X) X[c] = f->tasks[c].X;
+        if (Y) Y[c] = f->tasks[c].Y;
+        if (ms) ms[c] = f->ms_cls[c];
+        if (nquart) nquart[c] = f->tasks[c].nquart;
+    }
+    return NCLSPAIR;
 }
 
 extern "C" int gtf_fock_eri_flops(gtf_fock_dev_t *f, double *flops)

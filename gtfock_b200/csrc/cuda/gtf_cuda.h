@@ -75,6 +75,9 @@ void gtf_fock_release_onee(gtf_fock_dev_t *f, int which);
 int gtf_fock_set_precision(gtf_fock_dev_t *f, int prec, double fp32_cutoff);
 int gtf_fock_last_timing(gtf_fock_dev_t *f, double *ms_total, double *ms_eri, double *ms_other);
 int gtf_fock_eri_flops(gtf_fock_dev_t *f, double *flops);
+/* per angular class pair (21 of them for s/p/d): classes, ms of the last
+ * build, quartet counts; returns the number of class pairs */
+int gtf_fock_class_stats(gtf_fock_dev_t *f, int *X, int *Y, double *ms, double *nquart);
 void *gtf_fock_stream(gtf_fock_dev_t *f);
 size_t gtf_fock_device_bytes(gtf_fock_dev_t *f);
 
@@ -90,8 +93,14 @@ int gtf_purif_run_dev(gtf_purif_dev_t *p, const double *F_dev, double *D_dev, in
 /* one DIIS step: F (AO, host or device) in, extrapolated orthogonal F out */
 int gtf_diis_step(gtf_purif_dev_t *p, const double *D_host, double *F_host, int iter);
 int gtf_diis_step_dev(gtf_purif_dev_t *p, const double *D_dev, double *F_dev, int iter);
+void gtf_purif_reset(gtf_purif_dev_t *p);
 int gtf_purif_stats(gtf_purif_dev_t *p, double *ms_gemm, double *ms_total, double *errnorm,
                     double *idem_err, double *tr_err);
+
+/* bookkeeping (scf_dev.cu) */
+void gtf_note_launches(int n);
+unsigned long long gtf_launch_count(void);
+int gtf_fp64_peak(double *gflops);
 
 #ifdef __cplusplus
 }

@@ -324,9 +324,11 @@ __device__ __forceinline__ void digest(const R (&I)[ncart(LA) * ncart(LB) * ncar
 #pragma unroll
                     for (int ic = 0; ic < NC; ic++)
                         v = fma((double)I[ia + NA * (ibb + NB * (ic + NC * id))], dcd[ic + NC * id], v);
+                // the factor depends on the lane's ket (f2), so apply it before the reduction
+                v *= sJab;
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(GTF_FULL_MASK, v, o);
-                if (lane == 0) atomicAdd(Fj + (size_t)(fa + ia) * ld + fb + ibb, sJab * v);
+                if (lane == 0) atomicAdd(Fj + (size_t)(fa + ia) * ld + fb + ibb, v);
             }
         }
     }

@@ -39,6 +39,8 @@
         }                                                               \
     } while (0)
 
+extern "C" void gtf_note_launches(int n);
+
 struct gtf_purif_dev {
     int n, nocc;
     cudaStream_t st;
@@ -284,6 +286,16 @@ extern "C" void gtf_purif_destroy(gtf_purif_dev_t *p)
     delete p;
 }
 
+// forget the DIIS history (a new SCF solve starts)
+extern "C" void gtf_purif_reset(gtf_purif_dev_t *p)
+{
+    p->len_diis = 0;
+    p->bmax = DBL_MIN;
+    p->bmax_id = -1;
+    for (int i = 0; i < PUR_LDB; i++)
+        for (int j = 0; j < PUR_LDB; j++) p->b[i * PUR_LDB + j] = (i != j) ? -1.0 : 0.0;
+}
+
 extern "C" int gtf_purif_set_sx(gtf_purif_dev_t *p, const double *S_host, const double *X_host)
 {
     const size_t nn = (size_t)p->n * p->n;
@@ -314,6 +326,7 @@ extern "C" int gtf_purif_run_dev(gtf_purif_dev_t *p, const double *F_dev, double
     k_purif_init<<<1, 32, 0, st>>>(p->part, RED_BLOCKS, n, p->nocc, p->scal);
     k_purif_d0<<<ge, 256, 0, st>>>(F_dev, p->D, n, p->scal);
     CKP(cudaGetLastError());
+    gtf_note_launches(3);
     int it;
     double err = 0.0;
     for (it = 0; it < PUR_MAX_ITERS; it++) {
@@ -323,6 +336,7 @@ extern "C" int gtf_purif_run_dev(gtf_purif_dev_t *p, const double *F_dev, double
         k_purif_finish<<<1, 32, 0, st>>>(p->part, RED_BLOCKS, p->scal);
         k_purif_update<<<ge, 256, 0, st>>>(p->D, p->D2, p->D3, nn, p->scal);
         CKP(cudaGetLastError());
+        gtf_note_launches(3);
         CKP(cudaMemcpyAsync(p->h_scal + 6, p->scal + 6, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
         CKP(cudaStreamSynchronize(st));
         err = p->h_scal[6];
@@ -409,6 +423,7 @@ extern "C" int gtf_diis_step_dev(gtf_purif_dev_t *p, const double *D_dev, double
         if (gemm_abt(p, p->W, p->X, cur)) return GTF_ERR_CUDA;
         k_dots<<<RED_BLOCKS, RED_THREADS, 0, st>>>(cur, p->vecs, nn, p->len_diis, p->part);
         CKP(cudaGetLastError());
+        gtf_note_launches(2);
         static double hpart[RED_BLOCKS * PUR_MAX_DIIS];
         CKP(cudaMemcpyAsync(hpart, p->part, sizeof(double) * RED_BLOCKS * PUR_MAX_DIIS, cudaMemcpyDeviceToHost, st));
         CKP(cudaStreamSynchronize(st));
@@ -436,6 +451,7 @@ extern "C" int gtf_diis_step_dev(gtf_purif_dev_t *p, const double *D_dev, double
         for (int i = 0; i < PUR_MAX_DIIS; i++) c.c[i] = (i < p->len_diis) ? co[i] : 0.0;
         k_combine<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(F_dev, p->Fvecs, nn, p->len_diis, c);
         CKP(cudaGetLastError());
+        gtf_note_launches(1);
     }
     return GTF_OK;
 }

@@ -3,8 +3,12 @@
 #include <cuda_runtime.h>
 #include <stdio.h>
 
+#include <atomic>
+
 #include "gtf_cuda.h"
 
+// count of this library's own kernel launches (benchmark bookkeeping)
+static std::atomic<unsigned long long> g_launches{0};
 #define EN_BLOCKS 148
 #define EN_THREADS 256
 
@@ -58,6 +62,7 @@ extern "C" int gtf_dev_energy(double *F, const double *H, const double *D, int n
     }
     cudaStream_t st = (cudaStream_t)stream;
     k_energy<<<EN_BLOCKS, EN_THREADS, 0, st>>>(F, H, D, (size_t)n * n, part);
+    g_launches += 1;
     if (cudaGetLastError() != cudaSuccess) return GTF_ERR_CUDA;
     if (cudaMemcpyAsync(hpart, part, sizeof(double) * EN_BLOCKS, cudaMemcpyDeviceToHost, st) != cudaSuccess)
         return GTF_ERR_CUDA;
@@ -81,4 +86,57 @@ extern "C" int gtf_device_info(int *ndev, int *cc)
         }
     }
     return n > 0 ? 0 : -1;
+}
+
+extern "C" void gtf_note_launches(int n) { g_launches += (unsigned long long)n; }
+
+extern "C" unsigned long long gtf_launch_count(void) { return g_launches.load(); }
+
+// FP64 FMA throughput probe: FP64_CHAINS independent dependency chains per
+// thread keep the FP64 pipe busy; every FMA is 2 flops
+#define FP64_CHAINS 8
+__global__ void k_fp64_probe(double *out, int iters, double a, double b)
+{
+    double x[FP64_CHAINS];
+#pragma unroll
+    for (int c = 0; c < FP64_CHAINS; c++) x[c] = threadIdx.x * 1e-9 + c;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int c = 0; c < FP64_CHAINS; c++) x[c] = fma(x[c], a, b);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int c = 0; c < FP64_CHAINS; c++) s += x[c];
+    if (s == 1.2345e-300) out[0] = s;  // keeps the chains live
+}
+
+// measured FP64 FMA rate of this device in GFLOP/s (best of 3 runs)
+extern "C" int gtf_fp64_peak(double *gflops)
+{
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    double *out;
+    if (cudaMalloc((void **)&out, sizeof(double)) != cudaSuccess) return GTF_ERR_ALLOC;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int threads = 256, blocks = nsm * 8, iters = 4096;
+    k_fp64_probe<<<blocks, threads>>>(out, 64, 0.999999, 1e-7);
+    double best = 0.0;
+    for (int r = 0; r < 3; r++) {
+        cudaEventRecord(e0);
+        k_fp64_probe<<<blocks, threads>>>(out, iters, 0.999999, 1e-7);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        const double fl = 2.0 * FP64_CHAINS * (double)iters * threads * blocks;
+        if (fl / (ms * 1e6) > best) best = fl / (ms * 1e6);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    *gflops = best;
+    return cudaGetLastError() == cudaSuccess ? GTF_OK : GTF_ERR_CUDA;
 }

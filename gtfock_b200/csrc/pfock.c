@@ -387,6 +387,11 @@ PFockStatus_t gtf_pfock_timing(PFock_t pf, double *ms_total, double *ms_eri, dou
     return PFOCK_STATUS_SUCCESS;
 }
 
+int gtf_pfock_class_stats(PFock_t pf, int *X, int *Y, double *ms, double *nquart)
+{
+    return gtf_fock_class_stats(pf->dev, X, Y, ms, nquart);
+}
+
 PFockStatus_t gtf_pfock_set_precision(PFock_t pf, int mode, double fp32_cutoff)
 {
     return map_err(gtf_fock_set_precision(pf->dev, mode, fp32_cutoff));

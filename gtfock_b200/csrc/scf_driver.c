@@ -1,5 +1,5 @@
 /*
- * scf_driver.c -- native SCF driver (gtfock_b200.h: gtf_scf_run).
+ * scf_driver.c -- native SCF driver (gtfock_b200.h: gtf_scf_*).
  *
  * Runs the loop of pscf/scf.c:329-459 on one GPU: initial guess
  * (pscf/scf.c:34-76), Fock build, energy E = sum D (H + F)
@@ -7,6 +7,8 @@
  * |E - E_prev| < 1e-11 (pscf/scf.c:373).
  *   mode 0: every matrix crosses the C API in host memory, as scf.c does;
  *   mode 1: D, F, S, X, H stay in device memory between the steps.
+ * gtf_scf_create does the set-up of pscf/scf.c:298-314 and init_oedmat
+ * (pscf/scf.c:131-185) once; gtf_scf_solve can then run many solves.
  */
 #include <math.h>
 #include <stdio.h>
@@ -22,6 +24,16 @@ extern int gtf_dev_malloc(void **p, size_t bytes);
 extern void gtf_dev_free(void *p);
 extern int gtf_dev_copy(void *dst, const void *src, size_t bytes, int kind, void *stream);
 extern int gtf_dev_energy(double *F, const double *H, const double *D, int n, void *stream, double *energy);
+
+struct gtf_scf {
+    BasisSet_t basis;
+    PFock_t pf;
+    purif_t *pur;
+    int n;
+    double enuc;
+    double *D0;          /* initial guess (host) */
+    double *dD, *dF;     /* device-resident D and F (mode 1) */
+};
 
 static double wall(void)
 {
@@ -47,50 +59,88 @@ static void initial_density(BasisSet_t basis, double *D, int n)
     for (size_t k = 0; k < (size_t)n * n; k++) D[k] *= R / 2.0;
 }
 
-int gtf_scf_run(const char *bsfile, const char *xyzfile, double tolscr, int niters, int mode,
-                double *energies, double *timings)
+void gtf_scf_destroy(gtf_scf_t *s)
 {
-    if (!bsfile || !xyzfile || niters <= 0 || (mode != 0 && mode != 1)) return -1;
-    BasisSet_t basis;
-    CInt_createBasisSet(&basis);
-    if (CInt_loadBasisSet(basis, (char *)bsfile, (char *)xyzfile) != CINT_STATUS_SUCCESS) {
-        CInt_destroyBasisSet(basis);
-        return -2;
+    if (!s) return;
+    gtf_dev_free(s->dD);
+    gtf_dev_free(s->dF);
+    if (s->pf) {
+        PFock_destroyOvlMat(s->pf);
+        PFock_destroyCoreHMat(s->pf);
     }
-    const int n = CInt_getNumFuncs(basis);
-    const size_t nn = (size_t)n * n;
-    PFock_t pf;
-    if (PFock_create(basis, 1, 1, 4, tolscr, 1, 1, &pf) != PFOCK_STATUS_SUCCESS) {
-        CInt_destroyBasisSet(basis);
-        return -3;
+    if (s->pur) destroy_purif(s->pur);
+    if (s->pf) PFock_destroy(s->pf);
+    if (s->basis) CInt_destroyBasisSet(s->basis);
+    free(s->D0);
+    free(s);
+}
+
+gtf_scf_t *gtf_scf_create(const char *bsfile, const char *xyzfile, double tolscr)
+{
+    if (!bsfile || !xyzfile) return NULL;
+    gtf_scf_t *s = (gtf_scf_t *)calloc(1, sizeof(gtf_scf_t));
+    if (!s) return NULL;
+    CInt_createBasisSet(&s->basis);
+    if (CInt_loadBasisSet(s->basis, (char *)bsfile, (char *)xyzfile) != CINT_STATUS_SUCCESS) {
+        gtf_scf_destroy(s);
+        return NULL;
     }
-    purif_t *pur = create_purif(basis, 1, 1, 1);
-    if (!pur) {
-        PFock_destroy(pf);
-        CInt_destroyBasisSet(basis);
-        return -4;
+    s->n = CInt_getNumFuncs(s->basis);
+    s->enuc = CInt_getNucEnergy(s->basis);
+    const int n = s->n;
+    if (PFock_create(s->basis, 1, 1, 4, tolscr, 1, 1, &s->pf) != PFOCK_STATUS_SUCCESS) {
+        s->pf = NULL;
+        gtf_scf_destroy(s);
+        return NULL;
     }
-    const double enuc = CInt_getNucEnergy(basis);
-    double t_fock = 0.0, t_diis = 0.0, t_pur = 0.0;
+    s->pur = create_purif(s->basis, 1, 1, 1);
+    s->D0 = (double *)malloc(sizeof(double) * (size_t)n * n);
+    if (!s->pur || !s->D0 ||
+        gtf_dev_malloc((void **)&s->dD, sizeof(double) * (size_t)n * n) ||
+        gtf_dev_malloc((void **)&s->dF, sizeof(double) * (size_t)n * n)) {
+        gtf_scf_destroy(s);
+        return NULL;
+    }
+    /* init_oedmat, pscf/scf.c:131-185; the device copies are kept for mode 1 */
+    PFock_createOvlMat(s->pf, s->basis);
+    PFock_getOvlMat(s->pf, 0, n - 1, 0, n - 1, n, s->pur->S_block);
+    PFock_getOvlMat2(s->pf, 0, n - 1, 0, n - 1, n, s->pur->X_block);
+    PFock_createCoreHMat(s->pf, s->basis);
+    PFock_getCoreHMat(s->pf, 0, n - 1, 0, n - 1, n, s->pur->H_block);
+    PFock_setNumDenMat(1, s->pf);
+    initial_density(s->basis, s->D0, n);
+    return s;
+}
+
+int gtf_scf_nbf(gtf_scf_t *s) { return s ? s->n : -1; }
+
+int gtf_scf_solve(gtf_scf_t *s, int niters, int mode, double *energies, double *timings)
+{
+    if (!s || niters <= 0 || (mode != 0 && mode != 1)) return -1;
+    const int n = s->n;
+    const size_t nn = (size_t)n * n, mb = sizeof(double) * nn;
+    purif_t *pur = s->pur;
+    gtf_purif_dev_t *pd = (gtf_purif_dev_t *)pur->dev;
+    gtf_purif_reset(pd);
+    pur->len_diis = 0;
+    double t_fock = 0.0, t_diis = 0.0, t_pur = 0.0, h2d = 0.0, d2h = 0.0;
+    const unsigned long long l0 = gtf_launch_count();
     const double t_start = wall();
     int iter, ret = 0;
     double e0 = -1.0;
-    PFock_createOvlMat(pf, basis);
-    PFock_getOvlMat(pf, 0, n - 1, 0, n - 1, n, pur->S_block);
-    PFock_getOvlMat2(pf, 0, n - 1, 0, n - 1, n, pur->X_block);
-    PFock_createCoreHMat(pf, basis);
-    PFock_getCoreHMat(pf, 0, n - 1, 0, n - 1, n, pur->H_block);
-    PFock_setNumDenMat(1, pf);
-    initial_density(basis, pur->D_block, n);
+    memcpy(pur->D_block, s->D0, mb);
     if (mode == 0) {
-        PFock_destroyOvlMat(pf);
-        PFock_destroyCoreHMat(pf);
+        if (!pur->sx_uploaded) {
+            h2d += 2.0 * mb;   /* S and X read once by purif */
+        }
         for (iter = 0; iter < niters; iter++) {
             double t1 = wall();
-            PFock_putDenMat(0, n - 1, 0, n - 1, n, pur->D_block, 0, pf);
-            PFock_commitDenMats(pf);
-            if (PFock_computeFock(basis, pf) != PFOCK_STATUS_SUCCESS) { ret = -5; break; }
-            PFock_getMat(pf, PFOCK_MAT_TYPE_F, 0, 0, n - 1, 0, n - 1, n, pur->F_block);
+            PFock_putDenMat(0, n - 1, 0, n - 1, n, pur->D_block, 0, s->pf);
+            PFock_commitDenMats(s->pf);
+            if (PFock_computeFock(s->basis, s->pf) != PFOCK_STATUS_SUCCESS) { ret = -5; break; }
+            PFock_getMat(s->pf, PFOCK_MAT_TYPE_F, 0, 0, n - 1, 0, n - 1, n, pur->F_block);
+            h2d += mb;
+            d2h += mb;
             double e = 0.0;
             for (size_t k = 0; k < nn; k++) {
                 pur->F_block[k] += pur->H_block[k];
@@ -98,69 +148,80 @@ int gtf_scf_run(const char *bsfile, const char *xyzfile, double tolscr, int nite
             }
             double t2 = wall();
             t_fock += t2 - t1;
-            if (energies) energies[iter] = e + enuc;
+            if (energies) energies[iter] = e + s->enuc;
             if (iter > 0 && fabs(e - e0) < 1e-11) {
                 iter++;
                 break;
             }
             e0 = e;
             t1 = wall();
-            compute_diis(pf, pur, pur->D_block, pur->F_block, iter);
+            compute_diis(s->pf, pur, pur->D_block, pur->F_block, iter);
+            h2d += 2.0 * mb;
+            d2h += mb;
             t2 = wall();
             t_diis += t2 - t1;
             if (compute_purification(pur, pur->F_block, pur->D_block) < 0) { ret = -6; break; }
+            h2d += mb;
+            d2h += mb;
             t_pur += wall() - t2;
         }
     } else {
-        gtf_fock_dev_t *fd = gtf_pfock_device(pf);
+        gtf_fock_dev_t *fd = gtf_pfock_device(s->pf);
         void *st = gtf_fock_stream(fd);
-        gtf_purif_dev_t *pd = (gtf_purif_dev_t *)pur->dev;
-        double *dD = NULL, *dF = NULL;
-        if (gtf_dev_malloc((void **)&dD, sizeof(double) * nn) || gtf_dev_malloc((void **)&dF, sizeof(double) * nn)) {
-            ret = -7;
-            iter = 0;
-        } else {
-            gtf_purif_set_sx_dev(pd, gtf_fock_onee_dev(fd, 0), gtf_fock_onee_dev(fd, 1));
-            pur->sx_uploaded = 1;
-            const double *dH = gtf_fock_onee_dev(fd, 2);
-            gtf_dev_copy(dD, pur->D_block, sizeof(double) * nn, 0, st);
-            for (iter = 0; iter < niters; iter++) {
-                double t1 = wall();
-                const double *dFock = NULL;
-                if (gtf_pfock_compute_dev(pf, dD, &dFock) != PFOCK_STATUS_SUCCESS) { ret = -5; break; }
-                gtf_dev_copy(dF, dFock, sizeof(double) * nn, 2, st);
-                double e = 0.0;
-                gtf_dev_energy(dF, dH, dD, n, st, &e);
-                double t2 = wall();
-                t_fock += t2 - t1;
-                if (energies) energies[iter] = e + enuc;
-                if (iter > 0 && fabs(e - e0) < 1e-11) {
-                    iter++;
-                    break;
-                }
-                e0 = e;
-                t1 = wall();
-                gtf_diis_step_dev(pd, dD, dF, iter);
-                t2 = wall();
-                t_diis += t2 - t1;
-                int it = 0;
-                if (gtf_purif_run_dev(pd, dF, dD, &it) != GTF_OK) { ret = -6; break; }
-                t_pur += wall() - t2;
+        gtf_purif_set_sx_dev(pd, gtf_fock_onee_dev(fd, 0), gtf_fock_onee_dev(fd, 1));
+        pur->sx_uploaded = 1;
+        const double *dH = gtf_fock_onee_dev(fd, 2);
+        gtf_dev_copy(s->dD, s->D0, mb, 0, st);
+        h2d += mb;
+        for (iter = 0; iter < niters; iter++) {
+            double t1 = wall();
+            const double *dFock = NULL;
+            if (gtf_pfock_compute_dev(s->pf, s->dD, &dFock) != PFOCK_STATUS_SUCCESS) { ret = -5; break; }
+            gtf_dev_copy(s->dF, dFock, mb, 2, st);
+            double e = 0.0;
+            gtf_dev_energy(s->dF, dH, s->dD, n, st, &e);
+            double t2 = wall();
+            t_fock += t2 - t1;
+            if (energies) energies[iter] = e + s->enuc;
+            if (iter > 0 && fabs(e - e0) < 1e-11) {
+                iter++;
+                break;
             }
+            e0 = e;
+            t1 = wall();
+            gtf_diis_step_dev(pd, s->dD, s->dF, iter);
+            t2 = wall();
+            t_diis += t2 - t1;
+            int it = 0;
+            if (gtf_purif_run_dev(pd, s->dF, s->dD, &it) != GTF_OK) { ret = -6; break; }
+            t_pur += wall() - t2;
         }
-        gtf_dev_free(dD);
-        gtf_dev_free(dF);
-        PFock_destroyOvlMat(pf);
-        PFock_destroyCoreHMat(pf);
     }
     if (timings) {
         timings[0] = t_fock;
         timings[1] = t_diis;
         timings[2] = t_pur;
         timings[3] = wall() - t_start;
+        timings[4] = h2d;
+        timings[5] = d2h;
+        timings[6] = (double)(gtf_launch_count() - l0);
     }
-    destroy_purif(pur);
-    PFock_destroy(pf);
-    CInt_destroyBasisSet(basis);
     return ret < 0 ? ret : iter;
+}
+
+int gtf_scf_run(const char *bsfile, const char *xyzfile, double tolscr, int niters, int mode,
+                double *energies, double *timings)
+{
+    if (!bsfile || !xyzfile || niters <= 0 || (mode != 0 && mode != 1)) return -1;
+    const double t0 = wall();
+    gtf_scf_t *s = gtf_scf_create(bsfile, xyzfile, tolscr);
+    if (!s) return -3;
+    double t[8] = {0};
+    int it = gtf_scf_solve(s, niters, mode, energies, t);
+    gtf_scf_destroy(s);
+    if (timings) {
+        for (int k = 0; k < 7; k++) timings[k] = t[k];
+        timings[3] = wall() - t0;  /* whole job: set-up, solve, tear-down */
+    }
+    return it;
 }

@@ -33,6 +33,11 @@ PFockStatus_t gtf_pfock_screening(PFock_t pfock, int *shellptr, int *shellid,
 PFockStatus_t gtf_pfock_timing(PFock_t pfock, double *ms_total, double *ms_eri,
                                double *eri_flops);
 
+/* Per angular-class-pair statistics of the last build (21 pairs for s/p/d
+ * shells): bra / ket pair classes (ss=0 ps=1 pp=2 ds=3 dp=4 dd=5), CUDA-event
+ * ms of each class kernel and its quartet count.  Returns the pair count. */
+int gtf_pfock_class_stats(PFock_t pfock, int *X, int *Y, double *ms, double *nquart);
+
 /* Precision of the ERI kernels: 0 = FP64 (default), 1 = FP32 for quartets
  * whose Schwarz bound sqrt(v1 v2) is below fp32_cutoff. */
 PFockStatus_t gtf_pfock_set_precision(PFock_t pfock, int mode, double fp32_cutoff);
@@ -45,13 +50,29 @@ PFockStatus_t gtf_pfock_compute_dev(PFock_t pfock, const double *dev_D,
 
 /* Native SCF driver: the loop of pscf/scf.c:329-459 (Fock build, energy,
  * DIIS, purification) on one GPU for the molecule in xyzfile with basis
- * bsfile.  energies[k] = total energy (incl. nuclear) of iteration k.
- * mode 0: host D/F buffers cross the C API every iteration (as scf.c);
- * mode 1: D and F stay resident on the device.  Returns iterations run, or
- * a negative value on error.  timings (optional, 4 doubles): seconds in Fock
- * builds, DIIS, purification, total. */
+ * bsfile.  gtf_scf_create performs the set-up (basis, PFock_create with its
+ * screening, create_purif, S / X / H_core) once; gtf_scf_solve runs one SCF
+ * from the initial guess and may be called repeatedly.
+ *   mode 0: host D/F buffers cross the C API every iteration (as scf.c);
+ *   mode 1: D and F stay resident on the device.
+ * energies[k] = total energy (incl. nuclear) of iteration k.  timings
+ * (optional, 7 doubles): seconds in Fock builds, DIIS, purification, total;
+ * host->device bytes, device->host bytes, library kernel launches.
+ * Returns iterations run, or a negative value on error. */
+typedef struct gtf_scf gtf_scf_t;
+gtf_scf_t *gtf_scf_create(const char *bsfile, const char *xyzfile, double tolscr);
+int gtf_scf_solve(gtf_scf_t *s, int niters, int mode, double *energies, double *timings);
+int gtf_scf_nbf(gtf_scf_t *s);
+void gtf_scf_destroy(gtf_scf_t *s);
+/* create + solve + destroy; timings[3] covers the whole job */
 int gtf_scf_run(const char *bsfile, const char *xyzfile, double tolscr,
                 int niters, int mode, double *energies, double *timings);
+
+/* Number of this library's own kernel launches so far (all threads). */
+unsigned long long gtf_launch_count(void);
+
+/* Measured FP64 FMA throughput of device 0 in GFLOP/s (probe kernel). */
+int gtf_fp64_peak(double *gflops);
 
 /* Device and library identification for tests: number of CUDA devices seen
  * and the compute capability of device 0 (major*10+minor); -1 on error. */

@@ -175,11 +175,30 @@ static void update_F_full(int nbf, const double *I, int dimM, int dimN, int dimP
     }
 }
 
+/* One Fock build restricted to every `stride`-th MN pair of the task loop
+ * (stride 1 = the whole build); count_only skips the integrals and the
+ * digestion and only counts quartets.  Used for the timed CPU baseline on a
+ * bounded sample of a large build. */
+int or_fock_build_sample(BasisSet_t basis, double tolscr, int nthreads,
+                         const int *shellptr, const int *shellid, const int *shellrid,
+                         const double *shellvalue, const double *D, double *F,
+                         int stride, int count_only, double *usq_o, double *uitl_o);
+
 int or_fock_build(BasisSet_t basis, double tolscr, int nthreads,
                   const int *shellptr, const int *shellid, const int *shellrid,
                   const double *shellvalue,
                   const double *D, double *F, double *usq_o, double *uitl_o)
 {
+    return or_fock_build_sample(basis, tolscr, nthreads, shellptr, shellid, shellrid, shellvalue,
+                                D, F, 1, 0, usq_o, uitl_o);
+}
+
+int or_fock_build_sample(BasisSet_t basis, double tolscr, int nthreads,
+                         const int *shellptr, const int *shellid, const int *shellrid,
+                         const double *shellvalue, const double *D, double *F,
+                         int stride, int count_only, double *usq_o, double *uitl_o)
+{
+    if (stride < 1) stride = 1;
     const int nbf = basis->nbf;
     const int nshells = basis->nshells;
     const double tolscr2 = tolscr * tolscr;
@@ -200,6 +219,7 @@ int or_fock_build(BasisSet_t basis, double tolscr, int nthreads,
         double *K = Kt + nn * nt;
         #pragma omp for schedule(dynamic)
         for (int i = startMN; i < endMN; i++) {
+            if ((i - startMN) % stride != 0) continue;
             const int M = shellrid[i];
             const int N = shellid[i];
             const double value1 = shellvalue[i];
@@ -222,6 +242,7 @@ int or_fock_build(BasisSet_t basis, double tolscr, int nthreads,
                     double *ints;
                     usq += 1.0;
                     uitl += dimM * dimN * dimP * dimQ;
+                    if (count_only) continue;
                     CInt_computeShellQuartet(basis, erd, nt, M, N, P, Q, &ints, &nints);
                     if (nints != 0) {
                         update_F_full(nbf, ints, dimM, dimN, dimP, dimQ,

@@ -34,6 +34,14 @@ int or_fock_build(BasisSet_t basis, double tolscr, int nthreads,
                   const double *shellvalue,
                   const double *D, double *F, double *usq, double *uitl);
 
+/* The same build restricted to every stride-th MN pair (count_only: count
+ * quartets without computing them); the timed CPU baseline samples large
+ * builds this way. */
+int or_fock_build_sample(BasisSet_t basis, double tolscr, int nthreads,
+                         const int *shellptr, const int *shellid, const int *shellrid,
+                         const double *shellvalue, const double *D, double *F,
+                         int stride, int count_only, double *usq, double *uitl);
+
 /* S, H_core and X = U diag(1/sqrt(lambda)) U^T
  * (pfock/one_electron.c:28-119, pfock/pfock.c:1782-1867). */
 int or_one_electron(BasisSet_t basis, double *S, double *H, double *X);

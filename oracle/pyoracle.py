@@ -51,6 +51,11 @@ def lib():
         L.or_screening.argtypes = [vp, d, i, ctypes.POINTER(ip), ctypes.POINTER(ip),
                                    ctypes.POINTER(ip), ctypes.POINTER(dp), ip, dp]
         L.or_fock_build.argtypes = [vp, d, i, ip, ip, ip, dp, dp, dp, dp, dp]
+        L.or_fock_build_sample.argtypes = [vp, d, i, ip, ip, ip, dp, dp, dp, i, i, dp, dp]
+        L.or_diis_create.argtypes = [i]
+        L.or_diis_create.restype = vp
+        L.or_diis_destroy.argtypes = [vp]
+        L.or_diis_step.argtypes = [vp, dp, dp, dp, dp, i]
         L.or_one_electron.argtypes = [vp, dp, dp, dp]
         L.or_purification.argtypes = [i, i, dp, dp, dp]
         L.or_scf.argtypes = [vp, d, i, i, dp, dp, dp]
@@ -156,6 +161,45 @@ def fock_build(basis, tol, D, scr=None, nthreads=os.cpu_count()):
     if st != 0:
         raise RuntimeError("or_fock_build failed")
     return F, usq.value, uitl.value
+
+
+def fock_build_sample(basis, tol, D, stride, count_only=False, scr=None, nthreads=os.cpu_count()):
+    """Every stride-th MN pair of one Fock build: (usq, uitl, seconds)."""
+    import time
+    L = lib()
+    if scr is None:
+        scr = screening(basis, tol, nthreads)
+    shellptr, shellid, shellrid, shellvalue, _ = scr
+    D = np.ascontiguousarray(D, dtype=np.float64)
+    F = np.zeros_like(D)
+    usq = ctypes.c_double()
+    uitl = ctypes.c_double()
+    sid = np.ascontiguousarray(shellid, dtype=np.int32)
+    srid = np.ascontiguousarray(shellrid, dtype=np.int32)
+    sval = np.ascontiguousarray(shellvalue, dtype=np.float64)
+    sptr = np.ascontiguousarray(shellptr, dtype=np.int32)
+    t0 = time.perf_counter()
+    st = L.or_fock_build_sample(basis.h, tol, nthreads, _ip(sptr), _ip(sid), _ip(srid), _dp(sval),
+                                _dp(D), _dp(F), stride, 1 if count_only else 0,
+                                ctypes.byref(usq), ctypes.byref(uitl))
+    dt = time.perf_counter() - t0
+    if st != 0:
+        raise RuntimeError("or_fock_build_sample failed")
+    return usq.value, uitl.value, dt
+
+
+def diis_step_timed(X, S, D, F, it, state=None):
+    """One DIIS step (pscf/purif.c:491-641) on the CPU; returns (F_out, seconds, state)."""
+    import time
+    L = lib()
+    n = X.shape[0]
+    if state is None:
+        state = L.or_diis_create(n)
+    F = np.ascontiguousarray(F, dtype=np.float64).copy()
+    t0 = time.perf_counter()
+    L.or_diis_step(state, _dp(np.ascontiguousarray(X)), _dp(np.ascontiguousarray(S)),
+                   _dp(np.ascontiguousarray(D)), _dp(F), it)
+    return F, time.perf_counter() - t0, state
 
 
 def one_electron(basis):
