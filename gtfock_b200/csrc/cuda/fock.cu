@@ -414,6 +414,11 @@ __global__ void k_build_pairs(const int *__restrict__ idx, const int *__restrict
     pair_n[s] = r.n;
 }
 
+// Primitive pairs of each listed shell pair, compacted and sorted: pairs
+// whose prefactor |K| is below GTF_PRIM_EPS are dropped (their contribution
+// to any integral is below 1e-20 Hartree), the rest are stored in descending
+// |K| so that the quartet loop can stop once |K_ab K_cd| < GTF_PRIMQ_EPS.
+// pairs[s].n becomes the kept count (possibly 0); the slot keeps its size.
 __global__ void k_fill_primpairs(PairRec *__restrict__ pairs, const int *__restrict__ idx,
                                  const int *__restrict__ shellid, const int *__restrict__ shellrid,
                                  const int *__restrict__ pair_off, BasisDev b, int npairs, double *pp,
@@ -426,24 +431,37 @@ __global__ void k_fill_primpairs(PairRec *__restrict__ pairs, const int *__restr
     const int a = (b.sh_L[M] >= b.sh_L[N]) ? M : N;
     const int bb = (a == M) ? N : M;
     const int off = pair_off[s];
-    pairs[s].off = off;
     const double Ax = b.sh_xyz[3 * a], Ay = b.sh_xyz[3 * a + 1], Az = b.sh_xyz[3 * a + 2];
     const double Bx = b.sh_xyz[3 * bb], By = b.sh_xyz[3 * bb + 1], Bz = b.sh_xyz[3 * bb + 2];
     const double r2 = (Ax - Bx) * (Ax - Bx) + (Ay - By) * (Ay - By) + (Az - Bz) * (Az - Bz);
     const int na = b.sh_nprim[a], nb = b.sh_nprim[bb];
     const int pa = b.sh_pstart[a], pb = b.sh_pstart[bb];
+    const size_t np = (size_t)npp;
+    int kept = 0;
     for (int i = 0; i < na; i++) {
         for (int j = 0; j < nb; j++) {
             const double al = b.alpha[pa + i], be = b.alpha[pb + j];
             const double p = al + be, ip = 1.0 / p;
-            const int o = off + i * nb + j;
-            pp[o] = p;
-            pp[npp + o] = (al * Ax + be * Bx) * ip;
-            pp[2 * npp + o] = (al * Ay + be * By) * ip;
-            pp[3 * npp + o] = (al * Az + be * Bz) * ip;
-            pp[4 * npp + o] = GTF_PAIR_PREF * b.coef[pa + i] * b.coef[pb + j] * exp(-al * be * ip * r2) * ip;
+            const double K = GTF_PAIR_PREF * b.coef[pa + i] * b.coef[pb + j] * exp(-al * be * ip * r2) * ip;
+            if (fabs(K) < GTF_PRIM_EPS) continue;
+            // insertion into the descending-|K| list of the kept pairs
+            int o = kept;
+            while (o > 0 && fabs(pp[4 * np + off + o - 1]) < fabs(K)) {
+                const size_t src = (size_t)off + o - 1;
+                for (int f = 0; f < 5; f++) pp[f * np + src + 1] = pp[f * np + src];
+                o--;
+            }
+            const size_t d = (size_t)off + o;
+            pp[d] = p;
+            pp[np + d] = (al * Ax + be * Bx) * ip;
+            pp[2 * np + d] = (al * Ay + be * By) * ip;
+            pp[3 * np + d] = (al * Az + be * Bz) * ip;
+            pp[4 * np + d] = K;
+            kept++;
         }
     }
+    pairs[s].off = off;
+    pairs[s].n = kept;
 }
 
 // number of ket pairs of the ket class that pass v_bra * v_ket >= tol2
@@ -797,12 +815,12 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
             f->uitl += q * dims;
         }
     }
-    // Rys-model FLOPs per build: needs primitive counts per quartet, summed on the host
+    // Rys-model FLOPs per build (SURVEY-normalised work: every primitive
+    // quartet of every screened shell quartet, before primitive screening)
     {
-        std::vector<PairRec> hp(nnz > 0 ? nnz : 1);
-        std::vector<double> hv(nnz > 0 ? nnz : 1);
+        std::vector<int> hn(nnz > 0 ? nnz : 1);
         if (nnz > 0) {
-            CK(cudaMemcpyAsync(hp.data(), f->d_pairs, sizeof(PairRec) * nnz, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(hn.data(), d_pair_n, sizeof(int) * nnz, cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
         }
         double flops = 0.0;
@@ -813,14 +831,14 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
             CK(cudaMemcpy(nk.data(), t.d_nket, sizeof(int) * t.nbra, cudaMemcpyDeviceToHost));
             // prefix sums of ket primitive-pair counts
             std::vector<double> kpre(t.nketcls + 1, 0.0);
-            for (int j = 0; j < t.nketcls; j++) kpre[j + 1] = kpre[j] + hp[t.ket_start + j].n;
+            for (int j = 0; j < t.nketcls; j++) kpre[j + 1] = kpre[j] + hn[t.ket_start + j];
             double cpart;
             const double per_prim = class_flops_per_prim(t.X, t.Y, &cpart);
             const int la = k_cls_la[t.X], lb = k_cls_lb[t.X], lc = k_cls_la[t.Y], ld = k_cls_lb[t.Y];
             const double ns_ = (double)(b->pure && la == 2 ? 5 : ncart(la)) * (b->pure && lb == 2 ? 5 : ncart(lb)) *
                                (b->pure && lc == 2 ? 5 : ncart(lc)) * (b->pure && ld == 2 ? 5 : ncart(ld));
             for (int i = 0; i < t.nbra; i++) {
-                const double kb = hp[t.bra_start + i].n;
+                const double kb = hn[t.bra_start + i];
                 const double kk = kpre[nk[i]];
                 flops += kb * kk * per_prim + (cpart + 12.0 * ns_) * nk[i];
             }

@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(FOCK_THREADS)
         double acc[NQ];
 #pragma unroll
         for (int k = 0; k < NQ; k++) acc[k] = 0.0;
-        if (active) eri_accumulate<LA, LB, LC, LD>(src, pb, src, pk, acc);
+        if (active) eri_accumulate<LA, LB, LC, LD, true>(src, pb, src, pk, acc);
         const bool same = (bra_start + i) == (ket_start + j);
         digest<LA, LB, LC, LD, double>(acc, active, pb, pk, same, D, Fj, Fk, ld, lane);
     }

@@ -28,6 +28,13 @@
 // sqrt(2) * pi^(5/4): the per-pair share of 2 pi^(5/2) / (p q sqrt(p+q))
 #define GTF_PAIR_PREF 5.9149671727956130
 
+// primitive screening in the Fock build: a primitive pair is dropped when its
+// prefactor K is below GTF_PRIM_EPS; a primitive quartet is skipped when
+// |K_ab K_cd| is below GTF_PRIMQ_EPS (pairs are stored in descending |K|, so
+// the ket loop stops there).  Every dropped contribution is below 1e-20 Ha.
+#define GTF_PRIM_EPS 1e-24
+#define GTF_PRIMQ_EPS 1e-26
+
 // ---------------------------------------------------------------------------
 // Cartesian component tables (lexicographic: xx, xy, xz, yy, yz, zz)
 // ---------------------------------------------------------------------------
@@ -198,7 +205,9 @@ __device__ __forceinline__ void hrr_abcd(const double (&G)[LA + LB + 1][LC + LD 
 // ---------------------------------------------------------------------------
 // contracted Cartesian (ab|cd), accumulated into acc[ia + NA*(ib + NB*(ic + NC*id))]
 // ---------------------------------------------------------------------------
-template <int LA, int LB, int LC, int LD, class PPB, class PPK>
+// SKIP: primitive pairs are sorted by descending |K| (Fock-build pair list),
+// so the primitive-quartet cutoff may end the ket loop early
+template <int LA, int LB, int LC, int LD, bool SKIP = false, class PPB, class PPK>
 __device__ __forceinline__ void eri_accumulate(const PPB &bra, const PairRec &pb, const PPK &ket,
                                                const PairRec &pk,
                                                double (&acc)[ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD)])
@@ -213,6 +222,7 @@ __device__ __forceinline__ void eri_accumulate(const PPB &bra, const PairRec &pb
         for (int ik = 0; ik < pk.n; ik++) {
             double q, Qx, Qy, Qz, Kcd;
             ket.get(pk, ik, q, Qx, Qy, Qz, Kcd);
+            if (SKIP && fabs(Kab * Kcd) < GTF_PRIMQ_EPS) break;  // kets are in descending |K|
             const double rpq = rsqrt(p + q);
             const double ipq = rpq * rpq;
             const double PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
