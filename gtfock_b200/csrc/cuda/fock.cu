@@ -23,6 +23,7 @@
 #include <cub/cub.cuh>
 #include <cuda_runtime.h>
 #include <math.h>
+#include <pthread.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -1175,4 +1176,137 @@ extern "C" void gtf_fock_basis_dev(gtf_fock_dev_t *f, const int **sh_L, const in
     *natoms = f->natoms;
     *nbf = f->nbf;
     *pure = f->pure;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free Fock build
+//
+// Some callers cannot allocate device memory once they are running: a host
+// that hands every byte of the GPU to its own pool allocator, a real-time
+// loop that must not block on the driver's allocator, or a plugin whose
+// host process forbids new allocations after start-up.  For them this
+// variant of gtf_fock_compute keeps its scratch -- Cartesian D, the Coulomb
+// and exchange accumulators, spherical J and K, and the per-class unit
+// counters -- in one file-scope device array instead of the engine's
+// buffers.  The engine itself (pair lists, primitive pairs, task lists) is
+// still built by gtf_fock_create.
+//
+// Limits and sharing:
+//   * at most GTF_FIXED_MAX_FUNCS Cartesian (and spherical) functions;
+//     larger bases are rejected with GTF_ERR_INVALID and a message;
+//   * the array (about 5.9 MB) exists on every GPU that loads the library,
+//     for the life of the process;
+//   * every call on a device uses the same array, so calls whose work
+//     overlaps on that GPU (two streams, two threads, two engines) race;
+//     callers must order them;
+//   * the first call on a device looks up the array's device address
+//     (cudaGetSymbolAddress, with that device current); make that first call
+//     before any stream capture;
+//   * the accumulators and counters are cleared on every call (stream-ordered
+//     cudaMemsetAsync), so results never depend on the previous call.
+// ---------------------------------------------------------------------------
+#define GTF_FIXED_MAX_FUNCS 384
+#define GTF_FIXED_NN ((size_t)GTF_FIXED_MAX_FUNCS * GTF_FIXED_MAX_FUNCS)
+#define GTF_FIXED_DOUBLES (5 * GTF_FIXED_NN + NCLSPAIR + 3)
+#define GTF_FIXED_MAX_DEVICES 64
+
+static __device__ __align__(256) double g_fixed_scratch[GTF_FIXED_DOUBLES];
+
+static double *g_fixed_ptr[GTF_FIXED_MAX_DEVICES];
+static pthread_mutex_t g_fixed_lock = PTHREAD_MUTEX_INITIALIZER;
+
+// device address of g_fixed_scratch on the current device (looked up once)
+static int fixed_scratch(int dev, double **out)
+{
+    if (dev < 0 || dev >= GTF_FIXED_MAX_DEVICES) return GTF_ERR_INVALID;
+    pthread_mutex_lock(&g_fixed_lock);
+    if (g_fixed_ptr[dev] == nullptr) {
+        double *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress((void **)&p, g_fixed_scratch);
+        if (e != cudaSuccess || p == nullptr) {
+            pthread_mutex_unlock(&g_fixed_lock);
+            snprintf(g_errbuf, sizeof(g_errbuf), "cudaGetSymbolAddress(g_fixed_scratch): %s",
+                     cudaGetErrorString(e));
+            return GTF_ERR_CUDA;
+        }
+        g_fixed_ptr[dev] = p;
+    }
+    *out = g_fixed_ptr[dev];
+    pthread_mutex_unlock(&g_fixed_lock);
+    return GTF_OK;
+}
+
+extern "C" int gtf_fock_compute_fixed(gtf_fock_dev_t *f, const double *dev_D, double *dev_F)
+{
+    if (f == nullptr || dev_D == nullptr || dev_F == nullptr || f->max_numdmat <= 0) return GTF_ERR_INVALID;
+    const int nbf = f->nbf, nbfc = f->nbf_cart;
+    if (nbfc > GTF_FIXED_MAX_FUNCS || nbf > GTF_FIXED_MAX_FUNCS) {
+        snprintf(g_errbuf, sizeof(g_errbuf),
+                 "allocation-free Fock build: basis has %d Cartesian functions, limit is %d", nbfc,
+                 GTF_FIXED_MAX_FUNCS);
+        return GTF_ERR_INVALID;
+    }
+    int dev = -1;
+    CK(cudaGetDevice(&dev));
+    if (dev != f->dev) {
+        snprintf(g_errbuf, sizeof(g_errbuf), "allocation-free Fock build: current device %d, engine on %d", dev,
+                 f->dev);
+        return GTF_ERR_INVALID;
+    }
+    double *scr = nullptr;
+    int r = fixed_scratch(dev, &scr);
+    if (r) return r;
+    cudaStream_t st = f->stream;
+    const size_t nn = (size_t)nbf * nbf, nnc = (size_t)nbfc * nbfc;
+    double *Dc = scr;
+    double *Fj = scr + GTF_FIXED_NN;
+    double *Fk = scr + 2 * GTF_FIXED_NN;
+    double *J = scr + 3 * GTF_FIXED_NN;
+    double *K = scr + 4 * GTF_FIXED_NN;
+    unsigned long long *counters = (unsigned long long *)(scr + 5 * GTF_FIXED_NN);
+    const bool need_tr = f->pure && nbfc != nbf;
+    const double *Duse = dev_D;
+    if (need_tr) {
+        dim3 g((nbfc + 127) / 128, nbfc);
+        k_d_to_cart<<<g, 128, 0, st>>>(dev_D, Dc, f->d_cart2shell, f->d_sh_L, f->d_f_start, f->d_fc_start, nbf,
+                                       nbfc, f->pure);
+        CK(cudaGetLastError());
+        Duse = Dc;
+    }
+    CK(cudaMemsetAsync(Fj, 0, sizeof(double) * nnc, st));
+    CK(cudaMemsetAsync(Fk, 0, sizeof(double) * nnc, st));
+    CK(cudaMemsetAsync(counters, 0, sizeof(unsigned long long) * NCLSPAIR, st));
+    PrimPairs pp{f->d_pp, f->d_pp + f->nprimpairs, f->d_pp + 2 * (size_t)f->nprimpairs,
+                 f->d_pp + 3 * (size_t)f->nprimpairs, f->d_pp + 4 * (size_t)f->nprimpairs};
+    for (int c = 0; c < NCLSPAIR; c++) {
+        ClassPairTask &t = f->tasks[c];
+        if (t.nunits == 0) continue;
+        FockLaunch a;
+        a.pairs = f->d_pairs;
+        a.pp = pp;
+        a.nket = t.d_nket;
+        a.unit_prefix = t.d_unit_prefix;
+        a.nbra = t.nbra;
+        a.nunits = t.nunits;
+        a.bra_start = t.bra_start;
+        a.ket_start = t.ket_start;
+        a.counter = counters + c;
+        a.D = Duse;
+        a.Fj = Fj;
+        a.Fk = Fk;
+        a.ld = nbfc;
+        a.nsm = f->nsm;
+        if (launch_fock(t.X, t.Y, a, st) != 0) {
+            snprintf(g_errbuf, sizeof(g_errbuf), "allocation-free Fock build: launch for (%d,%d) failed: %s", t.X,
+                     t.Y, cudaGetErrorString(cudaGetLastError()));
+            return GTF_ERR_CUDA;
+        }
+    }
+    dim3 g2((nbf + 127) / 128, nbf);
+    k_f_to_sph<<<g2, 128, 0, st>>>(Fj, Fk, dev_F, J, K, f->d_sph2shell, f->d_sh_L, f->d_f_start, f->d_fc_start,
+                                   nbf, nbfc, f->pure);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
+    (void)nn;
+    return GTF_OK;
 }

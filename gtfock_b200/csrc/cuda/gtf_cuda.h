@@ -64,6 +64,10 @@ int gtf_fock_get_mat(gtf_fock_dev_t *f, int type, int index, int r0, int r1, int
                      int stride, double *host);
 const double *gtf_fock_mat_dev(gtf_fock_dev_t *f, int type, int index);
 
+/* Fock build with its scratch in a static device array (no allocation);
+ * dev_D in, dev_F (= J + K) out, both device pointers of nbf x nbf */
+int gtf_fock_compute_fixed(gtf_fock_dev_t *f, const double *dev_D, double *dev_F);
+
 /* one-electron matrices on the device: 0 S, 1 X = S^-1/2, 2 H_core */
 int gtf_fock_one_electron(gtf_fock_dev_t *f, int want_sx, int want_h);
 int gtf_fock_get_onee(gtf_fock_dev_t *f, int which, int r0, int r1, int c0, int c1,

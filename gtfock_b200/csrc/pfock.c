@@ -406,5 +406,13 @@ PFockStatus_t gtf_pfock_compute_dev(PFock_t pf, const double *dev_D, const doubl
     return PFOCK_STATUS_SUCCESS;
 }
 
+PFockStatus_t gtf_pfock_compute_noalloc(PFock_t pf, const double *dev_D, double *dev_F)
+{
+    if (pf == NULL) return PFOCK_STATUS_INVALID_VALUE;
+    int e = gtf_fock_compute_fixed(pf->dev, dev_D, dev_F);
+    if (e != GTF_OK) PFOCK_PRINTF(1, "%s\n", gtf_last_error());
+    return map_err(e);
+}
+
 /* internal accessors for scf_driver.c */
 gtf_fock_dev_t *gtf_pfock_device(PFock_t pf) { return pf->dev; }

@@ -48,6 +48,22 @@ PFockStatus_t gtf_pfock_set_precision(PFock_t pfock, int mode, double fp32_cutof
 PFockStatus_t gtf_pfock_compute_dev(PFock_t pfock, const double *dev_D,
                                     const double **dev_F);
 
+/* Fock build that allocates nothing.  No counterpart in the reference.
+ * For callers that may not allocate device memory while they run (a host
+ * whose own pool allocator owns the GPU memory, a real-time loop that must
+ * not wait on the driver's allocator, a plugin in a process that forbids
+ * allocation after start-up).  Same inputs and result as
+ * gtf_pfock_compute_dev: dev_D is the nbf x nbf density and dev_F receives
+ * F = J + K, both device pointers owned by the caller.  The scratch lives in
+ * one static device array of about 5.9 MB that every GPU loading the library
+ * keeps until exit; bases above 384 Cartesian functions are rejected with
+ * PFOCK_STATUS_INVALID_VALUE.  All calls on a GPU share that array: calls
+ * whose work overlaps on the GPU race and must be ordered by the caller.
+ * The first call on a device looks up the array's address; make it before
+ * any stream capture.  The engine must have been created on the current
+ * device. */
+PFockStatus_t gtf_pfock_compute_noalloc(PFock_t pfock, const double *dev_D, double *dev_F);
+
 /* Native SCF driver: the loop of pscf/scf.c:329-459 (Fock build, energy,
  * DIIS, purification) on one GPU for the molecule in xyzfile with basis
  * bsfile.  gtf_scf_create performs the set-up (basis, PFock_create with its
