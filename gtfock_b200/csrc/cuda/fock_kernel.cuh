@@ -28,6 +28,36 @@ struct FockLaunch {
 // ---------------------------------------------------------------------------
 // the Fock kernel: persistent warps claim units of 32 quartets
 // ---------------------------------------------------------------------------
+// Ket components per slice: quartets with up to 81 Cartesian integrals are
+// done in one pass; larger ones are split so that a slice keeps at most
+// ~54 accumulators in registers (the Rys roots and 2-D tables are
+// recomputed per slice, which costs less than spilling the accumulators).
+__host__ __device__ constexpr int fock_slice(int LA, int LB, int LC, int LD)
+{
+    const int nab = ncart(LA) * ncart(LB), ncd = ncart(LC) * ncart(LD);
+    if (nab * ncd <= 81) return ncd;
+    const int s = 54 / nab;
+    return s < 1 ? 1 : (s > ncd ? ncd : s);
+}
+
+template <int LA, int LB, int LC, int LD, int CD0>
+__device__ __forceinline__ void fock_slices(const PPStored &src, const PairRec &pb, const PairRec &pk, bool active,
+                                            bool same, const double *__restrict__ D, double *__restrict__ Fj,
+                                            double *__restrict__ Fk, int ld, int lane)
+{
+    constexpr int NCD = ncart(LC) * ncart(LD);
+    constexpr int S = fock_slice(LA, LB, LC, LD);
+    if constexpr (CD0 < NCD) {
+        constexpr int N = (NCD - CD0 < S) ? NCD - CD0 : S;
+        double acc[ncart(LA) * ncart(LB) * N];
+#pragma unroll
+        for (int k = 0; k < ncart(LA) * ncart(LB) * N; k++) acc[k] = 0.0;
+        if (active) eri_accumulate_cd<LA, LB, LC, LD, CD0, N, true>(src, pb, src, pk, acc);
+        digest_cd<LA, LB, LC, LD, CD0, N>(acc, active, pb, pk, same, D, Fj, Fk, ld, lane);
+        fock_slices<LA, LB, LC, LD, CD0 + N>(src, pb, pk, active, same, D, Fj, Fk, ld, lane);
+    }
+}
+
 template <int LA, int LB, int LC, int LD>
 __global__ void __launch_bounds__(FOCK_THREADS)
     k_fock(const PairRec *__restrict__ pairs, PrimPairs pp, const int *__restrict__ nket,
@@ -35,7 +65,6 @@ __global__ void __launch_bounds__(FOCK_THREADS)
            int ket_start, unsigned long long *__restrict__ counter, const double *__restrict__ D,
            double *__restrict__ Fj, double *__restrict__ Fk, int ld)
 {
-    constexpr int NQ = ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD);
     const int lane = threadIdx.x & 31;
     PPStored src{pp};
     for (;;) {
@@ -55,15 +84,10 @@ __global__ void __launch_bounds__(FOCK_THREADS)
         const bool active = j < __ldg(nket + i);
         const PairRec pb = pairs[bra_start + i];
         const PairRec pk = active ? pairs[ket_start + j] : pb;
-        double acc[NQ];
-#pragma unroll
-        for (int k = 0; k < NQ; k++) acc[k] = 0.0;
-        if (active) eri_accumulate<LA, LB, LC, LD, true>(src, pb, src, pk, acc);
         const bool same = (bra_start + i) == (ket_start + j);
-        digest<LA, LB, LC, LD, double>(acc, active, pb, pk, same, D, Fj, Fk, ld, lane);
+        fock_slices<LA, LB, LC, LD, 0>(src, pb, pk, active, same, D, Fj, Fk, ld, lane);
     }
 }
-
 
 template <int LA, int LB, int LC, int LD>
 int launch_fock_t(const FockLaunch &a, cudaStream_t st)

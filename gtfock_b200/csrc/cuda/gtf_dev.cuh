@@ -207,10 +207,12 @@ __device__ __forceinline__ void hrr_abcd(const double (&G)[LA + LB + 1][LC + LD 
 // ---------------------------------------------------------------------------
 // SKIP: primitive pairs are sorted by descending |K| (Fock-build pair list),
 // so the primitive-quartet cutoff may end the ket loop early
-template <int LA, int LB, int LC, int LD, bool SKIP = false, class PPB, class PPK>
-__device__ __forceinline__ void eri_accumulate(const PPB &bra, const PairRec &pb, const PPK &ket,
-                                               const PairRec &pk,
-                                               double (&acc)[ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD)])
+// Restricted to the ket components cd = CD0 .. CD0+N-1 (cd = ic + NC*id):
+// acc[ia + NA*(ib + NB*t)] with t = cd - CD0.  The output-split Fock kernels
+// call it once per slice so that a slice's accumulators fit in registers.
+template <int LA, int LB, int LC, int LD, int CD0, int N, bool SKIP, class PPB, class PPK>
+__device__ __forceinline__ void eri_accumulate_cd(const PPB &bra, const PairRec &pb, const PPK &ket,
+                                                  const PairRec &pk, double (&acc)[ncart(LA) * ncart(LB) * N])
 {
     constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
     constexpr int NI = LA + LB + 1, NK = LC + LD + 1;
@@ -252,24 +254,33 @@ __device__ __forceinline__ void eri_accumulate(const PPB &bra, const PairRec &pb
                 hrr_abcd<LA, LB, LC, LD>(Gy, Iy, pb.ABy, pk.ABy);
                 hrr_abcd<LA, LB, LC, LD>(Gz, Iz, pb.ABz, pk.ABz);
 #pragma unroll
-                for (int id = 0; id < ND; id++)
+                for (int t = 0; t < N; t++) {
+                    const int ic = (CD0 + t) % NC, id = (CD0 + t) / NC;
 #pragma unroll
-                    for (int ic = 0; ic < NC; ic++)
+                    for (int ibb = 0; ibb < NB; ibb++)
 #pragma unroll
-                        for (int ibb = 0; ibb < NB; ibb++)
-#pragma unroll
-                            for (int ia = 0; ia < NA; ia++) {
-                                const double xy =
-                                    Ix[cart_x(LA, ia)][cart_x(LB, ibb)][cart_x(LC, ic)][cart_x(LD, id)] *
-                                    Iy[cart_y(LA, ia)][cart_y(LB, ibb)][cart_y(LC, ic)][cart_y(LD, id)];
-                                double &dst = acc[ia + NA * (ibb + NB * (ic + NC * id))];
-                                dst = fma(xy,
-                                          Iz[cart_z(LA, ia)][cart_z(LB, ibb)][cart_z(LC, ic)][cart_z(LD, id)],
-                                          dst);
-                            }
+                        for (int ia = 0; ia < NA; ia++) {
+                            const double xy =
+                                Ix[cart_x(LA, ia)][cart_x(LB, ibb)][cart_x(LC, ic)][cart_x(LD, id)] *
+                                Iy[cart_y(LA, ia)][cart_y(LB, ibb)][cart_y(LC, ic)][cart_y(LD, id)];
+                            double &dst = acc[ia + NA * (ibb + NB * t)];
+                            dst = fma(xy, Iz[cart_z(LA, ia)][cart_z(LB, ibb)][cart_z(LC, ic)][cart_z(LD, id)],
+                                      dst);
+                        }
+                }
             }
         }
     }
+    (void)ND;
+}
+
+// the whole quartet: acc[ia + NA*(ib + NB*(ic + NC*id))]
+template <int LA, int LB, int LC, int LD, bool SKIP = false, class PPB, class PPK>
+__device__ __forceinline__ void eri_accumulate(const PPB &bra, const PairRec &pb, const PPK &ket,
+                                               const PairRec &pk,
+                                               double (&acc)[ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD)])
+{
+    eri_accumulate_cd<LA, LB, LC, LD, 0, ncart(LC) * ncart(LD), SKIP>(bra, pb, ket, pk, acc);
 }
 
 // primitive pairs read from the precomputed pair arrays
@@ -442,5 +453,150 @@ __device__ __forceinline__ void digest(const R (&I)[ncart(LA) * ncart(LB) * ncar
                         v = fma((double)I[ia + NA * (ibb + NB * (ic + NC * id))], dac[ia + NA * ic], v);
                 atomicAdd(Fk + (size_t)(fb + ibb) * ld + fd + id, sKbd * v);
             }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Digestion of one slice of a quartet (ket components cd = CD0 .. CD0+N-1),
+// same factors as digest<>.  Terms whose destination is summed over the
+// sliced index (Fj[a][b], Fk[a][c], Fk[b][c]) receive a partial sum per slice.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr bool slice_has_c(int CD0, int N, int NC, int ic)
+{
+    for (int t = 0; t < N; t++)
+        if ((CD0 + t) % NC == ic) return true;
+    return false;
+}
+
+__host__ __device__ constexpr bool slice_has_d(int CD0, int N, int NC, int id)
+{
+    for (int t = 0; t < N; t++)
+        if ((CD0 + t) / NC == id) return true;
+    return false;
+}
+
+template <int LA, int LB, int LC, int LD, int CD0, int N>
+__device__ __forceinline__ void digest_cd(const double (&I)[ncart(LA) * ncart(LB) * N], bool active,
+                                          const PairRec &pb, const PairRec &pk, bool same_pair,
+                                          const double *__restrict__ D, double *__restrict__ Fj,
+                                          double *__restrict__ Fk, int ld, int lane)
+{
+    constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    const int fa = pb.fa, fb = pb.fb, fc = pk.fa, fd = pk.fb;
+    const double f1 = (fa != fb) ? 1.0 : 0.0;
+    const double f2 = (fc != fd) ? 1.0 : 0.0;
+    const double f3 = same_pair ? 0.0 : 1.0;
+    const double sJab = 2.0 * (1.0 + f1) * (1.0 + f2);
+    const double sJcd = f3 * sJab;
+    const double sKac = -(1.0 + f3);
+    const double sKbc = f1 * sKac, sKad = f2 * sKac, sKbd = f1 * f2 * sKac;
+    // bra block J (warp-uniform destination), partial over the slice
+    {
+        double dcd[N];
+#pragma unroll
+        for (int t = 0; t < N; t++) {
+            const int ic = (CD0 + t) % NC, id = (CD0 + t) / NC;
+            dcd[t] = active ? __ldg(D + (size_t)(fc + ic) * ld + fd + id) : 0.0;
+        }
+#pragma unroll
+        for (int ibb = 0; ibb < NB; ibb++) {
+#pragma unroll
+            for (int ia = 0; ia < NA; ia++) {
+                double v = 0.0;
+#pragma unroll
+                for (int t = 0; t < N; t++) v = fma(I[ia + NA * (ibb + NB * t)], dcd[t], v);
+                v *= sJab;  // depends on the lane's ket
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(GTF_FULL_MASK, v, o);
+                if (lane == 0) atomicAdd(Fj + (size_t)(fa + ia) * ld + fb + ibb, v);
+            }
+        }
+    }
+    if (!active) return;
+    // ket block J: complete per (c, d)
+    if (f3 != 0.0) {
+        double dab[NA * NB];
+#pragma unroll
+        for (int ia = 0; ia < NA; ia++)
+#pragma unroll
+            for (int ibb = 0; ibb < NB; ibb++) dab[ia + NA * ibb] = __ldg(D + (size_t)(fa + ia) * ld + fb + ibb);
+#pragma unroll
+        for (int t = 0; t < N; t++) {
+            const int ic = (CD0 + t) % NC, id = (CD0 + t) / NC;
+            double v = 0.0;
+#pragma unroll
+            for (int ibb = 0; ibb < NB; ibb++)
+#pragma unroll
+                for (int ia = 0; ia < NA; ia++) v = fma(I[ia + NA * (ibb + NB * t)], dab[ia + NA * ibb], v);
+            atomicAdd(Fj + (size_t)(fc + ic) * ld + fd + id, sJcd * v);
+        }
+    }
+    // K[a][c] -= (1+f3) sum_bd D[b][d] I   and   K[b][c] -= f1 (1+f3) sum_ad D[a][d] I
+#pragma unroll
+    for (int ic = 0; ic < NC; ic++) {
+        if (!slice_has_c(CD0, N, NC, ic)) continue;
+#pragma unroll
+        for (int ia = 0; ia < NA; ia++) {
+            double v = 0.0;
+#pragma unroll
+            for (int t = 0; t < N; t++) {
+                if ((CD0 + t) % NC != ic) continue;
+                const int id = (CD0 + t) / NC;
+#pragma unroll
+                for (int ibb = 0; ibb < NB; ibb++)
+                    v = fma(I[ia + NA * (ibb + NB * t)], __ldg(D + (size_t)(fb + ibb) * ld + fd + id), v);
+            }
+            atomicAdd(Fk + (size_t)(fa + ia) * ld + fc + ic, sKac * v);
+        }
+        if (f1 != 0.0) {
+#pragma unroll
+            for (int ibb = 0; ibb < NB; ibb++) {
+                double v = 0.0;
+#pragma unroll
+                for (int t = 0; t < N; t++) {
+                    if ((CD0 + t) % NC != ic) continue;
+                    const int id = (CD0 + t) / NC;
+#pragma unroll
+                    for (int ia = 0; ia < NA; ia++)
+                        v = fma(I[ia + NA * (ibb + NB * t)], __ldg(D + (size_t)(fa + ia) * ld + fd + id), v);
+                }
+                atomicAdd(Fk + (size_t)(fb + ibb) * ld + fc + ic, sKbc * v);
+            }
+        }
+    }
+    // K[a][d] -= f2 (1+f3) sum_bc D[b][c] I   and   K[b][d] -= f1 f2 (1+f3) sum_ac D[a][c] I
+    if (f2 != 0.0) {
+#pragma unroll
+        for (int id = 0; id < ND; id++) {
+            if (!slice_has_d(CD0, N, NC, id)) continue;
+#pragma unroll
+            for (int ia = 0; ia < NA; ia++) {
+                double v = 0.0;
+#pragma unroll
+                for (int t = 0; t < N; t++) {
+                    if ((CD0 + t) / NC != id) continue;
+                    const int ic = (CD0 + t) % NC;
+#pragma unroll
+                    for (int ibb = 0; ibb < NB; ibb++)
+                        v = fma(I[ia + NA * (ibb + NB * t)], __ldg(D + (size_t)(fb + ibb) * ld + fc + ic), v);
+                }
+                atomicAdd(Fk + (size_t)(fa + ia) * ld + fd + id, sKad * v);
+            }
+            if (f1 != 0.0) {
+#pragma unroll
+                for (int ibb = 0; ibb < NB; ibb++) {
+                    double v = 0.0;
+#pragma unroll
+                    for (int t = 0; t < N; t++) {
+                        if ((CD0 + t) / NC != id) continue;
+                        const int ic = (CD0 + t) % NC;
+#pragma unroll
+                        for (int ia = 0; ia < NA; ia++)
+                            v = fma(I[ia + NA * (ibb + NB * t)], __ldg(D + (size_t)(fa + ia) * ld + fc + ic), v);
+                    }
+                    atomicAdd(Fk + (size_t)(fb + ibb) * ld + fd + id, sKbd * v);
+                }
+            }
+        }
     }
 }
