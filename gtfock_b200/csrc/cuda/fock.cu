@@ -32,6 +32,9 @@
 
 #include "gtf_cuda.h"
 #include "gtf_dev.cuh"
+// the Fock kernels live in fock_kernel.cuh, instantiated across several
+// translation units (fock_cls_*.cu) so that they compile in parallel
+#include "fock_kernel.cuh"
 
 
 #define NCLS 6
@@ -66,10 +69,11 @@ struct ClassPairTask {
     int X, Y;
     int bra_start, nbra;
     int ket_start, nketcls;
+    int seg[GTF_NBKT + 1];  // ket segments (primitive-count buckets), relative to ket_start
     long long nunits;
     double nquart;
-    int *d_nket;
-    long long *d_unit_prefix;
+    int *d_nket;               // [nbra][GTF_NBKT]
+    long long *d_unit_prefix;  // [nbra * GTF_NBKT + 1]
 };
 
 struct gtf_fock_dev {
@@ -93,7 +97,7 @@ struct gtf_fock_dev {
     PairRec *d_pairs;
     double *d_pair_v;
     int nprimpairs;
-    double *d_pp;   // 5 * nprimpairs: p, Px, Py, Pz, K
+    double *d_pp;   // 6 * nprimpairs: records {p, K, Px, Py, Pz, 0} (PPRec)
     ClassPairTask tasks[NCLSPAIR];
     unsigned long long *d_counters;
     double usq, uitl, eri_flops;
@@ -377,14 +381,43 @@ __global__ void k_sort_keys(const double *__restrict__ shellvalue, const int *__
     idx[k] = k;
 }
 
+// second sort key: angular class (high bits) and primitive-count bucket
 __global__ void k_gather_cls(const int *__restrict__ idx, const int *__restrict__ shellid,
-                             const int *__restrict__ shellrid, const int *__restrict__ sh_L, int nnz,
-                             int *__restrict__ kcls)
+                             const int *__restrict__ shellrid, const int *__restrict__ sh_L,
+                             const int *__restrict__ kept, int nnz, int *__restrict__ kcls)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nnz) return;
     const int k = idx[s];
-    kcls[s] = pair_class(sh_L[shellrid[k]], sh_L[shellid[k]]);
+    kcls[s] = pair_class(sh_L[shellrid[k]], sh_L[shellid[k]]) * 16 + gtf_prim_bucket(kept[k]);
+}
+
+// prefactor K of primitive pair (i, j) of shells (a, bb) at squared distance r2
+__device__ __forceinline__ double prim_pair_K(const BasisDev &b, int pa, int pb, int i, int j, double r2, double &p)
+{
+    const double al = b.alpha[pa + i], be = b.alpha[pb + j];
+    p = al + be;
+    const double ip = 1.0 / p;
+    return GTF_PAIR_PREF * b.coef[pa + i] * b.coef[pb + j] * exp(-al * be * ip * r2) * ip;
+}
+
+// number of primitive pairs of CSR entry k that survive |K| >= GTF_PRIM_EPS
+__global__ void k_prim_keep(const int *__restrict__ shellid, const int *__restrict__ shellrid, BasisDev b,
+                            int nnz, int *__restrict__ kept)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nnz) return;
+    const int M = shellrid[k], N = shellid[k];
+    const double dx = b.sh_xyz[3 * M] - b.sh_xyz[3 * N], dy = b.sh_xyz[3 * M + 1] - b.sh_xyz[3 * N + 1],
+                 dz = b.sh_xyz[3 * M + 2] - b.sh_xyz[3 * N + 2];
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    int c = 0;
+    for (int i = 0; i < b.sh_nprim[M]; i++)
+        for (int j = 0; j < b.sh_nprim[N]; j++) {
+            double p;
+            if (fabs(prim_pair_K(b, b.sh_pstart[M], b.sh_pstart[N], i, j, r2, p)) >= GTF_PRIM_EPS) c++;
+        }
+    kept[k] = c;
 }
 
 __global__ void k_build_pairs(const int *__restrict__ idx, const int *__restrict__ shellid,
@@ -420,10 +453,10 @@ __global__ void k_build_pairs(const int *__restrict__ idx, const int *__restrict
 // to any integral is below 1e-20 Hartree), the rest are stored in descending
 // |K| so that the quartet loop can stop once |K_ab K_cd| < GTF_PRIMQ_EPS.
 // pairs[s].n becomes the kept count (possibly 0); the slot keeps its size.
+// Records are {p, K, Px, Py, Pz, 0} (PPRec).
 __global__ void k_fill_primpairs(PairRec *__restrict__ pairs, const int *__restrict__ idx,
                                  const int *__restrict__ shellid, const int *__restrict__ shellrid,
-                                 const int *__restrict__ pair_off, BasisDev b, int npairs, double *pp,
-                                 int npp)
+                                 const int *__restrict__ pair_off, BasisDev b, int npairs, double *pp)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= npairs) return;
@@ -437,27 +470,28 @@ __global__ void k_fill_primpairs(PairRec *__restrict__ pairs, const int *__restr
     const double r2 = (Ax - Bx) * (Ax - Bx) + (Ay - By) * (Ay - By) + (Az - Bz) * (Az - Bz);
     const int na = b.sh_nprim[a], nb = b.sh_nprim[bb];
     const int pa = b.sh_pstart[a], pb = b.sh_pstart[bb];
-    const size_t np = (size_t)npp;
+    constexpr int W = 2 * GTF_PPREC_D2;
     int kept = 0;
     for (int i = 0; i < na; i++) {
         for (int j = 0; j < nb; j++) {
-            const double al = b.alpha[pa + i], be = b.alpha[pb + j];
-            const double p = al + be, ip = 1.0 / p;
-            const double K = GTF_PAIR_PREF * b.coef[pa + i] * b.coef[pb + j] * exp(-al * be * ip * r2) * ip;
+            double p;
+            const double K = prim_pair_K(b, pa, pb, i, j, r2, p);
             if (fabs(K) < GTF_PRIM_EPS) continue;
+            const double al = b.alpha[pa + i], be = b.alpha[pb + j], ip = 1.0 / p;
             // insertion into the descending-|K| list of the kept pairs
             int o = kept;
-            while (o > 0 && fabs(pp[4 * np + off + o - 1]) < fabs(K)) {
-                const size_t src = (size_t)off + o - 1;
-                for (int f = 0; f < 5; f++) pp[f * np + src + 1] = pp[f * np + src];
+            while (o > 0 && fabs(pp[W * ((size_t)off + o - 1) + 1]) < fabs(K)) {
+                const size_t src = W * ((size_t)off + o - 1);
+                for (int f = 0; f < W; f++) pp[src + W + f] = pp[src + f];
                 o--;
             }
-            const size_t d = (size_t)off + o;
-            pp[d] = p;
-            pp[np + d] = (al * Ax + be * Bx) * ip;
-            pp[2 * np + d] = (al * Ay + be * By) * ip;
-            pp[3 * np + d] = (al * Az + be * Bz) * ip;
-            pp[4 * np + d] = K;
+            double *d = pp + W * ((size_t)off + o);
+            d[0] = p;
+            d[1] = K;
+            d[2] = (al * Ax + be * Bx) * ip;
+            d[3] = (al * Ay + be * By) * ip;
+            d[4] = (al * Az + be * Bz) * ip;
+            d[5] = 0.0;
             kept++;
         }
     }
@@ -465,34 +499,44 @@ __global__ void k_fill_primpairs(PairRec *__restrict__ pairs, const int *__restr
     pairs[s].n = kept;
 }
 
-// number of ket pairs of the ket class that pass v_bra * v_ket >= tol2
-// (pfock/fock_task.c:192); the ket class is sorted by value, descending
+// number of ket pairs of segment b of the ket class that pass
+// v_bra * v_ket >= tol2 (pfock/fock_task.c:192): each segment is sorted by
+// value, descending, so they form a prefix.  For bra class == ket class only
+// kets at or before the bra in the class order count, so every unordered
+// pair of pairs is visited once.  Thread (i, b); segment 0 holds pairs whose
+// primitive pairs were all screened out: counted, but given no units.
+struct SegStarts {
+    int s[GTF_NBKT + 1];
+};
+
 __global__ void k_count_kets(const double *__restrict__ pair_v, int bra_start, int nbra, int ket_start,
-                             int nketcls, int same, double tol2, int *__restrict__ nket,
+                             SegStarts seg, int same, double tol2, int *__restrict__ nket,
                              long long *__restrict__ units)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i > nbra) return;
-    if (i == nbra) {
-        units[nbra] = 0;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nidx = nbra * GTF_NBKT;
+    if (t > nidx) return;
+    if (t == nidx) {
+        units[nidx] = 0;
         return;
     }
+    const int i = t / GTF_NBKT, b = t - i * GTF_NBKT;
     const double v = pair_v[bra_start + i];
-    int lo = 0, hi = nketcls;  // count = first index failing the test
+    const int s0 = seg.s[b], s1 = seg.s[b + 1];
+    int lo = s0, hi = s1;  // first index failing the test
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
         if (fabs(v * pair_v[ket_start + mid]) >= tol2) lo = mid + 1;
         else hi = mid;
     }
-    int c = lo;
-    if (same && c > i + 1) c = i + 1;
-    nket[i] = c;
-    units[i] = (c + 31) / 32;
+    int c = lo - s0;
+    if (same) {
+        const int lim = i - s0 + 1;  // kets j <= i
+        c = lim < 0 ? 0 : (c < lim ? c : lim);
+    }
+    nket[t] = c;
+    units[t] = b == 0 ? 0 : (c + 31) / 32;
 }
-
-// the Fock kernels live in fock_kernel.cuh, instantiated across several
-// translation units (fock_cls_*.cu) so that they compile in parallel
-#include "fock_kernel.cuh"
 
 typedef int (*fock_group_launch_t)(int la, int lb, int lc, int ld, const FockLaunch &a, cudaStream_t st);
 extern fock_group_launch_t gtf_fock_groups[];
@@ -698,7 +742,7 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
     // ---- device pair list: sort by class, then value descending ----
     f->npairs = nnz;
     unsigned long long *d_kval, *d_kval2;
-    int *d_kcls, *d_kcls2, *d_idx, *d_idx2, *d_pair_n, *d_pair_off;
+    int *d_kcls, *d_kcls2, *d_idx, *d_idx2, *d_pair_n, *d_pair_off, *d_kept;
     DALLOC(d_kval, nnz);
     DALLOC(d_kval2, nnz);
     DALLOC(d_kcls, nnz);
@@ -707,14 +751,17 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
     DALLOC(d_idx2, nnz);
     DALLOC(d_pair_n, nnz + 1);
     DALLOC(d_pair_off, nnz + 1);
+    DALLOC(d_kept, nnz);
     const unsigned gp = (unsigned)((nnz + 255) / 256 > 0 ? (nnz + 255) / 256 : 1);
     if (nnz > 0) {
         k_sort_keys<<<gp, 256, 0, st>>>(f->d_shellvalue, f->d_shellid, f->d_shellrid, f->d_sh_L, nnz,
                                         d_kval, d_kcls, d_idx);
         CK(cudaGetLastError());
+        k_prim_keep<<<gp, 256, 0, st>>>(f->d_shellid, f->d_shellrid, bd, nnz, d_kept);
+        CK(cudaGetLastError());
         size_t b1 = 0, b2 = 0;
         CK(cub::DeviceRadixSort::SortPairs(nullptr, b1, d_kval, d_kval2, d_idx, d_idx2, nnz, 0, 64, st));
-        CK(cub::DeviceRadixSort::SortPairs(nullptr, b2, d_kcls, d_kcls2, d_idx2, d_idx, nnz, 0, 3, st));
+        CK(cub::DeviceRadixSort::SortPairs(nullptr, b2, d_kcls, d_kcls2, d_idx2, d_idx, nnz, 0, 7, st));
         size_t need = b1 > b2 ? b1 : b2;
         if (need > tmp_cap) {
             cudaFree(d_tmp);
@@ -723,10 +770,10 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
         }
         b1 = tmp_cap;
         CK(cub::DeviceRadixSort::SortPairs(d_tmp, b1, d_kval, d_kval2, d_idx, d_idx2, nnz, 0, 64, st));
-        k_gather_cls<<<gp, 256, 0, st>>>(d_idx2, f->d_shellid, f->d_shellrid, f->d_sh_L, nnz, d_kcls);
+        k_gather_cls<<<gp, 256, 0, st>>>(d_idx2, f->d_shellid, f->d_shellrid, f->d_sh_L, d_kept, nnz, d_kcls);
         CK(cudaGetLastError());
         b2 = tmp_cap;
-        CK(cub::DeviceRadixSort::SortPairs(d_tmp, b2, d_kcls, d_kcls2, d_idx2, d_idx, nnz, 0, 3, st));
+        CK(cub::DeviceRadixSort::SortPairs(d_tmp, b2, d_kcls, d_kcls2, d_idx2, d_idx, nnz, 0, 7, st));
     }
     DALLOC(f->d_pairs, nnz);
     DALLOC(f->d_pair_v, nnz);
@@ -752,16 +799,18 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
         CK(cudaMemcpyAsync(cls_sorted.data(), d_kcls2, sizeof(int) * nnz, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     f->nprimpairs = npp;
-    DALLOC(f->d_pp, 5 * (size_t)(npp > 0 ? npp : 1));
+    DALLOC(f->d_pp, 2 * GTF_PPREC_D2 * (size_t)(npp > 0 ? npp : 1));
     if (nnz > 0) {
         k_fill_primpairs<<<gp, 256, 0, st>>>(f->d_pairs, d_idx, f->d_shellid, f->d_shellrid, d_pair_off, bd,
-                                             nnz, f->d_pp, npp);
+                                             nnz, f->d_pp);
         CK(cudaGetLastError());
     }
-    for (int c = 0; c <= NCLS; c++) f->cls_start[c] = nnz;
-    for (int s = nnz - 1; s >= 0; s--) f->cls_start[cls_sorted[s]] = s;
-    for (int c = NCLS - 1; c >= 0; c--)
-        if (f->cls_start[c] > f->cls_start[c + 1]) f->cls_start[c] = f->cls_start[c + 1];
+    // class and segment starts from the sorted keys (class * 16 + bucket)
+    std::vector<int> key_start(NCLS * 16 + 1, nnz);
+    for (int s2 = nnz - 1; s2 >= 0; s2--) key_start[cls_sorted[s2]] = s2;
+    for (int k = NCLS * 16 - 1; k >= 0; k--)
+        if (key_start[k] > key_start[k + 1]) key_start[k] = key_start[k + 1];
+    for (int c = 0; c <= NCLS; c++) f->cls_start[c] = key_start[c * 16];
 
     // ---- task lists per class pair ----
     f->usq = 0.0;
@@ -778,34 +827,38 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
             t.nbra = f->cls_start[X + 1] - f->cls_start[X];
             t.ket_start = f->cls_start[Y];
             t.nketcls = f->cls_start[Y + 1] - f->cls_start[Y];
+            SegStarts seg;
+            for (int bk = 0; bk <= GTF_NBKT; bk++) {
+                t.seg[bk] = key_start[Y * 16 + bk] - t.ket_start;
+                seg.s[bk] = t.seg[bk];
+            }
             t.nunits = 0;
             t.nquart = 0.0;
             if (t.nbra == 0 || t.nketcls == 0) continue;
-            DALLOC(t.d_nket, t.nbra);
-            DALLOC(t.d_unit_prefix, t.nbra + 1);
+            const int nidx = t.nbra * GTF_NBKT;
+            DALLOC(t.d_nket, nidx);
+            DALLOC(t.d_unit_prefix, nidx + 1);
             long long *d_units;
-            CK(cudaMalloc(&d_units, sizeof(long long) * (t.nbra + 1)));
-            k_count_kets<<<(t.nbra + 1 + 255) / 256, 256, 0, st>>>(f->d_pair_v, t.bra_start, t.nbra,
-                                                                  t.ket_start, t.nketcls, X == Y,
-                                                                  f->tolscr2, t.d_nket, d_units);
+            CK(cudaMalloc(&d_units, sizeof(long long) * (nidx + 1)));
+            k_count_kets<<<(nidx + 1 + 255) / 256, 256, 0, st>>>(f->d_pair_v, t.bra_start, t.nbra, t.ket_start,
+                                                                seg, X == Y, f->tolscr2, t.d_nket, d_units);
             CK(cudaGetLastError());
             size_t b4 = 0;
-            CK(cub::DeviceScan::ExclusiveSum(nullptr, b4, d_units, t.d_unit_prefix, t.nbra + 1, st));
+            CK(cub::DeviceScan::ExclusiveSum(nullptr, b4, d_units, t.d_unit_prefix, nidx + 1, st));
             if (b4 > tmp_cap) {
                 cudaFree(d_tmp);
                 tmp_cap = b4;
                 CK(cudaMalloc(&d_tmp, tmp_cap));
             }
             b4 = tmp_cap;
-            CK(cub::DeviceScan::ExclusiveSum(d_tmp, b4, d_units, t.d_unit_prefix, t.nbra + 1, st));
-            std::vector<int> nk(t.nbra);
-            CK(cudaMemcpyAsync(&t.nunits, t.d_unit_prefix + t.nbra, sizeof(long long), cudaMemcpyDeviceToHost,
-                               st));
-            CK(cudaMemcpyAsync(nk.data(), t.d_nket, sizeof(int) * t.nbra, cudaMemcpyDeviceToHost, st));
+            CK(cub::DeviceScan::ExclusiveSum(d_tmp, b4, d_units, t.d_unit_prefix, nidx + 1, st));
+            std::vector<int> nk(nidx);
+            CK(cudaMemcpyAsync(&t.nunits, t.d_unit_prefix + nidx, sizeof(long long), cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(nk.data(), t.d_nket, sizeof(int) * nidx, cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             cudaFree(d_units);
             double q = 0.0;
-            for (int i = 0; i < t.nbra; i++) q += nk[i];
+            for (int i = 0; i < nidx; i++) q += nk[i];
             t.nquart = q;
             const int la = k_cls_la[X], lb = k_cls_lb[X], lc = k_cls_la[Y], ld = k_cls_lb[Y];
             const double dims = (double)(b->pure ? (la == 2 ? 5 : ncart(la)) : ncart(la)) *
@@ -828,8 +881,9 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
         for (int c2 = 0; c2 < NCLSPAIR; c2++) {
             ClassPairTask &t = f->tasks[c2];
             if (t.nunits == 0) continue;
-            std::vector<int> nk(t.nbra);
-            CK(cudaMemcpy(nk.data(), t.d_nket, sizeof(int) * t.nbra, cudaMemcpyDeviceToHost));
+            const int nidx = t.nbra * GTF_NBKT;
+            std::vector<int> nk(nidx);
+            CK(cudaMemcpy(nk.data(), t.d_nket, sizeof(int) * nidx, cudaMemcpyDeviceToHost));
             // prefix sums of ket primitive-pair counts
             std::vector<double> kpre(t.nketcls + 1, 0.0);
             for (int j = 0; j < t.nketcls; j++) kpre[j + 1] = kpre[j] + hn[t.ket_start + j];
@@ -840,8 +894,11 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
                                (b->pure && lc == 2 ? 5 : ncart(lc)) * (b->pure && ld == 2 ? 5 : ncart(ld));
             for (int i = 0; i < t.nbra; i++) {
                 const double kb = hn[t.bra_start + i];
-                const double kk = kpre[nk[i]];
-                flops += kb * kk * per_prim + (cpart + 12.0 * ns_) * nk[i];
+                for (int bk = 0; bk < GTF_NBKT; bk++) {
+                    const int c = nk[i * GTF_NBKT + bk];
+                    const double kk = kpre[t.seg[bk] + c] - kpre[t.seg[bk]];
+                    flops += kb * kk * per_prim + (cpart + 12.0 * ns_) * c;
+                }
             }
         }
         f->eri_flops = flops;
@@ -856,6 +913,7 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
     cudaFree(d_idx2);
     cudaFree(d_pair_n);
     cudaFree(d_pair_off);
+    cudaFree(d_kept);
     cudaFree(d_idx);
     f->dev_bytes -= n2 * 2 * sizeof(int) + (size_t)nnz * (2 * 8 + 4 * 4) + (size_t)(nnz + 1) * 8;
 
@@ -993,6 +1051,23 @@ extern "C" int gtf_fock_set_precision(gtf_fock_dev_t *f, int prec, double fp32_c
     return GTF_OK;
 }
 
+// launch arguments of one class pair (counter, D and accumulators are set by the caller)
+static FockLaunch fock_launch_args(const gtf_fock_dev *f, const ClassPairTask &t)
+{
+    FockLaunch a;
+    memset(&a, 0, sizeof(a));
+    a.pairs = f->d_pairs;
+    a.pprec = reinterpret_cast<const double2 *>(f->d_pp);
+    a.nket = t.d_nket;
+    a.unit_prefix = t.d_unit_prefix;
+    a.nbra = t.nbra;
+    a.nunits = t.nunits;
+    a.bra_start = t.bra_start;
+    a.ket_start = t.ket_start;
+    for (int b = 0; b <= GTF_NBKT; b++) a.seg[b] = t.seg[b];
+    return a;
+}
+
 extern "C" int gtf_fock_compute(gtf_fock_dev_t *f, int numdmat)
 {
     if (numdmat <= 0 || numdmat > f->max_numdmat) return GTF_ERR_INVALID;
@@ -1000,8 +1075,6 @@ extern "C" int gtf_fock_compute(gtf_fock_dev_t *f, int numdmat)
     const int nbf = f->nbf, nbfc = f->nbf_cart;
     const size_t nn = (size_t)nbf * nbf, nnc = (size_t)nbfc * nbfc;
     const bool need_tr = f->pure && nbfc != nbf;
-    PrimPairs pp{f->d_pp, f->d_pp + f->nprimpairs, f->d_pp + 2 * (size_t)f->nprimpairs,
-                 f->d_pp + 3 * (size_t)f->nprimpairs, f->d_pp + 4 * (size_t)f->nprimpairs};
     CK(cudaEventRecord(f->ev0, st));
     float eri_ms_total = 0.0f;
     for (int d = 0; d < numdmat; d++) {
@@ -1023,15 +1096,7 @@ extern "C" int gtf_fock_compute(gtf_fock_dev_t *f, int numdmat)
             ClassPairTask &t = f->tasks[c];
             CK(cudaEventRecord(f->ev_cls[c], st));
             if (t.nunits == 0) continue;
-            FockLaunch a;
-            a.pairs = f->d_pairs;
-            a.pp = pp;
-            a.nket = t.d_nket;
-            a.unit_prefix = t.d_unit_prefix;
-            a.nbra = t.nbra;
-            a.nunits = t.nunits;
-            a.bra_start = t.bra_start;
-            a.ket_start = t.ket_start;
+            FockLaunch a = fock_launch_args(f, t);
             a.counter = f->d_counters + c;
             a.D = Dc;
             a.Fj = f->d_Fj;
@@ -1276,20 +1341,10 @@ extern "C" int gtf_fock_compute_fixed(gtf_fock_dev_t *f, const double *dev_D, do
     CK(cudaMemsetAsync(Fj, 0, sizeof(double) * nnc, st));
     CK(cudaMemsetAsync(Fk, 0, sizeof(double) * nnc, st));
     CK(cudaMemsetAsync(counters, 0, sizeof(unsigned long long) * NCLSPAIR, st));
-    PrimPairs pp{f->d_pp, f->d_pp + f->nprimpairs, f->d_pp + 2 * (size_t)f->nprimpairs,
-                 f->d_pp + 3 * (size_t)f->nprimpairs, f->d_pp + 4 * (size_t)f->nprimpairs};
     for (int c = 0; c < NCLSPAIR; c++) {
         ClassPairTask &t = f->tasks[c];
         if (t.nunits == 0) continue;
-        FockLaunch a;
-        a.pairs = f->d_pairs;
-        a.pp = pp;
-        a.nket = t.d_nket;
-        a.unit_prefix = t.d_unit_prefix;
-        a.nbra = t.nbra;
-        a.nunits = t.nunits;
-        a.bra_start = t.bra_start;
-        a.ket_start = t.ket_start;
+        FockLaunch a = fock_launch_args(f, t);
         a.counter = counters + c;
         a.D = Duse;
         a.Fj = Fj;

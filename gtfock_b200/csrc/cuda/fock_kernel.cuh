@@ -10,14 +10,36 @@
 
 #define FOCK_THREADS 128
 
+// Ket pairs of one angular class are stored in segments of similar
+// primitive-pair count (gtf_prim_bucket), each sorted by Schwarz bound, so the
+// 32 lanes of a warp loop over about the same number of primitive quartets.
+#define GTF_NBKT 15
+__host__ __device__ inline int gtf_prim_bucket(int n)
+{
+    if (n <= 2) return n < 0 ? 0 : n;
+    if (n <= 4) return 3;
+    if (n <= 6) return 4;
+    if (n <= 9) return 5;
+    if (n <= 12) return 6;
+    if (n <= 16) return 7;
+    if (n <= 20) return 8;
+    if (n <= 25) return 9;
+    if (n <= 32) return 10;
+    if (n <= 40) return 11;
+    if (n <= 48) return 12;
+    if (n <= 64) return 13;
+    return 14;
+}
+
 struct FockLaunch {
     const PairRec *pairs;
-    PrimPairs pp;
-    const int *nket;
-    const long long *unit_prefix;
+    const double2 *pprec;          // primitive-pair records (PPRec)
+    const int *nket;               // [nbra][GTF_NBKT] kets per (bra, segment)
+    const long long *unit_prefix;  // exclusive prefix of units over (bra, segment)
     int nbra;
     long long nunits;
     int bra_start, ket_start;
+    int seg[GTF_NBKT + 1];         // segment starts, relative to ket_start
     unsigned long long *counter;
     const double *D;
     double *Fj, *Fk;
@@ -28,20 +50,20 @@ struct FockLaunch {
 // ---------------------------------------------------------------------------
 // the Fock kernel: persistent warps claim units of 32 quartets
 // ---------------------------------------------------------------------------
-// Ket components per slice: quartets with up to 81 Cartesian integrals are
+// Ket components per slice: quartets with up to 64 Cartesian integrals are
 // done in one pass; larger ones are split so that a slice keeps at most
 // ~54 accumulators in registers (the Rys roots and 2-D tables are
 // recomputed per slice, which costs less than spilling the accumulators).
 __host__ __device__ constexpr int fock_slice(int LA, int LB, int LC, int LD)
 {
     const int nab = ncart(LA) * ncart(LB), ncd = ncart(LC) * ncart(LD);
-    if (nab * ncd <= 81) return ncd;
+    if (nab * ncd <= 64) return ncd;
     const int s = 54 / nab;
     return s < 1 ? 1 : (s > ncd ? ncd : s);
 }
 
 template <int LA, int LB, int LC, int LD, int CD0>
-__device__ __forceinline__ void fock_slices(const PPStored &src, const PairRec &pb, const PairRec &pk, bool active,
+__device__ __forceinline__ void fock_slices(const PPRec &src, const PairRec &pb, const PairRec &pk, bool active,
                                             bool same, const double *__restrict__ D, double *__restrict__ Fj,
                                             double *__restrict__ Fk, int ld, int lane)
 {
@@ -58,34 +80,34 @@ __device__ __forceinline__ void fock_slices(const PPStored &src, const PairRec &
     }
 }
 
+// unit u -> (bra i, segment b, chunk of 32 kets): binary search of the
+// exclusive unit prefix over the flattened (bra, segment) index
 template <int LA, int LB, int LC, int LD>
-__global__ void __launch_bounds__(FOCK_THREADS)
-    k_fock(const PairRec *__restrict__ pairs, PrimPairs pp, const int *__restrict__ nket,
-           const long long *__restrict__ unit_prefix, int nbra, long long nunits, int bra_start,
-           int ket_start, unsigned long long *__restrict__ counter, const double *__restrict__ D,
-           double *__restrict__ Fj, double *__restrict__ Fk, int ld)
+__global__ void __launch_bounds__(FOCK_THREADS) k_fock(const FockLaunch a)
 {
     const int lane = threadIdx.x & 31;
-    PPStored src{pp};
+    const PPRec src{a.pprec};
+    const int nidx = a.nbra * GTF_NBKT;
     for (;;) {
         unsigned long long u = 0;
-        if (lane == 0) u = atomicAdd(counter, 1ULL);
+        if (lane == 0) u = atomicAdd(a.counter, 1ULL);
         u = __shfl_sync(GTF_FULL_MASK, u, 0);
-        if (u >= (unsigned long long)nunits) break;
-        int lo = 0, hi = nbra;
+        if (u >= (unsigned long long)a.nunits) break;
+        int lo = 0, hi = nidx;
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
-            if (__ldg(unit_prefix + mid) <= (long long)u) lo = mid;
+            if (__ldg(a.unit_prefix + mid) <= (long long)u) lo = mid;
             else hi = mid;
         }
-        const int i = lo;
-        const long long chunk = (long long)u - __ldg(unit_prefix + i);
-        const int j = (int)(chunk * 32) + lane;
-        const bool active = j < __ldg(nket + i);
-        const PairRec pb = pairs[bra_start + i];
-        const PairRec pk = active ? pairs[ket_start + j] : pb;
-        const bool same = (bra_start + i) == (ket_start + j);
-        fock_slices<LA, LB, LC, LD, 0>(src, pb, pk, active, same, D, Fj, Fk, ld, lane);
+        const int i = lo / GTF_NBKT, b = lo - i * GTF_NBKT;
+        const long long chunk = (long long)u - __ldg(a.unit_prefix + lo);
+        const int jj = (int)(chunk * 32) + lane;
+        const bool active = jj < __ldg(a.nket + lo);
+        const int j = a.seg[b] + jj;
+        const PairRec pb = a.pairs[a.bra_start + i];
+        const PairRec pk = active ? a.pairs[a.ket_start + j] : pb;
+        const bool same = (a.bra_start + i) == (a.ket_start + j);
+        fock_slices<LA, LB, LC, LD, 0>(src, pb, pk, active, same, a.D, a.Fj, a.Fk, a.ld, lane);
     }
 }
 
@@ -100,8 +122,7 @@ int launch_fock_t(const FockLaunch &a, cudaStream_t st)
     long long grid = (long long)a.nsm * per_sm;
     if (want < grid) grid = want;
     if (grid < 1) grid = 1;
-    k<<<(unsigned)grid, FOCK_THREADS, 0, st>>>(a.pairs, a.pp, a.nket, a.unit_prefix, a.nbra, a.nunits,
-                                               a.bra_start, a.ket_start, a.counter, a.D, a.Fj, a.Fk, a.ld);
+    k<<<(unsigned)grid, FOCK_THREADS, 0, st>>>(a);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

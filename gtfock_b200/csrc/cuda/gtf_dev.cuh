@@ -10,7 +10,7 @@
 //     G(i,k) by the Rys recurrences (C00, C00', B10, B01, B00), horizontal
 //     transfer to (a b | c d) per Cartesian direction, and the product
 //     Ix*Iy*Iz accumulated in registers; integrals never leave the thread;
-//   * digest<...>: the six J/K updates of one unique quartet into F with
+//   * digest_cd<...>: the six J/K updates of one unique quartet into F with
 //     the reference's degeneracy factors; the bra block (uniform across a
 //     warp) is warp-reduced before its atomics.
 #pragma once
@@ -18,7 +18,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#define RYS_QUAL __device__
+#define RYS_QUAL __device__ __align__(16)
 #define RYS_QUAL_SMALL __constant__
 #include "rys_table.h"
 
@@ -104,13 +104,23 @@ __device__ __forceinline__ void rys_roots(double T, double (&u)[N], double (&w)[
     const int k = (int)(T * RYS_INV_H);
     const double s = T - ((double)k * RYS_H + 0.5 * RYS_H);
     const double *c = RYS_TABLE + RYS_OFF[N] + k * (RYS_DEG + 1) * (2 * N);
+    // rows of 2N coefficients start on 16-byte boundaries (even offsets)
+    const double2 *c2 = reinterpret_cast<const double2 *>(c);
     double a[2 * N];
 #pragma unroll
-    for (int f = 0; f < 2 * N; f++) a[f] = __ldg(c + RYS_DEG * 2 * N + f);
+    for (int f = 0; f < N; f++) {
+        const double2 t = __ldg(c2 + RYS_DEG * N + f);
+        a[2 * f] = t.x;
+        a[2 * f + 1] = t.y;
+    }
 #pragma unroll
     for (int j = RYS_DEG - 1; j >= 0; j--) {
 #pragma unroll
-        for (int f = 0; f < 2 * N; f++) a[f] = fma(a[f], s, __ldg(c + j * 2 * N + f));
+        for (int f = 0; f < N; f++) {
+            const double2 t = __ldg(c2 + j * N + f);
+            a[2 * f] = fma(a[2 * f], s, t.x);
+            a[2 * f + 1] = fma(a[2 * f + 1], s, t.y);
+        }
     }
 #pragma unroll
     for (int i = 0; i < N; i++) {
@@ -221,9 +231,12 @@ __device__ __forceinline__ void eri_accumulate_cd(const PPB &bra, const PairRec 
         double p, Px, Py, Pz, Kab;
         bra.get(pb, ib, p, Px, Py, Pz, Kab);
         const double PAx = Px - pb.Ax, PAy = Py - pb.Ay, PAz = Pz - pb.Az;
+        // the next ket primitive pair is loaded while the current one is used
+        double nq = 0.0, nQx = 0.0, nQy = 0.0, nQz = 0.0, nK = 0.0;
+        if (pk.n > 0) ket.get(pk, 0, nq, nQx, nQy, nQz, nK);
         for (int ik = 0; ik < pk.n; ik++) {
-            double q, Qx, Qy, Qz, Kcd;
-            ket.get(pk, ik, q, Qx, Qy, Qz, Kcd);
+            const double q = nq, Qx = nQx, Qy = nQy, Qz = nQz, Kcd = nK;
+            if (ik + 1 < pk.n) ket.get(pk, ik + 1, nq, nQx, nQy, nQz, nK);
             if (SKIP && fabs(Kab * Kcd) < GTF_PRIMQ_EPS) break;  // kets are in descending |K|
             const double rpq = rsqrt(p + q);
             const double ipq = rpq * rpq;
@@ -298,6 +311,72 @@ struct PPStored {
     }
 };
 
+// primitive pairs of the Fock build: one 48-byte record per pair,
+// {p, K}, {Px, Py}, {Pz, 0}, read with three 16-byte loads
+#define GTF_PPREC_D2 3
+struct PPRec {
+    const double2 *r;
+    __device__ __forceinline__ void get(const PairRec &pr, int i, double &p, double &Px, double &Py,
+                                        double &Pz, double &K) const
+    {
+        const double2 *q = r + (size_t)GTF_PPREC_D2 * (pr.off + i);
+        const double2 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+        p = a.x;
+        K = a.y;
+        Px = b.x;
+        Py = b.y;
+        Pz = c.x;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Warp sum of M values per lane (M <= 32) by recursive halving: at each of
+// the first log2(MP) butterfly steps a lane keeps half of its values and
+// sends the other half to its partner, so the whole reduction costs MP-1
+// shuffles (MP = M rounded up to a power of two) instead of 5 M.  Afterwards
+// lane l holds the total of value index m = l >> (5 - log2 MP); the lanes
+// with (l & (32/MP - 1)) == 0 and m < M each own one distinct total.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int pow2_ceil(int m) { return m <= 1 ? 1 : 2 * pow2_ceil((m + 1) / 2); }
+__host__ __device__ constexpr int ilog2c(int m) { return m <= 1 ? 0 : 1 + ilog2c(m / 2); }
+
+template <int M, class Sink>
+__device__ __forceinline__ void warp_sum_values(const double *v, int lane, Sink &&sink)
+{
+    static_assert(M >= 1 && M <= 32, "at most 32 values per call");
+    constexpr int MP = pow2_ceil(M), LG = ilog2c(MP);
+    double w[MP];
+#pragma unroll
+    for (int k = 0; k < MP; k++) w[k] = k < M ? v[k] : 0.0;
+    int m = 0;
+#pragma unroll
+    for (int st = 0; st < LG; st++) {
+        const int h = MP >> (st + 1), o = 16 >> st;
+        const bool up = (lane & o) != 0;
+#pragma unroll
+        for (int k = 0; k < h; k++) {
+            const double send = up ? w[k] : w[k + h];
+            const double keep = up ? w[k + h] : w[k];
+            w[k] = keep + __shfl_xor_sync(GTF_FULL_MASK, send, o);
+        }
+        if (up) m += h;
+    }
+#pragma unroll
+    for (int o = 16 >> LG; o >= 1; o >>= 1) w[0] += __shfl_xor_sync(GTF_FULL_MASK, w[0], o);
+    if ((lane & ((32 >> LG) - 1)) == 0 && m < M) sink(m, w[0]);
+}
+
+// any M: chunks of 32 values
+template <int M, int C0 = 0, class Sink>
+__device__ __forceinline__ void warp_sum_many(const double (&v)[M], int lane, Sink &&sink)
+{
+    if constexpr (C0 < M) {
+        constexpr int n = (M - C0 < 32) ? M - C0 : 32;
+        warp_sum_values<n>(v + C0, lane, [&](int m, double t) { sink(C0 + m, t); });
+        warp_sum_many<M, C0 + 32>(v, lane, sink);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // J/K digestion of one unique quartet (pfock/fock_task.c:29-117 semantics):
 //   Fj[a][b] += 2(1+f1)(1+f2)         sum_cd D[c][d] I
@@ -310,156 +389,10 @@ struct PPStored {
 // Fj and Fk afterwards (GA_Symmetrize, pfock/pfock.c:1719-1726).
 // The bra pair is shared by the 32 lanes of the warp; `active` lanes carry a
 // quartet, inactive lanes contribute zeros to the warp reductions.
-// ---------------------------------------------------------------------------
-template <int LA, int LB, int LC, int LD, typename R>
-__device__ __forceinline__ void digest(const R (&I)[ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD)],
-                                       bool active, const PairRec &pb, const PairRec &pk, bool same_pair,
-                                       const double *__restrict__ D, double *__restrict__ Fj,
-                                       double *__restrict__ Fk, int ld, int lane)
-{
-    constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
-    const int fa = pb.fa, fb = pb.fb, fc = pk.fa, fd = pk.fb;
-    const double f1 = (fa != fb) ? 1.0 : 0.0;
-    const double f2 = (fc != fd) ? 1.0 : 0.0;
-    const double f3 = same_pair ? 0.0 : 1.0;
-    const double sJab = 2.0 * (1.0 + f1) * (1.0 + f2);
-    const double sJcd = f3 * sJab;
-    const double sKac = -(1.0 + f3);
-    const double sKbc = f1 * sKac, sKad = f2 * sKac, sKbd = f1 * f2 * sKac;
-
-    // bra block J: warp-uniform destination
-    {
-        double dcd[NC * ND];
-#pragma unroll
-        for (int ic = 0; ic < NC; ic++)
-#pragma unroll
-            for (int id = 0; id < ND; id++)
-                dcd[ic + NC * id] = active ? __ldg(D + (size_t)(fc + ic) * ld + fd + id) : 0.0;
-#pragma unroll
-        for (int ibb = 0; ibb < NB; ibb++) {
-#pragma unroll
-            for (int ia = 0; ia < NA; ia++) {
-                double v = 0.0;
-#pragma unroll
-                for (int id = 0; id < ND; id++)
-#pragma unroll
-                    for (int ic = 0; ic < NC; ic++)
-                        v = fma((double)I[ia + NA * (ibb + NB * (ic + NC * id))], dcd[ic + NC * id], v);
-                // the factor depends on the lane's ket (f2), so apply it before the reduction
-                v *= sJab;
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(GTF_FULL_MASK, v, o);
-                if (lane == 0) atomicAdd(Fj + (size_t)(fa + ia) * ld + fb + ibb, v);
-            }
-        }
-    }
-    if (!active) return;
-    // ket block J
-    if (f3 != 0.0) {
-        double dab[NA * NB];
-#pragma unroll
-        for (int ia = 0; ia < NA; ia++)
-#pragma unroll
-            for (int ibb = 0; ibb < NB; ibb++) dab[ia + NA * ibb] = __ldg(D + (size_t)(fa + ia) * ld + fb + ibb);
-#pragma unroll
-        for (int id = 0; id < ND; id++)
-#pragma unroll
-            for (int ic = 0; ic < NC; ic++) {
-                double v = 0.0;
-#pragma unroll
-                for (int ibb = 0; ibb < NB; ibb++)
-#pragma unroll
-                    for (int ia = 0; ia < NA; ia++)
-                        v = fma((double)I[ia + NA * (ibb + NB * (ic + NC * id))], dab[ia + NA * ibb], v);
-                atomicAdd(Fj + (size_t)(fc + ic) * ld + fd + id, sJcd * v);
-            }
-    }
-    // K[a][c] -= (1+f3) sum_bd D[b][d] I
-    {
-        double dbd[NB * ND];
-#pragma unroll
-        for (int ibb = 0; ibb < NB; ibb++)
-#pragma unroll
-            for (int id = 0; id < ND; id++) dbd[ibb + NB * id] = __ldg(D + (size_t)(fb + ibb) * ld + fd + id);
-#pragma unroll
-        for (int ic = 0; ic < NC; ic++)
-#pragma unroll
-            for (int ia = 0; ia < NA; ia++) {
-                double v = 0.0;
-#pragma unroll
-                for (int id = 0; id < ND; id++)
-#pragma unroll
-                    for (int ibb = 0; ibb < NB; ibb++)
-                        v = fma((double)I[ia + NA * (ibb + NB * (ic + NC * id))], dbd[ibb + NB * id], v);
-                atomicAdd(Fk + (size_t)(fa + ia) * ld + fc + ic, sKac * v);
-            }
-    }
-    // K[b][c] -= f1 (1+f3) sum_ad D[a][d] I
-    if (f1 != 0.0) {
-        double dad[NA * ND];
-#pragma unroll
-        for (int ia = 0; ia < NA; ia++)
-#pragma unroll
-            for (int id = 0; id < ND; id++) dad[ia + NA * id] = __ldg(D + (size_t)(fa + ia) * ld + fd + id);
-#pragma unroll
-        for (int ic = 0; ic < NC; ic++)
-#pragma unroll
-            for (int ibb = 0; ibb < NB; ibb++) {
-                double v = 0.0;
-#pragma unroll
-                for (int id = 0; id < ND; id++)
-#pragma unroll
-                    for (int ia = 0; ia < NA; ia++)
-                        v = fma((double)I[ia + NA * (ibb + NB * (ic + NC * id))], dad[ia + NA * id], v);
-                atomicAdd(Fk + (size_t)(fb + ibb) * ld + fc + ic, sKbc * v);
-            }
-    }
-    // K[a][d] -= f2 (1+f3) sum_bc D[b][c] I
-    if (f2 != 0.0) {
-        double dbc[NB * NC];
-#pragma unroll
-        for (int ibb = 0; ibb < NB; ibb++)
-#pragma unroll
-            for (int ic = 0; ic < NC; ic++) dbc[ibb + NB * ic] = __ldg(D + (size_t)(fb + ibb) * ld + fc + ic);
-#pragma unroll
-        for (int id = 0; id < ND; id++)
-#pragma unroll
-            for (int ia = 0; ia < NA; ia++) {
-                double v = 0.0;
-#pragma unroll
-                for (int ic = 0; ic < NC; ic++)
-#pragma unroll
-                    for (int ibb = 0; ibb < NB; ibb++)
-                        v = fma((double)I[ia + NA * (ibb + NB * (ic + NC * id))], dbc[ibb + NB * ic], v);
-                atomicAdd(Fk + (size_t)(fa + ia) * ld + fd + id, sKad * v);
-            }
-    }
-    // K[b][d] -= f1 f2 (1+f3) sum_ac D[a][c] I
-    if (f1 != 0.0 && f2 != 0.0) {
-        double dac[NA * NC];
-#pragma unroll
-        for (int ia = 0; ia < NA; ia++)
-#pragma unroll
-            for (int ic = 0; ic < NC; ic++) dac[ia + NA * ic] = __ldg(D + (size_t)(fa + ia) * ld + fc + ic);
-#pragma unroll
-        for (int id = 0; id < ND; id++)
-#pragma unroll
-            for (int ibb = 0; ibb < NB; ibb++) {
-                double v = 0.0;
-#pragma unroll
-                for (int ic = 0; ic < NC; ic++)
-#pragma unroll
-                    for (int ia = 0; ia < NA; ia++)
-                        v = fma((double)I[ia + NA * (ibb + NB * (ic + NC * id))], dac[ia + NA * ic], v);
-                atomicAdd(Fk + (size_t)(fb + ibb) * ld + fd + id, sKbd * v);
-            }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Digestion of one slice of a quartet (ket components cd = CD0 .. CD0+N-1),
-// same factors as digest<>.  Terms whose destination is summed over the
-// sliced index (Fj[a][b], Fk[a][c], Fk[b][c]) receive a partial sum per slice.
+// digest_cd<..., CD0, N> digests the slice of ket components
+// cd = CD0 .. CD0+N-1 (cd = ic + NC*id) of the quartet; terms whose
+// destination sums over the sliced index (Fj[a][b], Fk[a][c], Fk[b][c])
+// receive a partial sum per slice.
 // ---------------------------------------------------------------------------
 __host__ __device__ constexpr bool slice_has_c(int CD0, int N, int NC, int ic)
 {
@@ -498,19 +431,17 @@ __device__ __forceinline__ void digest_cd(const double (&I)[ncart(LA) * ncart(LB
             const int ic = (CD0 + t) % NC, id = (CD0 + t) / NC;
             dcd[t] = active ? __ldg(D + (size_t)(fc + ic) * ld + fd + id) : 0.0;
         }
+        double vab[NA * NB];
 #pragma unroll
-        for (int ibb = 0; ibb < NB; ibb++) {
+        for (int k = 0; k < NA * NB; k++) {
+            double v = 0.0;
 #pragma unroll
-            for (int ia = 0; ia < NA; ia++) {
-                double v = 0.0;
-#pragma unroll
-                for (int t = 0; t < N; t++) v = fma(I[ia + NA * (ibb + NB * t)], dcd[t], v);
-                v *= sJab;  // depends on the lane's ket
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(GTF_FULL_MASK, v, o);
-                if (lane == 0) atomicAdd(Fj + (size_t)(fa + ia) * ld + fb + ibb, v);
-            }
+            for (int t = 0; t < N; t++) v = fma(I[k + NA * NB * t], dcd[t], v);
+            vab[k] = v * sJab;  // the factor depends on the lane's ket
         }
+        warp_sum_many<NA * NB>(vab, lane, [&](int k, double t) {
+            atomicAdd(Fj + (size_t)(fa + k % NA) * ld + fb + k / NA, t);
+        });
     }
     if (!active) return;
     // ket block J: complete per (c, d)
