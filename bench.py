@@ -287,16 +287,20 @@ def profile_fock(args):
     import gtfock_b200 as gb
     from gtfock_b200 import molecules as mol
     atoms = {"c12h26": mol.alkane(12), "c54h18": mol.graphene_flake(2),
-             "c96h24": mol.graphene_flake(3)}[args.profile_fock]
+             "c96h24": mol.graphene_flake(3), "w64": mol.water_cluster(64, 2024)}[args.profile_fock]
     with tempfile.TemporaryDirectory() as td:
         xyz = mol.write_xyz(atoms, os.path.join(td, args.profile_fock + ".xyz"))
-        b = gb.BasisSet(mol.basis_file("cc-pvdz"), xyz)
+        b = gb.BasisSet(mol.basis_file("6-31g" if args.profile_fock == "w64" else "cc-pvdz"), xyz)
         pf = gb.PFock(b, tolscr=TOL)
+        if args.fp32_cutoff is not None:
+            pf.set_precision(1, args.fp32_cutoff)
         D = np.eye(b.nbf) * 0.3
         for _ in range(args.builds):
             pf.compute_fock(D)
         tm = pf.timing()
+        nq32, nq = pf.precision_stats()
         out = {"molecule": args.profile_fock, "nbf": b.nbf, "counts": pf.counts(), "timing": tm,
+               "fp32_cutoff": args.fp32_cutoff, "fp32_share": nq32 / nq if nq else 0.0,
                "classes": [{"bra": x, "ket": y, "ms": ms, "quartets": q}
                            for x, y, ms, q in pf.class_stats() if q > 0]}
         pf.close()
@@ -310,8 +314,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gtfock_b200", choices=["gtfock_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile-fock", choices=["c12h26", "c54h18", "c96h24"], default=None)
+    ap.add_argument("--profile-fock", choices=["c12h26", "c54h18", "c96h24", "w64"], default=None)
     ap.add_argument("--builds", type=int, default=2)
+    ap.add_argument("--fp32-cutoff", type=float, default=None,
+                    help="with --profile-fock: FP32 for quartets with Schwarz bound below this")
     args = ap.parse_args()
     if args.profile_fock:
         profile_fock(args)

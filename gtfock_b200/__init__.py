@@ -91,11 +91,14 @@ def load():
     _sig(L, "gtf_pfock_screening", [_vp, _ip, _ip, _ip, _dp])
     _sig(L, "gtf_pfock_timing", [_vp, _dp, _dp, _dp])
     _sig(L, "gtf_pfock_set_precision", [_vp, _i, _d])
+    _sig(L, "gtf_pfock_precision_stats", [_vp, _dp, _dp])
     _sig(L, "gtf_pfock_class_stats", [_vp, _ip, _ip, _dp, _dp])
     _sig(L, "gtf_scf_run", [_cp, _cp, _d, _i, _i, _dp, _dp])
     _sig(L, "gtf_scf_create", [_cp, _cp, _d], _vp)
     _sig(L, "gtf_scf_solve", [_vp, _i, _i, _dp, _dp])
     _sig(L, "gtf_scf_nbf", [_vp])
+    _sig(L, "gtf_scf_set_options", [_vp, _i, _d, _d])
+    _sig(L, "gtf_scf_get_density", [_vp, _dp])
     _sig(L, "gtf_scf_destroy", [_vp], None)
     _sig(L, "gtf_launch_count", [], ctypes.c_ulonglong)
     _sig(L, "gtf_fp64_peak", [_dp])
@@ -232,8 +235,17 @@ class PFock:
         return [(int(X[i]), int(Y[i]), float(ms[i]), float(nq[i])) for i in range(n)]
 
     def set_precision(self, mode, fp32_cutoff=0.0):
+        """mode 0: FP64; mode 1: FP32 for quartets with Schwarz bound < fp32_cutoff."""
         self._check(load().gtf_pfock_set_precision(self.h, mode, fp32_cutoff),
                     "gtf_pfock_set_precision")
+
+    def precision_stats(self):
+        """(quartets evaluated in FP32, all quartets) under the current mode."""
+        a = np.zeros(1)
+        b = np.zeros(1)
+        self._check(load().gtf_pfock_precision_stats(self.h, _dptr(a), _dptr(b)),
+                    "gtf_pfock_precision_stats")
+        return float(a[0]), float(b[0])
 
     def one_electron(self):
         """(S, X, H) as PFock_createOvlMat/getOvlMat/getOvlMat2/createCoreHMat produce them."""
@@ -339,6 +351,20 @@ class SCFSolver:
         if it < 0:
             raise GtfError("gtf_scf_solve failed (%d)" % it)
         return e[:it], _timings(t)
+
+    def set_options(self, precision=0, fp32_cutoff=0.0, etol=1e-11):
+        """precision 0: FP64 ERIs; 1: FP32 for quartets with Schwarz bound <
+        fp32_cutoff.  The solve stops when |E_k - E_k-1| < etol."""
+        r = load().gtf_scf_set_options(self.h, precision, fp32_cutoff, etol)
+        if r != 0:
+            raise GtfError("gtf_scf_set_options failed (%d)" % r)
+
+    def density(self):
+        """Density of the last solve (half density, AO basis)."""
+        D = np.zeros((self.nbf, self.nbf))
+        if load().gtf_scf_get_density(self.h, _dptr(D)) != 0:
+            raise GtfError("gtf_scf_get_density failed")
+        return D
 
     def close(self):
         if getattr(self, "h", None) and _lib is not None:

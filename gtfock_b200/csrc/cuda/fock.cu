@@ -70,10 +70,12 @@ struct ClassPairTask {
     int bra_start, nbra;
     int ket_start, nketcls;
     int seg[GTF_NBKT + 1];  // ket segments (primitive-count buckets), relative to ket_start
-    long long nunits;
-    double nquart;
-    int *d_nket;               // [nbra][GTF_NBKT]
-    long long *d_unit_prefix;  // [nbra * GTF_NBKT + 1]
+    long long nunits, nunits32;  // units of the FP64 and the FP32 launch
+    double nquart, nquart32;     // quartets in all, of which evaluated in FP32
+    int *d_nket;                 // [nbra][GTF_NBKT] kets per (bra, segment)
+    int *d_n64;                  // [nbra][GTF_NBKT] of which FP64 (a prefix)
+    long long *d_unit_prefix;    // [nbra * GTF_NBKT + 1], FP64 launch
+    long long *d_unit_prefix32;  // [nbra * GTF_NBKT + 1], FP32 launch
 };
 
 struct gtf_fock_dev {
@@ -509,33 +511,48 @@ struct SegStarts {
     int s[GTF_NBKT + 1];
 };
 
+// cut2 > 0 (mixed precision): the kets with v_bra * v_ket < cut2, i.e. a
+// Schwarz bound sqrt(v_bra v_ket) below the FP32 cutoff, form the tail of each
+// prefix and go to the FP32 launch; n64 counts the FP64 head.
 __global__ void k_count_kets(const double *__restrict__ pair_v, int bra_start, int nbra, int ket_start,
-                             SegStarts seg, int same, double tol2, int *__restrict__ nket,
-                             long long *__restrict__ units)
+                             SegStarts seg, int same, double tol2, double cut2, int *__restrict__ nket,
+                             int *__restrict__ n64, long long *__restrict__ units64,
+                             long long *__restrict__ units32)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int nidx = nbra * GTF_NBKT;
     if (t > nidx) return;
     if (t == nidx) {
-        units[nidx] = 0;
+        units64[nidx] = 0;
+        units32[nidx] = 0;
         return;
     }
     const int i = t / GTF_NBKT, b = t - i * GTF_NBKT;
     const double v = pair_v[bra_start + i];
     const int s0 = seg.s[b], s1 = seg.s[b + 1];
-    int lo = s0, hi = s1;  // first index failing the test
+    int lo = s0, hi = s1;  // first index failing the Schwarz test
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
         if (fabs(v * pair_v[ket_start + mid]) >= tol2) lo = mid + 1;
         else hi = mid;
     }
     int c = lo - s0;
+    int lo2 = s0, hi2 = s0 + c;  // first index below the FP32 cutoff
+    while (lo2 < hi2) {
+        const int mid = (lo2 + hi2) >> 1;
+        if (fabs(v * pair_v[ket_start + mid]) >= cut2) lo2 = mid + 1;
+        else hi2 = mid;
+    }
+    int c64 = lo2 - s0;
     if (same) {
         const int lim = i - s0 + 1;  // kets j <= i
         c = lim < 0 ? 0 : (c < lim ? c : lim);
+        c64 = c64 < c ? c64 : c;
     }
     nket[t] = c;
-    units[t] = b == 0 ? 0 : (c + 31) / 32;
+    n64[t] = c64;
+    units64[t] = b == 0 ? 0 : (c64 + 31) / 32;
+    units32[t] = b == 0 ? 0 : (c - c64 + 31) / 32;
 }
 
 typedef int (*fock_group_launch_t)(int la, int lb, int lc, int ld, const FockLaunch &a, cudaStream_t st);
@@ -639,6 +656,58 @@ extern "C" int gtf_basis_dev_create(const gtf_basis_view_t *b, gtf_fock_dev_t **
     f->max_numdmat = 0;
     *out = f;
     return upload_basis(f, b);
+}
+
+// Per class pair and (bra, segment): ket counts, the FP64 / FP32 split for
+// the current precision mode and the unit prefixes of both launches.
+static int build_units(gtf_fock_dev *f)
+{
+    cudaStream_t st = f->stream;
+    const double cut2 = f->prec == GTF_PREC_MIXED ? f->fp32_cutoff * f->fp32_cutoff : 0.0;
+    void *d_tmp = nullptr;
+    size_t tmp_cap = 0;
+    for (int c = 0; c < NCLSPAIR; c++) {
+        ClassPairTask &t = f->tasks[c];
+        t.nunits = t.nunits32 = 0;
+        t.nquart = t.nquart32 = 0.0;
+        if (t.nbra == 0 || t.nketcls == 0) continue;
+        const int nidx = t.nbra * GTF_NBKT;
+        SegStarts seg;
+        for (int bk = 0; bk <= GTF_NBKT; bk++) seg.s[bk] = t.seg[bk];
+        long long *d_units;
+        CK(cudaMalloc(&d_units, sizeof(long long) * 2 * (nidx + 1)));
+        k_count_kets<<<(nidx + 1 + 255) / 256, 256, 0, st>>>(f->d_pair_v, t.bra_start, t.nbra, t.ket_start, seg,
+                                                            t.X == t.Y, f->tolscr2, cut2, t.d_nket, t.d_n64,
+                                                            d_units, d_units + nidx + 1);
+        CK(cudaGetLastError());
+        size_t b4 = 0;
+        CK(cub::DeviceScan::ExclusiveSum(nullptr, b4, d_units, t.d_unit_prefix, nidx + 1, st));
+        if (b4 > tmp_cap) {
+            if (d_tmp) cudaFree(d_tmp);
+            tmp_cap = b4;
+            CK(cudaMalloc(&d_tmp, tmp_cap));
+        }
+        b4 = tmp_cap;
+        CK(cub::DeviceScan::ExclusiveSum(d_tmp, b4, d_units, t.d_unit_prefix, nidx + 1, st));
+        b4 = tmp_cap;
+        CK(cub::DeviceScan::ExclusiveSum(d_tmp, b4, d_units + nidx + 1, t.d_unit_prefix32, nidx + 1, st));
+        std::vector<int> nk(nidx), n64(nidx);
+        CK(cudaMemcpyAsync(&t.nunits, t.d_unit_prefix + nidx, sizeof(long long), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&t.nunits32, t.d_unit_prefix32 + nidx, sizeof(long long), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(nk.data(), t.d_nket, sizeof(int) * nidx, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(n64.data(), t.d_n64, sizeof(int) * nidx, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        cudaFree(d_units);
+        double q = 0.0, q32 = 0.0;
+        for (int i = 0; i < nidx; i++) {
+            q += nk[i];
+            q32 += nk[i] - n64[i];
+        }
+        t.nquart = q;
+        t.nquart32 = q32;
+    }
+    if (d_tmp) cudaFree(d_tmp);
+    return GTF_OK;
 }
 
 extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max_numdmat,
@@ -816,7 +885,7 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
     f->usq = 0.0;
     f->uitl = 0.0;
     f->eri_flops = 0.0;
-    DALLOC(f->d_counters, NCLSPAIR);
+    DALLOC(f->d_counters, 2 * NCLSPAIR);
     int cp = 0;
     for (int X = 0; X < NCLS; X++) {
         for (int Y = 0; Y <= X; Y++, cp++) {
@@ -827,39 +896,27 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
             t.nbra = f->cls_start[X + 1] - f->cls_start[X];
             t.ket_start = f->cls_start[Y];
             t.nketcls = f->cls_start[Y + 1] - f->cls_start[Y];
-            SegStarts seg;
-            for (int bk = 0; bk <= GTF_NBKT; bk++) {
-                t.seg[bk] = key_start[Y * 16 + bk] - t.ket_start;
-                seg.s[bk] = t.seg[bk];
-            }
-            t.nunits = 0;
-            t.nquart = 0.0;
+            for (int bk = 0; bk <= GTF_NBKT; bk++) t.seg[bk] = key_start[Y * 16 + bk] - t.ket_start;
+            t.nunits = t.nunits32 = 0;
+            t.nquart = t.nquart32 = 0.0;
             if (t.nbra == 0 || t.nketcls == 0) continue;
             const int nidx = t.nbra * GTF_NBKT;
             DALLOC(t.d_nket, nidx);
+            DALLOC(t.d_n64, nidx);
             DALLOC(t.d_unit_prefix, nidx + 1);
-            long long *d_units;
-            CK(cudaMalloc(&d_units, sizeof(long long) * (nidx + 1)));
-            k_count_kets<<<(nidx + 1 + 255) / 256, 256, 0, st>>>(f->d_pair_v, t.bra_start, t.nbra, t.ket_start,
-                                                                seg, X == Y, f->tolscr2, t.d_nket, d_units);
-            CK(cudaGetLastError());
-            size_t b4 = 0;
-            CK(cub::DeviceScan::ExclusiveSum(nullptr, b4, d_units, t.d_unit_prefix, nidx + 1, st));
-            if (b4 > tmp_cap) {
-                cudaFree(d_tmp);
-                tmp_cap = b4;
-                CK(cudaMalloc(&d_tmp, tmp_cap));
-            }
-            b4 = tmp_cap;
-            CK(cub::DeviceScan::ExclusiveSum(d_tmp, b4, d_units, t.d_unit_prefix, nidx + 1, st));
-            std::vector<int> nk(nidx);
-            CK(cudaMemcpyAsync(&t.nunits, t.d_unit_prefix + nidx, sizeof(long long), cudaMemcpyDeviceToHost, st));
-            CK(cudaMemcpyAsync(nk.data(), t.d_nket, sizeof(int) * nidx, cudaMemcpyDeviceToHost, st));
-            CK(cudaStreamSynchronize(st));
-            cudaFree(d_units);
-            double q = 0.0;
-            for (int i = 0; i < nidx; i++) q += nk[i];
-            t.nquart = q;
+            DALLOC(t.d_unit_prefix32, nidx + 1);
+        }
+    }
+    {
+        const int r = build_units(f);
+        if (r != GTF_OK) return r;
+    }
+    cp = 0;
+    for (int X = 0; X < NCLS; X++) {
+        for (int Y = 0; Y <= X; Y++, cp++) {
+            ClassPairTask &t = f->tasks[cp];
+            if (t.nbra == 0 || t.nketcls == 0) continue;
+            const double q = t.nquart;
             const int la = k_cls_la[X], lb = k_cls_lb[X], lc = k_cls_la[Y], ld = k_cls_lb[Y];
             const double dims = (double)(b->pure ? (la == 2 ? 5 : ncart(la)) : ncart(la)) *
                                 (b->pure ? (lb == 2 ? 5 : ncart(lb)) : ncart(lb)) *
@@ -880,7 +937,7 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
         double flops = 0.0;
         for (int c2 = 0; c2 < NCLSPAIR; c2++) {
             ClassPairTask &t = f->tasks[c2];
-            if (t.nunits == 0) continue;
+            if (t.nbra == 0 || t.nketcls == 0) continue;
             const int nidx = t.nbra * GTF_NBKT;
             std::vector<int> nk(nidx);
             CK(cudaMemcpy(nk.data(), t.d_nket, sizeof(int) * nidx, cudaMemcpyDeviceToHost));
@@ -950,6 +1007,8 @@ extern "C" void gtf_fock_destroy(gtf_fock_dev_t *f)
     for (int c = 0; c < NCLSPAIR; c++) {
         if (f->tasks[c].d_nket) cudaFree(f->tasks[c].d_nket);
         if (f->tasks[c].d_unit_prefix) cudaFree(f->tasks[c].d_unit_prefix);
+        if (f->tasks[c].d_n64) cudaFree(f->tasks[c].d_n64);
+        if (f->tasks[c].d_unit_prefix32) cudaFree(f->tasks[c].d_unit_prefix32);
     }
     if (f->d_host_stage) cudaFreeHost(f->d_host_stage);
     cudaEventDestroy(f->ev0);
@@ -1046,26 +1105,50 @@ extern "C" int gtf_fock_put_density_dev(gtf_fock_dev_t *f, int index, const doub
 extern "C" int gtf_fock_set_precision(gtf_fock_dev_t *f, int prec, double fp32_cutoff)
 {
     if (prec != GTF_PREC_FP64 && prec != GTF_PREC_MIXED) return GTF_ERR_INVALID;
+    if (prec == GTF_PREC_MIXED && !(fp32_cutoff >= 0.0)) return GTF_ERR_INVALID;
     f->prec = prec;
     f->fp32_cutoff = fp32_cutoff;
-    return GTF_OK;
+    return build_units(f);
 }
 
-// launch arguments of one class pair (counter, D and accumulators are set by the caller)
-static FockLaunch fock_launch_args(const gtf_fock_dev *f, const ClassPairTask &t)
+// Launches the Fock kernels of class pair c: the FP64 part of every ket
+// range, then (mixed precision) the FP32 tail.  counters holds two slots per
+// class pair.  Returns the number of launches, or -1 on a launch error.
+static int launch_class(const gtf_fock_dev *f, int c, const double *D, double *Fj, double *Fk,
+                        unsigned long long *counters, cudaStream_t st)
 {
-    FockLaunch a;
-    memset(&a, 0, sizeof(a));
-    a.pairs = f->d_pairs;
-    a.pprec = reinterpret_cast<const double2 *>(f->d_pp);
-    a.nket = t.d_nket;
-    a.unit_prefix = t.d_unit_prefix;
-    a.nbra = t.nbra;
-    a.nunits = t.nunits;
-    a.bra_start = t.bra_start;
-    a.ket_start = t.ket_start;
-    for (int b = 0; b <= GTF_NBKT; b++) a.seg[b] = t.seg[b];
-    return a;
+    const ClassPairTask &t = f->tasks[c];
+    int n = 0;
+    for (int part = 0; part < 2; part++) {
+        const long long nu = part ? t.nunits32 : t.nunits;
+        if (nu == 0) continue;
+        FockLaunch a;
+        memset(&a, 0, sizeof(a));
+        a.pairs = f->d_pairs;
+        a.pprec = reinterpret_cast<const double2 *>(f->d_pp);
+        a.nlo = part ? t.d_n64 : nullptr;
+        a.nket = part ? t.d_nket : t.d_n64;
+        a.unit_prefix = part ? t.d_unit_prefix32 : t.d_unit_prefix;
+        a.nbra = t.nbra;
+        a.nunits = nu;
+        a.bra_start = t.bra_start;
+        a.ket_start = t.ket_start;
+        for (int b = 0; b <= GTF_NBKT; b++) a.seg[b] = t.seg[b];
+        a.counter = counters + 2 * c + part;
+        a.D = D;
+        a.Fj = Fj;
+        a.Fk = Fk;
+        a.ld = f->nbf_cart;
+        a.nsm = f->nsm;
+        a.fp32 = part;
+        if (launch_fock(t.X, t.Y, a, st) != 0) {
+            snprintf(g_errbuf, sizeof(g_errbuf), "Fock kernel launch for class pair (%d,%d)%s failed: %s", t.X, t.Y,
+                     part ? " (FP32)" : "", cudaGetErrorString(cudaGetLastError()));
+            return -1;
+        }
+        n++;
+    }
+    return n;
 }
 
 extern "C" int gtf_fock_compute(gtf_fock_dev_t *f, int numdmat)
@@ -1090,26 +1173,15 @@ extern "C" int gtf_fock_compute(gtf_fock_dev_t *f, int numdmat)
         }
         CK(cudaMemsetAsync(f->d_Fj, 0, sizeof(double) * nnc, st));
         CK(cudaMemsetAsync(f->d_Fk, 0, sizeof(double) * nnc, st));
-        CK(cudaMemsetAsync(f->d_counters, 0, sizeof(unsigned long long) * NCLSPAIR, st));
+        CK(cudaMemsetAsync(f->d_counters, 0, sizeof(unsigned long long) * 2 * NCLSPAIR, st));
         CK(cudaEventRecord(f->ev1, st));
         for (int c = 0; c < NCLSPAIR; c++) {
             ClassPairTask &t = f->tasks[c];
             CK(cudaEventRecord(f->ev_cls[c], st));
-            if (t.nunits == 0) continue;
-            FockLaunch a = fock_launch_args(f, t);
-            a.counter = f->d_counters + c;
-            a.D = Dc;
-            a.Fj = f->d_Fj;
-            a.Fk = f->d_Fk;
-            a.ld = nbfc;
-            a.nsm = f->nsm;
-            const int r = launch_fock(t.X, t.Y, a, st);
-            gtf_note_launches(1);
-            if (r != 0) {
-                snprintf(g_errbuf, sizeof(g_errbuf), "Fock kernel launch for class pair (%d,%d) failed: %d (%s)",
-                         t.X, t.Y, r, cudaGetErrorString(cudaGetLastError()));
-                return GTF_ERR_CUDA;
-            }
+            (void)t;
+            const int r = launch_class(f, c, Dc, f->d_Fj, f->d_Fk, f->d_counters, st);
+            if (r < 0) return GTF_ERR_CUDA;
+            gtf_note_launches(r);
         }
         CK(cudaEventRecord(f->ev_cls[NCLSPAIR], st));
         CK(cudaEventRecord(f->ev2, st));
@@ -1178,6 +1250,18 @@ extern "C" int gtf_fock_class_stats(gtf_fock_dev_t *f, int *X, int *Y, double *m
         if (nquart) nquart[c] = f->tasks[c].nquart;
     }
     return NCLSPAIR;
+}
+
+extern "C" int gtf_fock_fp32_quartets(gtf_fock_dev_t *f, double *nq32, double *nq)
+{
+    double a = 0.0, b = 0.0;
+    for (int c = 0; c < NCLSPAIR; c++) {
+        a += f->tasks[c].nquart32;
+        b += f->tasks[c].nquart;
+    }
+    if (nq32) *nq32 = a;
+    if (nq) *nq = b;
+    return GTF_OK;
 }
 
 extern "C" int gtf_fock_eri_flops(gtf_fock_dev_t *f, double *flops)
@@ -1272,7 +1356,7 @@ extern "C" void gtf_fock_basis_dev(gtf_fock_dev_t *f, const int **sh_L, const in
 // ---------------------------------------------------------------------------
 #define GTF_FIXED_MAX_FUNCS 384
 #define GTF_FIXED_NN ((size_t)GTF_FIXED_MAX_FUNCS * GTF_FIXED_MAX_FUNCS)
-#define GTF_FIXED_DOUBLES (5 * GTF_FIXED_NN + NCLSPAIR + 3)
+#define GTF_FIXED_DOUBLES (5 * GTF_FIXED_NN + 2 * NCLSPAIR + 3)
 #define GTF_FIXED_MAX_DEVICES 64
 
 static __device__ __align__(256) double g_fixed_scratch[GTF_FIXED_DOUBLES];
@@ -1340,23 +1424,9 @@ extern "C" int gtf_fock_compute_fixed(gtf_fock_dev_t *f, const double *dev_D, do
     }
     CK(cudaMemsetAsync(Fj, 0, sizeof(double) * nnc, st));
     CK(cudaMemsetAsync(Fk, 0, sizeof(double) * nnc, st));
-    CK(cudaMemsetAsync(counters, 0, sizeof(unsigned long long) * NCLSPAIR, st));
-    for (int c = 0; c < NCLSPAIR; c++) {
-        ClassPairTask &t = f->tasks[c];
-        if (t.nunits == 0) continue;
-        FockLaunch a = fock_launch_args(f, t);
-        a.counter = counters + c;
-        a.D = Duse;
-        a.Fj = Fj;
-        a.Fk = Fk;
-        a.ld = nbfc;
-        a.nsm = f->nsm;
-        if (launch_fock(t.X, t.Y, a, st) != 0) {
-            snprintf(g_errbuf, sizeof(g_errbuf), "allocation-free Fock build: launch for (%d,%d) failed: %s", t.X,
-                     t.Y, cudaGetErrorString(cudaGetLastError()));
-            return GTF_ERR_CUDA;
-        }
-    }
+    CK(cudaMemsetAsync(counters, 0, sizeof(unsigned long long) * 2 * NCLSPAIR, st));
+    for (int c = 0; c < NCLSPAIR; c++)
+        if (launch_class(f, c, Duse, Fj, Fk, counters, st) < 0) return GTF_ERR_CUDA;
     dim3 g2((nbf + 127) / 128, nbf);
     k_f_to_sph<<<g2, 128, 0, st>>>(Fj, Fk, dev_F, J, K, f->d_sph2shell, f->d_sh_L, f->d_f_start, f->d_fc_start,
                                    nbf, nbfc, f->pure);

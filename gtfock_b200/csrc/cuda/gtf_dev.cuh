@@ -85,6 +85,11 @@ struct PrimPairs {
     const double *K;   // GTF_PAIR_PREF * ca * cb * exp(-ab/p |AB|^2) / p
 };
 
+__device__ __forceinline__ double gfma(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float gfma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double grsqrt(double x) { return rsqrt(x); }
+__device__ __forceinline__ float grsqrt(float x) { return rsqrtf(x); }
+
 // ---------------------------------------------------------------------------
 // Rys roots and weights
 // ---------------------------------------------------------------------------
@@ -129,21 +134,61 @@ __device__ __forceinline__ void rys_roots(double T, double (&u)[N], double (&w)[
     }
 }
 
+// FP32 form for quartets evaluated in single precision: degree-7 fit of the
+// same functions on the same intervals (RYS32_TABLE), same large-T form
+template <int N>
+__device__ __forceinline__ void rys_roots(float T, float (&u)[N], float (&w)[N])
+{
+    if (T >= (float)RYS_TMAX[N]) {
+        const float it = 1.0f / T;
+        const float rs = rsqrtf(T);
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            u[i] = (float)RYS_LARGE_X2[N][i] * it;
+            w[i] = (float)RYS_LARGE_W[N][i] * rs;
+        }
+        return;
+    }
+    const int k = (int)(T * RYS32_INV_H);
+    const float s = T - ((float)k * (float)RYS32_H + 0.5f * (float)RYS32_H);
+    const float2 *c2 = reinterpret_cast<const float2 *>(RYS32_TABLE + RYS32_OFF[N] + k * (RYS32_DEG + 1) * (2 * N));
+    float a[2 * N];
+#pragma unroll
+    for (int f = 0; f < N; f++) {
+        const float2 t = __ldg(c2 + RYS32_DEG * N + f);
+        a[2 * f] = t.x;
+        a[2 * f + 1] = t.y;
+    }
+#pragma unroll
+    for (int j = RYS32_DEG - 1; j >= 0; j--) {
+#pragma unroll
+        for (int f = 0; f < N; f++) {
+            const float2 t = __ldg(c2 + j * N + f);
+            a[2 * f] = fmaf(a[2 * f], s, t.x);
+            a[2 * f + 1] = fmaf(a[2 * f + 1], s, t.y);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        u[i] = a[i];
+        w[i] = a[N + i];
+    }
+}
+
 // ---------------------------------------------------------------------------
 // one-dimensional horizontal transfer:
 // t(a, b+1) = t(a+1, b) + dist * t(a, b); input v[0..L1+L2], output o[a][b]
 // ---------------------------------------------------------------------------
-template <int L1, int L2>
-__device__ __forceinline__ void hrr1d(const double (&v)[L1 + L2 + 1], double (&o)[L1 + 1][L2 + 1],
-                                      double dist)
+template <int L1, int L2, typename R>
+__device__ __forceinline__ void hrr1d(const R (&v)[L1 + L2 + 1], R (&o)[L1 + 1][L2 + 1], R dist)
 {
-    double t[L1 + L2 + 1][L2 + 1];
+    R t[L1 + L2 + 1][L2 + 1];
 #pragma unroll
     for (int a = 0; a <= L1 + L2; a++) t[a][0] = v[a];
 #pragma unroll
     for (int b = 0; b < L2; b++) {
 #pragma unroll
-        for (int a = 0; a <= L1 + L2 - b - 1; a++) t[a][b + 1] = fma(dist, t[a][b], t[a + 1][b]);
+        for (int a = 0; a <= L1 + L2 - b - 1; a++) t[a][b + 1] = gfma(dist, t[a][b], t[a + 1][b]);
     }
 #pragma unroll
     for (int a = 0; a <= L1; a++) {
@@ -153,42 +198,40 @@ __device__ __forceinline__ void hrr1d(const double (&v)[L1 + L2 + 1], double (&o
 }
 
 // 2-D Rys integrals G[i][k] (i on centre A, k on centre C) for one direction
-template <int NI, int NK>
-__device__ __forceinline__ void rys_2d(double (&G)[NI][NK], double g00, double C00, double C0p,
-                                      double B10, double B01, double B00)
+template <int NI, int NK, typename R>
+__device__ __forceinline__ void rys_2d(R (&G)[NI][NK], R g00, R C00, R C0p, R B10, R B01, R B00)
 {
     G[0][0] = g00;
     if (NI > 1) G[1][0] = C00 * g00;
 #pragma unroll
-    for (int i = 1; i < NI - 1; i++) G[i + 1][0] = fma(C00, G[i][0], i * B10 * G[i - 1][0]);
+    for (int i = 1; i < NI - 1; i++) G[i + 1][0] = gfma(C00, G[i][0], (R)i * B10 * G[i - 1][0]);
     if (NK > 1) G[0][1] = C0p * g00;
 #pragma unroll
-    for (int k = 1; k < NK - 1; k++) G[0][k + 1] = fma(C0p, G[0][k], k * B01 * G[0][k - 1]);
+    for (int k = 1; k < NK - 1; k++) G[0][k + 1] = gfma(C0p, G[0][k], (R)k * B01 * G[0][k - 1]);
 #pragma unroll
     for (int k = 1; k < NK; k++) {
 #pragma unroll
         for (int i = 0; i < NI - 1; i++) {
-            double v = fma(C00, G[i][k], k * B00 * G[i][k - 1]);
-            if (i > 0) v = fma(i * B10, G[i - 1][k], v);
+            R v = gfma(C00, G[i][k], (R)k * B00 * G[i][k - 1]);
+            if (i > 0) v = gfma((R)i * B10, G[i - 1][k], v);
             G[i + 1][k] = v;
         }
     }
 }
 
 // full 1-D transfer: G[i][k] -> I[a][b][c][d]
-template <int LA, int LB, int LC, int LD>
-__device__ __forceinline__ void hrr_abcd(const double (&G)[LA + LB + 1][LC + LD + 1],
-                                         double (&I)[LA + 1][LB + 1][LC + 1][LD + 1],
-                                         double ab, double cd)
+template <int LA, int LB, int LC, int LD, typename R>
+__device__ __forceinline__ void hrr_abcd(const R (&G)[LA + LB + 1][LC + LD + 1],
+                                         R (&I)[LA + 1][LB + 1][LC + 1][LD + 1], R ab, R cd)
 {
     constexpr int NI = LA + LB + 1;
-    double K[NI][LC + 1][LD + 1];
+    R K[NI][LC + 1][LD + 1];
 #pragma unroll
     for (int i = 0; i < NI; i++) {
-        double v[LC + LD + 1];
+        R v[LC + LD + 1];
 #pragma unroll
         for (int k = 0; k <= LC + LD; k++) v[k] = G[i][k];
-        double o[LC + 1][LD + 1];
+        R o[LC + 1][LD + 1];
         hrr1d<LC, LD>(v, o, cd);
 #pragma unroll
         for (int c = 0; c <= LC; c++)
@@ -199,10 +242,10 @@ __device__ __forceinline__ void hrr_abcd(const double (&G)[LA + LB + 1][LC + LD 
     for (int c = 0; c <= LC; c++) {
 #pragma unroll
         for (int d = 0; d <= LD; d++) {
-            double v[NI];
+            R v[NI];
 #pragma unroll
             for (int i = 0; i < NI; i++) v[i] = K[i][c][d];
-            double o[LA + 1][LB + 1];
+            R o[LA + 1][LB + 1];
             hrr1d<LA, LB>(v, o, ab);
 #pragma unroll
             for (int a = 0; a <= LA; a++)
@@ -220,17 +263,22 @@ __device__ __forceinline__ void hrr_abcd(const double (&G)[LA + LB + 1][LC + LD 
 // Restricted to the ket components cd = CD0 .. CD0+N-1 (cd = ic + NC*id):
 // acc[ia + NA*(ib + NB*t)] with t = cd - CD0.  The output-split Fock kernels
 // call it once per slice so that a slice's accumulators fit in registers.
-template <int LA, int LB, int LC, int LD, int CD0, int N, bool SKIP, class PPB, class PPK>
+// R = double, or float for quartets evaluated in single precision (the
+// differences of centres are formed in double first, then rounded).
+template <int LA, int LB, int LC, int LD, int CD0, int N, bool SKIP, class PPB, class PPK, typename R>
 __device__ __forceinline__ void eri_accumulate_cd(const PPB &bra, const PairRec &pb, const PPK &ket,
-                                                  const PairRec &pk, double (&acc)[ncart(LA) * ncart(LB) * N])
+                                                  const PairRec &pk, R (&acc)[ncart(LA) * ncart(LB) * N])
 {
     constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
     constexpr int NI = LA + LB + 1, NK = LC + LD + 1;
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    const R ABx = (R)pb.ABx, ABy = (R)pb.ABy, ABz = (R)pb.ABz;
+    const R CDx = (R)pk.ABx, CDy = (R)pk.ABy, CDz = (R)pk.ABz;
     for (int ib = 0; ib < pb.n; ib++) {
         double p, Px, Py, Pz, Kab;
         bra.get(pb, ib, p, Px, Py, Pz, Kab);
-        const double PAx = Px - pb.Ax, PAy = Py - pb.Ay, PAz = Pz - pb.Az;
+        const R PAx = (R)(Px - pb.Ax), PAy = (R)(Py - pb.Ay), PAz = (R)(Pz - pb.Az);
+        const R p_ = (R)p;
         // the next ket primitive pair is loaded while the current one is used
         double nq = 0.0, nQx = 0.0, nQy = 0.0, nQz = 0.0, nK = 0.0;
         if (pk.n > 0) ket.get(pk, 0, nq, nQx, nQy, nQz, nK);
@@ -238,34 +286,35 @@ __device__ __forceinline__ void eri_accumulate_cd(const PPB &bra, const PairRec 
             const double q = nq, Qx = nQx, Qy = nQy, Qz = nQz, Kcd = nK;
             if (ik + 1 < pk.n) ket.get(pk, ik + 1, nq, nQx, nQy, nQz, nK);
             if (SKIP && fabs(Kab * Kcd) < GTF_PRIMQ_EPS) break;  // kets are in descending |K|
-            const double rpq = rsqrt(p + q);
-            const double ipq = rpq * rpq;
-            const double PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
-            const double rho = p * q * ipq;
-            const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
-            const double pref = Kab * Kcd * rpq;
-            double u[NR], w[NR];
+            const R q_ = (R)q;
+            const R rpq = grsqrt((R)(p + q));
+            const R ipq = rpq * rpq;
+            const R PQx = (R)(Px - Qx), PQy = (R)(Py - Qy), PQz = (R)(Pz - Qz);
+            const R rho = p_ * q_ * ipq;
+            const R T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
+            const R pref = (R)(Kab * Kcd) * rpq;
+            R u[NR], w[NR];
             rys_roots<NR>(T, u, w);
-            const double QCx = Qx - pk.Ax, QCy = Qy - pk.Ay, QCz = Qz - pk.Az;
-            const double h2p = 0.5 / p, h2q = 0.5 / q;
-            const double qf = q * ipq, pf = p * ipq;
+            const R QCx = (R)(Qx - pk.Ax), QCy = (R)(Qy - pk.Ay), QCz = (R)(Qz - pk.Az);
+            const R h2p = (R)0.5 / p_, h2q = (R)0.5 / q_;
+            const R qf = q_ * ipq, pf = p_ * ipq;
 #pragma unroll
             for (int r = 0; r < NR; r++) {
-                const double ur = u[r];
-                const double B00 = 0.5 * ur * ipq;
-                const double B10 = h2p * (1.0 - qf * ur);
-                const double B01 = h2q * (1.0 - pf * ur);
-                const double cq = qf * ur, cp = pf * ur;
-                double Gx[NI][NK], Gy[NI][NK], Gz[NI][NK];
-                rys_2d<NI, NK>(Gx, 1.0, PAx - cq * PQx, QCx + cp * PQx, B10, B01, B00);
-                rys_2d<NI, NK>(Gy, 1.0, PAy - cq * PQy, QCy + cp * PQy, B10, B01, B00);
+                const R ur = u[r];
+                const R B00 = (R)0.5 * ur * ipq;
+                const R B10 = h2p * ((R)1 - qf * ur);
+                const R B01 = h2q * ((R)1 - pf * ur);
+                const R cq = qf * ur, cp = pf * ur;
+                R Gx[NI][NK], Gy[NI][NK], Gz[NI][NK];
+                rys_2d<NI, NK>(Gx, (R)1, PAx - cq * PQx, QCx + cp * PQx, B10, B01, B00);
+                rys_2d<NI, NK>(Gy, (R)1, PAy - cq * PQy, QCy + cp * PQy, B10, B01, B00);
                 rys_2d<NI, NK>(Gz, w[r] * pref, PAz - cq * PQz, QCz + cp * PQz, B10, B01, B00);
-                double Ix[LA + 1][LB + 1][LC + 1][LD + 1];
-                double Iy[LA + 1][LB + 1][LC + 1][LD + 1];
-                double Iz[LA + 1][LB + 1][LC + 1][LD + 1];
-                hrr_abcd<LA, LB, LC, LD>(Gx, Ix, pb.ABx, pk.ABx);
-                hrr_abcd<LA, LB, LC, LD>(Gy, Iy, pb.ABy, pk.ABy);
-                hrr_abcd<LA, LB, LC, LD>(Gz, Iz, pb.ABz, pk.ABz);
+                R Ix[LA + 1][LB + 1][LC + 1][LD + 1];
+                R Iy[LA + 1][LB + 1][LC + 1][LD + 1];
+                R Iz[LA + 1][LB + 1][LC + 1][LD + 1];
+                hrr_abcd<LA, LB, LC, LD>(Gx, Ix, ABx, CDx);
+                hrr_abcd<LA, LB, LC, LD>(Gy, Iy, ABy, CDy);
+                hrr_abcd<LA, LB, LC, LD>(Gz, Iz, ABz, CDz);
 #pragma unroll
                 for (int t = 0; t < N; t++) {
                     const int ic = (CD0 + t) % NC, id = (CD0 + t) / NC;
@@ -273,12 +322,11 @@ __device__ __forceinline__ void eri_accumulate_cd(const PPB &bra, const PairRec 
                     for (int ibb = 0; ibb < NB; ibb++)
 #pragma unroll
                         for (int ia = 0; ia < NA; ia++) {
-                            const double xy =
-                                Ix[cart_x(LA, ia)][cart_x(LB, ibb)][cart_x(LC, ic)][cart_x(LD, id)] *
-                                Iy[cart_y(LA, ia)][cart_y(LB, ibb)][cart_y(LC, ic)][cart_y(LD, id)];
-                            double &dst = acc[ia + NA * (ibb + NB * t)];
-                            dst = fma(xy, Iz[cart_z(LA, ia)][cart_z(LB, ibb)][cart_z(LC, ic)][cart_z(LD, id)],
-                                      dst);
+                            const R xy = Ix[cart_x(LA, ia)][cart_x(LB, ibb)][cart_x(LC, ic)][cart_x(LD, id)] *
+                                         Iy[cart_y(LA, ia)][cart_y(LB, ibb)][cart_y(LC, ic)][cart_y(LD, id)];
+                            R &dst = acc[ia + NA * (ibb + NB * t)];
+                            dst = gfma(xy, Iz[cart_z(LA, ia)][cart_z(LB, ibb)][cart_z(LC, ic)][cart_z(LD, id)],
+                                       dst);
                         }
                 }
             }
@@ -408,8 +456,8 @@ __host__ __device__ constexpr bool slice_has_d(int CD0, int N, int NC, int id)
     return false;
 }
 
-template <int LA, int LB, int LC, int LD, int CD0, int N>
-__device__ __forceinline__ void digest_cd(const double (&I)[ncart(LA) * ncart(LB) * N], bool active,
+template <int LA, int LB, int LC, int LD, int CD0, int N, typename R>
+__device__ __forceinline__ void digest_cd(const R (&I)[ncart(LA) * ncart(LB) * N], bool active,
                                           const PairRec &pb, const PairRec &pk, bool same_pair,
                                           const double *__restrict__ D, double *__restrict__ Fj,
                                           double *__restrict__ Fk, int ld, int lane)
@@ -436,7 +484,7 @@ __device__ __forceinline__ void digest_cd(const double (&I)[ncart(LA) * ncart(LB
         for (int k = 0; k < NA * NB; k++) {
             double v = 0.0;
 #pragma unroll
-            for (int t = 0; t < N; t++) v = fma(I[k + NA * NB * t], dcd[t], v);
+            for (int t = 0; t < N; t++) v = fma((double)I[k + NA * NB * t], dcd[t], v);
             vab[k] = v * sJab;  // the factor depends on the lane's ket
         }
         warp_sum_many<NA * NB>(vab, lane, [&](int k, double t) {
@@ -458,7 +506,7 @@ __device__ __forceinline__ void digest_cd(const double (&I)[ncart(LA) * ncart(LB
 #pragma unroll
             for (int ibb = 0; ibb < NB; ibb++)
 #pragma unroll
-                for (int ia = 0; ia < NA; ia++) v = fma(I[ia + NA * (ibb + NB * t)], dab[ia + NA * ibb], v);
+                for (int ia = 0; ia < NA; ia++) v = fma((double)I[ia + NA * (ibb + NB * t)], dab[ia + NA * ibb], v);
             atomicAdd(Fj + (size_t)(fc + ic) * ld + fd + id, sJcd * v);
         }
     }
@@ -475,7 +523,7 @@ __device__ __forceinline__ void digest_cd(const double (&I)[ncart(LA) * ncart(LB
                 const int id = (CD0 + t) / NC;
 #pragma unroll
                 for (int ibb = 0; ibb < NB; ibb++)
-                    v = fma(I[ia + NA * (ibb + NB * t)], __ldg(D + (size_t)(fb + ibb) * ld + fd + id), v);
+                    v = fma((double)I[ia + NA * (ibb + NB * t)], __ldg(D + (size_t)(fb + ibb) * ld + fd + id), v);
             }
             atomicAdd(Fk + (size_t)(fa + ia) * ld + fc + ic, sKac * v);
         }
@@ -489,7 +537,7 @@ __device__ __forceinline__ void digest_cd(const double (&I)[ncart(LA) * ncart(LB
                     const int id = (CD0 + t) / NC;
 #pragma unroll
                     for (int ia = 0; ia < NA; ia++)
-                        v = fma(I[ia + NA * (ibb + NB * t)], __ldg(D + (size_t)(fa + ia) * ld + fd + id), v);
+                        v = fma((double)I[ia + NA * (ibb + NB * t)], __ldg(D + (size_t)(fa + ia) * ld + fd + id), v);
                 }
                 atomicAdd(Fk + (size_t)(fb + ibb) * ld + fc + ic, sKbc * v);
             }
@@ -509,7 +557,7 @@ __device__ __forceinline__ void digest_cd(const double (&I)[ncart(LA) * ncart(LB
                     const int ic = (CD0 + t) % NC;
 #pragma unroll
                     for (int ibb = 0; ibb < NB; ibb++)
-                        v = fma(I[ia + NA * (ibb + NB * t)], __ldg(D + (size_t)(fb + ibb) * ld + fc + ic), v);
+                        v = fma((double)I[ia + NA * (ibb + NB * t)], __ldg(D + (size_t)(fb + ibb) * ld + fc + ic), v);
                 }
                 atomicAdd(Fk + (size_t)(fa + ia) * ld + fd + id, sKad * v);
             }
@@ -523,7 +571,7 @@ __device__ __forceinline__ void digest_cd(const double (&I)[ncart(LA) * ncart(LB
                         const int ic = (CD0 + t) % NC;
 #pragma unroll
                         for (int ia = 0; ia < NA; ia++)
-                            v = fma(I[ia + NA * (ibb + NB * t)], __ldg(D + (size_t)(fa + ia) * ld + fc + ic), v);
+                            v = fma((double)I[ia + NA * (ibb + NB * t)], __ldg(D + (size_t)(fa + ia) * ld + fc + ic), v);
                     }
                     atomicAdd(Fk + (size_t)(fb + ibb) * ld + fd + id, sKbd * v);
                 }

@@ -397,6 +397,11 @@ PFockStatus_t gtf_pfock_set_precision(PFock_t pf, int mode, double fp32_cutoff)
     return map_err(gtf_fock_set_precision(pf->dev, mode, fp32_cutoff));
 }
 
+PFockStatus_t gtf_pfock_precision_stats(PFock_t pf, double *nquart_fp32, double *nquart)
+{
+    return map_err(gtf_fock_fp32_quartets(pf->dev, nquart_fp32, nquart));
+}
+
 PFockStatus_t gtf_pfock_compute_dev(PFock_t pf, const double *dev_D, const double **dev_F)
 {
     int e = gtf_fock_put_density_dev(pf->dev, 0, dev_D);

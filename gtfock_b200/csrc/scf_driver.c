@@ -33,6 +33,8 @@ struct gtf_scf {
     double enuc;
     double *D0;          /* initial guess (host) */
     double *dD, *dF;     /* device-resident D and F (mode 1) */
+    double etol;         /* stop when |E_k - E_k-1| < etol */
+    int last_mode;       /* where the last solve left D: 0 host, 1 device */
 };
 
 static double wall(void)
@@ -109,7 +111,29 @@ gtf_scf_t *gtf_scf_create(const char *bsfile, const char *xyzfile, double tolscr
     PFock_getCoreHMat(s->pf, 0, n - 1, 0, n - 1, n, s->pur->H_block);
     PFock_setNumDenMat(1, s->pf);
     initial_density(s->basis, s->D0, n);
+    s->etol = 1e-11;
+    s->last_mode = 0;
     return s;
+}
+
+int gtf_scf_set_options(gtf_scf_t *s, int prec_mode, double fp32_cutoff, double etol)
+{
+    if (!s || !(etol >= 0.0)) return -1;
+    if (gtf_pfock_set_precision(s->pf, prec_mode, fp32_cutoff) != PFOCK_STATUS_SUCCESS) return -2;
+    s->etol = etol;
+    return 0;
+}
+
+int gtf_scf_get_density(gtf_scf_t *s, double *D)
+{
+    if (!s || !D) return -1;
+    const size_t mb = sizeof(double) * (size_t)s->n * s->n;
+    if (s->last_mode == 1) {
+        void *st = gtf_fock_stream(gtf_pfock_device(s->pf));
+        return gtf_dev_copy(D, s->dD, mb, 1, st) == 0 ? 0 : -2;
+    }
+    memcpy(D, s->pur->D_block, mb);
+    return 0;
 }
 
 int gtf_scf_nbf(gtf_scf_t *s) { return s ? s->n : -1; }
@@ -117,6 +141,7 @@ int gtf_scf_nbf(gtf_scf_t *s) { return s ? s->n : -1; }
 int gtf_scf_solve(gtf_scf_t *s, int niters, int mode, double *energies, double *timings)
 {
     if (!s || niters <= 0 || (mode != 0 && mode != 1)) return -1;
+    s->last_mode = mode;
     const int n = s->n;
     const size_t nn = (size_t)n * n, mb = sizeof(double) * nn;
     purif_t *pur = s->pur;
@@ -149,7 +174,7 @@ int gtf_scf_solve(gtf_scf_t *s, int niters, int mode, double *energies, double *
             double t2 = wall();
             t_fock += t2 - t1;
             if (energies) energies[iter] = e + s->enuc;
-            if (iter > 0 && fabs(e - e0) < 1e-11) {
+            if (iter > 0 && fabs(e - e0) < s->etol) {
                 iter++;
                 break;
             }
@@ -183,7 +208,7 @@ int gtf_scf_solve(gtf_scf_t *s, int niters, int mode, double *energies, double *
             double t2 = wall();
             t_fock += t2 - t1;
             if (energies) energies[iter] = e + s->enuc;
-            if (iter > 0 && fabs(e - e0) < 1e-11) {
+            if (iter > 0 && fabs(e - e0) < s->etol) {
                 iter++;
                 break;
             }

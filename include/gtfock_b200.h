@@ -39,8 +39,13 @@ PFockStatus_t gtf_pfock_timing(PFock_t pfock, double *ms_total, double *ms_eri,
 int gtf_pfock_class_stats(PFock_t pfock, int *X, int *Y, double *ms, double *nquart);
 
 /* Precision of the ERI kernels: 0 = FP64 (default), 1 = FP32 for quartets
- * whose Schwarz bound sqrt(v1 v2) is below fp32_cutoff. */
+ * whose Schwarz bound sqrt(v1 v2) is below fp32_cutoff (Rys roots, 2-D
+ * integrals and the primitive sum in FP32; D, the J/K digestion and every
+ * accumulation into F stay FP64).  Rebuilds the task lists. */
 PFockStatus_t gtf_pfock_set_precision(PFock_t pfock, int mode, double fp32_cutoff);
+
+/* Quartets evaluated in FP32 under the current mode, and all quartets. */
+PFockStatus_t gtf_pfock_precision_stats(PFock_t pfock, double *nquart_fp32, double *nquart);
 
 /* Device-resident Fock build for callers that keep D on the GPU: dev_D is a
  * device pointer to the nbf x nbf density; the result stays on the device
@@ -79,6 +84,13 @@ typedef struct gtf_scf gtf_scf_t;
 gtf_scf_t *gtf_scf_create(const char *bsfile, const char *xyzfile, double tolscr);
 int gtf_scf_solve(gtf_scf_t *s, int niters, int mode, double *energies, double *timings);
 int gtf_scf_nbf(gtf_scf_t *s);
+/* ERI precision of the engine (as gtf_pfock_set_precision) and the energy
+ * convergence tolerance: a solve stops once |E_k - E_k-1| < etol (default
+ * 1e-11).  0 on success. */
+int gtf_scf_set_options(gtf_scf_t *s, int prec_mode, double fp32_cutoff, double etol);
+/* Copy of the density (half density, AO basis, nbf x nbf) left by the last
+ * solve.  0 on success. */
+int gtf_scf_get_density(gtf_scf_t *s, double *D);
 void gtf_scf_destroy(gtf_scf_t *s);
 /* create + solve + destroy; timings[3] covers the whole job */
 int gtf_scf_run(const char *bsfile, const char *xyzfile, double tolscr,
