@@ -563,9 +563,9 @@ static int launch_fock(int X, int Y, const FockLaunch &a, cudaStream_t st)
 {
     for (int g = 0; g < gtf_fock_ngroups; g++) {
         int r = gtf_fock_groups[g](k_cls_la[X], k_cls_lb[X], k_cls_la[Y], k_cls_lb[Y], a, st);
-        if (r != 1) return r;  // 0 launched, <0 error
+        if (r != GTF_NOT_IN_GROUP) return r;  // launches, or -1 on error
     }
-    return GTF_ERR_INVALID;
+    return -1;
 }
 
 // Rys-model FLOPs of one quartet of a class (normalisation used for the roofline):
@@ -885,7 +885,7 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
     f->usq = 0.0;
     f->uitl = 0.0;
     f->eri_flops = 0.0;
-    DALLOC(f->d_counters, 2 * NCLSPAIR);
+    DALLOC(f->d_counters, 2 * NCLSPAIR * GTF_MAX_SLICES);
     int cp = 0;
     for (int X = 0; X < NCLS; X++) {
         for (int Y = 0; Y <= X; Y++, cp++) {
@@ -1112,8 +1112,9 @@ extern "C" int gtf_fock_set_precision(gtf_fock_dev_t *f, int prec, double fp32_c
 }
 
 // Launches the Fock kernels of class pair c: the FP64 part of every ket
-// range, then (mixed precision) the FP32 tail.  counters holds two slots per
-// class pair.  Returns the number of launches, or -1 on a launch error.
+// range, then (mixed precision) the FP32 tail.  counters holds
+// GTF_MAX_SLICES zeroed slots per (class pair, part), one per slice launch.
+// Returns the number of launches, or -1 on a launch error.
 static int launch_class(const gtf_fock_dev *f, int c, const double *D, double *Fj, double *Fk,
                         unsigned long long *counters, cudaStream_t st)
 {
@@ -1134,19 +1135,20 @@ static int launch_class(const gtf_fock_dev *f, int c, const double *D, double *F
         a.bra_start = t.bra_start;
         a.ket_start = t.ket_start;
         for (int b = 0; b <= GTF_NBKT; b++) a.seg[b] = t.seg[b];
-        a.counter = counters + 2 * c + part;
+        a.counter = counters + (size_t)(2 * c + part) * GTF_MAX_SLICES;
         a.D = D;
         a.Fj = Fj;
         a.Fk = Fk;
         a.ld = f->nbf_cart;
         a.nsm = f->nsm;
         a.fp32 = part;
-        if (launch_fock(t.X, t.Y, a, st) != 0) {
+        const int r = launch_fock(t.X, t.Y, a, st);
+        if (r < 0) {
             snprintf(g_errbuf, sizeof(g_errbuf), "Fock kernel launch for class pair (%d,%d)%s failed: %s", t.X, t.Y,
                      part ? " (FP32)" : "", cudaGetErrorString(cudaGetLastError()));
             return -1;
         }
-        n++;
+        n += r;
     }
     return n;
 }
@@ -1173,7 +1175,7 @@ extern "C" int gtf_fock_compute(gtf_fock_dev_t *f, int numdmat)
         }
         CK(cudaMemsetAsync(f->d_Fj, 0, sizeof(double) * nnc, st));
         CK(cudaMemsetAsync(f->d_Fk, 0, sizeof(double) * nnc, st));
-        CK(cudaMemsetAsync(f->d_counters, 0, sizeof(unsigned long long) * 2 * NCLSPAIR, st));
+        CK(cudaMemsetAsync(f->d_counters, 0, sizeof(unsigned long long) * 2 * NCLSPAIR * GTF_MAX_SLICES, st));
         CK(cudaEventRecord(f->ev1, st));
         for (int c = 0; c < NCLSPAIR; c++) {
             ClassPairTask &t = f->tasks[c];
@@ -1356,7 +1358,7 @@ extern "C" void gtf_fock_basis_dev(gtf_fock_dev_t *f, const int **sh_L, const in
 // ---------------------------------------------------------------------------
 #define GTF_FIXED_MAX_FUNCS 384
 #define GTF_FIXED_NN ((size_t)GTF_FIXED_MAX_FUNCS * GTF_FIXED_MAX_FUNCS)
-#define GTF_FIXED_DOUBLES (5 * GTF_FIXED_NN + 2 * NCLSPAIR + 3)
+#define GTF_FIXED_DOUBLES (5 * GTF_FIXED_NN + 2 * NCLSPAIR * GTF_MAX_SLICES + 3)
 #define GTF_FIXED_MAX_DEVICES 64
 
 static __device__ __align__(256) double g_fixed_scratch[GTF_FIXED_DOUBLES];
@@ -1424,7 +1426,7 @@ extern "C" int gtf_fock_compute_fixed(gtf_fock_dev_t *f, const double *dev_D, do
     }
     CK(cudaMemsetAsync(Fj, 0, sizeof(double) * nnc, st));
     CK(cudaMemsetAsync(Fk, 0, sizeof(double) * nnc, st));
-    CK(cudaMemsetAsync(counters, 0, sizeof(unsigned long long) * 2 * NCLSPAIR, st));
+    CK(cudaMemsetAsync(counters, 0, sizeof(unsigned long long) * 2 * NCLSPAIR * GTF_MAX_SLICES, st));
     for (int c = 0; c < NCLSPAIR; c++)
         if (launch_class(f, c, Duse, Fj, Fk, counters, st) < 0) return GTF_ERR_CUDA;
     dim3 g2((nbf + 127) / 128, nbf);

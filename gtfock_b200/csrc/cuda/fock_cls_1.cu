@@ -8,5 +8,5 @@ extern "C" int gtf_fock_group_1(int la, int lb, int lc, int ld, const FockLaunch
     FOCK_GROUP_CASE(2,1,1,0)
     FOCK_GROUP_CASE(2,1,1,1)
     FOCK_GROUP_CASE(2,1,2,0)
-    return 1;
+    return GTF_NOT_IN_GROUP;
 }

@@ -5,5 +5,5 @@
 extern "C" int gtf_fock_group_5(int la, int lb, int lc, int ld, const FockLaunch &a, cudaStream_t st)
 {
     FOCK_GROUP_CASE(2,2,2,2)
-    return 1;
+    return GTF_NOT_IN_GROUP;
 }

@@ -67,29 +67,24 @@ __host__ __device__ constexpr int fock_slice(int LA, int LB, int LC, int LD, int
     return s < 1 ? 1 : (s > ncd ? ncd : s);
 }
 
+// One launch per slice (CD0 = first ket component of the slice): each
+// kernel holds the code of a single slice, which keeps the instruction
+// footprint of the d-class kernels small.  The Rys table block of this class
+// (NR roots, precision R) is staged in shared memory by every block.
 template <int LA, int LB, int LC, int LD, typename R, int CD0>
-__device__ __forceinline__ void fock_slices(const PPRec &src, const PairRec &pb, const PairRec &pk, bool active,
-                                            bool same, const double *__restrict__ D, double *__restrict__ Fj,
-                                            double *__restrict__ Fk, int ld, int lane)
-{
-    constexpr int NCD = ncart(LC) * ncart(LD);
-    constexpr int S = fock_slice(LA, LB, LC, LD, sizeof(R) == 4 ? 1 : 0);
-    if constexpr (CD0 < NCD) {
-        constexpr int N = (NCD - CD0 < S) ? NCD - CD0 : S;
-        R acc[ncart(LA) * ncart(LB) * N];
-#pragma unroll
-        for (int k = 0; k < ncart(LA) * ncart(LB) * N; k++) acc[k] = (R)0;
-        if (active) eri_accumulate_cd<LA, LB, LC, LD, CD0, N, true>(src, pb, src, pk, acc);
-        digest_cd<LA, LB, LC, LD, CD0, N>(acc, active, pb, pk, same, D, Fj, Fk, ld, lane);
-        fock_slices<LA, LB, LC, LD, R, CD0 + N>(src, pb, pk, active, same, D, Fj, Fk, ld, lane);
-    }
-}
-
-// unit u -> (bra i, segment b, chunk of 32 kets): binary search of the
-// exclusive unit prefix over the flattened (bra, segment) index
-template <int LA, int LB, int LC, int LD, typename R>
 __global__ void __launch_bounds__(FOCK_THREADS) k_fock(const FockLaunch a)
 {
+    constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
+    constexpr int NCD = ncart(LC) * ncart(LD);
+    constexpr int S = fock_slice(LA, LB, LC, LD, sizeof(R) == 4 ? 1 : 0);
+    constexpr int N = (NCD - CD0 < S) ? NCD - CD0 : S;
+    constexpr int TL = RysTab<R>::len(NR);
+    __shared__ __align__(16) R tab[TL];
+    {
+        const R *g = RysTab<R>::ptr(NR);
+        for (int k = threadIdx.x; k < TL; k += blockDim.x) tab[k] = g[k];
+        __syncthreads();
+    }
     const int lane = threadIdx.x & 31;
     const PPRec src{a.pprec};
     const int nidx = a.nbra * GTF_NBKT;
@@ -98,6 +93,8 @@ __global__ void __launch_bounds__(FOCK_THREADS) k_fock(const FockLaunch a)
         if (lane == 0) u = atomicAdd(a.counter, 1ULL);
         u = __shfl_sync(GTF_FULL_MASK, u, 0);
         if (u >= (unsigned long long)a.nunits) break;
+        // unit u -> (bra i, segment b, chunk of 32 kets): binary search of the
+        // exclusive unit prefix over the flattened (bra, segment) index
         int lo = 0, hi = nidx;
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
@@ -113,26 +110,59 @@ __global__ void __launch_bounds__(FOCK_THREADS) k_fock(const FockLaunch a)
         const PairRec pb = a.pairs[a.bra_start + i];
         const PairRec pk = active ? a.pairs[a.ket_start + j] : pb;
         const bool same = (a.bra_start + i) == (a.ket_start + j);
-        fock_slices<LA, LB, LC, LD, R, 0>(src, pb, pk, active, same, a.D, a.Fj, a.Fk, a.ld, lane);
+        R acc[ncart(LA) * ncart(LB) * N];
+#pragma unroll
+        for (int k = 0; k < ncart(LA) * ncart(LB) * N; k++) acc[k] = (R)0;
+        if (active) eri_accumulate_cd<LA, LB, LC, LD, CD0, N, true>(src, pb, src, pk, acc, tab);
+        digest_cd<LA, LB, LC, LD, CD0, N>(acc, active, pb, pk, same, a.D, a.Fj, a.Fk, a.ld, lane);
     }
 }
 
+// Number of slice launches of a class pair; a.counter points at that many
+// zeroed counters.
+__host__ __device__ constexpr int fock_nslices(int LA, int LB, int LC, int LD, int fp32)
+{
+    const int ncd = ncart(LC) * ncart(LD), s = fock_slice(LA, LB, LC, LD, fp32);
+    return (ncd + s - 1) / s;
+}
+#define GTF_MAX_SLICES 64
+
+template <int LA, int LB, int LC, int LD, typename R, int CD0>
+int launch_fock_slices(const FockLaunch &a, cudaStream_t st, int slice)
+{
+    constexpr int NCD = ncart(LC) * ncart(LD);
+    if constexpr (CD0 < NCD) {
+        constexpr int S = fock_slice(LA, LB, LC, LD, sizeof(R) == 4 ? 1 : 0);
+        auto k = k_fock<LA, LB, LC, LD, R, CD0>;
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k, FOCK_THREADS, 0);
+        if (per_sm < 1) per_sm = 1;
+        long long want = (a.nunits + (FOCK_THREADS / 32) - 1) / (FOCK_THREADS / 32);
+        long long grid = (long long)a.nsm * per_sm;
+        if (want < grid) grid = want;
+        if (grid < 1) grid = 1;
+        FockLaunch b = a;
+        b.counter = a.counter + slice;
+        k<<<(unsigned)grid, FOCK_THREADS, 0, st>>>(b);
+        if (cudaGetLastError() != cudaSuccess) return -1;
+        const int r = launch_fock_slices<LA, LB, LC, LD, R, CD0 + S>(a, st, slice + 1);
+        return r < 0 ? r : r + 1;
+    } else {
+        return 0;
+    }
+}
+
+// returns the number of kernels launched, or -1 on a launch error
 template <int LA, int LB, int LC, int LD, typename R>
 int launch_fock_t(const FockLaunch &a, cudaStream_t st)
 {
-    auto k = k_fock<LA, LB, LC, LD, R>;
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k, FOCK_THREADS, 0);
-    if (per_sm < 1) per_sm = 1;
-    long long want = (a.nunits + (FOCK_THREADS / 32) - 1) / (FOCK_THREADS / 32);
-    long long grid = (long long)a.nsm * per_sm;
-    if (want < grid) grid = want;
-    if (grid < 1) grid = 1;
-    k<<<(unsigned)grid, FOCK_THREADS, 0, st>>>(a);
-    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    static_assert(fock_nslices(LA, LB, LC, LD, sizeof(R) == 4 ? 1 : 0) <= GTF_MAX_SLICES, "slice counters");
+    return launch_fock_slices<LA, LB, LC, LD, R, 0>(a, st, 0);
 }
 
-// returns 0 when launched, -1 on a launch error, 1 when the class pair is not in this group
+// returns the number of launches, -1 on a launch error, GTF_NOT_IN_GROUP when the
+// class pair is not in this group
+#define GTF_NOT_IN_GROUP (-2)
 #define FOCK_GROUP_CASE(A, B, C, D) \
     if (la == A && lb == B && lc == C && ld == D)                                                       \
         return a.fp32 ? launch_fock_t<A, B, C, D, float>(a, st) : launch_fock_t<A, B, C, D, double>(a, st);

@@ -93,8 +93,34 @@ __device__ __forceinline__ float grsqrt(float x) { return rsqrtf(x); }
 // ---------------------------------------------------------------------------
 // Rys roots and weights
 // ---------------------------------------------------------------------------
+// The N-root block of each table is [off(N), off(N+1)); its extent is known
+// at compile time so kernels can stage it in shared memory.
+template <typename R>
+struct RysTab;
+template <>
+struct RysTab<double> {
+    static __host__ __device__ constexpr int off(int n)
+    {
+        constexpr int o[] = {RYS_OFF_LIST, RYS_TABLE_LEN};
+        return o[n];
+    }
+    static __host__ __device__ constexpr int len(int n) { return off(n + 1) - off(n); }
+    static __device__ __forceinline__ const double *ptr(int n) { return RYS_TABLE + off(n); }
+};
+template <>
+struct RysTab<float> {
+    static __host__ __device__ constexpr int off(int n)
+    {
+        constexpr int o[] = {RYS32_OFF_LIST, RYS32_TABLE_LEN};
+        return o[n];
+    }
+    static __host__ __device__ constexpr int len(int n) { return off(n + 1) - off(n); }
+    static __device__ __forceinline__ const float *ptr(int n) { return RYS32_TABLE + off(n); }
+};
+
+// tab: the N-root block of RYS_TABLE (global or a shared-memory copy)
 template <int N>
-__device__ __forceinline__ void rys_roots(double T, double (&u)[N], double (&w)[N])
+__device__ __forceinline__ void rys_roots(double T, double (&u)[N], double (&w)[N], const double *tab)
 {
     if (T >= RYS_TMAX[N]) {
         const double it = 1.0 / T;
@@ -108,13 +134,13 @@ __device__ __forceinline__ void rys_roots(double T, double (&u)[N], double (&w)[
     }
     const int k = (int)(T * RYS_INV_H);
     const double s = T - ((double)k * RYS_H + 0.5 * RYS_H);
-    const double *c = RYS_TABLE + RYS_OFF[N] + k * (RYS_DEG + 1) * (2 * N);
+    const double *c = tab + k * (RYS_DEG + 1) * (2 * N);
     // rows of 2N coefficients start on 16-byte boundaries (even offsets)
     const double2 *c2 = reinterpret_cast<const double2 *>(c);
     double a[2 * N];
 #pragma unroll
     for (int f = 0; f < N; f++) {
-        const double2 t = __ldg(c2 + RYS_DEG * N + f);
+        const double2 t = c2[RYS_DEG * N + f];
         a[2 * f] = t.x;
         a[2 * f + 1] = t.y;
     }
@@ -122,7 +148,7 @@ __device__ __forceinline__ void rys_roots(double T, double (&u)[N], double (&w)[
     for (int j = RYS_DEG - 1; j >= 0; j--) {
 #pragma unroll
         for (int f = 0; f < N; f++) {
-            const double2 t = __ldg(c2 + j * N + f);
+            const double2 t = c2[j * N + f];
             a[2 * f] = fma(a[2 * f], s, t.x);
             a[2 * f + 1] = fma(a[2 * f + 1], s, t.y);
         }
@@ -137,7 +163,7 @@ __device__ __forceinline__ void rys_roots(double T, double (&u)[N], double (&w)[
 // FP32 form for quartets evaluated in single precision: degree-7 fit of the
 // same functions on the same intervals (RYS32_TABLE), same large-T form
 template <int N>
-__device__ __forceinline__ void rys_roots(float T, float (&u)[N], float (&w)[N])
+__device__ __forceinline__ void rys_roots(float T, float (&u)[N], float (&w)[N], const float *tab)
 {
     if (T >= (float)RYS_TMAX[N]) {
         const float it = 1.0f / T;
@@ -151,11 +177,11 @@ __device__ __forceinline__ void rys_roots(float T, float (&u)[N], float (&w)[N])
     }
     const int k = (int)(T * RYS32_INV_H);
     const float s = T - ((float)k * (float)RYS32_H + 0.5f * (float)RYS32_H);
-    const float2 *c2 = reinterpret_cast<const float2 *>(RYS32_TABLE + RYS32_OFF[N] + k * (RYS32_DEG + 1) * (2 * N));
+    const float2 *c2 = reinterpret_cast<const float2 *>(tab + k * (RYS32_DEG + 1) * (2 * N));
     float a[2 * N];
 #pragma unroll
     for (int f = 0; f < N; f++) {
-        const float2 t = __ldg(c2 + RYS32_DEG * N + f);
+        const float2 t = c2[RYS32_DEG * N + f];
         a[2 * f] = t.x;
         a[2 * f + 1] = t.y;
     }
@@ -163,7 +189,7 @@ __device__ __forceinline__ void rys_roots(float T, float (&u)[N], float (&w)[N])
     for (int j = RYS32_DEG - 1; j >= 0; j--) {
 #pragma unroll
         for (int f = 0; f < N; f++) {
-            const float2 t = __ldg(c2 + j * N + f);
+            const float2 t = c2[j * N + f];
             a[2 * f] = fmaf(a[2 * f], s, t.x);
             a[2 * f + 1] = fmaf(a[2 * f + 1], s, t.y);
         }
@@ -265,9 +291,11 @@ __device__ __forceinline__ void hrr_abcd(const R (&G)[LA + LB + 1][LC + LD + 1],
 // call it once per slice so that a slice's accumulators fit in registers.
 // R = double, or float for quartets evaluated in single precision (the
 // differences of centres are formed in double first, then rounded).
+// rtab: the NR-root block of the Rys table of precision R.
 template <int LA, int LB, int LC, int LD, int CD0, int N, bool SKIP, class PPB, class PPK, typename R>
 __device__ __forceinline__ void eri_accumulate_cd(const PPB &bra, const PairRec &pb, const PPK &ket,
-                                                  const PairRec &pk, R (&acc)[ncart(LA) * ncart(LB) * N])
+                                                  const PairRec &pk, R (&acc)[ncart(LA) * ncart(LB) * N],
+                                                  const R *rtab)
 {
     constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
     constexpr int NI = LA + LB + 1, NK = LC + LD + 1;
@@ -294,7 +322,7 @@ __device__ __forceinline__ void eri_accumulate_cd(const PPB &bra, const PairRec 
             const R T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
             const R pref = (R)(Kab * Kcd) * rpq;
             R u[NR], w[NR];
-            rys_roots<NR>(T, u, w);
+            rys_roots<NR>(T, u, w, rtab);
             const R QCx = (R)(Qx - pk.Ax), QCy = (R)(Qy - pk.Ay), QCz = (R)(Qz - pk.Az);
             const R h2p = (R)0.5 / p_, h2q = (R)0.5 / q_;
             const R qf = q_ * ipq, pf = p_ * ipq;
@@ -341,7 +369,9 @@ __device__ __forceinline__ void eri_accumulate(const PPB &bra, const PairRec &pb
                                                const PairRec &pk,
                                                double (&acc)[ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD)])
 {
-    eri_accumulate_cd<LA, LB, LC, LD, 0, ncart(LC) * ncart(LD), SKIP>(bra, pb, ket, pk, acc);
+    constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
+    eri_accumulate_cd<LA, LB, LC, LD, 0, ncart(LC) * ncart(LD), SKIP>(bra, pb, ket, pk, acc,
+                                                                      RysTab<double>::ptr(NR));
 }
 
 // primitive pairs read from the precomputed pair arrays

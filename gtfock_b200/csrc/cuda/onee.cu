@@ -40,7 +40,7 @@ template <int N>
 __device__ void nuclear_rys(double T, double (&u)[3], double (&w)[3])
 {
     double uu[N], ww[N];
-    rys_roots<N>(T, uu, ww);
+    rys_roots<N>(T, uu, ww, RysTab<double>::ptr(N));
 #pragma unroll
     for (int i = 0; i < N; i++) {
         u[i] = uu[i];

@@ -159,6 +159,7 @@ def main(out_path=None):
       ", ".join("%.1f" % TMAX[n] for n in range(1, NMAX + 1)))
     w("RYS_QUAL_SMALL const int RYS_OFF[RYS_NMAX + 1] = {0, %s};" %
       ", ".join(str(offs[n]) for n in range(1, NMAX + 1)))
+    w("#define RYS_OFF_LIST 0, %s" % ", ".join(str(offs[n]) for n in range(1, NMAX + 1)))
     w("#define RYS_TABLE_LEN %d" % len(flat))
     w("RYS_QUAL const double RYS_TABLE[RYS_TABLE_LEN] = {")
     for i in range(0, len(flat), 4):
@@ -176,6 +177,7 @@ def main(out_path=None):
         off = len(flat32)
     w("RYS_QUAL_SMALL const int RYS32_OFF[RYS_NMAX + 1] = {0, %s};" %
       ", ".join(str(offs32[n]) for n in range(1, NMAX + 1)))
+    w("#define RYS32_OFF_LIST 0, %s" % ", ".join(str(offs32[n]) for n in range(1, NMAX + 1)))
     w("#define RYS32_TABLE_LEN %d" % len(flat32))
     w("RYS_QUAL const float RYS32_TABLE[RYS32_TABLE_LEN] = {")
     for i in range(0, len(flat32), 6):
