@@ -301,8 +301,9 @@ def profile_fock(args):
         nq32, nq = pf.precision_stats()
         out = {"molecule": args.profile_fock, "nbf": b.nbf, "counts": pf.counts(), "timing": tm,
                "fp32_cutoff": args.fp32_cutoff, "fp32_share": nq32 / nq if nq else 0.0,
-               "classes": [{"bra": x, "ket": y, "ms": ms, "quartets": q}
-                           for x, y, ms, q in pf.class_stats() if q > 0]}
+               "classes": [{"bra": x, "ket": y, "ms": ms, "quartets": q, "gflop": w[0] / 1e9,
+                            "primq": w[1], "tflops": w[0] / ms / 1e9 if ms > 0 else 0.0}
+                           for (x, y, ms, q), w in zip(pf.class_stats(), pf.class_work()) if q > 0]}
         pf.close()
     print(json.dumps(out), flush=True)
 

@@ -93,6 +93,7 @@ def load():
     _sig(L, "gtf_pfock_set_precision", [_vp, _i, _d])
     _sig(L, "gtf_pfock_precision_stats", [_vp, _dp, _dp])
     _sig(L, "gtf_pfock_class_stats", [_vp, _ip, _ip, _dp, _dp])
+    _sig(L, "gtf_pfock_class_work", [_vp, _dp, _dp])
     _sig(L, "gtf_scf_run", [_cp, _cp, _d, _i, _i, _dp, _dp])
     _sig(L, "gtf_scf_create", [_cp, _cp, _d], _vp)
     _sig(L, "gtf_scf_solve", [_vp, _i, _i, _dp, _dp])
@@ -233,6 +234,13 @@ class PFock:
         nq = np.zeros(32)
         n = load().gtf_pfock_class_stats(self.h, _iptr(X), _iptr(Y), _dptr(ms), _dptr(nq))
         return [(int(X[i]), int(Y[i]), float(ms[i]), float(nq[i])) for i in range(n)]
+
+    def class_work(self):
+        """[(Rys-model FLOPs, primitive quartets)] per class pair, same order."""
+        fl = np.zeros(32)
+        npq = np.zeros(32)
+        n = load().gtf_pfock_class_work(self.h, _dptr(fl), _dptr(npq))
+        return [(float(fl[i]), float(npq[i])) for i in range(n)]
 
     def set_precision(self, mode, fp32_cutoff=0.0):
         """mode 0: FP64; mode 1: FP32 for quartets with Schwarz bound < fp32_cutoff."""

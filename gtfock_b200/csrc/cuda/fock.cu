@@ -71,6 +71,7 @@ struct ClassPairTask {
     int ket_start, nketcls;
     int seg[GTF_NBKT + 1];  // ket segments (primitive-count buckets), relative to ket_start
     long long nunits, nunits32;  // units of the FP64 and the FP32 launch
+    double flops, nprimq;        // Rys-model FLOPs and primitive quartets (before primitive screening)
     double nquart, nquart32;     // quartets in all, of which evaluated in FP32
     int *d_nket;                 // [nbra][GTF_NBKT] kets per (bra, segment)
     int *d_n64;                  // [nbra][GTF_NBKT] of which FP64 (a prefix)
@@ -99,7 +100,7 @@ struct gtf_fock_dev {
     PairRec *d_pairs;
     double *d_pair_v;
     int nprimpairs;
-    double *d_pp;   // 6 * nprimpairs: records {p, K, Px, Py, Pz, 0} (PPRec)
+    double *d_pp;   // 6 * nprimpairs: records {p, K, Px, Py, Pz, 1/(2p)} (PPRec)
     ClassPairTask tasks[NCLSPAIR];
     unsigned long long *d_counters;
     double usq, uitl, eri_flops;
@@ -455,7 +456,7 @@ __global__ void k_build_pairs(const int *__restrict__ idx, const int *__restrict
 // to any integral is below 1e-20 Hartree), the rest are stored in descending
 // |K| so that the quartet loop can stop once |K_ab K_cd| < GTF_PRIMQ_EPS.
 // pairs[s].n becomes the kept count (possibly 0); the slot keeps its size.
-// Records are {p, K, Px, Py, Pz, 0} (PPRec).
+// Records are {p, K, Px, Py, Pz, 1/(2p)} (PPRec).
 __global__ void k_fill_primpairs(PairRec *__restrict__ pairs, const int *__restrict__ idx,
                                  const int *__restrict__ shellid, const int *__restrict__ shellrid,
                                  const int *__restrict__ pair_off, BasisDev b, int npairs, double *pp)
@@ -493,7 +494,7 @@ __global__ void k_fill_primpairs(PairRec *__restrict__ pairs, const int *__restr
             d[2] = (al * Ax + be * Bx) * ip;
             d[3] = (al * Ay + be * By) * ip;
             d[4] = (al * Az + be * Bz) * ip;
-            d[5] = 0.0;
+            d[5] = 0.5 * ip;
             kept++;
         }
     }
@@ -949,14 +950,19 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
             const int la = k_cls_la[t.X], lb = k_cls_lb[t.X], lc = k_cls_la[t.Y], ld = k_cls_lb[t.Y];
             const double ns_ = (double)(b->pure && la == 2 ? 5 : ncart(la)) * (b->pure && lb == 2 ? 5 : ncart(lb)) *
                                (b->pure && lc == 2 ? 5 : ncart(lc)) * (b->pure && ld == 2 ? 5 : ncart(ld));
+            double cf = 0.0, cq = 0.0;
             for (int i = 0; i < t.nbra; i++) {
                 const double kb = hn[t.bra_start + i];
                 for (int bk = 0; bk < GTF_NBKT; bk++) {
                     const int c = nk[i * GTF_NBKT + bk];
                     const double kk = kpre[t.seg[bk] + c] - kpre[t.seg[bk]];
-                    flops += kb * kk * per_prim + (cpart + 12.0 * ns_) * c;
+                    cf += kb * kk * per_prim + (cpart + 12.0 * ns_) * c;
+                    cq += kb * kk;
                 }
             }
+            t.flops = cf;
+            t.nprimq = cq;
+            flops += cf;
         }
         f->eri_flops = flops;
     }
@@ -1250,6 +1256,15 @@ extern "C" int gtf_fock_class_stats(gtf_fock_dev_t *f, int *X, int *Y, double *m
         if (Y) Y[c] = f->tasks[c].Y;
         if (ms) ms[c] = f->ms_cls[c];
         if (nquart) nquart[c] = f->tasks[c].nquart;
+    }
+    return NCLSPAIR;
+}
+
+extern "C" int gtf_fock_class_work(gtf_fock_dev_t *f, double *flops, double *nprimq)
+{
+    for (int c = 0; c < NCLSPAIR; c++) {
+        if (flops) flops[c] = f->tasks[c].flops;
+        if (nprimq) nprimq[c] = f->tasks[c].nprimq;
     }
     return NCLSPAIR;
 }

@@ -79,6 +79,8 @@ void gtf_fock_release_onee(gtf_fock_dev_t *f, int which);
 int gtf_fock_set_precision(gtf_fock_dev_t *f, int prec, double fp32_cutoff);
 int gtf_fock_last_timing(gtf_fock_dev_t *f, double *ms_total, double *ms_eri, double *ms_other);
 int gtf_fock_eri_flops(gtf_fock_dev_t *f, double *flops);
+/* per class pair: Rys-model FLOPs and primitive quartets of one build */
+int gtf_fock_class_work(gtf_fock_dev_t *f, double *flops, double *nprimq);
 /* quartets evaluated in FP32 under the current precision mode, and all */
 int gtf_fock_fp32_quartets(gtf_fock_dev_t *f, double *nq32, double *nq);
 /* per angular class pair (21 of them for s/p/d): classes, ms of the last

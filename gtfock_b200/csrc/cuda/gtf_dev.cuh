@@ -85,6 +85,12 @@ struct PrimPairs {
     const double *K;   // GTF_PAIR_PREF * ca * cb * exp(-ab/p |AB|^2) / p
 };
 
+// one primitive pair: exponent sum p, centre P, prefactor K, h = 1/(2p)
+struct PrimVals {
+    double p, Px, Py, Pz, K, h;
+};
+
+
 __device__ __forceinline__ double gfma(double a, double b, double c) { return fma(a, b, c); }
 __device__ __forceinline__ float gfma(float a, float b, float c) { return fmaf(a, b, c); }
 __device__ __forceinline__ double grsqrt(double x) { return rsqrt(x); }
@@ -292,6 +298,9 @@ __device__ __forceinline__ void hrr_abcd(const R (&G)[LA + LB + 1][LC + LD + 1],
 // R = double, or float for quartets evaluated in single precision (the
 // differences of centres are formed in double first, then rounded).
 // rtab: the NR-root block of the Rys table of precision R.
+// Loop order: ket primitive pairs outside (one per lane), bra primitive pairs
+// inside -- the bra is shared by the warp, so its records are warp-uniform
+// loads that stay in L1, and each lane reads its ket's records once.
 template <int LA, int LB, int LC, int LD, int CD0, int N, bool SKIP, class PPB, class PPK, typename R>
 __device__ __forceinline__ void eri_accumulate_cd(const PPB &bra, const PairRec &pb, const PPK &ket,
                                                   const PairRec &pk, R (&acc)[ncart(LA) * ncart(LB) * N],
@@ -300,31 +309,34 @@ __device__ __forceinline__ void eri_accumulate_cd(const PPB &bra, const PairRec 
     constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
     constexpr int NI = LA + LB + 1, NK = LC + LD + 1;
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    if (pb.n <= 0) return;
     const R ABx = (R)pb.ABx, ABy = (R)pb.ABy, ABz = (R)pb.ABz;
     const R CDx = (R)pk.ABx, CDy = (R)pk.ABy, CDz = (R)pk.ABz;
-    for (int ib = 0; ib < pb.n; ib++) {
-        double p, Px, Py, Pz, Kab;
-        bra.get(pb, ib, p, Px, Py, Pz, Kab);
-        const R PAx = (R)(Px - pb.Ax), PAy = (R)(Py - pb.Ay), PAz = (R)(Pz - pb.Az);
-        const R p_ = (R)p;
-        // the next ket primitive pair is loaded while the current one is used
-        double nq = 0.0, nQx = 0.0, nQy = 0.0, nQz = 0.0, nK = 0.0;
-        if (pk.n > 0) ket.get(pk, 0, nq, nQx, nQy, nQz, nK);
-        for (int ik = 0; ik < pk.n; ik++) {
-            const double q = nq, Qx = nQx, Qy = nQy, Qz = nQz, Kcd = nK;
-            if (ik + 1 < pk.n) ket.get(pk, ik + 1, nq, nQx, nQy, nQz, nK);
-            if (SKIP && fabs(Kab * Kcd) < GTF_PRIMQ_EPS) break;  // kets are in descending |K|
-            const R q_ = (R)q;
-            const R rpq = grsqrt((R)(p + q));
+    const PrimVals b0 = bra.get(pb, 0);
+    PrimVals nk;
+    if (pk.n > 0) nk = ket.get(pk, 0);
+    for (int ik = 0; ik < pk.n; ik++) {
+        const PrimVals kq = nk;
+        if (ik + 1 < pk.n) nk = ket.get(pk, ik + 1);
+        if (SKIP && fabs(b0.K * kq.K) < GTF_PRIMQ_EPS) break;  // both lists are in descending |K|
+        const R q_ = (R)kq.p, h2q = (R)kq.h;
+        const R QCx = (R)(kq.Px - pk.Ax), QCy = (R)(kq.Py - pk.Ay), QCz = (R)(kq.Pz - pk.Az);
+        // the next bra primitive pair is loaded while the current one is used
+        PrimVals nb = b0;
+        for (int ib = 0; ib < pb.n; ib++) {
+            const PrimVals bq = nb;
+            if (ib + 1 < pb.n) nb = bra.get(pb, ib + 1);
+            if (SKIP && fabs(bq.K * kq.K) < GTF_PRIMQ_EPS) break;
+            const R p_ = (R)bq.p, h2p = (R)bq.h;
+            const R PAx = (R)(bq.Px - pb.Ax), PAy = (R)(bq.Py - pb.Ay), PAz = (R)(bq.Pz - pb.Az);
+            const R rpq = grsqrt((R)(bq.p + kq.p));
             const R ipq = rpq * rpq;
-            const R PQx = (R)(Px - Qx), PQy = (R)(Py - Qy), PQz = (R)(Pz - Qz);
+            const R PQx = (R)(bq.Px - kq.Px), PQy = (R)(bq.Py - kq.Py), PQz = (R)(bq.Pz - kq.Pz);
             const R rho = p_ * q_ * ipq;
             const R T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
-            const R pref = (R)(Kab * Kcd) * rpq;
+            const R pref = (R)(bq.K * kq.K) * rpq;
             R u[NR], w[NR];
             rys_roots<NR>(T, u, w, rtab);
-            const R QCx = (R)(Qx - pk.Ax), QCy = (R)(Qy - pk.Ay), QCz = (R)(Qz - pk.Az);
-            const R h2p = (R)0.5 / p_, h2q = (R)0.5 / q_;
             const R qf = q_ * ipq, pf = p_ * ipq;
 #pragma unroll
             for (int r = 0; r < NR; r++) {
@@ -374,36 +386,40 @@ __device__ __forceinline__ void eri_accumulate(const PPB &bra, const PairRec &pb
                                                                       RysTab<double>::ptr(NR));
 }
 
-// primitive pairs read from the precomputed pair arrays
+// primitive pairs read from the precomputed pair arrays (SoA)
 struct PPStored {
     PrimPairs pp;
-    __device__ __forceinline__ void get(const PairRec &pr, int i, double &p, double &Px, double &Py,
-                                        double &Pz, double &K) const
+    __device__ __forceinline__ PrimVals get(const PairRec &pr, int i) const
     {
         const int k = pr.off + i;
-        p = __ldg(pp.p + k);
-        Px = __ldg(pp.Px + k);
-        Py = __ldg(pp.Py + k);
-        Pz = __ldg(pp.Pz + k);
-        K = __ldg(pp.K + k);
+        PrimVals v;
+        v.p = __ldg(pp.p + k);
+        v.Px = __ldg(pp.Px + k);
+        v.Py = __ldg(pp.Py + k);
+        v.Pz = __ldg(pp.Pz + k);
+        v.K = __ldg(pp.K + k);
+        v.h = 0.5 / v.p;
+        return v;
     }
 };
 
 // primitive pairs of the Fock build: one 48-byte record per pair,
-// {p, K}, {Px, Py}, {Pz, 0}, read with three 16-byte loads
+// {p, K}, {Px, Py}, {Pz, 1/(2p)}, read with three 16-byte loads
 #define GTF_PPREC_D2 3
 struct PPRec {
     const double2 *r;
-    __device__ __forceinline__ void get(const PairRec &pr, int i, double &p, double &Px, double &Py,
-                                        double &Pz, double &K) const
+    __device__ __forceinline__ PrimVals get(const PairRec &pr, int i) const
     {
         const double2 *q = r + (size_t)GTF_PPREC_D2 * (pr.off + i);
         const double2 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
-        p = a.x;
-        K = a.y;
-        Px = b.x;
-        Py = b.y;
-        Pz = c.x;
+        PrimVals v;
+        v.p = a.x;
+        v.K = a.y;
+        v.Px = b.x;
+        v.Py = b.y;
+        v.Pz = c.x;
+        v.h = c.y;
+        return v;
     }
 };
 

@@ -392,6 +392,11 @@ int gtf_pfock_class_stats(PFock_t pf, int *X, int *Y, double *ms, double *nquart
     return gtf_fock_class_stats(pf->dev, X, Y, ms, nquart);
 }
 
+int gtf_pfock_class_work(PFock_t pf, double *flops, double *nprimq)
+{
+    return gtf_fock_class_work(pf->dev, flops, nprimq);
+}
+
 PFockStatus_t gtf_pfock_set_precision(PFock_t pf, int mode, double fp32_cutoff)
 {
     return map_err(gtf_fock_set_precision(pf->dev, mode, fp32_cutoff));

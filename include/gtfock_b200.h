@@ -38,6 +38,10 @@ PFockStatus_t gtf_pfock_timing(PFock_t pfock, double *ms_total, double *ms_eri,
  * ms of each class kernel and its quartet count.  Returns the pair count. */
 int gtf_pfock_class_stats(PFock_t pfock, int *X, int *Y, double *ms, double *nquart);
 
+/* Per class pair (same order): Rys-model FLOPs of one build and the number of
+ * primitive quartets before primitive screening.  Returns the pair count. */
+int gtf_pfock_class_work(PFock_t pfock, double *flops, double *nprimq);
+
 /* Precision of the ERI kernels: 0 = FP64 (default), 1 = FP32 for quartets
  * whose Schwarz bound sqrt(v1 v2) is below fp32_cutoff (Rys roots, 2-D
  * integrals and the primitive sum in FP32; D, the J/K digestion and every
