@@ -71,8 +71,20 @@ __host__ __device__ constexpr int fock_slice(int LA, int LB, int LC, int LD, int
 // kernel holds the code of a single slice, which keeps the instruction
 // footprint of the d-class kernels small.  The Rys table block of this class
 // (NR roots, precision R) is staged in shared memory by every block.
+// Blocks per SM the register allocation must allow: small quartets run
+// latency-bound dependency chains (Rys polynomial, recurrences), so more
+// resident warps pay off more than the registers they give up.
+__host__ __device__ constexpr int fock_min_blocks(int LA, int LB, int LC, int LD, int slice)
+{
+    const int nq = ncart(LA) * ncart(LB) * slice;
+    return nq <= 3 ? 6 : nq <= 9 ? 4 : nq <= 27 ? 3 : 2;
+}
+
 template <int LA, int LB, int LC, int LD, typename R, int CD0>
-__global__ void __launch_bounds__(FOCK_THREADS) k_fock(const FockLaunch a)
+__global__ void __launch_bounds__(FOCK_THREADS,
+                                  fock_min_blocks(LA, LB, LC, LD,
+                                                  fock_slice(LA, LB, LC, LD, sizeof(R) == 4 ? 1 : 0)))
+    k_fock(const FockLaunch a)
 {
     constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
     constexpr int NCD = ncart(LC) * ncart(LD);
