@@ -102,6 +102,16 @@ def load():
     _sig(L, "gtf_scf_get_density", [_vp, _dp])
     _sig(L, "gtf_scf_destroy", [_vp], None)
     _sig(L, "gtf_launch_count", [], ctypes.c_ulonglong)
+    _sig(L, "gtf_batch_create", [_i], _vp)
+    _sig(L, "gtf_batch_add", [_vp, _cp, _cp, _d, _i, _d, _i, _d])
+    _sig(L, "gtf_batch_step", [_vp])
+    _sig(L, "gtf_batch_run", [_vp])
+    _sig(L, "gtf_batch_result", [_vp, _i, _dp, _ip, _ip])
+    _sig(L, "gtf_batch_density", [_vp, _i, _dp])
+    _sig(L, "gtf_batch_remove", [_vp, _i])
+    _sig(L, "gtf_batch_info", [_vp, _ip, _ip, _dp, _dp, ctypes.POINTER(ctypes.c_size_t)])
+    _sig(L, "gtf_batch_job_bytes", [_i], ctypes.c_size_t)
+    _sig(L, "gtf_batch_destroy", [_vp], None)
     _sig(L, "gtf_fp64_peak", [_dp])
     _sig(L, "gtf_device_info", [_ip, _ip])
     _lib = L
@@ -377,6 +387,81 @@ class SCFSolver:
     def close(self):
         if getattr(self, "h", None) and _lib is not None:
             _lib.gtf_scf_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+
+class Batch:
+    """Many SCF jobs iterated in lock-step on one GPU (gtf_batch_*).
+
+    add() sets a job up in a free slot and returns the slot; step() runs one
+    SCF iteration of every running job and returns how many still run;
+    result(slot) gives (energies, done).  Jobs may be added and removed
+    between steps (continuous batching)."""
+
+    def __init__(self, capacity):
+        self.h = load().gtf_batch_create(capacity)
+        if not self.h:
+            raise GtfError("gtf_batch_create failed")
+        self.capacity = capacity
+        self.max_iters = {}
+
+    def add(self, gbs, xyz, tolscr=1e-10, precision=0, fp32_cutoff=0.0, max_iters=30, etol=1e-11):
+        slot = load().gtf_batch_add(self.h, gbs.encode(), xyz.encode(), tolscr, precision, fp32_cutoff,
+                                    max_iters, etol)
+        if slot < 0:
+            raise GtfError("gtf_batch_add failed (%d)" % slot)
+        self.max_iters[slot] = max_iters
+        return slot
+
+    def step(self):
+        r = load().gtf_batch_step(self.h)
+        if r < 0:
+            raise GtfError("gtf_batch_step failed (%d)" % r)
+        return r
+
+    def run(self):
+        r = load().gtf_batch_run(self.h)
+        if r < 0:
+            raise GtfError("gtf_batch_run failed (%d)" % r)
+
+    def result(self, slot):
+        e = np.zeros(self.max_iters[slot])
+        n = ctypes.c_int()
+        done = ctypes.c_int()
+        r = load().gtf_batch_result(self.h, slot, _dptr(e), ctypes.byref(n), ctypes.byref(done))
+        if r != 0:
+            raise GtfError("gtf_batch_result failed (%d)" % r)
+        return e[:n.value].copy(), bool(done.value)
+
+    def density(self, slot, nbf):
+        D = np.zeros((nbf, nbf))
+        if load().gtf_batch_density(self.h, slot, _dptr(D)) != 0:
+            raise GtfError("gtf_batch_density failed")
+        return D
+
+    def remove(self, slot):
+        if load().gtf_batch_remove(self.h, slot) != 0:
+            raise GtfError("gtf_batch_remove failed")
+        self.max_iters.pop(slot, None)
+
+    def info(self):
+        r, u = ctypes.c_int(), ctypes.c_int()
+        mf, mr = ctypes.c_double(), ctypes.c_double()
+        by = ctypes.c_size_t()
+        load().gtf_batch_info(self.h, ctypes.byref(r), ctypes.byref(u), ctypes.byref(mf), ctypes.byref(mr),
+                              ctypes.byref(by))
+        return {"running": r.value, "used": u.value, "ms_fock": mf.value, "ms_rest": mr.value,
+                "device_bytes": by.value}
+
+    @staticmethod
+    def job_bytes(nbf):
+        return int(load().gtf_batch_job_bytes(nbf))
+
+    def close(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.gtf_batch_destroy(self.h)
             self.h = None
 
     __del__ = close

@@ -1,0 +1,859 @@
+// batch_scf.cu -- many SCF jobs (molecules of different sizes) iterated in
+// lock-step on one GPU.
+//
+// Every step runs one SCF iteration (pscf/scf.c:348-459) of every running
+// job: one batched Fock build (one launch per class pair, precision part and
+// slice for all jobs, gtf_fock_batch_compute), the energy of
+// pscf/scf.c:80-102, DIIS (pscf/purif.c:491-641) and canonical purification
+// (pscf/purif.c:257-488), each as a few launches that cover all jobs.  The
+// dense products are batched tiled DGEMMs over per-job descriptors; the
+// reductions (energy, DIIS dots, purification traces and norms) use one block
+// per job in a fixed order, so a job's numbers do not depend on its
+// neighbours.  The DIIS bookkeeping (bordered matrix, replacement of the
+// vector with the largest error, the small solve) stays on the host as in the
+// single-job path.
+//
+// Jobs may join (gtf_batch_add) and leave (gtf_batch_remove) between steps:
+// the serving loop admits a request as soon as a slot and device memory are
+// free, and its iterations then interleave with those of the jobs already
+// running.
+#include <cuda_runtime.h>
+#include <float.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "gtf_cuda.h"
+#include "gtfock_b200.h"
+
+extern "C" gtf_fock_dev_t *gtf_pfock_device(PFock_t pf);
+extern "C" int gtf_initial_density(BasisSet_t basis, double *D, int n);
+extern "C" void gtf_note_launches(int n);
+extern "C" const char *gtf_last_error(void);
+
+#define BJ_MAX_DIIS 10
+#define BJ_THREADS 256
+#define BJ_TILE 64
+#define BJ_KT 16
+#define BJ_PUR_MAX 200
+#define BJ_PUR_CHECK 8
+
+// ---------------------------------------------------------------------------
+// device side
+// ---------------------------------------------------------------------------
+struct JobDev {
+    double *D, *F;                 // engine density (AO, input of the Fock build) and Fock matrix
+    const double *H, *S, *X;
+    double *P, *P2, *P3, *W, *W2;  // purification (orthogonal basis) and scratch
+    double *vecs, *Fvecs;          // DIIS error vectors and Fock matrices
+    int n, nocc;
+    int cur;                       // DIIS slot of this iteration (-1: no DIIS)
+    int len;                       // DIIS vectors in use
+};
+
+struct GemmDesc {
+    const double *A, *B;
+    double *C;
+    int n;
+    int job;                       // index into the active flags (-1: always)
+};
+
+// C = A B^T (TB) or C = A B, row-major n x n.  Block t of the launch is tile
+// (ti, tj) of descriptor d, found in the exclusive tile prefix.
+template <bool TB>
+__global__ void __launch_bounds__(BJ_THREADS) k_bgemm(const GemmDesc *__restrict__ ds,
+                                                     const int *__restrict__ tile_prefix, int nd,
+                                                     const int *__restrict__ active)
+{
+    __shared__ double As[BJ_KT][BJ_TILE];
+    __shared__ double Bs[BJ_KT][BJ_TILE];
+    const int t = blockIdx.x;
+    int lo = 0, hi = nd;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (tile_prefix[mid] <= t) lo = mid;
+        else hi = mid;
+    }
+    const GemmDesc g = ds[lo];
+    if (g.job >= 0 && active && !active[g.job]) return;
+    const int n = g.n;
+    const int nt = (n + BJ_TILE - 1) / BJ_TILE;
+    const int local = t - tile_prefix[lo];
+    const int r0 = (local / nt) * BJ_TILE, c0 = (local % nt) * BJ_TILE;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    double acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
+    for (int k0 = 0; k0 < n; k0 += BJ_KT) {
+        // 64 x 16 tiles of A (rows r0..) and of op(B) (columns c0..)
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int e = threadIdx.x + q * BJ_THREADS;  // 0..1023
+            const int kk = e & 15, rr = e >> 4;
+            const int ar = r0 + rr, ak = k0 + kk;
+            As[kk][rr] = (ar < n && ak < n) ? g.A[(size_t)ar * n + ak] : 0.0;
+            if (TB) {
+                const int bc = c0 + rr;
+                Bs[kk][rr] = (bc < n && ak < n) ? g.B[(size_t)bc * n + ak] : 0.0;
+            } else {
+                const int bk = k0 + (e >> 6), bc = c0 + (e & 63);
+                Bs[e >> 6][e & 63] = (bk < n && bc < n) ? g.B[(size_t)bk * n + bc] : 0.0;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < BJ_KT; kk++) {
+            double a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) a[i] = As[kk][ty * 4 + i];
+#pragma unroll
+            for (int j = 0; j < 4; j++) b[j] = Bs[kk][tx * 4 + j];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int r = r0 + ty * 4 + i;
+        if (r >= n) continue;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int c = c0 + tx * 4 + j;
+            if (c < n) g.C[(size_t)r * n + c] = acc[i][j];
+        }
+    }
+}
+
+__device__ __forceinline__ double block_sum(double v, double *sh)
+{
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int s = BJ_THREADS / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    const double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+// job blockIdx.x: F += H, energy = sum D (H + F) (pscf/scf.c:80-102)
+__global__ void __launch_bounds__(BJ_THREADS) k_j_energy(const JobDev *__restrict__ jobs, double *__restrict__ energy)
+{
+    __shared__ double sh[BJ_THREADS];
+    const JobDev j = jobs[blockIdx.x];
+    const size_t nn = (size_t)j.n * j.n;
+    double e = 0.0;
+    for (size_t k = threadIdx.x; k < nn; k += BJ_THREADS) {
+        const double f = j.F[k] + j.H[k];
+        j.F[k] = f;
+        e += j.D[k] * (j.H[k] + f);
+    }
+    e = block_sum(e, sh);
+    if (threadIdx.x == 0) energy[blockIdx.x] = e;
+}
+
+// cur = W2 - W2^T into the DIIS slot (pscf/purif.c:553-558); jobs with cur < 0 skip
+__global__ void k_j_antisym(const JobDev *__restrict__ jobs)
+{
+    const JobDev j = jobs[blockIdx.y];
+    if (j.cur < 0) return;
+    const size_t nn = (size_t)j.n * j.n;
+    double *cur = j.vecs + nn * j.cur;
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += (size_t)gridDim.x * blockDim.x) {
+        const int r = (int)(k / j.n), c = (int)(k % j.n);
+        cur[k] = j.W2[k] - j.W2[(size_t)c * j.n + r];
+    }
+}
+
+// dots[job][i] = <vecs[cur], vecs[i]>, i < len
+__global__ void __launch_bounds__(BJ_THREADS) k_j_dots(const JobDev *__restrict__ jobs, double *__restrict__ dots)
+{
+    __shared__ double sh[BJ_THREADS];
+    const JobDev j = jobs[blockIdx.x];
+    if (j.cur < 0) return;
+    const size_t nn = (size_t)j.n * j.n;
+    const double *a = j.vecs + nn * j.cur;
+    for (int i = 0; i < j.len; i++) {
+        const double *b = j.vecs + nn * i;
+        double v = 0.0;
+        for (size_t k = threadIdx.x; k < nn; k += BJ_THREADS) v += a[k] * b[k];
+        v = block_sum(v, sh);
+        if (threadIdx.x == 0) dots[blockIdx.x * BJ_MAX_DIIS + i] = v;
+    }
+}
+
+// F = sum_i c_i Fvecs_i
+__global__ void k_j_combine(const JobDev *__restrict__ jobs, const double *__restrict__ coef)
+{
+    const JobDev j = jobs[blockIdx.y];
+    if (j.cur < 0) return;
+    const size_t nn = (size_t)j.n * j.n;
+    const double *c = coef + blockIdx.y * BJ_MAX_DIIS;
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += (size_t)gridDim.x * blockDim.x) {
+        double v = 0.0;
+        for (int i = 0; i < j.len; i++) v += c[i] * j.Fvecs[nn * i + k];
+        j.F[k] = v;
+    }
+}
+
+// Gershgorin bounds and trace of F (orthogonal basis), initial P
+// (pscf/purif.c:309-373); scal[job*8 + 0..1] hold the two coefficients
+__global__ void __launch_bounds__(BJ_THREADS) k_j_pur_init(const JobDev *__restrict__ jobs, double *__restrict__ scal,
+                                                          int *__restrict__ active)
+{
+    __shared__ double sh[BJ_THREADS];
+    __shared__ double c01[2];
+    const JobDev j = jobs[blockIdx.x];
+    const int n = j.n;
+    double lmin = DBL_MAX, lmax = -DBL_MAX, ltr = 0.0;
+    for (int i = threadIdx.x; i < n; i += BJ_THREADS) {
+        double off = 0.0, dg = 0.0;
+        for (int r = 0; r < n; r++) {
+            const double v = j.F[(size_t)r * n + i];
+            off += fabs(v);
+            if (r == i) dg = v;
+        }
+        off -= fabs(dg);
+        lmin = fmin(lmin, dg - off);
+        lmax = fmax(lmax, dg + off);
+        ltr += dg;
+    }
+    // min / max / sum reductions in a fixed order
+    sh[threadIdx.x] = lmin;
+    __syncthreads();
+    for (int s = BJ_THREADS / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] = fmin(sh[threadIdx.x], sh[threadIdx.x + s]);
+        __syncthreads();
+    }
+    const double hmin = sh[0];
+    __syncthreads();
+    sh[threadIdx.x] = lmax;
+    __syncthreads();
+    for (int s = BJ_THREADS / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + s]);
+        __syncthreads();
+    }
+    const double hmax = sh[0];
+    __syncthreads();
+    const double trF = block_sum(ltr, sh);
+    if (threadIdx.x == 0) {
+        const double mu_bar = trF / (double)n;
+        const double lambda = fmin((double)j.nocc / (hmax - mu_bar), (double)(n - j.nocc) / (mu_bar - hmin));
+        c01[0] = -lambda / n;
+        c01[1] = lambda * mu_bar / (double)n + (double)j.nocc / n;
+        scal[blockIdx.x * 8 + 0] = c01[0];
+        scal[blockIdx.x * 8 + 1] = c01[1];
+        active[blockIdx.x] = 1;
+    }
+    __syncthreads();
+    const size_t nn = (size_t)n * n;
+    for (size_t k = threadIdx.x; k < nn; k += BJ_THREADS) {
+        double v = j.F[k] * c01[0];
+        if (k / n == k % n) v += c01[1];
+        j.P[k] = v;
+    }
+}
+
+// ||P - P2||_F, c = tr(P2 - P3) / tr(P - P2), then the trace-conserving
+// update (pscf/purif.c:394-455); a job stops once ||P - P2||_F < 1e-11
+__global__ void __launch_bounds__(BJ_THREADS) k_j_pur_step(const JobDev *__restrict__ jobs, double *__restrict__ scal,
+                                                          int *__restrict__ active, int *__restrict__ iters)
+{
+    __shared__ double sh[BJ_THREADS];
+    if (!active[blockIdx.x]) return;
+    const JobDev j = jobs[blockIdx.x];
+    const int n = j.n;
+    const size_t nn = (size_t)n * n;
+    double e = 0.0, t = 0.0, t2 = 0.0;
+    for (size_t k = threadIdx.x; k < nn; k += BJ_THREADS) {
+        const double d = j.P[k] - j.P2[k];
+        e += d * d;
+    }
+    for (int i = threadIdx.x; i < n; i += BJ_THREADS) {
+        const size_t k = (size_t)i * n + i;
+        t += j.P2[k] - j.P3[k];
+        t2 += j.P[k] - j.P2[k];
+    }
+    e = block_sum(e, sh);
+    t = block_sum(t, sh);
+    t2 = block_sum(t2, sh);
+    const double err = sqrt(e), c = t / t2;
+    for (size_t k = threadIdx.x; k < nn; k += BJ_THREADS) {
+        if (c < 0.5) j.P[k] = ((1.0 - 2.0 * c) * j.P[k] + (1.0 + c) * j.P2[k] - j.P3[k]) / (1.0 - c);
+        else j.P[k] = ((1.0 + c) * j.P2[k] - j.P3[k]) / c;
+    }
+    if (threadIdx.x == 0) {
+        scal[blockIdx.x * 8 + 2] = err;
+        iters[blockIdx.x] += 1;
+        if (err < 1e-11) active[blockIdx.x] = 0;
+    }
+}
+
+__global__ void k_j_count(const int *__restrict__ active, int m, int *__restrict__ out)
+{
+    __shared__ int sh[BJ_THREADS];
+    int c = 0;
+    for (int i = threadIdx.x; i < m; i += BJ_THREADS) c += active[i];
+    sh[threadIdx.x] = c;
+    __syncthreads();
+    for (int s = BJ_THREADS / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = sh[0];
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+struct BJob {
+    int used;
+    int n, nocc, nbf_cart;
+    double enuc;
+    BasisSet_t basis;
+    PFock_t pf;
+    gtf_fock_dev_t *eng;
+    double *mem;
+    size_t bytes;
+    JobDev dv;
+    // SCF state
+    int iter, max_iters, done, failed;
+    double etol, e_prev;
+    std::vector<double> energies;
+    // DIIS state (pscf/purif.c:491-641)
+    int len_diis, bmax_id;
+    double bmax;
+    double b[BJ_MAX_DIIS + 1][BJ_MAX_DIIS + 1];
+    int pur_iters;
+};
+
+struct gtf_batch {
+    int capacity;
+    std::vector<BJob> jobs;
+    cudaStream_t st;
+    gtf_fock_batch_t *fb;
+    std::vector<int> fb_members;   // slots in the current Fock batch
+    int dirty;
+    // device arrays (capacity-sized)
+    JobDev *d_jobs;
+    GemmDesc *d_gd;                // 10 call sets x capacity
+    int *d_tp;                     // 10 call sets x (capacity + 1)
+    double *d_energy, *d_dots, *d_coef, *d_scal;
+    int *d_active, *d_iters, *d_count;
+    // pinned mirrors
+    JobDev *h_jobs;
+    GemmDesc *h_gd;
+    int *h_tp;
+    double *h_energy, *h_dots, *h_coef;
+    int *h_iters, *h_count;
+    size_t dev_bytes_jobs;
+    double ms_fock, ms_rest;
+    cudaEvent_t e0, e1, e2;
+};
+
+#define CKH(call)                                                                          \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess) {                                                           \
+            fprintf(stderr, "gtfock_b200 batch %s:%d %s\n", __FILE__, __LINE__, cudaGetErrorString(e_)); \
+            return GTF_ERR_CUDA;                                                           \
+        }                                                                                  \
+    } while (0)
+
+static const int NSETS = 10;
+
+// device bytes of one job's batch buffers (beyond its Fock engine)
+static size_t job_buffer_bytes(int n) { return sizeof(double) * (size_t)n * n * (5 + 2 * BJ_MAX_DIIS); }
+
+extern "C" size_t gtf_batch_job_bytes(int nbf) { return job_buffer_bytes(nbf); }
+
+static void job_free(BJob &j)
+{
+    if (j.mem) cudaFree(j.mem);
+    if (j.pf) {
+        PFock_destroyOvlMat(j.pf);
+        PFock_destroyCoreHMat(j.pf);
+        PFock_destroy(j.pf);
+    }
+    if (j.basis) CInt_destroyBasisSet(j.basis);
+    j = BJob();
+}
+
+extern "C" void gtf_batch_destroy(gtf_batch_t *b)
+{
+    if (!b) return;
+    cudaStreamSynchronize(b->st);
+    if (b->fb) gtf_fock_batch_destroy(b->fb);
+    for (auto &j : b->jobs)
+        if (j.used) job_free(j);
+    void *dp[] = {b->d_jobs, b->d_gd, b->d_tp, b->d_energy, b->d_dots, b->d_coef, b->d_scal, b->d_active,
+                  b->d_iters, b->d_count};
+    for (void *p : dp)
+        if (p) cudaFree(p);
+    void *hp[] = {b->h_jobs, b->h_gd, b->h_tp, b->h_energy, b->h_dots, b->h_coef, b->h_iters, b->h_count};
+    for (void *p : hp)
+        if (p) cudaFreeHost(p);
+    cudaEventDestroy(b->e0);
+    cudaEventDestroy(b->e1);
+    cudaEventDestroy(b->e2);
+    cudaStreamDestroy(b->st);
+    delete b;
+}
+
+extern "C" gtf_batch_t *gtf_batch_create(int capacity)
+{
+    if (capacity <= 0) return nullptr;
+    gtf_batch *b = new gtf_batch();
+    b->capacity = capacity;
+    b->jobs.resize(capacity);
+    b->fb = nullptr;
+    b->dirty = 1;
+    b->ms_fock = b->ms_rest = 0.0;
+    bool ok = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) == cudaSuccess;
+    ok = ok && cudaEventCreate(&b->e0) == cudaSuccess && cudaEventCreate(&b->e1) == cudaSuccess &&
+         cudaEventCreate(&b->e2) == cudaSuccess;
+    const size_t C = capacity;
+    ok = ok && cudaMalloc(&b->d_jobs, sizeof(JobDev) * C) == cudaSuccess;
+    ok = ok && cudaMalloc(&b->d_gd, sizeof(GemmDesc) * C * NSETS) == cudaSuccess;
+    ok = ok && cudaMalloc(&b->d_tp, sizeof(int) * (C + 1) * NSETS) == cudaSuccess;
+    ok = ok && cudaMalloc(&b->d_energy, sizeof(double) * C) == cudaSuccess;
+    ok = ok && cudaMalloc(&b->d_dots, sizeof(double) * C * BJ_MAX_DIIS) == cudaSuccess;
+    ok = ok && cudaMalloc(&b->d_coef, sizeof(double) * C * BJ_MAX_DIIS) == cudaSuccess;
+    ok = ok && cudaMalloc(&b->d_scal, sizeof(double) * C * 8) == cudaSuccess;
+    ok = ok && cudaMalloc(&b->d_active, sizeof(int) * C) == cudaSuccess;
+    ok = ok && cudaMalloc(&b->d_iters, sizeof(int) * C) == cudaSuccess;
+    ok = ok && cudaMalloc(&b->d_count, sizeof(int)) == cudaSuccess;
+    ok = ok && cudaMallocHost(&b->h_jobs, sizeof(JobDev) * C) == cudaSuccess;
+    ok = ok && cudaMallocHost(&b->h_gd, sizeof(GemmDesc) * C * NSETS) == cudaSuccess;
+    ok = ok && cudaMallocHost(&b->h_tp, sizeof(int) * (C + 1) * NSETS) == cudaSuccess;
+    ok = ok && cudaMallocHost(&b->h_energy, sizeof(double) * C) == cudaSuccess;
+    ok = ok && cudaMallocHost(&b->h_dots, sizeof(double) * C * BJ_MAX_DIIS) == cudaSuccess;
+    ok = ok && cudaMallocHost(&b->h_coef, sizeof(double) * C * BJ_MAX_DIIS) == cudaSuccess;
+    ok = ok && cudaMallocHost(&b->h_iters, sizeof(int) * C) == cudaSuccess;
+    ok = ok && cudaMallocHost(&b->h_count, sizeof(int)) == cudaSuccess;
+    if (!ok) {
+        fprintf(stderr, "gtfock_b200: batch allocation failed\n");
+        gtf_batch_destroy(b);
+        return nullptr;
+    }
+    return b;
+}
+
+static void diis_reset(BJob &j)
+{
+    j.len_diis = 0;
+    j.bmax = DBL_MIN;
+    j.bmax_id = -1;
+    for (int r = 0; r <= BJ_MAX_DIIS; r++)
+        for (int c = 0; c <= BJ_MAX_DIIS; c++) j.b[r][c] = (r != c) ? -1.0 : 0.0;
+}
+
+// Set-up of one SCF job (pscf/scf.c:298-314, init_oedmat pscf/scf.c:131-185)
+// in a free slot; returns the slot or a negative error.
+extern "C" int gtf_batch_add(gtf_batch_t *b, const char *bsfile, const char *xyzfile, double tolscr, int prec_mode,
+                             double fp32_cutoff, int max_iters, double etol)
+{
+    if (!b || !bsfile || !xyzfile || max_iters <= 0 || !(etol >= 0.0)) return -1;
+    int slot = -1;
+    for (int s = 0; s < b->capacity; s++)
+        if (!b->jobs[s].used) {
+            slot = s;
+            break;
+        }
+    if (slot < 0) return -2;
+    BJob &j = b->jobs[slot];
+    j = BJob();
+    if (CInt_createBasisSet(&j.basis) != CINT_STATUS_SUCCESS ||
+        CInt_loadBasisSet(j.basis, (char *)bsfile, (char *)xyzfile) != CINT_STATUS_SUCCESS) {
+        if (j.basis) CInt_destroyBasisSet(j.basis);
+        j = BJob();
+        return -3;
+    }
+    j.n = CInt_getNumFuncs(j.basis);
+    j.nocc = CInt_getNumOccOrb(j.basis);
+    j.enuc = CInt_getNucEnergy(j.basis);
+    if (PFock_create(j.basis, 1, 1, 4, tolscr, 1, 1, &j.pf) != PFOCK_STATUS_SUCCESS) {
+        j.pf = nullptr;
+        job_free(j);
+        return -4;
+    }
+    j.used = 1;
+    j.eng = gtf_pfock_device(j.pf);
+    if ((prec_mode != 0 && gtf_pfock_set_precision(j.pf, prec_mode, fp32_cutoff) != PFOCK_STATUS_SUCCESS) ||
+        PFock_createOvlMat(j.pf, j.basis) != PFOCK_STATUS_SUCCESS ||
+        PFock_createCoreHMat(j.pf, j.basis) != PFOCK_STATUS_SUCCESS) {
+        job_free(j);
+        return -5;
+    }
+    const size_t nn = (size_t)j.n * j.n;
+    j.bytes = job_buffer_bytes(j.n);
+    if (cudaMalloc(&j.mem, j.bytes) != cudaSuccess) {
+        j.mem = nullptr;
+        job_free(j);
+        return -6;
+    }
+    JobDev &d = j.dv;
+    d.D = const_cast<double *>(gtf_fock_mat_dev(j.eng, 0, 0));
+    d.F = const_cast<double *>(gtf_fock_mat_dev(j.eng, 1, 0));
+    d.S = gtf_fock_onee_dev(j.eng, 0);
+    d.X = gtf_fock_onee_dev(j.eng, 1);
+    d.H = gtf_fock_onee_dev(j.eng, 2);
+    d.P = j.mem;
+    d.P2 = d.P + nn;
+    d.P3 = d.P2 + nn;
+    d.W = d.P3 + nn;
+    d.W2 = d.W + nn;
+    d.vecs = d.W2 + nn;
+    d.Fvecs = d.vecs + nn * BJ_MAX_DIIS;
+    d.n = j.n;
+    d.nocc = j.nocc;
+    d.cur = -1;
+    d.len = 0;
+    // initial guess (pscf/scf.c:34-76) into the engine's density buffer
+    std::vector<double> D0(nn);
+    gtf_initial_density(j.basis, D0.data(), j.n);
+    if (cudaMemcpy(d.D, D0.data(), sizeof(double) * nn, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaDeviceSynchronize() != cudaSuccess) {
+        job_free(j);
+        return -7;
+    }
+    j.iter = 0;
+    j.max_iters = max_iters;
+    j.etol = etol;
+    j.e_prev = 0.0;
+    j.done = 0;
+    j.failed = 0;
+    diis_reset(j);
+    b->dirty = 1;
+    return slot;
+}
+
+extern "C" int gtf_batch_remove(gtf_batch_t *b, int slot)
+{
+    if (!b || slot < 0 || slot >= b->capacity || !b->jobs[slot].used) return -1;
+    cudaStreamSynchronize(b->st);
+    job_free(b->jobs[slot]);
+    b->dirty = 1;
+    return 0;
+}
+
+extern "C" int gtf_batch_result(gtf_batch_t *b, int slot, double *energies, int *niters, int *done)
+{
+    if (!b || slot < 0 || slot >= b->capacity || !b->jobs[slot].used) return -1;
+    const BJob &j = b->jobs[slot];
+    if (energies)
+        for (size_t k = 0; k < j.energies.size(); k++) energies[k] = j.energies[k];
+    if (niters) *niters = (int)j.energies.size();
+    if (done) *done = j.done;
+    return j.failed ? -2 : 0;
+}
+
+extern "C" int gtf_batch_density(gtf_batch_t *b, int slot, double *D)
+{
+    if (!b || slot < 0 || slot >= b->capacity || !b->jobs[slot].used || !D) return -1;
+    CKH(cudaStreamSynchronize(b->st));
+    const BJob &j = b->jobs[slot];
+    CKH(cudaMemcpy(D, j.dv.D, sizeof(double) * j.n * j.n, cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+// one call set of batched GEMMs: descriptors of set `s` for `m` jobs
+static int run_gemm(gtf_batch *b, int s, int m, bool tb, const int *active, int *launches)
+{
+    if (m == 0) return GTF_OK;
+    const int ntiles = b->h_tp[s * (b->capacity + 1) + m];
+    if (ntiles == 0) return GTF_OK;
+    const GemmDesc *gd = b->d_gd + (size_t)s * b->capacity;
+    const int *tp = b->d_tp + (size_t)s * (b->capacity + 1);
+    if (tb) k_bgemm<true><<<ntiles, BJ_THREADS, 0, b->st>>>(gd, tp, m, active);
+    else k_bgemm<false><<<ntiles, BJ_THREADS, 0, b->st>>>(gd, tp, m, active);
+    CKH(cudaGetLastError());
+    (*launches)++;
+    return GTF_OK;
+}
+
+static void set_gemm(gtf_batch *b, int s, int k, const double *A, const double *B, double *C, int n, int job)
+{
+    GemmDesc &g = b->h_gd[(size_t)s * b->capacity + k];
+    g.A = A;
+    g.B = B;
+    g.C = C;
+    g.n = n;
+    g.job = job;
+    const int nt = (n + BJ_TILE - 1) / BJ_TILE;
+    int *tp = b->h_tp + (size_t)s * (b->capacity + 1);
+    if (k == 0) tp[0] = 0;
+    tp[k + 1] = tp[k] + nt * nt;
+}
+
+// inverse of the bordered DIIS matrix by Gauss-Jordan with partial pivoting;
+// coeffs[i] = -inv[i][m] (as the single-job path)
+static void diis_coeffs(const double (&bm)[BJ_MAX_DIIS + 1][BJ_MAX_DIIS + 1], int m, double *coeffs)
+{
+    const int s = m + 1;
+    double a[BJ_MAX_DIIS + 1][2 * (BJ_MAX_DIIS + 1)];
+    for (int i = 0; i < s; i++)
+        for (int j = 0; j < s; j++) {
+            a[i][j] = bm[i][j];
+            a[i][s + j] = (i == j) ? 1.0 : 0.0;
+        }
+    for (int c = 0; c < s; c++) {
+        int piv = c;
+        for (int r = c + 1; r < s; r++)
+            if (fabs(a[r][c]) > fabs(a[piv][c])) piv = r;
+        if (piv != c)
+            for (int j = 0; j < 2 * s; j++) {
+                const double t = a[c][j];
+                a[c][j] = a[piv][j];
+                a[piv][j] = t;
+            }
+        const double d = a[c][c];
+        for (int j = 0; j < 2 * s; j++) a[c][j] /= d;
+        for (int r = 0; r < s; r++) {
+            if (r == c) continue;
+            const double f = a[r][c];
+            if (f == 0.0) continue;
+            for (int j = 0; j < 2 * s; j++) a[r][j] -= f * a[c][j];
+        }
+    }
+    for (int i = 0; i < s; i++) coeffs[i] = -a[i][s + s - 1];
+}
+
+// The bordered matrix lives in the top-left (len+1) x (len+1) block with the
+// border in row/column len (pscf/purif.c:600-620).  The single-job path keeps
+// it the same way: entries b[i][j] for i, j < len are error dot products,
+// the rest -1 off the diagonal and 0 on it.
+static void diis_update(BJob &j, int cur_idx, const double *dots)
+{
+    for (int i = 0; i < j.len_diis; i++) j.b[cur_idx][i] = dots[i];
+    j.bmax = -DBL_MAX;
+    for (int i = 0; i < j.len_diis; i++) {
+        j.b[i][cur_idx] = j.b[cur_idx][i];
+        if (j.bmax < j.b[i][i]) {
+            j.bmax = j.b[i][i];
+            j.bmax_id = i;
+        }
+    }
+}
+
+// One SCF iteration of every running job.  Returns the number of jobs still
+// running afterwards, or a negative error.
+extern "C" int gtf_batch_step(gtf_batch_t *b)
+{
+    if (!b) return -1;
+    std::vector<int> run;
+    for (int s = 0; s < b->capacity; s++)
+        if (b->jobs[s].used && !b->jobs[s].done) run.push_back(s);
+    if (run.empty()) return 0;
+    int launches = 0;
+    // ---- Fock build of every running job ----
+    if (b->dirty || run != b->fb_members) {
+        if (b->fb) gtf_fock_batch_destroy(b->fb);
+        b->fb = nullptr;
+        std::vector<gtf_fock_dev_t *> eng;
+        for (int s : run) eng.push_back(b->jobs[s].eng);
+        if (gtf_fock_batch_create(eng.data(), (int)eng.size(), b->st, &b->fb) != GTF_OK) {
+            fprintf(stderr, "gtfock_b200: batched Fock set-up failed: %s\n", gtf_last_error());
+            return -2;
+        }
+        b->fb_members = run;
+        b->dirty = 0;
+    }
+    CKH(cudaEventRecord(b->e0, b->st));
+    if (gtf_fock_batch_compute(b->fb) < 0) {
+        fprintf(stderr, "gtfock_b200: batched Fock build failed: %s\n", gtf_last_error());
+        return -3;
+    }
+    CKH(cudaEventRecord(b->e1, b->st));
+    // ---- energies (pscf/scf.c:80-102, 339-375) ----
+    const int M = (int)run.size();
+    for (int k = 0; k < M; k++) {
+        BJob &j = b->jobs[run[k]];
+        j.dv.cur = -1;
+        j.dv.len = j.len_diis;
+        b->h_jobs[k] = j.dv;
+    }
+    CKH(cudaMemcpyAsync(b->d_jobs, b->h_jobs, sizeof(JobDev) * M, cudaMemcpyHostToDevice, b->st));
+    k_j_energy<<<M, BJ_THREADS, 0, b->st>>>(b->d_jobs, b->d_energy);
+    CKH(cudaGetLastError());
+    launches++;
+    CKH(cudaMemcpyAsync(b->h_energy, b->d_energy, sizeof(double) * M, cudaMemcpyDeviceToHost, b->st));
+    CKH(cudaStreamSynchronize(b->st));
+    // jobs that continue with DIIS + purification
+    std::vector<int> cont;   // indices into run
+    for (int k = 0; k < M; k++) {
+        BJob &j = b->jobs[run[k]];
+        const double e = b->h_energy[k];
+        j.energies.push_back(e + j.enuc);
+        const int it = j.iter++;
+        if ((it > 0 && fabs(e - j.e_prev) < j.etol) || j.iter >= j.max_iters) {
+            j.done = 1;
+            continue;
+        }
+        j.e_prev = e;
+        cont.push_back(k);
+    }
+    const int C = (int)cont.size();
+    if (C > 0) {
+        // ---- DIIS (pscf/purif.c:491-641) ----
+        // call sets: 0 W=F D^T, 1 W2=W S^T, 2 W=X cur^T, 3 cur=W X^T (DIIS jobs);
+        //            4 W=X F^T, 5 target=W X^T (all); 6 P2=P P^T, 7 P3=P P2,
+        //            8 W=X P^T, 9 D=W X^T (purification)
+        int nd = 0;
+        for (int q = 0; q < C; q++) {
+            BJob &j = b->jobs[run[cont[q]]];
+            JobDev &d = j.dv;
+            const int it = j.iter - 1;   // this iteration's index
+            const size_t nn = (size_t)j.n * j.n;
+            d.cur = -1;
+            double *target = d.F;
+            if (it > 1) {
+                int cur_idx;
+                if (j.len_diis < BJ_MAX_DIIS) {
+                    cur_idx = j.len_diis;
+                    j.len_diis++;
+                } else {
+                    cur_idx = j.bmax_id;
+                }
+                d.cur = cur_idx;
+                double *cur = d.vecs + nn * cur_idx;
+                target = d.Fvecs + nn * cur_idx;
+                set_gemm(b, 0, nd, d.F, d.D, d.W, j.n, -1);
+                set_gemm(b, 1, nd, d.W, d.S, d.W2, j.n, -1);
+                set_gemm(b, 2, nd, d.X, cur, d.W, j.n, -1);
+                set_gemm(b, 3, nd, d.W, d.X, cur, j.n, -1);
+                nd++;
+            }
+            d.len = j.len_diis;
+            set_gemm(b, 4, q, d.X, d.F, d.W, j.n, -1);
+            set_gemm(b, 5, q, d.W, d.X, target, j.n, -1);
+            set_gemm(b, 6, q, d.P, d.P, d.P2, j.n, q);
+            set_gemm(b, 7, q, d.P, d.P2, d.P3, j.n, q);
+            set_gemm(b, 8, q, d.X, d.P, d.W, j.n, -1);
+            set_gemm(b, 9, q, d.W, d.X, d.D, j.n, -1);
+            b->h_jobs[q] = d;
+        }
+        // DIIS-set descriptors come first in `cont` order: remap antisym /
+        // dots / combine through JobDev.cur (jobs without DIIS have cur < 0)
+        const size_t C1 = b->capacity + 1;
+        CKH(cudaMemcpyAsync(b->d_jobs, b->h_jobs, sizeof(JobDev) * C, cudaMemcpyHostToDevice, b->st));
+        CKH(cudaMemcpyAsync(b->d_gd, b->h_gd, sizeof(GemmDesc) * b->capacity * NSETS, cudaMemcpyHostToDevice, b->st));
+        CKH(cudaMemcpyAsync(b->d_tp, b->h_tp, sizeof(int) * C1 * NSETS, cudaMemcpyHostToDevice, b->st));
+        int maxn = 0;
+        for (int q = 0; q < C; q++) maxn = b->h_jobs[q].n > maxn ? b->h_jobs[q].n : maxn;
+        const unsigned ge = (unsigned)(((size_t)maxn * maxn + 255) / 256 < 1024 ? ((size_t)maxn * maxn + 255) / 256 : 1024);
+        if (nd > 0) {
+            if (run_gemm(b, 0, nd, true, nullptr, &launches) || run_gemm(b, 1, nd, true, nullptr, &launches))
+                return -4;
+            k_j_antisym<<<dim3(ge, C), 256, 0, b->st>>>(b->d_jobs);
+            CKH(cudaGetLastError());
+            launches++;
+            if (run_gemm(b, 2, nd, true, nullptr, &launches) || run_gemm(b, 3, nd, true, nullptr, &launches))
+                return -4;
+            k_j_dots<<<C, BJ_THREADS, 0, b->st>>>(b->d_jobs, b->d_dots);
+            CKH(cudaGetLastError());
+            launches++;
+            CKH(cudaMemcpyAsync(b->h_dots, b->d_dots, sizeof(double) * C * BJ_MAX_DIIS, cudaMemcpyDeviceToHost,
+                                b->st));
+        }
+        // F' = X F X^T (pscf/purif.c:620-636)
+        if (run_gemm(b, 4, C, true, nullptr, &launches) || run_gemm(b, 5, C, true, nullptr, &launches)) return -4;
+        if (nd > 0) {
+            CKH(cudaStreamSynchronize(b->st));
+            for (int q = 0; q < C; q++) {
+                BJob &j = b->jobs[run[cont[q]]];
+                const int cur_idx = b->h_jobs[q].cur;
+                double *co = b->h_coef + q * BJ_MAX_DIIS;
+                for (int i = 0; i < BJ_MAX_DIIS; i++) co[i] = 0.0;
+                if (cur_idx < 0) continue;
+                diis_update(j, cur_idx, b->h_dots + q * BJ_MAX_DIIS);
+                double cf[BJ_MAX_DIIS + 1];
+                // the bordered system: copy with the border at index len
+                double bm[BJ_MAX_DIIS + 1][BJ_MAX_DIIS + 1];
+                const int L = j.len_diis;
+                for (int r = 0; r <= L; r++)
+                    for (int c = 0; c <= L; c++)
+                        bm[r][c] = (r < L && c < L) ? j.b[r][c] : ((r == c) ? 0.0 : -1.0);
+                diis_coeffs(bm, L, cf);
+                for (int i = 0; i < L; i++) co[i] = cf[i];
+            }
+            CKH(cudaMemcpyAsync(b->d_coef, b->h_coef, sizeof(double) * C * BJ_MAX_DIIS, cudaMemcpyHostToDevice,
+                                b->st));
+            k_j_combine<<<dim3(ge, C), 256, 0, b->st>>>(b->d_jobs, b->d_coef);
+            CKH(cudaGetLastError());
+            launches++;
+        }
+        // ---- canonical purification (pscf/purif.c:257-488) ----
+        CKH(cudaMemsetAsync(b->d_iters, 0, sizeof(int) * C, b->st));
+        k_j_pur_init<<<C, BJ_THREADS, 0, b->st>>>(b->d_jobs, b->d_scal, b->d_active);
+        CKH(cudaGetLastError());
+        launches++;
+        for (int step = 0; step < BJ_PUR_MAX; step++) {
+            if (run_gemm(b, 6, C, true, b->d_active, &launches) || run_gemm(b, 7, C, false, b->d_active, &launches))
+                return -4;
+            k_j_pur_step<<<C, BJ_THREADS, 0, b->st>>>(b->d_jobs, b->d_scal, b->d_active, b->d_iters);
+            CKH(cudaGetLastError());
+            launches++;
+            if ((step + 1) % BJ_PUR_CHECK == 0) {
+                k_j_count<<<1, BJ_THREADS, 0, b->st>>>(b->d_active, C, b->d_count);
+                launches++;
+                CKH(cudaMemcpyAsync(b->h_count, b->d_count, sizeof(int), cudaMemcpyDeviceToHost, b->st));
+                CKH(cudaStreamSynchronize(b->st));
+                if (*b->h_count == 0) break;
+            }
+        }
+        // D_AO = X P X^T (pscf/purif.c:469-476), into the engine's density
+        if (run_gemm(b, 8, C, true, nullptr, &launches) || run_gemm(b, 9, C, true, nullptr, &launches)) return -4;
+        CKH(cudaMemcpyAsync(b->h_iters, b->d_iters, sizeof(int) * C, cudaMemcpyDeviceToHost, b->st));
+    }
+    CKH(cudaEventRecord(b->e2, b->st));
+    CKH(cudaStreamSynchronize(b->st));
+    for (int q = 0; q < C; q++) b->jobs[run[cont[q]]].pur_iters = b->h_iters[q];
+    float ms1 = 0.0f, ms2 = 0.0f;
+    cudaEventElapsedTime(&ms1, b->e0, b->e1);
+    cudaEventElapsedTime(&ms2, b->e1, b->e2);
+    b->ms_fock += ms1;
+    b->ms_rest += ms2;
+    gtf_note_launches(launches);
+    int left = 0;
+    for (int s = 0; s < b->capacity; s++)
+        if (b->jobs[s].used && !b->jobs[s].done) left++;
+    return left;
+}
+
+extern "C" int gtf_batch_run(gtf_batch_t *b)
+{
+    int r;
+    while ((r = gtf_batch_step(b)) > 0) {
+    }
+    return r;
+}
+
+extern "C" int gtf_batch_info(gtf_batch_t *b, int *nrunning, int *nused, double *ms_fock, double *ms_rest,
+                              size_t *job_bytes)
+{
+    if (!b) return -1;
+    int r = 0, u = 0;
+    size_t by = 0;
+    for (auto &j : b->jobs)
+        if (j.used) {
+            u++;
+            if (!j.done) r++;
+            by += j.bytes + gtf_fock_device_bytes(j.eng);
+        }
+    if (nrunning) *nrunning = r;
+    if (nused) *nused = u;
+    if (ms_fock) *ms_fock = b->ms_fock;
+    if (ms_rest) *ms_rest = b->ms_rest;
+    if (job_bytes) *job_bytes = by;
+    return 0;
+}

@@ -163,14 +163,11 @@ __device__ __forceinline__ double sph_coef(int L, int pure, int m, int c)
 __device__ __forceinline__ int nsph_of(int L, int pure) { return (pure && L == 2) ? 5 : ncart(L); }
 
 // D_cart[i][j] = sum_{m,n} T[m][i] T[n][j] D[m][n]
-__global__ void k_d_to_cart(const double *__restrict__ D, double *__restrict__ Dc,
-                            const int *__restrict__ cart2shell, const int *__restrict__ sh_L,
-                            const int *__restrict__ f_start, const int *__restrict__ fc_start,
-                            int nbf, int nbfc, int pure)
+__device__ __forceinline__ void d_to_cart_elem(const double *__restrict__ D, double *__restrict__ Dc,
+                                               const int *__restrict__ cart2shell, const int *__restrict__ sh_L,
+                                               const int *__restrict__ f_start, const int *__restrict__ fc_start,
+                                               int nbf, int nbfc, int pure, int i, int j)
 {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = blockIdx.y;
-    if (j >= nbfc) return;
     const int si = cart2shell[i], sj = cart2shell[j];
     const int ci = i - fc_start[si], cj = j - fc_start[sj];
     const int Li = sh_L[si], Lj = sh_L[sj];
@@ -189,16 +186,24 @@ __global__ void k_d_to_cart(const double *__restrict__ D, double *__restrict__ D
     Dc[(size_t)i * nbfc + j] = v;
 }
 
-// J = T sym(Fj) T^T, K = T sym(Fk) T^T, F = J + K (pfock/pfock.c:1719-1726, 1161-1185)
-__global__ void k_f_to_sph(const double *__restrict__ Fj, const double *__restrict__ Fk,
-                           double *__restrict__ F, double *__restrict__ J, double *__restrict__ K,
-                           const int *__restrict__ sph2shell, const int *__restrict__ sh_L,
-                           const int *__restrict__ f_start, const int *__restrict__ fc_start,
-                           int nbf, int nbfc, int pure)
+__global__ void k_d_to_cart(const double *__restrict__ D, double *__restrict__ Dc,
+                            const int *__restrict__ cart2shell, const int *__restrict__ sh_L,
+                            const int *__restrict__ f_start, const int *__restrict__ fc_start,
+                            int nbf, int nbfc, int pure)
 {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    const int m = blockIdx.y;
-    if (n >= nbf) return;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y;
+    if (j >= nbfc) return;
+    d_to_cart_elem(D, Dc, cart2shell, sh_L, f_start, fc_start, nbf, nbfc, pure, i, j);
+}
+
+// J = T sym(Fj) T^T, K = T sym(Fk) T^T, F = J + K (pfock/pfock.c:1719-1726, 1161-1185)
+__device__ __forceinline__ void f_to_sph_elem(const double *__restrict__ Fj, const double *__restrict__ Fk,
+                                              double *__restrict__ F, double *__restrict__ J, double *__restrict__ K,
+                                              const int *__restrict__ sph2shell, const int *__restrict__ sh_L,
+                                              const int *__restrict__ f_start, const int *__restrict__ fc_start,
+                                              int nbf, int nbfc, int pure, int m, int n)
+{
     const int sm = sph2shell[m], sn = sph2shell[n];
     const int cm = m - f_start[sm], cn = n - f_start[sn];
     const int Lm = sh_L[sm], Ln = sh_L[sn];
@@ -221,6 +226,18 @@ __global__ void k_f_to_sph(const double *__restrict__ Fj, const double *__restri
     J[o] = j;
     K[o] = k;
     F[o] = j + k;
+}
+
+__global__ void k_f_to_sph(const double *__restrict__ Fj, const double *__restrict__ Fk,
+                           double *__restrict__ F, double *__restrict__ J, double *__restrict__ K,
+                           const int *__restrict__ sph2shell, const int *__restrict__ sh_L,
+                           const int *__restrict__ f_start, const int *__restrict__ fc_start,
+                           int nbf, int nbfc, int pure)
+{
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = blockIdx.y;
+    if (n >= nbf) return;
+    f_to_sph_elem(Fj, Fk, F, J, K, sph2shell, sh_L, f_start, fc_start, nbf, nbfc, pure, m, n);
 }
 
 // ---------------------------------------------------------------------------
@@ -556,14 +573,14 @@ __global__ void k_count_kets(const double *__restrict__ pair_v, int bra_start, i
     units32[t] = b == 0 ? 0 : (c - c64 + 31) / 32;
 }
 
-typedef int (*fock_group_launch_t)(int la, int lb, int lc, int ld, const FockLaunch &a, cudaStream_t st);
+typedef int (*fock_group_launch_t)(int la, int lb, int lc, int ld, const FockGrid &g, cudaStream_t st);
 extern fock_group_launch_t gtf_fock_groups[];
 extern const int gtf_fock_ngroups;
 
-static int launch_fock(int X, int Y, const FockLaunch &a, cudaStream_t st)
+static int launch_fock(int X, int Y, const FockGrid &fg, cudaStream_t st)
 {
     for (int g = 0; g < gtf_fock_ngroups; g++) {
-        int r = gtf_fock_groups[g](k_cls_la[X], k_cls_lb[X], k_cls_la[Y], k_cls_lb[Y], a, st);
+        int r = gtf_fock_groups[g](k_cls_la[X], k_cls_lb[X], k_cls_la[Y], k_cls_lb[Y], fg, st);
         if (r != GTF_NOT_IN_GROUP) return r;  // launches, or -1 on error
     }
     return -1;
@@ -1117,6 +1134,29 @@ extern "C" int gtf_fock_set_precision(gtf_fock_dev_t *f, int prec, double fp32_c
     return build_units(f);
 }
 
+// The descriptor of class pair c, part 0 (FP64 head of every ket range) or
+// part 1 (FP32 tail), of one engine.
+static void fill_launch(const gtf_fock_dev *f, int c, int part, const double *D, double *Fj, double *Fk,
+                        FockLaunch &a)
+{
+    const ClassPairTask &t = f->tasks[c];
+    memset(&a, 0, sizeof(a));
+    a.pairs = f->d_pairs;
+    a.pprec = reinterpret_cast<const double2 *>(f->d_pp);
+    a.nlo = part ? t.d_n64 : nullptr;
+    a.nket = part ? t.d_nket : t.d_n64;
+    a.unit_prefix = part ? t.d_unit_prefix32 : t.d_unit_prefix;
+    a.nbra = t.nbra;
+    a.nunits = part ? t.nunits32 : t.nunits;
+    a.bra_start = t.bra_start;
+    a.ket_start = t.ket_start;
+    for (int b = 0; b <= GTF_NBKT; b++) a.seg[b] = t.seg[b];
+    a.D = D;
+    a.Fj = Fj;
+    a.Fk = Fk;
+    a.ld = f->nbf_cart;
+}
+
 // Launches the Fock kernels of class pair c: the FP64 part of every ket
 // range, then (mixed precision) the FP32 tail.  counters holds
 // GTF_MAX_SLICES zeroed slots per (class pair, part), one per slice launch.
@@ -1129,26 +1169,15 @@ static int launch_class(const gtf_fock_dev *f, int c, const double *D, double *F
     for (int part = 0; part < 2; part++) {
         const long long nu = part ? t.nunits32 : t.nunits;
         if (nu == 0) continue;
-        FockLaunch a;
-        memset(&a, 0, sizeof(a));
-        a.pairs = f->d_pairs;
-        a.pprec = reinterpret_cast<const double2 *>(f->d_pp);
-        a.nlo = part ? t.d_n64 : nullptr;
-        a.nket = part ? t.d_nket : t.d_n64;
-        a.unit_prefix = part ? t.d_unit_prefix32 : t.d_unit_prefix;
-        a.nbra = t.nbra;
-        a.nunits = nu;
-        a.bra_start = t.bra_start;
-        a.ket_start = t.ket_start;
-        for (int b = 0; b <= GTF_NBKT; b++) a.seg[b] = t.seg[b];
-        a.counter = counters + (size_t)(2 * c + part) * GTF_MAX_SLICES;
-        a.D = D;
-        a.Fj = Fj;
-        a.Fk = Fk;
-        a.ld = f->nbf_cart;
-        a.nsm = f->nsm;
-        a.fp32 = part;
-        const int r = launch_fock(t.X, t.Y, a, st);
+        FockGrid g;
+        memset(&g, 0, sizeof(g));
+        fill_launch(f, c, part, D, Fj, Fk, g.one);
+        g.nmol = 1;
+        g.nunits = nu;
+        g.counter = counters + (size_t)(2 * c + part) * GTF_MAX_SLICES;
+        g.nsm = f->nsm;
+        g.fp32 = part;
+        const int r = launch_fock(t.X, t.Y, g, st);
         if (r < 0) {
             snprintf(g_errbuf, sizeof(g_errbuf), "Fock kernel launch for class pair (%d,%d)%s failed: %s", t.X, t.Y,
                      part ? " (FP32)" : "", cudaGetErrorString(cudaGetLastError()));
@@ -1451,4 +1480,203 @@ extern "C" int gtf_fock_compute_fixed(gtf_fock_dev_t *f, const double *dev_D, do
     CK(cudaStreamSynchronize(st));
     (void)nn;
     return GTF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Batched Fock builds: many engines (molecules of any size) share one launch
+// per (class pair, precision part, slice); pre- and post-transforms run as one
+// kernel over all molecules.  Each engine reads its D from its own density
+// buffer (gtf_fock_mat_dev(f, 0, 0)) and leaves F, J, K in its own result
+// buffers, as gtf_fock_compute does.
+// ---------------------------------------------------------------------------
+struct XformDesc {
+    const double *D;
+    double *Dc, *Fj, *Fk, *F, *J, *K;
+    const int *cart2shell, *sph2shell, *sh_L, *f_start, *fc_start;
+    int nbf, nbfc, pure, need_tr;
+};
+
+// molecule blockIdx.z: Dc = T D T^T (when spherical), Fj = Fk = 0
+__global__ void k_b_prep(const XformDesc *__restrict__ xs)
+{
+    const XformDesc x = xs[blockIdx.z];
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int i = blockIdx.y; i < x.nbfc; i += gridDim.y) {
+        if (j >= x.nbfc) continue;
+        const size_t o = (size_t)i * x.nbfc + j;
+        x.Fj[o] = 0.0;
+        x.Fk[o] = 0.0;
+        if (x.need_tr) d_to_cart_elem(x.D, x.Dc, x.cart2shell, x.sh_L, x.f_start, x.fc_start, x.nbf, x.nbfc, x.pure, i, j);
+    }
+}
+
+// molecule blockIdx.z: symmetrise and transform back, F = J + K
+__global__ void k_b_post(const XformDesc *__restrict__ xs)
+{
+    const XformDesc x = xs[blockIdx.z];
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int m = blockIdx.y; m < x.nbf; m += gridDim.y) {
+        if (n >= x.nbf) continue;
+        f_to_sph_elem(x.Fj, x.Fk, x.F, x.J, x.K, x.sph2shell, x.sh_L, x.f_start, x.fc_start, x.nbf, x.nbfc, x.pure,
+                      m, n);
+    }
+}
+
+struct gtf_fock_batch {
+    int M;
+    std::vector<gtf_fock_dev *> eng;
+    cudaStream_t st;
+    int nsm, maxn, maxnc;
+    XformDesc *d_xf;
+    FockLaunch *d_desc[NCLSPAIR][2];
+    long long *d_prefix[NCLSPAIR][2];
+    FockLaunch one[NCLSPAIR][2];
+    int nmol[NCLSPAIR][2];
+    long long total[NCLSPAIR][2];
+    unsigned long long *d_counters;
+};
+
+extern "C" void gtf_fock_batch_destroy(gtf_fock_batch_t *b)
+{
+    if (!b) return;
+    cudaStreamSynchronize(b->st);
+    cudaFree(b->d_xf);
+    cudaFree(b->d_counters);
+    for (int c = 0; c < NCLSPAIR; c++)
+        for (int p = 0; p < 2; p++) {
+            cudaFree(b->d_desc[c][p]);
+            cudaFree(b->d_prefix[c][p]);
+        }
+    delete b;
+}
+
+#define CKB_(call)                                                                        \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) {                                                          \
+            snprintf(g_errbuf, sizeof(g_errbuf), "%s:%d %s: %s", __FILE__, __LINE__, #call, \
+                     cudaGetErrorString(e_));                                             \
+            gtf_fock_batch_destroy(b);                                                    \
+            return GTF_ERR_CUDA;                                                          \
+        }                                                                                 \
+    } while (0)
+
+// The engines must live on the current device and outlive the batch; their
+// precision modes are read now (rebuild the batch after changing one).
+extern "C" int gtf_fock_batch_create(gtf_fock_dev_t *const *engines, int M, void *stream, gtf_fock_batch_t **out)
+{
+    *out = nullptr;
+    if (M <= 0 || !engines) return GTF_ERR_INVALID;
+    gtf_fock_batch *b = new gtf_fock_batch();
+    memset(b->d_desc, 0, sizeof(b->d_desc));
+    memset(b->d_prefix, 0, sizeof(b->d_prefix));
+    b->d_xf = nullptr;
+    b->d_counters = nullptr;
+    b->M = M;
+    b->eng.assign(engines, engines + M);
+    b->st = (cudaStream_t)stream;
+    b->nsm = engines[0]->nsm;
+    b->maxn = b->maxnc = 0;
+    std::vector<XformDesc> xf(M);
+    for (int m = 0; m < M; m++) {
+        gtf_fock_dev *f = engines[m];
+        if (!f || f->max_numdmat < 1) {
+            gtf_fock_batch_destroy(b);
+            return GTF_ERR_INVALID;
+        }
+        XformDesc &x = xf[m];
+        x.D = f->d_D;
+        x.Dc = f->d_Dc;
+        x.Fj = f->d_Fj;
+        x.Fk = f->d_Fk;
+        x.F = f->d_F;
+        x.J = f->d_J;
+        x.K = f->d_K;
+        x.cart2shell = f->d_cart2shell;
+        x.sph2shell = f->d_sph2shell;
+        x.sh_L = f->d_sh_L;
+        x.f_start = f->d_f_start;
+        x.fc_start = f->d_fc_start;
+        x.nbf = f->nbf;
+        x.nbfc = f->nbf_cart;
+        x.pure = f->pure;
+        x.need_tr = f->pure && f->nbf_cart != f->nbf;
+        if (f->nbf > b->maxn) b->maxn = f->nbf;
+        if (f->nbf_cart > b->maxnc) b->maxnc = f->nbf_cart;
+    }
+    CKB_(cudaMalloc(&b->d_xf, sizeof(XformDesc) * M));
+    CKB_(cudaMemcpy(b->d_xf, xf.data(), sizeof(XformDesc) * M, cudaMemcpyHostToDevice));
+    CKB_(cudaMalloc(&b->d_counters, sizeof(unsigned long long) * 2 * NCLSPAIR * GTF_MAX_SLICES));
+    for (int c = 0; c < NCLSPAIR; c++)
+        for (int p = 0; p < 2; p++) {
+            std::vector<FockLaunch> d;
+            std::vector<long long> pre(1, 0);
+            for (int m = 0; m < M; m++) {
+                gtf_fock_dev *f = engines[m];
+                const ClassPairTask &t = f->tasks[c];
+                const long long nu = p ? t.nunits32 : t.nunits;
+                if (nu == 0) continue;
+                const bool need_tr = f->pure && f->nbf_cart != f->nbf;
+                FockLaunch a;
+                fill_launch(f, c, p, need_tr ? f->d_Dc : f->d_D, f->d_Fj, f->d_Fk, a);
+                d.push_back(a);
+                pre.push_back(pre.back() + nu);
+            }
+            b->nmol[c][p] = (int)d.size();
+            b->total[c][p] = pre.back();
+            if (d.empty()) continue;
+            b->one[c][p] = d[0];
+            CKB_(cudaMalloc(&b->d_desc[c][p], sizeof(FockLaunch) * d.size()));
+            CKB_(cudaMalloc(&b->d_prefix[c][p], sizeof(long long) * pre.size()));
+            CKB_(cudaMemcpy(b->d_desc[c][p], d.data(), sizeof(FockLaunch) * d.size(), cudaMemcpyHostToDevice));
+            CKB_(cudaMemcpy(b->d_prefix[c][p], pre.data(), sizeof(long long) * pre.size(), cudaMemcpyHostToDevice));
+        }
+    *out = b;
+    return GTF_OK;
+}
+
+// One Fock build of every engine of the batch; returns the number of kernels
+// launched (>= 0) or a negative error.  Stream-ordered: no host wait.
+extern "C" int gtf_fock_batch_compute(gtf_fock_batch_t *b)
+{
+    cudaStream_t st = b->st;
+    int launches = 0;
+    {
+        dim3 g((b->maxnc + 127) / 128, b->maxnc < 1024 ? b->maxnc : 1024, b->M);
+        k_b_prep<<<g, 128, 0, st>>>(b->d_xf);
+        CK(cudaGetLastError());
+        launches++;
+    }
+    CK(cudaMemsetAsync(b->d_counters, 0, sizeof(unsigned long long) * 2 * NCLSPAIR * GTF_MAX_SLICES, st));
+    for (int c = 0; c < NCLSPAIR; c++) {
+        const ClassPairTask &t0 = b->eng[0]->tasks[c];
+        for (int p = 0; p < 2; p++) {
+            if (b->total[c][p] == 0) continue;
+            FockGrid g;
+            memset(&g, 0, sizeof(g));
+            g.one = b->one[c][p];
+            g.mols = b->d_desc[c][p];
+            g.mol_prefix = b->d_prefix[c][p];
+            g.nmol = b->nmol[c][p];
+            g.nunits = b->total[c][p];
+            g.counter = b->d_counters + (size_t)(2 * c + p) * GTF_MAX_SLICES;
+            g.nsm = b->nsm;
+            g.fp32 = p;
+            const int r = launch_fock(t0.X, t0.Y, g, st);
+            if (r < 0) {
+                snprintf(g_errbuf, sizeof(g_errbuf), "batched Fock launch for class pair %d part %d failed: %s", c, p,
+                         cudaGetErrorString(cudaGetLastError()));
+                return GTF_ERR_CUDA;
+            }
+            launches += r;
+        }
+    }
+    {
+        dim3 g((b->maxn + 127) / 128, b->maxn < 1024 ? b->maxn : 1024, b->M);
+        k_b_post<<<g, 128, 0, st>>>(b->d_xf);
+        CK(cudaGetLastError());
+        launches++;
+    }
+    gtf_note_launches(launches);
+    return launches;
 }

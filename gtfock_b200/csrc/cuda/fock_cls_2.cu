@@ -2,7 +2,7 @@
 // angular class pairs (split for parallel compilation).
 #include "fock_kernel.cuh"
 
-extern "C" int gtf_fock_group_2(int la, int lb, int lc, int ld, const FockLaunch &a, cudaStream_t st)
+extern "C" int gtf_fock_group_2(int la, int lb, int lc, int ld, const FockGrid &g, cudaStream_t st)
 {
     FOCK_GROUP_CASE(2,1,2,1)
     FOCK_GROUP_CASE(2,2,0,0)

@@ -31,6 +31,8 @@ __host__ __device__ inline int gtf_prim_bucket(int n)
     return 14;
 }
 
+// One molecule's part of a class-pair launch (its task lists, pair data, D
+// and accumulators).
 struct FockLaunch {
     const PairRec *pairs;
     const double2 *pprec;          // primitive-pair records (PPRec)
@@ -41,12 +43,23 @@ struct FockLaunch {
     long long nunits;
     int bra_start, ket_start;
     int seg[GTF_NBKT + 1];         // segment starts, relative to ket_start
-    unsigned long long *counter;
     const double *D;
     double *Fj, *Fk;
     int ld;
+};
+
+// A launch over one molecule (nmol == 1: `one`) or a batch of molecules
+// (mols[0..nmol), units concatenated in mol_prefix order): the persistent
+// warps of one kernel serve every molecule of the batch.
+struct FockGrid {
+    FockLaunch one;
+    const FockLaunch *mols;         // device array, nmol > 1
+    const long long *mol_prefix;    // device, [nmol + 1] exclusive prefix of units
+    int nmol;
+    long long nunits;               // all units of the launch
+    unsigned long long *counter;    // GTF_MAX_SLICES zeroed counters, one per slice launch
     int nsm;
-    int fp32;                      // evaluate the integrals in FP32 (digestion stays FP64)
+    int fp32;                       // evaluate the integrals in FP32 (digestion stays FP64)
 };
 
 // ---------------------------------------------------------------------------
@@ -84,7 +97,7 @@ template <int LA, int LB, int LC, int LD, typename R, int CD0>
 __global__ void __launch_bounds__(FOCK_THREADS,
                                   fock_min_blocks(LA, LB, LC, LD,
                                                   fock_slice(LA, LB, LC, LD, sizeof(R) == 4 ? 1 : 0)))
-    k_fock(const FockLaunch a)
+    k_fock(const FockGrid g, unsigned long long *counter)
 {
     constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
     constexpr int NCD = ncart(LC) * ncart(LD);
@@ -93,20 +106,32 @@ __global__ void __launch_bounds__(FOCK_THREADS,
     constexpr int TL = RysTab<R>::len(NR);
     __shared__ __align__(16) R tab[TL];
     {
-        const R *g = RysTab<R>::ptr(NR);
-        for (int k = threadIdx.x; k < TL; k += blockDim.x) tab[k] = g[k];
+        const R *gt = RysTab<R>::ptr(NR);
+        for (int k = threadIdx.x; k < TL; k += blockDim.x) tab[k] = gt[k];
         __syncthreads();
     }
     const int lane = threadIdx.x & 31;
-    const PPRec src{a.pprec};
-    const int nidx = a.nbra * GTF_NBKT;
     for (;;) {
         unsigned long long u = 0;
-        if (lane == 0) u = atomicAdd(a.counter, 1ULL);
+        if (lane == 0) u = atomicAdd(counter, 1ULL);
         u = __shfl_sync(GTF_FULL_MASK, u, 0);
-        if (u >= (unsigned long long)a.nunits) break;
+        if (u >= (unsigned long long)g.nunits) break;
+        // molecule of the unit (batched launches)
+        const FockLaunch *ap = &g.one;
+        if (g.nmol > 1) {
+            int lo = 0, hi = g.nmol;
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (__ldg(g.mol_prefix + mid) <= (long long)u) lo = mid;
+                else hi = mid;
+            }
+            ap = g.mols + lo;
+            u -= (unsigned long long)__ldg(g.mol_prefix + lo);
+        }
+        const FockLaunch &a = *ap;
         // unit u -> (bra i, segment b, chunk of 32 kets): binary search of the
         // exclusive unit prefix over the flattened (bra, segment) index
+        const int nidx = a.nbra * GTF_NBKT;
         int lo = 0, hi = nidx;
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
@@ -122,6 +147,7 @@ __global__ void __launch_bounds__(FOCK_THREADS,
         const PairRec pb = a.pairs[a.bra_start + i];
         const PairRec pk = active ? a.pairs[a.ket_start + j] : pb;
         const bool same = (a.bra_start + i) == (a.ket_start + j);
+        const PPRec src{a.pprec};
         R acc[ncart(LA) * ncart(LB) * N];
 #pragma unroll
         for (int k = 0; k < ncart(LA) * ncart(LB) * N; k++) acc[k] = (R)0;
@@ -130,7 +156,7 @@ __global__ void __launch_bounds__(FOCK_THREADS,
     }
 }
 
-// Number of slice launches of a class pair; a.counter points at that many
+// Number of slice launches of a class pair; g.counter points at that many
 // zeroed counters.
 __host__ __device__ constexpr int fock_nslices(int LA, int LB, int LC, int LD, int fp32)
 {
@@ -140,7 +166,7 @@ __host__ __device__ constexpr int fock_nslices(int LA, int LB, int LC, int LD, i
 #define GTF_MAX_SLICES 64
 
 template <int LA, int LB, int LC, int LD, typename R, int CD0>
-int launch_fock_slices(const FockLaunch &a, cudaStream_t st, int slice)
+int launch_fock_slices(const FockGrid &g, cudaStream_t st, int slice)
 {
     constexpr int NCD = ncart(LC) * ncart(LD);
     if constexpr (CD0 < NCD) {
@@ -149,15 +175,13 @@ int launch_fock_slices(const FockLaunch &a, cudaStream_t st, int slice)
         int per_sm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k, FOCK_THREADS, 0);
         if (per_sm < 1) per_sm = 1;
-        long long want = (a.nunits + (FOCK_THREADS / 32) - 1) / (FOCK_THREADS / 32);
-        long long grid = (long long)a.nsm * per_sm;
+        long long want = (g.nunits + (FOCK_THREADS / 32) - 1) / (FOCK_THREADS / 32);
+        long long grid = (long long)g.nsm * per_sm;
         if (want < grid) grid = want;
         if (grid < 1) grid = 1;
-        FockLaunch b = a;
-        b.counter = a.counter + slice;
-        k<<<(unsigned)grid, FOCK_THREADS, 0, st>>>(b);
+        k<<<(unsigned)grid, FOCK_THREADS, 0, st>>>(g, g.counter + slice);
         if (cudaGetLastError() != cudaSuccess) return -1;
-        const int r = launch_fock_slices<LA, LB, LC, LD, R, CD0 + S>(a, st, slice + 1);
+        const int r = launch_fock_slices<LA, LB, LC, LD, R, CD0 + S>(g, st, slice + 1);
         return r < 0 ? r : r + 1;
     } else {
         return 0;
@@ -166,10 +190,10 @@ int launch_fock_slices(const FockLaunch &a, cudaStream_t st, int slice)
 
 // returns the number of kernels launched, or -1 on a launch error
 template <int LA, int LB, int LC, int LD, typename R>
-int launch_fock_t(const FockLaunch &a, cudaStream_t st)
+int launch_fock_t(const FockGrid &g, cudaStream_t st)
 {
     static_assert(fock_nslices(LA, LB, LC, LD, sizeof(R) == 4 ? 1 : 0) <= GTF_MAX_SLICES, "slice counters");
-    return launch_fock_slices<LA, LB, LC, LD, R, 0>(a, st, 0);
+    return launch_fock_slices<LA, LB, LC, LD, R, 0>(g, st, 0);
 }
 
 // returns the number of launches, -1 on a launch error, GTF_NOT_IN_GROUP when the
@@ -177,4 +201,4 @@ int launch_fock_t(const FockLaunch &a, cudaStream_t st)
 #define GTF_NOT_IN_GROUP (-2)
 #define FOCK_GROUP_CASE(A, B, C, D) \
     if (la == A && lb == B && lc == C && ld == D)                                                       \
-        return a.fp32 ? launch_fock_t<A, B, C, D, float>(a, st) : launch_fock_t<A, B, C, D, double>(a, st);
+        return g.fp32 ? launch_fock_t<A, B, C, D, float>(g, st) : launch_fock_t<A, B, C, D, double>(g, st);

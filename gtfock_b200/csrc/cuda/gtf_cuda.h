@@ -79,6 +79,13 @@ void gtf_fock_release_onee(gtf_fock_dev_t *f, int which);
 int gtf_fock_set_precision(gtf_fock_dev_t *f, int prec, double fp32_cutoff);
 int gtf_fock_last_timing(gtf_fock_dev_t *f, double *ms_total, double *ms_eri, double *ms_other);
 int gtf_fock_eri_flops(gtf_fock_dev_t *f, double *flops);
+/* batched Fock builds over many engines (molecules): one launch per class
+ * pair, precision part and slice for the whole batch.  Each engine reads its
+ * own density buffer (gtf_fock_mat_dev(f, 0, 0)) and fills its own F/J/K. */
+typedef struct gtf_fock_batch gtf_fock_batch_t;
+int gtf_fock_batch_create(gtf_fock_dev_t *const *engines, int M, void *stream, gtf_fock_batch_t **out);
+int gtf_fock_batch_compute(gtf_fock_batch_t *b);
+void gtf_fock_batch_destroy(gtf_fock_batch_t *b);
 /* per class pair: Rys-model FLOPs and primitive quartets of one build */
 int gtf_fock_class_work(gtf_fock_dev_t *f, double *flops, double *nprimq);
 /* quartets evaluated in FP32 under the current precision mode, and all */

@@ -44,7 +44,9 @@ static double wall(void)
     return ts.tv_sec + 1e-9 * ts.tv_nsec;
 }
 
-static void initial_density(BasisSet_t basis, double *D, int n)
+/* initial guess of pscf/scf.c:34-76 (half density from the per-atom guess
+ * blocks, scaled by R/2); also used by the batched driver */
+int gtf_initial_density(BasisSet_t basis, double *D, int n)
 {
     memset(D, 0, sizeof(double) * (size_t)n * n);
     double R = 1.0;
@@ -59,6 +61,7 @@ static void initial_density(BasisSet_t basis, double *D, int n)
             for (int c = sp; c <= ep; c++) D[(size_t)r * n + c] = g[(r - sp) * ld + (c - sp)];
     }
     for (size_t k = 0; k < (size_t)n * n; k++) D[k] *= R / 2.0;
+    return 0;
 }
 
 void gtf_scf_destroy(gtf_scf_t *s)
@@ -110,7 +113,7 @@ gtf_scf_t *gtf_scf_create(const char *bsfile, const char *xyzfile, double tolscr
     PFock_createCoreHMat(s->pf, s->basis);
     PFock_getCoreHMat(s->pf, 0, n - 1, 0, n - 1, n, s->pur->H_block);
     PFock_setNumDenMat(1, s->pf);
-    initial_density(s->basis, s->D0, n);
+    gtf_initial_density(s->basis, s->D0, n);
     s->etol = 1e-11;
     s->last_mode = 0;
     return s;

@@ -100,6 +100,41 @@ void gtf_scf_destroy(gtf_scf_t *s);
 int gtf_scf_run(const char *bsfile, const char *xyzfile, double tolscr,
                 int niters, int mode, double *energies, double *timings);
 
+/* Batched and served SCF: many molecules (jobs) of different sizes iterated
+ * in lock-step on one GPU.  Each gtf_batch_step runs one SCF iteration of
+ * every running job: one batched Fock build (one launch per class pair,
+ * precision part and slice covering all jobs), the energy, DIIS and canonical
+ * purification as launches that cover all jobs.  Jobs join (gtf_batch_add)
+ * and leave (gtf_batch_remove) between steps, so a serving loop can admit a
+ * request as soon as a slot and device memory are free.
+ *   gtf_batch_create(capacity): at most `capacity` jobs at a time.
+ *   gtf_batch_add: set-up of one job (basis, screening, S, X, H_core,
+ *     initial guess) with its ERI precision (as gtf_pfock_set_precision),
+ *     at most max_iters iterations, stopping once |E_k - E_k-1| < etol;
+ *     returns the job's slot (>= 0) or a negative error (-2: no free slot).
+ *   gtf_batch_step: returns the number of jobs still running, or < 0.
+ *   gtf_batch_run: steps until every job is done.
+ *   gtf_batch_result: energies (total, incl. nuclear) of the iterations run
+ *     so far, their count, and whether the job is done.
+ *   gtf_batch_density: the job's current density (AO basis, nbf x nbf).
+ *   gtf_batch_info: running / used slots, accumulated ms of the Fock builds
+ *     and of the rest of the steps, device bytes held by the jobs.
+ *   gtf_batch_job_bytes: device bytes of a job's batch buffers for nbf
+ *     functions (admission estimate; the Fock engine comes on top). */
+typedef struct gtf_batch gtf_batch_t;
+gtf_batch_t *gtf_batch_create(int capacity);
+int gtf_batch_add(gtf_batch_t *b, const char *bsfile, const char *xyzfile, double tolscr, int prec_mode,
+                  double fp32_cutoff, int max_iters, double etol);
+int gtf_batch_step(gtf_batch_t *b);
+int gtf_batch_run(gtf_batch_t *b);
+int gtf_batch_result(gtf_batch_t *b, int slot, double *energies, int *niters, int *done);
+int gtf_batch_density(gtf_batch_t *b, int slot, double *D);
+int gtf_batch_remove(gtf_batch_t *b, int slot);
+int gtf_batch_info(gtf_batch_t *b, int *nrunning, int *nused, double *ms_fock, double *ms_rest,
+                   size_t *job_bytes);
+size_t gtf_batch_job_bytes(int nbf);
+void gtf_batch_destroy(gtf_batch_t *b);
+
 /* Number of this library's own kernel launches so far (all threads). */
 unsigned long long gtf_launch_count(void);
 
