@@ -40,6 +40,11 @@ extern "C" const char *gtf_last_error(void);
 #define BJ_KT 16
 #define BJ_PUR_MAX 200
 #define BJ_PUR_CHECK 8
+#define BJ_EBLOCKS 64   // blocks per job of the energy reduction
+// Jobs above BJ_BIG functions run DIIS and purification through the single-job
+// path (cuBLAS DGEMM, multi-block reductions) on the batch's stream: their
+// products are large enough to fill the GPU alone.
+#define BJ_BIG 256
 
 // ---------------------------------------------------------------------------
 // device side
@@ -145,20 +150,21 @@ __device__ __forceinline__ double block_sum(double v, double *sh)
     return r;
 }
 
-// job blockIdx.x: F += H, energy = sum D (H + F) (pscf/scf.c:80-102)
-__global__ void __launch_bounds__(BJ_THREADS) k_j_energy(const JobDev *__restrict__ jobs, double *__restrict__ energy)
+// job blockIdx.y: F += H and block partials of sum D (H + F) (pscf/scf.c:80-102);
+// the host adds the BJ_EBLOCKS partials of a job in order
+__global__ void __launch_bounds__(BJ_THREADS) k_j_energy(const JobDev *__restrict__ jobs, double *__restrict__ part)
 {
     __shared__ double sh[BJ_THREADS];
-    const JobDev j = jobs[blockIdx.x];
+    const JobDev j = jobs[blockIdx.y];
     const size_t nn = (size_t)j.n * j.n;
     double e = 0.0;
-    for (size_t k = threadIdx.x; k < nn; k += BJ_THREADS) {
+    for (size_t k = (size_t)blockIdx.x * BJ_THREADS + threadIdx.x; k < nn; k += (size_t)BJ_EBLOCKS * BJ_THREADS) {
         const double f = j.F[k] + j.H[k];
         j.F[k] = f;
         e += j.D[k] * (j.H[k] + f);
     }
     e = block_sum(e, sh);
-    if (threadIdx.x == 0) energy[blockIdx.x] = e;
+    if (threadIdx.x == 0) part[blockIdx.y * BJ_EBLOCKS + blockIdx.x] = e;
 }
 
 // cur = W2 - W2^T into the DIIS slot (pscf/purif.c:553-558); jobs with cur < 0 skip
@@ -322,6 +328,7 @@ struct BJob {
     BasisSet_t basis;
     PFock_t pf;
     gtf_fock_dev_t *eng;
+    gtf_purif_dev_t *pd;           // jobs above BJ_BIG functions: single-job DIIS / purification
     double *mem;
     size_t bytes;
     JobDev dv;
@@ -379,6 +386,7 @@ extern "C" size_t gtf_batch_job_bytes(int nbf) { return job_buffer_bytes(nbf); }
 static void job_free(BJob &j)
 {
     if (j.mem) cudaFree(j.mem);
+    if (j.pd) gtf_purif_destroy(j.pd);
     if (j.pf) {
         PFock_destroyOvlMat(j.pf);
         PFock_destroyCoreHMat(j.pf);
@@ -425,7 +433,7 @@ extern "C" gtf_batch_t *gtf_batch_create(int capacity)
     ok = ok && cudaMalloc(&b->d_jobs, sizeof(JobDev) * C) == cudaSuccess;
     ok = ok && cudaMalloc(&b->d_gd, sizeof(GemmDesc) * C * NSETS) == cudaSuccess;
     ok = ok && cudaMalloc(&b->d_tp, sizeof(int) * (C + 1) * NSETS) == cudaSuccess;
-    ok = ok && cudaMalloc(&b->d_energy, sizeof(double) * C) == cudaSuccess;
+    ok = ok && cudaMalloc(&b->d_energy, sizeof(double) * C * BJ_EBLOCKS) == cudaSuccess;
     ok = ok && cudaMalloc(&b->d_dots, sizeof(double) * C * BJ_MAX_DIIS) == cudaSuccess;
     ok = ok && cudaMalloc(&b->d_coef, sizeof(double) * C * BJ_MAX_DIIS) == cudaSuccess;
     ok = ok && cudaMalloc(&b->d_scal, sizeof(double) * C * 8) == cudaSuccess;
@@ -435,7 +443,7 @@ extern "C" gtf_batch_t *gtf_batch_create(int capacity)
     ok = ok && cudaMallocHost(&b->h_jobs, sizeof(JobDev) * C) == cudaSuccess;
     ok = ok && cudaMallocHost(&b->h_gd, sizeof(GemmDesc) * C * NSETS) == cudaSuccess;
     ok = ok && cudaMallocHost(&b->h_tp, sizeof(int) * (C + 1) * NSETS) == cudaSuccess;
-    ok = ok && cudaMallocHost(&b->h_energy, sizeof(double) * C) == cudaSuccess;
+    ok = ok && cudaMallocHost(&b->h_energy, sizeof(double) * C * BJ_EBLOCKS) == cudaSuccess;
     ok = ok && cudaMallocHost(&b->h_dots, sizeof(double) * C * BJ_MAX_DIIS) == cudaSuccess;
     ok = ok && cudaMallocHost(&b->h_coef, sizeof(double) * C * BJ_MAX_DIIS) == cudaSuccess;
     ok = ok && cudaMallocHost(&b->h_iters, sizeof(int) * C) == cudaSuccess;
@@ -496,24 +504,33 @@ extern "C" int gtf_batch_add(gtf_batch_t *b, const char *bsfile, const char *xyz
     }
     const size_t nn = (size_t)j.n * j.n;
     j.bytes = job_buffer_bytes(j.n);
-    if (cudaMalloc(&j.mem, j.bytes) != cudaSuccess) {
+    JobDev &d = j.dv;
+    d.S = gtf_fock_onee_dev(j.eng, 0);
+    d.X = gtf_fock_onee_dev(j.eng, 1);
+    if (j.n > BJ_BIG) {
+        if (gtf_purif_create(j.n, j.nocc, b->st, &j.pd) != GTF_OK ||
+            gtf_purif_set_sx_dev(j.pd, d.S, d.X) != GTF_OK) {
+            j.pd = nullptr;
+            job_free(j);
+            return -6;
+        }
+    } else if (cudaMalloc(&j.mem, j.bytes) != cudaSuccess) {
         j.mem = nullptr;
         job_free(j);
         return -6;
     }
-    JobDev &d = j.dv;
     d.D = const_cast<double *>(gtf_fock_mat_dev(j.eng, 0, 0));
     d.F = const_cast<double *>(gtf_fock_mat_dev(j.eng, 1, 0));
-    d.S = gtf_fock_onee_dev(j.eng, 0);
-    d.X = gtf_fock_onee_dev(j.eng, 1);
     d.H = gtf_fock_onee_dev(j.eng, 2);
-    d.P = j.mem;
-    d.P2 = d.P + nn;
-    d.P3 = d.P2 + nn;
-    d.W = d.P3 + nn;
-    d.W2 = d.W + nn;
-    d.vecs = d.W2 + nn;
-    d.Fvecs = d.vecs + nn * BJ_MAX_DIIS;
+    if (j.mem) {
+        d.P = j.mem;
+        d.P2 = d.P + nn;
+        d.P3 = d.P2 + nn;
+        d.W = d.P3 + nn;
+        d.W2 = d.W + nn;
+        d.vecs = d.W2 + nn;
+        d.Fvecs = d.vecs + nn * BJ_MAX_DIIS;
+    }
     d.n = j.n;
     d.nocc = j.nocc;
     d.cur = -1;
@@ -683,16 +700,17 @@ extern "C" int gtf_batch_step(gtf_batch_t *b)
         b->h_jobs[k] = j.dv;
     }
     CKH(cudaMemcpyAsync(b->d_jobs, b->h_jobs, sizeof(JobDev) * M, cudaMemcpyHostToDevice, b->st));
-    k_j_energy<<<M, BJ_THREADS, 0, b->st>>>(b->d_jobs, b->d_energy);
+    k_j_energy<<<dim3(BJ_EBLOCKS, M), BJ_THREADS, 0, b->st>>>(b->d_jobs, b->d_energy);
     CKH(cudaGetLastError());
     launches++;
-    CKH(cudaMemcpyAsync(b->h_energy, b->d_energy, sizeof(double) * M, cudaMemcpyDeviceToHost, b->st));
+    CKH(cudaMemcpyAsync(b->h_energy, b->d_energy, sizeof(double) * M * BJ_EBLOCKS, cudaMemcpyDeviceToHost, b->st));
     CKH(cudaStreamSynchronize(b->st));
-    // jobs that continue with DIIS + purification
-    std::vector<int> cont;   // indices into run
+    // jobs that continue with DIIS + purification: batched (cont) or one by one (big)
+    std::vector<int> cont, big;   // indices into run
     for (int k = 0; k < M; k++) {
         BJob &j = b->jobs[run[k]];
-        const double e = b->h_energy[k];
+        double e = 0.0;
+        for (int q = 0; q < BJ_EBLOCKS; q++) e += b->h_energy[k * BJ_EBLOCKS + q];
         j.energies.push_back(e + j.enuc);
         const int it = j.iter++;
         if ((it > 0 && fabs(e - j.e_prev) < j.etol) || j.iter >= j.max_iters) {
@@ -700,7 +718,8 @@ extern "C" int gtf_batch_step(gtf_batch_t *b)
             continue;
         }
         j.e_prev = e;
-        cont.push_back(k);
+        if (j.pd) big.push_back(k);
+        else cont.push_back(k);
     }
     const int C = (int)cont.size();
     if (C > 0) {
@@ -814,6 +833,17 @@ extern "C" int gtf_batch_step(gtf_batch_t *b)
         // D_AO = X P X^T (pscf/purif.c:469-476), into the engine's density
         if (run_gemm(b, 8, C, true, nullptr, &launches) || run_gemm(b, 9, C, true, nullptr, &launches)) return -4;
         CKH(cudaMemcpyAsync(b->h_iters, b->d_iters, sizeof(int) * C, cudaMemcpyDeviceToHost, b->st));
+    }
+    // jobs above BJ_BIG functions: the single-job DIIS and purification
+    for (int k : big) {
+        BJob &j = b->jobs[run[k]];
+        int it = 0;
+        if (gtf_diis_step_dev(j.pd, j.dv.D, j.dv.F, j.iter - 1) != GTF_OK ||
+            gtf_purif_run_dev(j.pd, j.dv.F, j.dv.D, &it) != GTF_OK) {
+            j.failed = 1;
+            j.done = 1;
+        }
+        j.pur_iters = it;
     }
     CKH(cudaEventRecord(b->e2, b->st));
     CKH(cudaStreamSynchronize(b->st));
