@@ -40,6 +40,7 @@ sys.path.insert(0, ROOT)
 
 TOL = 1e-10
 NITER = 10
+MIXED_CUTOFF = 1e-6
 METRIC = "SCF solves/s (C54H18 cc-pVDZ, 10 iterations, FP64)"
 WORKLOAD = "C54H18 graphene flake / cc-pVDZ (846 bf), Schwarz 1e-10, 10 SCF iterations, FP64"
 
@@ -217,6 +218,14 @@ def run(args):
             pg.all_reduce(t, op=pg.ReduceOp.MAX)
             dt = float(t.item())
         clocks = clk.summary()
+        # the same solves with FP32 quartets below a Schwarz bound of 1e-6
+        solver.set_options(precision=1, fp32_cutoff=MIXED_CUTOFF, etol=1e-11)
+        solver.solve(NITER, device_resident=True)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e_mixed, tm_m = solver.solve(NITER, device_resident=True)
+        dt_mixed = time.perf_counter() - t0
+        solver.set_options(precision=0, etol=1e-11)
         # one Fock build's ERI kernels for the roofline
         pf_basis = gb.BasisSet(gbs, xyz)
         pf = gb.PFock(pf_basis, tolscr=TOL)
@@ -267,6 +276,11 @@ def run(args):
                      "work": "Rys-model FLOPs per build %.4g" % eri_flops,
                      "eri_ms_per_build": eri_s * 1e3},
         "clocks": clocks,
+        "mixed_precision": {"value": world * args.steps / dt_mixed, "unit": "solves/s",
+                            "fp32_cutoff": MIXED_CUTOFF,
+                            "dE_last_vs_fp64": float(abs(e_mixed[-1] - energies[-1])),
+                            "note": "FP32 ERIs for quartets with Schwarz bound below the cutoff; "
+                                    "digestion and F accumulation FP64"},
     }
     if rank == 0 and not args.no_cpu_baseline:
         with tempfile.TemporaryDirectory() as td2:
@@ -338,7 +352,9 @@ def run_batched(args):
             info = b.info()
             res[tag] = [b.result(s)[0] for s in slots]
             out[tag] = {"solves_per_s": len(files) / (t2 - t1), "solve_s": t2 - t1, "setup_s": t1 - t0,
-                        "ms_fock": info["ms_fock"], "ms_rest": info["ms_rest"],
+                        "ms_fock": info["ms_fock"], "ms_energy": info["ms_energy"], "ms_diis": info["ms_diis"],
+                        "ms_purification": info["ms_purification"],
+                        "purification_steps": info["purification_steps"], "steps": info["steps"],
                         "launches": gb.launch_count() - l0}
             b.close()
         # the plain FP64 GPU path, one molecule after another

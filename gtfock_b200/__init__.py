@@ -111,6 +111,7 @@ def load():
     _sig(L, "gtf_batch_remove", [_vp, _i])
     _sig(L, "gtf_batch_info", [_vp, _ip, _ip, _dp, _dp, ctypes.POINTER(ctypes.c_size_t)])
     _sig(L, "gtf_batch_job_bytes", [_i], ctypes.c_size_t)
+    _sig(L, "gtf_batch_stats", [_vp, _dp, _i])
     _sig(L, "gtf_batch_destroy", [_vp], None)
     _sig(L, "gtf_fp64_peak", [_dp])
     _sig(L, "gtf_device_info", [_ip, _ip])
@@ -452,8 +453,11 @@ class Batch:
         by = ctypes.c_size_t()
         load().gtf_batch_info(self.h, ctypes.byref(r), ctypes.byref(u), ctypes.byref(mf), ctypes.byref(mr),
                               ctypes.byref(by))
+        st = np.zeros(6)
+        load().gtf_batch_stats(self.h, _dptr(st), 6)
         return {"running": r.value, "used": u.value, "ms_fock": mf.value, "ms_rest": mr.value,
-                "device_bytes": by.value}
+                "device_bytes": by.value, "ms_energy": st[1], "ms_diis": st[2], "ms_purification": st[3],
+                "purification_steps": st[4], "steps": st[5]}
 
     @staticmethod
     def job_bytes(nbf):

@@ -44,7 +44,7 @@ extern "C" const char *gtf_last_error(void);
 // Jobs above BJ_BIG functions run DIIS and purification through the single-job
 // path (cuBLAS DGEMM, multi-block reductions) on the batch's stream: their
 // products are large enough to fill the GPU alone.
-#define BJ_BIG 256
+#define BJ_BIG 640
 
 // ---------------------------------------------------------------------------
 // device side
@@ -271,12 +271,15 @@ __global__ void __launch_bounds__(BJ_THREADS) k_j_pur_init(const JobDev *__restr
 
 // ||P - P2||_F, c = tr(P2 - P3) / tr(P - P2), then the trace-conserving
 // update (pscf/purif.c:394-455); a job stops once ||P - P2||_F < 1e-11
-__global__ void __launch_bounds__(BJ_THREADS) k_j_pur_step(const JobDev *__restrict__ jobs, double *__restrict__ scal,
-                                                          int *__restrict__ active, int *__restrict__ iters)
+// Block b serves job list[b] (the jobs still purifying).
+__global__ void __launch_bounds__(BJ_THREADS) k_j_pur_step(const JobDev *__restrict__ jobs, const int *__restrict__ list,
+                                                          double *__restrict__ scal, int *__restrict__ active,
+                                                          int *__restrict__ iters)
 {
     __shared__ double sh[BJ_THREADS];
-    if (!active[blockIdx.x]) return;
-    const JobDev j = jobs[blockIdx.x];
+    const int q = list[blockIdx.x];
+    if (!active[q]) return;
+    const JobDev j = jobs[q];
     const int n = j.n;
     const size_t nn = (size_t)n * n;
     double e = 0.0, t = 0.0, t2 = 0.0;
@@ -292,30 +295,17 @@ __global__ void __launch_bounds__(BJ_THREADS) k_j_pur_step(const JobDev *__restr
     e = block_sum(e, sh);
     t = block_sum(t, sh);
     t2 = block_sum(t2, sh);
-    const double err = sqrt(e), c = t / t2;
-    for (size_t k = threadIdx.x; k < nn; k += BJ_THREADS) {
+    const double c = t / t2;
+    const double err = isfinite(c) ? sqrt(e) : 0.0;   // 0/0 at an idempotent P: stop, as the one-job path
+    for (size_t k = threadIdx.x; k < nn && isfinite(c); k += BJ_THREADS) {
         if (c < 0.5) j.P[k] = ((1.0 - 2.0 * c) * j.P[k] + (1.0 + c) * j.P2[k] - j.P3[k]) / (1.0 - c);
         else j.P[k] = ((1.0 + c) * j.P2[k] - j.P3[k]) / c;
     }
     if (threadIdx.x == 0) {
-        scal[blockIdx.x * 8 + 2] = err;
-        iters[blockIdx.x] += 1;
-        if (err < 1e-11) active[blockIdx.x] = 0;
+        scal[q * 8 + 2] = err;
+        iters[q] += 1;
+        if (err < 1e-11) active[q] = 0;
     }
-}
-
-__global__ void k_j_count(const int *__restrict__ active, int m, int *__restrict__ out)
-{
-    __shared__ int sh[BJ_THREADS];
-    int c = 0;
-    for (int i = threadIdx.x; i < m; i += BJ_THREADS) c += active[i];
-    sh[threadIdx.x] = c;
-    __syncthreads();
-    for (int s = BJ_THREADS / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) *out = sh[0];
 }
 
 // ---------------------------------------------------------------------------
@@ -355,16 +345,16 @@ struct gtf_batch {
     GemmDesc *d_gd;                // 10 call sets x capacity
     int *d_tp;                     // 10 call sets x (capacity + 1)
     double *d_energy, *d_dots, *d_coef, *d_scal;
-    int *d_active, *d_iters, *d_count;
+    int *d_active, *d_iters, *d_count, *d_list;
     // pinned mirrors
     JobDev *h_jobs;
     GemmDesc *h_gd;
     int *h_tp;
     double *h_energy, *h_dots, *h_coef;
-    int *h_iters, *h_count;
+    int *h_iters, *h_count, *h_act, *h_list;
     size_t dev_bytes_jobs;
-    double ms_fock, ms_rest;
-    cudaEvent_t e0, e1, e2;
+    double ms_fock, ms_rest, ms_energy, ms_diis, ms_pur, pur_steps, nsteps;
+    cudaEvent_t e0, e1, e2, e3, e4;
 };
 
 #define CKH(call)                                                                          \
@@ -404,15 +394,18 @@ extern "C" void gtf_batch_destroy(gtf_batch_t *b)
     for (auto &j : b->jobs)
         if (j.used) job_free(j);
     void *dp[] = {b->d_jobs, b->d_gd, b->d_tp, b->d_energy, b->d_dots, b->d_coef, b->d_scal, b->d_active,
-                  b->d_iters, b->d_count};
+                  b->d_iters, b->d_count, b->d_list};
     for (void *p : dp)
         if (p) cudaFree(p);
-    void *hp[] = {b->h_jobs, b->h_gd, b->h_tp, b->h_energy, b->h_dots, b->h_coef, b->h_iters, b->h_count};
+    void *hp[] = {b->h_jobs, b->h_gd, b->h_tp, b->h_energy, b->h_dots, b->h_coef, b->h_iters, b->h_count,
+                  b->h_act, b->h_list};
     for (void *p : hp)
         if (p) cudaFreeHost(p);
     cudaEventDestroy(b->e0);
     cudaEventDestroy(b->e1);
     cudaEventDestroy(b->e2);
+    cudaEventDestroy(b->e3);
+    cudaEventDestroy(b->e4);
     cudaStreamDestroy(b->st);
     delete b;
 }
@@ -425,10 +418,11 @@ extern "C" gtf_batch_t *gtf_batch_create(int capacity)
     b->jobs.resize(capacity);
     b->fb = nullptr;
     b->dirty = 1;
-    b->ms_fock = b->ms_rest = 0.0;
+    b->ms_fock = b->ms_rest = b->ms_energy = b->ms_diis = b->ms_pur = b->pur_steps = b->nsteps = 0.0;
     bool ok = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) == cudaSuccess;
     ok = ok && cudaEventCreate(&b->e0) == cudaSuccess && cudaEventCreate(&b->e1) == cudaSuccess &&
-         cudaEventCreate(&b->e2) == cudaSuccess;
+         cudaEventCreate(&b->e2) == cudaSuccess && cudaEventCreate(&b->e3) == cudaSuccess &&
+         cudaEventCreate(&b->e4) == cudaSuccess;
     const size_t C = capacity;
     ok = ok && cudaMalloc(&b->d_jobs, sizeof(JobDev) * C) == cudaSuccess;
     ok = ok && cudaMalloc(&b->d_gd, sizeof(GemmDesc) * C * NSETS) == cudaSuccess;
@@ -440,6 +434,9 @@ extern "C" gtf_batch_t *gtf_batch_create(int capacity)
     ok = ok && cudaMalloc(&b->d_active, sizeof(int) * C) == cudaSuccess;
     ok = ok && cudaMalloc(&b->d_iters, sizeof(int) * C) == cudaSuccess;
     ok = ok && cudaMalloc(&b->d_count, sizeof(int)) == cudaSuccess;
+    ok = ok && cudaMalloc(&b->d_list, sizeof(int) * C) == cudaSuccess;
+    ok = ok && cudaMallocHost(&b->h_act, sizeof(int) * C) == cudaSuccess;
+    ok = ok && cudaMallocHost(&b->h_list, sizeof(int) * C) == cudaSuccess;
     ok = ok && cudaMallocHost(&b->h_jobs, sizeof(JobDev) * C) == cudaSuccess;
     ok = ok && cudaMallocHost(&b->h_gd, sizeof(GemmDesc) * C * NSETS) == cudaSuccess;
     ok = ok && cudaMallocHost(&b->h_tp, sizeof(int) * (C + 1) * NSETS) == cudaSuccess;
@@ -704,6 +701,8 @@ extern "C" int gtf_batch_step(gtf_batch_t *b)
     CKH(cudaGetLastError());
     launches++;
     CKH(cudaMemcpyAsync(b->h_energy, b->d_energy, sizeof(double) * M * BJ_EBLOCKS, cudaMemcpyDeviceToHost, b->st));
+    CKH(cudaEventRecord(b->e3, b->st));
+    CKH(cudaEventRecord(b->e4, b->st));
     CKH(cudaStreamSynchronize(b->st));
     // jobs that continue with DIIS + purification: batched (cont) or one by one (big)
     std::vector<int> cont, big;   // indices into run
@@ -803,7 +802,9 @@ extern "C" int gtf_batch_step(gtf_batch_t *b)
                     for (int c = 0; c <= L; c++)
                         bm[r][c] = (r < L && c < L) ? j.b[r][c] : ((r == c) ? 0.0 : -1.0);
                 diis_coeffs(bm, L, cf);
-                for (int i = 0; i < L; i++) co[i] = cf[i];
+                bool finite = true;
+                for (int i = 0; i < L; i++) finite = finite && isfinite(cf[i]);
+                for (int i = 0; i < L; i++) co[i] = finite ? cf[i] : (i == cur_idx ? 1.0 : 0.0);
             }
             CKH(cudaMemcpyAsync(b->d_coef, b->h_coef, sizeof(double) * C * BJ_MAX_DIIS, cudaMemcpyHostToDevice,
                                 b->st));
@@ -812,24 +813,49 @@ extern "C" int gtf_batch_step(gtf_batch_t *b)
             launches++;
         }
         // ---- canonical purification (pscf/purif.c:257-488) ----
+        CKH(cudaEventRecord(b->e4, b->st));
         CKH(cudaMemsetAsync(b->d_iters, 0, sizeof(int) * C, b->st));
         k_j_pur_init<<<C, BJ_THREADS, 0, b->st>>>(b->d_jobs, b->d_scal, b->d_active);
         CKH(cudaGetLastError());
         launches++;
-        for (int step = 0; step < BJ_PUR_MAX; step++) {
-            if (run_gemm(b, 6, C, true, b->d_active, &launches) || run_gemm(b, 7, C, false, b->d_active, &launches))
+        // the launches cover the jobs still purifying: every BJ_PUR_CHECK steps
+        // the active flags come back and the job list and the descriptors of
+        // the two products are compacted to the jobs that remain
+        int nact = C;
+        for (int q = 0; q < C; q++) b->h_list[q] = q;
+        CKH(cudaMemcpyAsync(b->d_list, b->h_list, sizeof(int) * C, cudaMemcpyHostToDevice, b->st));
+        int step;
+        for (step = 0; step < BJ_PUR_MAX; step++) {
+            if (run_gemm(b, 6, nact, true, b->d_active, &launches) ||
+                run_gemm(b, 7, nact, false, b->d_active, &launches))
                 return -4;
-            k_j_pur_step<<<C, BJ_THREADS, 0, b->st>>>(b->d_jobs, b->d_scal, b->d_active, b->d_iters);
+            k_j_pur_step<<<nact, BJ_THREADS, 0, b->st>>>(b->d_jobs, b->d_list, b->d_scal, b->d_active, b->d_iters);
             CKH(cudaGetLastError());
             launches++;
             if ((step + 1) % BJ_PUR_CHECK == 0) {
-                k_j_count<<<1, BJ_THREADS, 0, b->st>>>(b->d_active, C, b->d_count);
-                launches++;
-                CKH(cudaMemcpyAsync(b->h_count, b->d_count, sizeof(int), cudaMemcpyDeviceToHost, b->st));
+                CKH(cudaMemcpyAsync(b->h_act, b->d_active, sizeof(int) * C, cudaMemcpyDeviceToHost, b->st));
                 CKH(cudaStreamSynchronize(b->st));
-                if (*b->h_count == 0) break;
+                int m = 0;
+                for (int q = 0; q < C; q++)
+                    if (b->h_act[q]) {
+                        const JobDev &d = b->h_jobs[q];
+                        set_gemm(b, 6, m, d.P, d.P, d.P2, d.n, q);
+                        set_gemm(b, 7, m, d.P, d.P2, d.P3, d.n, q);
+                        b->h_list[m++] = q;
+                    }
+                if (m == 0) break;
+                if (m < nact) {
+                    nact = m;
+                    const size_t C1 = b->capacity + 1;
+                    CKH(cudaMemcpyAsync(b->d_gd + 6 * (size_t)b->capacity, b->h_gd + 6 * (size_t)b->capacity,
+                                        sizeof(GemmDesc) * 2 * b->capacity, cudaMemcpyHostToDevice, b->st));
+                    CKH(cudaMemcpyAsync(b->d_tp + 6 * C1, b->h_tp + 6 * C1, sizeof(int) * 2 * C1,
+                                        cudaMemcpyHostToDevice, b->st));
+                    CKH(cudaMemcpyAsync(b->d_list, b->h_list, sizeof(int) * nact, cudaMemcpyHostToDevice, b->st));
+                }
             }
         }
+        b->pur_steps += step + 1;
         // D_AO = X P X^T (pscf/purif.c:469-476), into the engine's density
         if (run_gemm(b, 8, C, true, nullptr, &launches) || run_gemm(b, 9, C, true, nullptr, &launches)) return -4;
         CKH(cudaMemcpyAsync(b->h_iters, b->d_iters, sizeof(int) * C, cudaMemcpyDeviceToHost, b->st));
@@ -848,11 +874,17 @@ extern "C" int gtf_batch_step(gtf_batch_t *b)
     CKH(cudaEventRecord(b->e2, b->st));
     CKH(cudaStreamSynchronize(b->st));
     for (int q = 0; q < C; q++) b->jobs[run[cont[q]]].pur_iters = b->h_iters[q];
-    float ms1 = 0.0f, ms2 = 0.0f;
+    float ms1 = 0.0f, ms2 = 0.0f, ms3 = 0.0f, ms4 = 0.0f;
     cudaEventElapsedTime(&ms1, b->e0, b->e1);
     cudaEventElapsedTime(&ms2, b->e1, b->e2);
+    cudaEventElapsedTime(&ms3, b->e1, b->e3);
+    cudaEventElapsedTime(&ms4, b->e4, b->e2);
     b->ms_fock += ms1;
     b->ms_rest += ms2;
+    b->ms_energy += ms3;
+    b->ms_pur += ms4;
+    b->ms_diis += ms2 - ms3 - ms4;
+    b->nsteps += 1;
     gtf_note_launches(launches);
     int left = 0;
     for (int s = 0; s < b->capacity; s++)
@@ -886,4 +918,16 @@ extern "C" int gtf_batch_info(gtf_batch_t *b, int *nrunning, int *nused, double 
     if (ms_rest) *ms_rest = b->ms_rest;
     if (job_bytes) *job_bytes = by;
     return 0;
+}
+
+// accumulated statistics: [0] ms of Fock builds, [1] energies, [2] DIIS,
+// [3] purification (incl. jobs on the one-job path), [4] purification steps
+// of the batched jobs, [5] batch steps; returns the number written
+extern "C" int gtf_batch_stats(gtf_batch_t *b, double *out, int n)
+{
+    if (!b || !out) return -1;
+    const double v[6] = {b->ms_fock, b->ms_energy, b->ms_diis, b->ms_pur, b->pur_steps, b->nsteps};
+    const int m = n < 6 ? n : 6;
+    for (int k = 0; k < m; k++) out[k] = v[k];
+    return m;
 }

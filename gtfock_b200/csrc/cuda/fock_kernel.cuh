@@ -93,7 +93,7 @@ __host__ __device__ constexpr int fock_min_blocks(int LA, int LB, int LC, int LD
     return nq <= 3 ? 6 : nq <= 9 ? 4 : nq <= 27 ? 3 : 2;
 }
 
-template <int LA, int LB, int LC, int LD, typename R, int CD0>
+template <int LA, int LB, int LC, int LD, typename R, int CD0, bool BATCH>
 __global__ void __launch_bounds__(FOCK_THREADS,
                                   fock_min_blocks(LA, LB, LC, LD,
                                                   fock_slice(LA, LB, LC, LD, sizeof(R) == 4 ? 1 : 0)))
@@ -116,43 +116,52 @@ __global__ void __launch_bounds__(FOCK_THREADS,
         if (lane == 0) u = atomicAdd(counter, 1ULL);
         u = __shfl_sync(GTF_FULL_MASK, u, 0);
         if (u >= (unsigned long long)g.nunits) break;
-        // molecule of the unit (batched launches)
-        const FockLaunch *ap = &g.one;
-        if (g.nmol > 1) {
+        // molecule of the unit (batched launches); the fields are read from
+        // the kernel parameter (one molecule, no registers held for them) or
+        // from the descriptor array
+        constexpr bool bt = BATCH;
+        const FockLaunch *mp = g.mols;
+        if constexpr (BATCH) {
             int lo = 0, hi = g.nmol;
             while (hi - lo > 1) {
                 const int mid = (lo + hi) >> 1;
                 if (__ldg(g.mol_prefix + mid) <= (long long)u) lo = mid;
                 else hi = mid;
             }
-            ap = g.mols + lo;
+            mp += lo;
             u -= (unsigned long long)__ldg(g.mol_prefix + lo);
         }
-        const FockLaunch &a = *ap;
+#define GTF_FLD(x) (bt ? mp->x : g.one.x)
+        const long long *unit_prefix = GTF_FLD(unit_prefix);
         // unit u -> (bra i, segment b, chunk of 32 kets): binary search of the
         // exclusive unit prefix over the flattened (bra, segment) index
-        const int nidx = a.nbra * GTF_NBKT;
+        const int nidx = GTF_FLD(nbra) * GTF_NBKT;
         int lo = 0, hi = nidx;
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
-            if (__ldg(a.unit_prefix + mid) <= (long long)u) lo = mid;
+            if (__ldg(unit_prefix + mid) <= (long long)u) lo = mid;
             else hi = mid;
         }
         const int i = lo / GTF_NBKT, b = lo - i * GTF_NBKT;
-        const long long chunk = (long long)u - __ldg(a.unit_prefix + lo);
+        const long long chunk = (long long)u - __ldg(unit_prefix + lo);
         const int jj = (int)(chunk * 32) + lane;
-        const int k0 = a.nlo ? __ldg(a.nlo + lo) : 0;
-        const bool active = jj < __ldg(a.nket + lo) - k0;
-        const int j = a.seg[b] + k0 + jj;
-        const PairRec pb = a.pairs[a.bra_start + i];
-        const PairRec pk = active ? a.pairs[a.ket_start + j] : pb;
-        const bool same = (a.bra_start + i) == (a.ket_start + j);
-        const PPRec src{a.pprec};
+        const int *nlo = GTF_FLD(nlo);
+        const int k0 = nlo ? __ldg(nlo + lo) : 0;
+        const bool active = jj < __ldg(GTF_FLD(nket) + lo) - k0;
+        const int j = GTF_FLD(seg[b]) + k0 + jj;
+        const PairRec *pairs = GTF_FLD(pairs);
+        const int bra_start = GTF_FLD(bra_start), ket_start = GTF_FLD(ket_start);
+        const PairRec pb = pairs[bra_start + i];
+        const PairRec pk = active ? pairs[ket_start + j] : pb;
+        const bool same = (bra_start + i) == (ket_start + j);
+        const PPRec src{GTF_FLD(pprec)};
         R acc[ncart(LA) * ncart(LB) * N];
 #pragma unroll
         for (int k = 0; k < ncart(LA) * ncart(LB) * N; k++) acc[k] = (R)0;
         if (active) eri_accumulate_cd<LA, LB, LC, LD, CD0, N, true>(src, pb, src, pk, acc, tab);
-        digest_cd<LA, LB, LC, LD, CD0, N>(acc, active, pb, pk, same, a.D, a.Fj, a.Fk, a.ld, lane);
+        digest_cd<LA, LB, LC, LD, CD0, N>(acc, active, pb, pk, same, GTF_FLD(D), GTF_FLD(Fj), GTF_FLD(Fk),
+                                          GTF_FLD(ld), lane);
+#undef GTF_FLD
     }
 }
 
@@ -171,7 +180,7 @@ int launch_fock_slices(const FockGrid &g, cudaStream_t st, int slice)
     constexpr int NCD = ncart(LC) * ncart(LD);
     if constexpr (CD0 < NCD) {
         constexpr int S = fock_slice(LA, LB, LC, LD, sizeof(R) == 4 ? 1 : 0);
-        auto k = k_fock<LA, LB, LC, LD, R, CD0>;
+        auto k = g.nmol > 1 ? k_fock<LA, LB, LC, LD, R, CD0, true> : k_fock<LA, LB, LC, LD, R, CD0, false>;
         int per_sm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k, FOCK_THREADS, 0);
         if (per_sm < 1) per_sm = 1;

@@ -174,7 +174,10 @@ __global__ void k_purif_stats(const double *__restrict__ D, const double *__rest
     }
 }
 
-// scal[6] = errnorm, scal[7] = c = tr(D2-D3)/tr(D-D2) (pscf/purif.c:394-440)
+// scal[6] = errnorm, scal[7] = c = tr(D2-D3)/tr(D-D2) (pscf/purif.c:394-440).
+// Where the reference would divide 0/0 (an exactly idempotent D) and write NaN
+// into D, the iteration stops instead: errnorm is reported as 0 and the
+// update below is skipped.
 __global__ void k_purif_finish(const double *__restrict__ part, int nblk, double *scal)
 {
     if (threadIdx.x != 0) return;
@@ -184,8 +187,9 @@ __global__ void k_purif_finish(const double *__restrict__ part, int nblk, double
         t += part[3 * b + 1];
         t2 += part[3 * b + 2];
     }
-    scal[6] = sqrt(e);
-    scal[7] = t / t2;
+    const double c = t / t2;
+    scal[6] = isfinite(c) ? sqrt(e) : 0.0;
+    scal[7] = c;
 }
 
 // D update (pscf/purif.c:441-455)
@@ -195,6 +199,7 @@ __global__ void k_purif_update(double *__restrict__ D, const double *__restrict_
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nn) return;
     const double c = scal[7];
+    if (!isfinite(c)) return;
     if (c < 0.5) D[k] = ((1.0 - 2.0 * c) * D[k] + (1.0 + c) * D2[k] - D3[k]) / (1.0 - c);
     else D[k] = ((1.0 + c) * D2[k] - D3[k]) / c;
 }
@@ -447,6 +452,12 @@ extern "C" int gtf_diis_step_dev(gtf_purif_dev_t *p, const double *D_dev, double
     if (iter > 1) {
         double co[PUR_MAX_DIIS + 1];
         diis_coeffs(p->b, p->len_diis, co);
+        // a singular bordered system (two identical error vectors) gives
+        // non-finite coefficients: keep this iteration's F unextrapolated
+        bool finite = true;
+        for (int i = 0; i < p->len_diis; i++) finite = finite && isfinite(co[i]);
+        if (!finite)
+            for (int i = 0; i < p->len_diis; i++) co[i] = (cur_F == p->Fvecs + nn * i) ? 1.0 : 0.0;
         Coeffs c;
         for (int i = 0; i < PUR_MAX_DIIS; i++) c.c[i] = (i < p->len_diis) ? co[i] : 0.0;
         k_combine<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(F_dev, p->Fvecs, nn, p->len_diis, c);

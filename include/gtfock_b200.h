@@ -133,6 +133,10 @@ int gtf_batch_remove(gtf_batch_t *b, int slot);
 int gtf_batch_info(gtf_batch_t *b, int *nrunning, int *nused, double *ms_fock, double *ms_rest,
                    size_t *job_bytes);
 size_t gtf_batch_job_bytes(int nbf);
+/* Accumulated statistics of a batch: [0] ms of the Fock builds, [1] of the
+ * energies, [2] of DIIS, [3] of purification, [4] purification steps of the
+ * batched jobs, [5] batch steps.  Writes min(n, 6) values, returns that count. */
+int gtf_batch_stats(gtf_batch_t *b, double *out, int n);
 void gtf_batch_destroy(gtf_batch_t *b);
 
 /* Number of this library's own kernel launches so far (all threads). */
