@@ -41,6 +41,9 @@ sys.path.insert(0, ROOT)
 TOL = 1e-10
 NITER = 10
 MIXED_CUTOFF = 1e-6
+# DRAM bytes (read + write) of all k_fock launches of one C54H18 build, from one
+# ncu capture (profiles/fock_c54h18_dram_traffic.md); the kernels are FP64 bound
+FOCK_BUILD_DRAM_BYTES = 786.6e6 + 0.8e6
 METRIC = "SCF solves/s (C54H18 cc-pVDZ, 10 iterations, FP64)"
 WORKLOAD = "C54H18 graphene flake / cc-pVDZ (846 bf), Schwarz 1e-10, 10 SCF iterations, FP64"
 
@@ -269,7 +272,8 @@ def run(args):
                 "h2d_bytes_per_step": int(e2e_bytes[0]), "d2h_bytes_per_step": int(e2e_bytes[1])},
         "gpu_launches": int(launches),
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak, "traffic": FOCK_BUILD_DRAM_BYTES,
+                     "traffic_unit": "bytes per build (ncu dram__bytes_read + write, profiles/)",
                      "kernel": "k_fock<*> (all class pairs of one Fock build)",
                      "peak_source": "FP64 FMA probe kernel measured in this run "
                                     "(MEASURED_PEAKS.json has no FP64 figure)",
