@@ -75,8 +75,9 @@ struct ClassPairTask {
     double nquart, nquart32;     // quartets in all, of which evaluated in FP32
     int *d_nket;                 // [nbra][GTF_NBKT] kets per (bra, segment)
     int *d_n64;                  // [nbra][GTF_NBKT] of which FP64 (a prefix)
-    long long *d_unit_prefix;    // [nbra * GTF_NBKT + 1], FP64 launch
-    long long *d_unit_prefix32;  // [nbra * GTF_NBKT + 1], FP32 launch
+    int *d_cum64, *d_cum32;      // [nbra][GTF_CUM] per-bra segment prefixes of the two launches
+    long long *d_unit_prefix;    // [nbra + 1], FP64 launch
+    long long *d_unit_prefix32;  // [nbra + 1], FP32 launch
 };
 
 struct gtf_fock_dev {
@@ -534,17 +535,11 @@ struct SegStarts {
 // prefix and go to the FP32 launch; n64 counts the FP64 head.
 __global__ void k_count_kets(const double *__restrict__ pair_v, int bra_start, int nbra, int ket_start,
                              SegStarts seg, int same, double tol2, double cut2, int *__restrict__ nket,
-                             int *__restrict__ n64, long long *__restrict__ units64,
-                             long long *__restrict__ units32)
+                             int *__restrict__ n64)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int nidx = nbra * GTF_NBKT;
-    if (t > nidx) return;
-    if (t == nidx) {
-        units64[nidx] = 0;
-        units32[nidx] = 0;
-        return;
-    }
+    if (t >= nidx) return;
     const int i = t / GTF_NBKT, b = t - i * GTF_NBKT;
     const double v = pair_v[bra_start + i];
     const int s0 = seg.s[b], s1 = seg.s[b + 1];
@@ -569,8 +564,36 @@ __global__ void k_count_kets(const double *__restrict__ pair_v, int bra_start, i
     }
     nket[t] = c;
     n64[t] = c64;
-    units64[t] = b == 0 ? 0 : (c64 + 31) / 32;
-    units32[t] = b == 0 ? 0 : (c - c64 + 31) / 32;
+}
+
+// Per bra: the kets of all segments (in segment order, segment 0 left out)
+// form one list per launch part, so a warp's 32 lanes are filled across
+// segment boundaries.  cum[i][b] is the exclusive prefix of the segment
+// counts (cum[i][GTF_NBKT] = the bra's total); units[i] = ceil(total / 32).
+__global__ void k_pack_units(int nbra, const int *__restrict__ nket, const int *__restrict__ n64,
+                             int *__restrict__ cum64, int *__restrict__ cum32, long long *__restrict__ units64,
+                             long long *__restrict__ units32)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > nbra) return;
+    if (i == nbra) {
+        units64[nbra] = 0;
+        units32[nbra] = 0;
+        return;
+    }
+    int a = 0, c = 0;
+    for (int b = 0; b < GTF_NBKT; b++) {
+        cum64[i * GTF_CUM + b] = a;
+        cum32[i * GTF_CUM + b] = c;
+        if (b == 0) continue;  // pairs whose primitive pairs were all screened out
+        const int n = nket[i * GTF_NBKT + b], h = n64[i * GTF_NBKT + b];
+        a += h;
+        c += n - h;
+    }
+    cum64[i * GTF_CUM + GTF_NBKT] = a;
+    cum32[i * GTF_CUM + GTF_NBKT] = c;
+    units64[i] = (a + 31) / 32;
+    units32[i] = (c + 31) / 32;
 }
 
 typedef int (*fock_group_launch_t)(int la, int lb, int lc, int ld, const FockGrid &g, cudaStream_t st);
@@ -692,26 +715,29 @@ static int build_units(gtf_fock_dev *f)
         const int nidx = t.nbra * GTF_NBKT;
         SegStarts seg;
         for (int bk = 0; bk <= GTF_NBKT; bk++) seg.s[bk] = t.seg[bk];
+        const int nb1 = t.nbra + 1;
         long long *d_units;
-        CK(cudaMalloc(&d_units, sizeof(long long) * 2 * (nidx + 1)));
-        k_count_kets<<<(nidx + 1 + 255) / 256, 256, 0, st>>>(f->d_pair_v, t.bra_start, t.nbra, t.ket_start, seg,
-                                                            t.X == t.Y, f->tolscr2, cut2, t.d_nket, t.d_n64,
-                                                            d_units, d_units + nidx + 1);
+        CK(cudaMalloc(&d_units, sizeof(long long) * 2 * nb1));
+        k_count_kets<<<(nidx + 255) / 256, 256, 0, st>>>(f->d_pair_v, t.bra_start, t.nbra, t.ket_start, seg,
+                                                        t.X == t.Y, f->tolscr2, cut2, t.d_nket, t.d_n64);
+        CK(cudaGetLastError());
+        k_pack_units<<<(nb1 + 255) / 256, 256, 0, st>>>(t.nbra, t.d_nket, t.d_n64, t.d_cum64, t.d_cum32, d_units,
+                                                       d_units + nb1);
         CK(cudaGetLastError());
         size_t b4 = 0;
-        CK(cub::DeviceScan::ExclusiveSum(nullptr, b4, d_units, t.d_unit_prefix, nidx + 1, st));
+        CK(cub::DeviceScan::ExclusiveSum(nullptr, b4, d_units, t.d_unit_prefix, nb1, st));
         if (b4 > tmp_cap) {
             if (d_tmp) cudaFree(d_tmp);
             tmp_cap = b4;
             CK(cudaMalloc(&d_tmp, tmp_cap));
         }
         b4 = tmp_cap;
-        CK(cub::DeviceScan::ExclusiveSum(d_tmp, b4, d_units, t.d_unit_prefix, nidx + 1, st));
+        CK(cub::DeviceScan::ExclusiveSum(d_tmp, b4, d_units, t.d_unit_prefix, nb1, st));
         b4 = tmp_cap;
-        CK(cub::DeviceScan::ExclusiveSum(d_tmp, b4, d_units + nidx + 1, t.d_unit_prefix32, nidx + 1, st));
+        CK(cub::DeviceScan::ExclusiveSum(d_tmp, b4, d_units + nb1, t.d_unit_prefix32, nb1, st));
         std::vector<int> nk(nidx), n64(nidx);
-        CK(cudaMemcpyAsync(&t.nunits, t.d_unit_prefix + nidx, sizeof(long long), cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(&t.nunits32, t.d_unit_prefix32 + nidx, sizeof(long long), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&t.nunits, t.d_unit_prefix + t.nbra, sizeof(long long), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&t.nunits32, t.d_unit_prefix32 + t.nbra, sizeof(long long), cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(nk.data(), t.d_nket, sizeof(int) * nidx, cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(n64.data(), t.d_n64, sizeof(int) * nidx, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
@@ -921,8 +947,10 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
             const int nidx = t.nbra * GTF_NBKT;
             DALLOC(t.d_nket, nidx);
             DALLOC(t.d_n64, nidx);
-            DALLOC(t.d_unit_prefix, nidx + 1);
-            DALLOC(t.d_unit_prefix32, nidx + 1);
+            DALLOC(t.d_cum64, (size_t)t.nbra * GTF_CUM);
+            DALLOC(t.d_cum32, (size_t)t.nbra * GTF_CUM);
+            DALLOC(t.d_unit_prefix, t.nbra + 1);
+            DALLOC(t.d_unit_prefix32, t.nbra + 1);
         }
     }
     {
@@ -1031,6 +1059,8 @@ extern "C" void gtf_fock_destroy(gtf_fock_dev_t *f)
         if (f->tasks[c].d_nket) cudaFree(f->tasks[c].d_nket);
         if (f->tasks[c].d_unit_prefix) cudaFree(f->tasks[c].d_unit_prefix);
         if (f->tasks[c].d_n64) cudaFree(f->tasks[c].d_n64);
+        if (f->tasks[c].d_cum64) cudaFree(f->tasks[c].d_cum64);
+        if (f->tasks[c].d_cum32) cudaFree(f->tasks[c].d_cum32);
         if (f->tasks[c].d_unit_prefix32) cudaFree(f->tasks[c].d_unit_prefix32);
     }
     if (f->d_host_stage) cudaFreeHost(f->d_host_stage);
@@ -1144,7 +1174,7 @@ static void fill_launch(const gtf_fock_dev *f, int c, int part, const double *D,
     a.pairs = f->d_pairs;
     a.pprec = reinterpret_cast<const double2 *>(f->d_pp);
     a.nlo = part ? t.d_n64 : nullptr;
-    a.nket = part ? t.d_nket : t.d_n64;
+    a.cum = part ? t.d_cum32 : t.d_cum64;
     a.unit_prefix = part ? t.d_unit_prefix32 : t.d_unit_prefix;
     a.nbra = t.nbra;
     a.nunits = part ? t.nunits32 : t.nunits;

@@ -14,6 +14,7 @@
 // primitive-pair count (gtf_prim_bucket), each sorted by Schwarz bound, so the
 // 32 lanes of a warp loop over about the same number of primitive quartets.
 #define GTF_NBKT 15
+#define GTF_CUM 16   // per-bra segment prefix: GTF_NBKT + 1 entries
 __host__ __device__ inline int gtf_prim_bucket(int n)
 {
     if (n <= 2) return n < 0 ? 0 : n;
@@ -36,9 +37,9 @@ __host__ __device__ inline int gtf_prim_bucket(int n)
 struct FockLaunch {
     const PairRec *pairs;
     const double2 *pprec;          // primitive-pair records (PPRec)
-    const int *nlo;                // [nbra][GTF_NBKT] first ket of this launch in the segment prefix (null: 0)
-    const int *nket;               // [nbra][GTF_NBKT] end of this launch's kets in the segment prefix
-    const long long *unit_prefix;  // exclusive prefix of units over (bra, segment)
+    const int *nlo;                // [nbra][GTF_NBKT] first ket of this launch in each segment prefix (null: 0)
+    const int *cum;                // [nbra][GTF_CUM] exclusive prefix over segments of this launch's kets
+    const long long *unit_prefix;  // [nbra + 1] exclusive prefix of units (32 kets) over bras
     int nbra;
     long long nunits;
     int bra_start, ket_start;
@@ -133,22 +134,34 @@ __global__ void __launch_bounds__(FOCK_THREADS,
         }
 #define GTF_FLD(x) (bt ? mp->x : g.one.x)
         const long long *unit_prefix = GTF_FLD(unit_prefix);
-        // unit u -> (bra i, segment b, chunk of 32 kets): binary search of the
-        // exclusive unit prefix over the flattened (bra, segment) index
-        const int nidx = GTF_FLD(nbra) * GTF_NBKT;
-        int lo = 0, hi = nidx;
+        // unit u -> (bra i, chunk of 32 kets) by binary search of the unit
+        // prefix over bras; lane v of the chunk -> segment b and position in
+        // it from the bra's segment prefix (the kets of consecutive segments
+        // share a warp)
+        const int nbra = GTF_FLD(nbra);
+        int lo = 0, hi = nbra;
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
             if (__ldg(unit_prefix + mid) <= (long long)u) lo = mid;
             else hi = mid;
         }
-        const int i = lo / GTF_NBKT, b = lo - i * GTF_NBKT;
-        const long long chunk = (long long)u - __ldg(unit_prefix + lo);
-        const int jj = (int)(chunk * 32) + lane;
+        const int i = lo;
+        const int v = (int)((long long)u - __ldg(unit_prefix + i)) * 32 + lane;
+        const int4 *cq = reinterpret_cast<const int4 *>(GTF_FLD(cum) + (size_t)i * GTF_CUM);
+        const int4 c0 = __ldg(cq), c1 = __ldg(cq + 1), c2 = __ldg(cq + 2), c3 = __ldg(cq + 3);
+        const int cum[GTF_CUM] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w,
+                                  c2.x, c2.y, c2.z, c2.w, c3.x, c3.y, c3.z, c3.w};
+        const bool active = v < cum[GTF_NBKT];
+        int b = 0, cb = 0;
+#pragma unroll
+        for (int k = 1; k < GTF_NBKT; k++)
+            if (cum[k] <= v) {
+                b = k;
+                cb = cum[k];
+            }
         const int *nlo = GTF_FLD(nlo);
-        const int k0 = nlo ? __ldg(nlo + lo) : 0;
-        const bool active = jj < __ldg(GTF_FLD(nket) + lo) - k0;
-        const int j = GTF_FLD(seg[b]) + k0 + jj;
+        const int k0 = nlo ? __ldg(nlo + (size_t)i * GTF_NBKT + b) : 0;
+        const int j = GTF_FLD(seg[b]) + k0 + (v - cb);
         const PairRec *pairs = GTF_FLD(pairs);
         const int bra_start = GTF_FLD(bra_start), ket_start = GTF_FLD(ket_start);
         const PairRec pb = pairs[bra_start + i];
