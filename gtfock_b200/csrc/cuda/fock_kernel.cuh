@@ -71,13 +71,13 @@ struct FockGrid {
 // ~54 accumulators in registers (the Rys roots and 2-D tables are
 // recomputed per slice, which costs less than spilling the accumulators).
 // FP32 values take one register each, so the FP32 kernels keep quartets of
-// up to 81 integrals in one pass; larger FP32 slices spill like the FP64 ones
-// (the FP32 2-D tables and roots are live at the same time).
+// up to 81 integrals in one pass and slices of up to ~72 accumulators (wider
+// FP32 slices spill, as FP64 slices wider than ~54 do).
 __host__ __device__ constexpr int fock_slice(int LA, int LB, int LC, int LD, int fp32)
 {
     const int nab = ncart(LA) * ncart(LB), ncd = ncart(LC) * ncart(LD);
     if (nab * ncd <= (fp32 ? 81 : 64)) return ncd;
-    const int s = 54 / nab;
+    const int s = (fp32 ? 72 : 54) / nab;
     return s < 1 ? 1 : (s > ncd ? ncd : s);
 }
 
