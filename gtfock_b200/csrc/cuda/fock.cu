@@ -121,6 +121,9 @@ struct gtf_fock_dev {
     int prec;
     double fp32_cutoff;
     size_t dev_bytes;
+    // non-symmetric densities (PFock_create with symm = 0)
+    int nosymm;
+    double *d_Ds, *d_Da, *d_Dca, *d_Fka;
 };
 
 template <typename T>
@@ -199,11 +202,14 @@ __global__ void k_d_to_cart(const double *__restrict__ D, double *__restrict__ D
 }
 
 // J = T sym(Fj) T^T, K = T sym(Fk) T^T, F = J + K (pfock/pfock.c:1719-1726, 1161-1185)
+// Fka (non-symmetric densities only, else null): exchange accumulator of the
+// antisymmetric part of D, whose full contribution is (Fka - Fka^T) / 2
 __device__ __forceinline__ void f_to_sph_elem(const double *__restrict__ Fj, const double *__restrict__ Fk,
                                               double *__restrict__ F, double *__restrict__ J, double *__restrict__ K,
                                               const int *__restrict__ sph2shell, const int *__restrict__ sh_L,
                                               const int *__restrict__ f_start, const int *__restrict__ fc_start,
-                                              int nbf, int nbfc, int pure, int m, int n)
+                                              int nbf, int nbfc, int pure, int m, int n,
+                                              const double *__restrict__ Fka = nullptr)
 {
     const int sm = sph2shell[m], sn = sph2shell[n];
     const int cm = m - f_start[sm], cn = n - f_start[sn];
@@ -221,6 +227,7 @@ __device__ __forceinline__ void f_to_sph_elem(const double *__restrict__ Fj, con
             const size_t ba = (size_t)(fn + b) * nbfc + fm + a;
             j += ta * tb * (0.5 * (Fj[ab] + Fj[ba]));
             k += ta * tb * (0.5 * (Fk[ab] + Fk[ba]));
+            if (Fka) k += ta * tb * (0.5 * (Fka[ab] - Fka[ba]));
         }
     }
     const size_t o = (size_t)m * nbf + n;
@@ -233,12 +240,23 @@ __global__ void k_f_to_sph(const double *__restrict__ Fj, const double *__restri
                            double *__restrict__ F, double *__restrict__ J, double *__restrict__ K,
                            const int *__restrict__ sph2shell, const int *__restrict__ sh_L,
                            const int *__restrict__ f_start, const int *__restrict__ fc_start,
-                           int nbf, int nbfc, int pure)
+                           int nbf, int nbfc, int pure, const double *__restrict__ Fka = nullptr)
 {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     const int m = blockIdx.y;
     if (n >= nbf) return;
-    f_to_sph_elem(Fj, Fk, F, J, K, sph2shell, sh_L, f_start, fc_start, nbf, nbfc, pure, m, n);
+    f_to_sph_elem(Fj, Fk, F, J, K, sph2shell, sh_L, f_start, fc_start, nbf, nbfc, pure, m, n, Fka);
+}
+
+// non-symmetric D: Ds = (D + D^T) / 2, Da = (D - D^T) / 2
+__global__ void k_split_density(const double *__restrict__ D, double *__restrict__ Ds, double *__restrict__ Da, int n)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y;
+    if (j >= n) return;
+    const double a = D[(size_t)i * n + j], t = D[(size_t)j * n + i];
+    Ds[(size_t)i * n + j] = 0.5 * (a + t);
+    Da[(size_t)i * n + j] = 0.5 * (a - t);
 }
 
 // ---------------------------------------------------------------------------
@@ -1052,7 +1070,7 @@ extern "C" void gtf_fock_destroy(gtf_fock_dev_t *f)
                     f->d_cart2shell, f->d_Z, f->d_sh_xyz, f->d_alpha, f->d_coef, f->d_atom_xyz, f->d_sq,
                     f->d_shellptr, f->d_shellid, f->d_shellrid, f->d_shellvalue, f->d_pairs, f->d_pair_v,
                     f->d_pp, f->d_counters, f->d_D, f->d_Dc, f->d_Fj, f->d_Fk, f->d_F, f->d_J, f->d_K,
-                    f->d_S, f->d_X, f->d_H};
+                    f->d_S, f->d_X, f->d_H, f->d_Ds, f->d_Da, f->d_Dca, f->d_Fka};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (int c = 0; c < NCLSPAIR; c++) {
@@ -1155,6 +1173,25 @@ extern "C" int gtf_fock_put_density_dev(gtf_fock_dev_t *f, int index, const doub
     return GTF_OK;
 }
 
+// Non-symmetric densities (PFock_create with symm = 0): buffers for the
+// symmetric and antisymmetric parts and the second exchange accumulator.
+extern "C" int gtf_fock_set_nosymm(gtf_fock_dev_t *f, int on)
+{
+    if (!on) {
+        f->nosymm = 0;
+        return GTF_OK;
+    }
+    if (!f->d_Fka) {
+        const size_t nn = (size_t)f->nbf * f->nbf, nnc = (size_t)f->nbf_cart * f->nbf_cart;
+        DALLOC(f->d_Ds, nn);
+        DALLOC(f->d_Da, nn);
+        DALLOC(f->d_Dca, nnc);
+        DALLOC(f->d_Fka, nnc);
+    }
+    f->nosymm = 1;
+    return GTF_OK;
+}
+
 extern "C" int gtf_fock_set_precision(gtf_fock_dev_t *f, int prec, double fp32_cutoff)
 {
     if (prec != GTF_PREC_FP64 && prec != GTF_PREC_MIXED) return GTF_ERR_INVALID;
@@ -1167,7 +1204,7 @@ extern "C" int gtf_fock_set_precision(gtf_fock_dev_t *f, int prec, double fp32_c
 // The descriptor of class pair c, part 0 (FP64 head of every ket range) or
 // part 1 (FP32 tail), of one engine.
 static void fill_launch(const gtf_fock_dev *f, int c, int part, const double *D, double *Fj, double *Fk,
-                        FockLaunch &a)
+                        FockLaunch &a, int konly = 0)
 {
     const ClassPairTask &t = f->tasks[c];
     memset(&a, 0, sizeof(a));
@@ -1185,6 +1222,7 @@ static void fill_launch(const gtf_fock_dev *f, int c, int part, const double *D,
     a.Fj = Fj;
     a.Fk = Fk;
     a.ld = f->nbf_cart;
+    a.konly = konly;
 }
 
 // Launches the Fock kernels of class pair c: the FP64 part of every ket
@@ -1192,7 +1230,7 @@ static void fill_launch(const gtf_fock_dev *f, int c, int part, const double *D,
 // GTF_MAX_SLICES zeroed slots per (class pair, part), one per slice launch.
 // Returns the number of launches, or -1 on a launch error.
 static int launch_class(const gtf_fock_dev *f, int c, const double *D, double *Fj, double *Fk,
-                        unsigned long long *counters, cudaStream_t st)
+                        unsigned long long *counters, cudaStream_t st, int konly = 0)
 {
     const ClassPairTask &t = f->tasks[c];
     int n = 0;
@@ -1201,7 +1239,7 @@ static int launch_class(const gtf_fock_dev *f, int c, const double *D, double *F
         if (nu == 0) continue;
         FockGrid g;
         memset(&g, 0, sizeof(g));
-        fill_launch(f, c, part, D, Fj, Fk, g.one);
+        fill_launch(f, c, part, D, Fj, Fk, g.one, konly);
         g.nmol = 1;
         g.nunits = nu;
         g.counter = counters + (size_t)(2 * c + part) * GTF_MAX_SLICES;
@@ -1229,6 +1267,16 @@ extern "C" int gtf_fock_compute(gtf_fock_dev_t *f, int numdmat)
     float eri_ms_total = 0.0f;
     for (int d = 0; d < numdmat; d++) {
         const double *D = f->d_D + nn * d;
+        if (f->nosymm) {
+            // exact 2 J[D] - K[D] for a general D: the symmetric part goes
+            // through the usual build, the antisymmetric part only through
+            // the exchange terms (it has no Coulomb contribution)
+            dim3 g((nbf + 127) / 128, nbf);
+            k_split_density<<<g, 128, 0, st>>>(D, f->d_Ds, f->d_Da, nbf);
+            CK(cudaGetLastError());
+            gtf_note_launches(1);
+            D = f->d_Ds;
+        }
         const double *Dc = D;
         if (need_tr) {
             dim3 g((nbfc + 127) / 128, nbfc);
@@ -1250,12 +1298,30 @@ extern "C" int gtf_fock_compute(gtf_fock_dev_t *f, int numdmat)
             if (r < 0) return GTF_ERR_CUDA;
             gtf_note_launches(r);
         }
+        if (f->nosymm) {
+            const double *Dca = f->d_Da;
+            if (need_tr) {
+                dim3 g((nbfc + 127) / 128, nbfc);
+                k_d_to_cart<<<g, 128, 0, st>>>(f->d_Da, f->d_Dca, f->d_cart2shell, f->d_sh_L, f->d_f_start,
+                                               f->d_fc_start, nbf, nbfc, f->pure);
+                CK(cudaGetLastError());
+                gtf_note_launches(1);
+                Dca = f->d_Dca;
+            }
+            CK(cudaMemsetAsync(f->d_Fka, 0, sizeof(double) * nnc, st));
+            CK(cudaMemsetAsync(f->d_counters, 0, sizeof(unsigned long long) * 2 * NCLSPAIR * GTF_MAX_SLICES, st));
+            for (int c = 0; c < NCLSPAIR; c++) {
+                const int r = launch_class(f, c, Dca, f->d_Fj, f->d_Fka, f->d_counters, st, 1);
+                if (r < 0) return GTF_ERR_CUDA;
+                gtf_note_launches(r);
+            }
+        }
         CK(cudaEventRecord(f->ev_cls[NCLSPAIR], st));
         CK(cudaEventRecord(f->ev2, st));
         dim3 g2((nbf + 127) / 128, nbf);
         k_f_to_sph<<<g2, 128, 0, st>>>(f->d_Fj, f->d_Fk, f->d_F + nn * d, f->d_J + nn * d, f->d_K + nn * d,
                                        f->d_sph2shell, f->d_sh_L, f->d_f_start, f->d_fc_start, nbf, nbfc,
-                                       f->pure);
+                                       f->pure, f->nosymm ? f->d_Fka : nullptr);
         CK(cudaGetLastError());
         gtf_note_launches(1);
         CK(cudaEventSynchronize(f->ev2));
@@ -1463,6 +1529,10 @@ static int fixed_scratch(int dev, double **out)
 
 extern "C" int gtf_fock_compute_fixed(gtf_fock_dev_t *f, const double *dev_D, double *dev_F)
 {
+    if (f->nosymm) {
+        snprintf(g_errbuf, sizeof(g_errbuf), "allocation-free Fock build: non-symmetric densities are not supported");
+        return GTF_ERR_INVALID;
+    }
     if (f == nullptr || dev_D == nullptr || dev_F == nullptr || f->max_numdmat <= 0) return GTF_ERR_INVALID;
     const int nbf = f->nbf, nbfc = f->nbf_cart;
     if (nbfc > GTF_FIXED_MAX_FUNCS || nbf > GTF_FIXED_MAX_FUNCS) {

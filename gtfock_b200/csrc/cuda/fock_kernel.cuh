@@ -47,6 +47,7 @@ struct FockLaunch {
     const double *D;
     double *Fj, *Fk;
     int ld;
+    int konly;                     // exchange terms only (antisymmetric part of a non-symmetric D)
 };
 
 // A launch over one molecule (nmol == 1: `one`) or a batch of molecules
@@ -173,7 +174,7 @@ __global__ void __launch_bounds__(FOCK_THREADS,
         for (int k = 0; k < ncart(LA) * ncart(LB) * N; k++) acc[k] = (R)0;
         if (active) eri_accumulate_cd<LA, LB, LC, LD, CD0, N, true>(src, pb, src, pk, acc, tab);
         digest_cd<LA, LB, LC, LD, CD0, N>(acc, active, pb, pk, same, GTF_FLD(D), GTF_FLD(Fj), GTF_FLD(Fk),
-                                          GTF_FLD(ld), lane);
+                                          GTF_FLD(ld), lane, GTF_FLD(konly) != 0);
 #undef GTF_FLD
     }
 }

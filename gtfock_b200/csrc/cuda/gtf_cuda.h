@@ -77,6 +77,8 @@ void gtf_fock_release_onee(gtf_fock_dev_t *f, int which);
 
 /* precision control and statistics */
 int gtf_fock_set_precision(gtf_fock_dev_t *f, int prec, double fp32_cutoff);
+/* non-symmetric densities: F = 2 J[D] - K[D] exactly for a general D */
+int gtf_fock_set_nosymm(gtf_fock_dev_t *f, int on);
 int gtf_fock_last_timing(gtf_fock_dev_t *f, double *ms_total, double *ms_eri, double *ms_other);
 int gtf_fock_eri_flops(gtf_fock_dev_t *f, double *flops);
 /* batched Fock builds over many engines (molecules): one launch per class

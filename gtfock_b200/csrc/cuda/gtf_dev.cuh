@@ -506,7 +506,7 @@ template <int LA, int LB, int LC, int LD, int CD0, int N, typename R>
 __device__ __forceinline__ void digest_cd(const R (&I)[ncart(LA) * ncart(LB) * N], bool active,
                                           const PairRec &pb, const PairRec &pk, bool same_pair,
                                           const double *__restrict__ D, double *__restrict__ Fj,
-                                          double *__restrict__ Fk, int ld, int lane)
+                                          double *__restrict__ Fk, int ld, int lane, bool konly = false)
 {
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     const int fa = pb.fa, fb = pb.fb, fc = pk.fa, fd = pk.fb;
@@ -517,8 +517,9 @@ __device__ __forceinline__ void digest_cd(const R (&I)[ncart(LA) * ncart(LB) * N
     const double sJcd = f3 * sJab;
     const double sKac = -(1.0 + f3);
     const double sKbc = f1 * sKac, sKad = f2 * sKac, sKbd = f1 * f2 * sKac;
-    // bra block J (warp-uniform destination), partial over the slice
-    {
+    // bra block J (warp-uniform destination), partial over the slice; konly
+    // (warp-uniform) skips both Coulomb terms
+    if (!konly) {
         double dcd[N];
 #pragma unroll
         for (int t = 0; t < N; t++) {
@@ -539,7 +540,7 @@ __device__ __forceinline__ void digest_cd(const R (&I)[ncart(LA) * ncart(LB) * N
     }
     if (!active) return;
     // ket block J: complete per (c, d)
-    if (f3 != 0.0) {
+    if (f3 != 0.0 && !konly) {
         double dab[NA * NB];
 #pragma unroll
         for (int ia = 0; ia < NA; ia++)

@@ -103,11 +103,6 @@ PFockStatus_t PFock_create(BasisSet_t basis, int nprow, int npcol, int ntasks,
         PFOCK_PRINTF(1, "Invalid number of density matrices\n");
         return PFOCK_STATUS_INVALID_VALUE;
     }
-    if (symm == 0) {
-        /* non-symmetric densities (pfock/pfock.c:1704-1718) are not built */
-        PFOCK_PRINTF(1, "Non-symmetric density matrices are not supported\n");
-        return PFOCK_STATUS_INVALID_VALUE;
-    }
     PFock_t pf = (PFock_t)calloc(1, sizeof(struct PFock));
     if (pf == NULL) {
         PFOCK_PRINTF(1, "Failed to allocate memory: %zu\n", sizeof(struct PFock));
@@ -131,6 +126,19 @@ PFockStatus_t PFock_create(BasisSet_t basis, int nprow, int npcol, int ntasks,
         if (pf->dev) gtf_fock_destroy(pf->dev);
         free(pf);
         return map_err(e);
+    }
+    /* symm = 0 (pfock/pfock.c:828): densities may be non-symmetric.  The
+     * engine forms F = 2 J[D] - K[D] exactly for a general D: the symmetric
+     * part of D through the usual build, the antisymmetric part through the
+     * exchange terms only.  For a symmetric D this is the symm = 1 result. */
+    if (symm == 0) {
+        e = gtf_fock_set_nosymm(pf->dev, 1);
+        if (e != GTF_OK) {
+            gtf_fock_destroy(pf->dev);
+            free(pf);
+            return map_err(e);
+        }
+        pf->nosymm = 1;
     }
     pf->mem_cpu = sizeof(struct PFock) + (double)gtf_fock_device_bytes(pf->dev);
     *_pfock = pf;

@@ -9,7 +9,9 @@
  *                  density read from <D.bin> (nbf*nbf doubles, row-major)
  * Test infrastructure only.
  *
- * usage: ref_probe <basis.gbs> <mol.xyz> <tolscr> <ntasks> <D.bin> <out>
+ * usage: ref_probe <basis.gbs> <mol.xyz> <tolscr> <ntasks> <D.bin> <out> [symm]
+ * symm 0 runs the reference's non-symmetric-density path (PFock_create's
+ * symm argument, pfock/pfock.c:828, 1117-1121, 1704-1718).
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -20,10 +22,11 @@
 
 int main(int argc, char **argv)
 {
-    if (argc != 7) {
-        fprintf(stderr, "usage: %s basis xyz tolscr ntasks D.bin out\n", argv[0]);
+    if (argc != 7 && argc != 8) {
+        fprintf(stderr, "usage: %s basis xyz tolscr ntasks D.bin out [symm]\n", argv[0]);
         return 2;
     }
+    const int symm = argc == 8 ? atoi(argv[7]) : 1;
     int provided;
     MPI_Init_thread(&argc, &argv, MPI_THREAD_MULTIPLE, &provided);
     BasisSet_t basis;
@@ -32,7 +35,7 @@ int main(int argc, char **argv)
     double tol = atof(argv[3]);
     int ntasks = atoi(argv[4]);
     PFock_t pf;
-    if (PFock_create(basis, 1, 1, ntasks, tol, 1, 1, &pf) != PFOCK_STATUS_SUCCESS) return 4;
+    if (PFock_create(basis, 1, 1, ntasks, tol, 1, symm, &pf) != PFOCK_STATUS_SUCCESS) return 4;
     int nshells = pf->nshells, nnz = pf->nnz, nbf = pf->nbf;
     char path[2048];
     snprintf(path, sizeof(path), "%s.screen", argv[6]);
