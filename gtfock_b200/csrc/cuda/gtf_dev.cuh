@@ -124,10 +124,24 @@ struct RysTab<float> {
     static __device__ __forceinline__ const float *ptr(int n) { return RYS32_TABLE + off(n); }
 };
 
+// interval width and polynomial degree of the N-root FP64 table
+__host__ __device__ constexpr double rys_h(int n)
+{
+    constexpr double h[] = {RYS_H_LIST};
+    return h[n];
+}
+__host__ __device__ constexpr int rys_deg(int n)
+{
+    constexpr int d[] = {RYS_DEG_LIST};
+    return d[n];
+}
+
 // tab: the N-root block of RYS_TABLE (global or a shared-memory copy)
 template <int N>
 __device__ __forceinline__ void rys_roots(double T, double (&u)[N], double (&w)[N], const double *tab)
 {
+    constexpr double H = rys_h(N), INV_H = 1.0 / rys_h(N);
+    constexpr int DEG = rys_deg(N);
     if (T >= RYS_TMAX[N]) {
         const double it = 1.0 / T;
         const double rs = rsqrt(T);
@@ -138,20 +152,20 @@ __device__ __forceinline__ void rys_roots(double T, double (&u)[N], double (&w)[
         }
         return;
     }
-    const int k = (int)(T * RYS_INV_H);
-    const double s = T - ((double)k * RYS_H + 0.5 * RYS_H);
-    const double *c = tab + k * (RYS_DEG + 1) * (2 * N);
+    const int k = (int)(T * INV_H);
+    const double s = T - ((double)k * H + 0.5 * H);
+    const double *c = tab + k * (DEG + 1) * (2 * N);
     // rows of 2N coefficients start on 16-byte boundaries (even offsets)
     const double2 *c2 = reinterpret_cast<const double2 *>(c);
     double a[2 * N];
 #pragma unroll
     for (int f = 0; f < N; f++) {
-        const double2 t = c2[RYS_DEG * N + f];
+        const double2 t = c2[DEG * N + f];
         a[2 * f] = t.x;
         a[2 * f + 1] = t.y;
     }
 #pragma unroll
-    for (int j = RYS_DEG - 1; j >= 0; j--) {
+    for (int j = DEG - 1; j >= 0; j--) {
 #pragma unroll
         for (int f = 0; f < N; f++) {
             const double2 t = c2[j * N + f];

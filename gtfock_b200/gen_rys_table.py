@@ -11,13 +11,16 @@ Method (published, restated here):
   * Jacobi matrix from the moments by Gautschi's Chebyshev algorithm
     (W. Gautschi, "Orthogonal Polynomials: Computation and Approximation",
     Oxford 2004, sec. 2.1.7), nodes and weights by Golub-Welsch;
-  * on each interval [T0, T0 + H) every u_i(T) and w_i(T) is interpolated at
-    DEG+1 Chebyshev points and stored as a monomial series in s = T - (T0+H/2);
+  * on each interval [T0, T0 + H_n) every u_i(T) and w_i(T) is interpolated at
+    DEG_n+1 Chebyshev points and stored as a monomial series in
+    s = T - (T0+H_n/2); the interval and degree depend on the root count n
+    (narrower intervals and lower degrees for the few-root tables, which the
+    light shell classes evaluate most often);
   * for T >= TMAX[n] the large-T form is exact to double precision:
     u_i = x_i^2 / T, w_i = W_i / sqrt(T) with x_i > 0 the roots of the Hermite
     polynomial H_2n and W_i their Gauss-Hermite weights.
 Accuracy of the double table against the 60-digit values: <= 1e-15 relative
-(checked by tests/test_rys_table.py against values recomputed here).
+(checked by tests/test_oracle.py against values recomputed here).
 
 Run:  python -m gtfock_b200.gen_rys_table   (about a minute on 8 cores)
 """
@@ -28,8 +31,12 @@ import sys
 import mpmath as mp
 
 NMAX = 5            # roots needed for (dd|dd): L = 8 -> n = 5
-H = 2.0             # interval width in T
-DEG = 13            # polynomial degree per interval
+# interval width in T and polynomial degree per root count n (FP64 table):
+# each choice fits u_i and w_i to <= 6e-16 relative (measured at 9 points per
+# interval on sample intervals); the N-root block must fit in 48 KB of
+# shared memory, which keeps n = 5 on the wider intervals
+H64 = {1: 0.5, 2: 0.5, 3: 2.0, 4: 1.0, 5: 2.0}
+DEG64 = {1: 9, 2: 9, 3: 13, 4: 11, 5: 13}
 TMAX = {1: 40.0, 2: 48.0, 3: 56.0, 4: 62.0, 5: 70.0}
 # single-precision table for the mixed-precision kernels
 H32 = 2.0
@@ -103,10 +110,13 @@ def fit_interval(args):
 
 
 def build_table(h, deg, pool):
+    """h, deg: per root count (dict) or one value for all"""
     tables = {}
     for n in range(1, NMAX + 1):
-        nint = int(round(TMAX[n] / h))
-        res = pool.map(fit_interval, [(n, k * h, h, deg) for k in range(nint)])
+        hn = h[n] if isinstance(h, dict) else h
+        dn = deg[n] if isinstance(deg, dict) else deg
+        nint = int(round(TMAX[n] / hn))
+        res = pool.map(fit_interval, [(n, k * hn, hn, dn) for k in range(nint)])
         tables[n] = res
     return tables
 
@@ -122,15 +132,17 @@ def main(out_path=None):
         out_path = os.path.join(os.path.dirname(os.path.abspath(__file__)),
                                 "csrc", "cuda", "rys_table.h")
     with mproc.get_context("spawn").Pool(os.cpu_count()) as pool:
-        t64 = build_table(H, DEG, pool)
+        t64 = build_table(H64, DEG64, pool)
         t32 = build_table(H32, DEG32, pool)
     lines = []
     w = lines.append
     w("/* rys_table.h -- generated by gtfock_b200/gen_rys_table.py; do not edit.")
     w(" * Rys quadrature for the Boys weight: per root count n, per interval of")
-    w(" * width RYS_H in T, DEG+1 monomial coefficients in s = T - (T0 + H/2) for")
-    w(" * u_1..u_n then w_1..w_n, stored [interval][coef][func]; above RYS_TMAX[n]")
-    w(" * the Hermite large-T form u = x^2/T, w = W/sqrt(T) applies. */")
+    w(" * width H_n in T (RYS_H_LIST), DEG_n+1 monomial coefficients (RYS_DEG_LIST)")
+    w(" * in s = T - (T0 + H_n/2) for u_1..u_n then w_1..w_n, stored")
+    w(" * [interval][coef][func]; above RYS_TMAX[n] the Hermite large-T form")
+    w(" * u = x^2/T, w = W/sqrt(T) applies.  The FP32 table uses RYS32_H and")
+    w(" * RYS32_DEG for every n. */")
     w("#pragma once")
     w("#ifndef RYS_QUAL")
     w("#define RYS_QUAL static")
@@ -139,9 +151,8 @@ def main(out_path=None):
     w("#define RYS_QUAL_SMALL static")
     w("#endif")
     w("#define RYS_NMAX %d" % NMAX)
-    w("#define RYS_H %.1f" % H)
-    w("#define RYS_INV_H %.17e" % (1.0 / H))
-    w("#define RYS_DEG %d" % DEG)
+    w("#define RYS_H_LIST 0.0, %s" % ", ".join("%.2f" % H64[n] for n in range(1, NMAX + 1)))
+    w("#define RYS_DEG_LIST 0, %s" % ", ".join("%d" % DEG64[n] for n in range(1, NMAX + 1)))
     w("#define RYS32_H %.1f" % H32)
     w("#define RYS32_INV_H %.9ef" % (1.0 / H32))
     w("#define RYS32_DEG %d" % DEG32)
@@ -151,7 +162,7 @@ def main(out_path=None):
     for n in range(1, NMAX + 1):
         offs[n] = off
         for iv in t64[n]:
-            for j in range(DEG + 1):
+            for j in range(DEG64[n] + 1):
                 for f in range(2 * n):
                     flat.append(iv[f][j])
         off = len(flat)

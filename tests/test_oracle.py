@@ -163,3 +163,31 @@ def test_nosymm_fixtures_pinned():
         n = z["D_ns"].shape[0]
         assert z["F_ns"].shape == (n, n)
         assert np.abs(z["D_ns"] - z["D_ns"].T).max() > 1e-3
+
+
+def test_rys_table_accuracy():
+    """The FP64 Rys table of the CUDA kernels (csrc/cuda/rys_table.h) against
+    the 60-digit Gauss rule recomputed by its generator, at a few T per root
+    count (both ends of the interval range, interior points, interval
+    midpoints and edges)."""
+    import re
+    from gtfock_b200 import gen_rys_table as G
+    hdr = open(os.path.join(ROOT, "gtfock_b200", "csrc", "cuda", "rys_table.h")).read()
+    hl = [float(x) for x in re.search(r"#define RYS_H_LIST (.*)", hdr).group(1).split(",")]
+    dl = [int(x) for x in re.search(r"#define RYS_DEG_LIST (.*)", hdr).group(1).split(",")]
+    offs = [int(x) for x in re.search(r"#define RYS_OFF_LIST (.*)", hdr).group(1).split(",")]
+    body = hdr[hdr.index("RYS_TABLE[RYS_TABLE_LEN] = {") + 28:]
+    body = body[:body.index("};")]
+    tab = np.array([float(x) for x in body.replace("\n", " ").split(",") if x.strip()])
+    worst = 0.0
+    for n in range(1, 6):
+        h, deg = hl[n], dl[n]
+        for T in (0.0, 0.3 * h, 2.6, 11.0 + 0.5 * h, 23.7, G.TMAX[n] - 1e-3):
+            k = int(T / h)
+            s = T - (k * h + 0.5 * h)
+            c = tab[offs[n] + k * (deg + 1) * 2 * n:][:(deg + 1) * 2 * n].reshape(deg + 1, 2 * n)
+            vals = np.polynomial.polynomial.polyval(s, c)   # c[j][f]: coefficient j of function f
+            u, w = G.gauss_rule(T, n)
+            ref = np.array([float(x) for x in list(u) + list(w)])
+            worst = max(worst, float(np.max(np.abs(vals - ref) / np.abs(ref))))
+    assert worst < 2e-15, worst
