@@ -102,6 +102,7 @@ struct gtf_fock_dev {
     double *d_pair_v;
     int nprimpairs;
     double *d_pp;   // 6 * nprimpairs: records {p, K, Px, Py, Pz, 1/(2p)} (PPRec)
+    float *d_pp32;  // 8 * nprimpairs: FP32 records {p, K, PA, 1/(2p), 0, 0} (PPRec32)
     ClassPairTask tasks[NCLSPAIR];
     unsigned long long *d_counters;
     double usq, uitl, eri_flops;
@@ -538,6 +539,29 @@ __global__ void k_fill_primpairs(PairRec *__restrict__ pairs, const int *__restr
     pairs[s].n = kept;
 }
 
+// FP32 records of the kept primitive pairs: centre relative to the pair's
+// first shell, so that single precision keeps the small differences
+__global__ void k_fill_pp32(const PairRec *__restrict__ pairs, int npairs, const double *__restrict__ pp,
+                            float *__restrict__ pp32)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= npairs) return;
+    const PairRec r = pairs[s];
+    constexpr int W = 2 * GTF_PPREC_D2;
+    for (int i = 0; i < r.n; i++) {
+        const double *d = pp + W * ((size_t)r.off + i);
+        float *o = pp32 + 8 * ((size_t)r.off + i);
+        o[0] = (float)d[0];
+        o[1] = (float)d[1];
+        o[2] = (float)(d[2] - r.Ax);
+        o[3] = (float)(d[3] - r.Ay);
+        o[4] = (float)(d[4] - r.Az);
+        o[5] = (float)d[5];
+        o[6] = 0.0f;
+        o[7] = 0.0f;
+    }
+}
+
 // number of ket pairs of segment b of the ket class that pass
 // v_bra * v_ket >= tol2 (pfock/fock_task.c:192): each segment is sorted by
 // value, descending, so they form a prefix.  For bra class == ket class only
@@ -931,9 +955,12 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
     CK(cudaStreamSynchronize(st));
     f->nprimpairs = npp;
     DALLOC(f->d_pp, 2 * GTF_PPREC_D2 * (size_t)(npp > 0 ? npp : 1));
+    DALLOC(f->d_pp32, 8 * (size_t)(npp > 0 ? npp : 1));
     if (nnz > 0) {
         k_fill_primpairs<<<gp, 256, 0, st>>>(f->d_pairs, d_idx, f->d_shellid, f->d_shellrid, d_pair_off, bd,
                                              nnz, f->d_pp);
+        CK(cudaGetLastError());
+        k_fill_pp32<<<gp, 256, 0, st>>>(f->d_pairs, nnz, f->d_pp, f->d_pp32);
         CK(cudaGetLastError());
     }
     // class and segment starts from the sorted keys (class * 16 + bucket)
@@ -1069,7 +1096,7 @@ extern "C" void gtf_fock_destroy(gtf_fock_dev_t *f)
     void *ptrs[] = {f->d_sh_L, f->d_sh_nprim, f->d_sh_pstart, f->d_f_start, f->d_fc_start, f->d_sph2shell,
                     f->d_cart2shell, f->d_Z, f->d_sh_xyz, f->d_alpha, f->d_coef, f->d_atom_xyz, f->d_sq,
                     f->d_shellptr, f->d_shellid, f->d_shellrid, f->d_shellvalue, f->d_pairs, f->d_pair_v,
-                    f->d_pp, f->d_counters, f->d_D, f->d_Dc, f->d_Fj, f->d_Fk, f->d_F, f->d_J, f->d_K,
+                    f->d_pp, f->d_pp32, f->d_counters, f->d_D, f->d_Dc, f->d_Fj, f->d_Fk, f->d_F, f->d_J, f->d_K,
                     f->d_S, f->d_X, f->d_H, f->d_Ds, f->d_Da, f->d_Dca, f->d_Fka};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -1210,6 +1237,7 @@ static void fill_launch(const gtf_fock_dev *f, int c, int part, const double *D,
     memset(&a, 0, sizeof(a));
     a.pairs = f->d_pairs;
     a.pprec = reinterpret_cast<const double2 *>(f->d_pp);
+    a.pprec32 = reinterpret_cast<const float4 *>(f->d_pp32);
     a.nlo = part ? t.d_n64 : nullptr;
     a.cum = part ? t.d_cum32 : t.d_cum64;
     a.unit_prefix = part ? t.d_unit_prefix32 : t.d_unit_prefix;

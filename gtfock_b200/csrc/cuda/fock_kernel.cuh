@@ -37,6 +37,7 @@ __host__ __device__ inline int gtf_prim_bucket(int n)
 struct FockLaunch {
     const PairRec *pairs;
     const double2 *pprec;          // primitive-pair records (PPRec)
+    const float4 *pprec32;         // FP32 primitive-pair records (PPRec32)
     const int *nlo;                // [nbra][GTF_NBKT] first ket of this launch in each segment prefix (null: 0)
     const int *cum;                // [nbra][GTF_CUM] exclusive prefix over segments of this launch's kets
     const long long *unit_prefix;  // [nbra + 1] exclusive prefix of units (32 kets) over bras
@@ -168,11 +169,16 @@ __global__ void __launch_bounds__(FOCK_THREADS,
         const PairRec pb = pairs[bra_start + i];
         const PairRec pk = active ? pairs[ket_start + j] : pb;
         const bool same = (bra_start + i) == (ket_start + j);
-        const PPRec src{GTF_FLD(pprec)};
         R acc[ncart(LA) * ncart(LB) * N];
 #pragma unroll
         for (int k = 0; k < ncart(LA) * ncart(LB) * N; k++) acc[k] = (R)0;
-        if (active) eri_accumulate_cd<LA, LB, LC, LD, CD0, N, true>(src, pb, src, pk, acc, tab);
+        if constexpr (sizeof(R) == 4) {
+            const PPRec32 src{GTF_FLD(pprec32)};
+            if (active) eri_accumulate_cd32<LA, LB, LC, LD, CD0, N, true>(src, pb, pk, acc, tab);
+        } else {
+            const PPRec src{GTF_FLD(pprec)};
+            if (active) eri_accumulate_cd<LA, LB, LC, LD, CD0, N, true>(src, pb, src, pk, acc, tab);
+        }
         digest_cd<LA, LB, LC, LD, CD0, N>(acc, active, pb, pk, same, GTF_FLD(D), GTF_FLD(Fj), GTF_FLD(Fk),
                                           GTF_FLD(ld), lane, GTF_FLD(konly) != 0);
 #undef GTF_FLD

@@ -90,6 +90,28 @@ struct PrimVals {
     double p, Px, Py, Pz, K, h;
 };
 
+// FP32 form of a primitive pair, centre relative to the pair's first shell:
+// {p, K, PAx, PAy}, {PAz, 1/(2p), 0, 0} (32 bytes, two 16-byte loads)
+struct PrimVals32 {
+    float p, K, PAx, PAy, PAz, h;
+};
+struct PPRec32 {
+    const float4 *r;
+    __device__ __forceinline__ PrimVals32 get(const PairRec &pr, int i) const
+    {
+        const float4 *q = r + 2 * (size_t)(pr.off + i);
+        const float4 a = __ldg(q), b = __ldg(q + 1);
+        PrimVals32 v;
+        v.p = a.x;
+        v.K = a.y;
+        v.PAx = a.z;
+        v.PAy = a.w;
+        v.PAz = b.x;
+        v.h = b.y;
+        return v;
+    }
+};
+
 
 __device__ __forceinline__ double gfma(double a, double b, double c) { return fma(a, b, c); }
 __device__ __forceinline__ float gfma(float a, float b, float c) { return fmaf(a, b, c); }
@@ -387,6 +409,81 @@ __device__ __forceinline__ void eri_accumulate_cd(const PPB &bra, const PairRec 
         }
     }
     (void)ND;
+}
+
+// FP32 quartets: everything in single precision, from the FP32 records (centres
+// relative to each pair's first shell; P - Q = PA - QC + (A - C) with A - C
+// formed in double once per quartet).  Same structure as eri_accumulate_cd.
+template <int LA, int LB, int LC, int LD, int CD0, int N, bool SKIP>
+__device__ __forceinline__ void eri_accumulate_cd32(const PPRec32 &src, const PairRec &pb, const PairRec &pk,
+                                                    float (&acc)[ncart(LA) * ncart(LB) * N], const float *rtab)
+{
+    constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
+    constexpr int NI = LA + LB + 1, NK = LC + LD + 1;
+    constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC);
+    if (pb.n <= 0) return;
+    const float ABx = (float)pb.ABx, ABy = (float)pb.ABy, ABz = (float)pb.ABz;
+    const float CDx = (float)pk.ABx, CDy = (float)pk.ABy, CDz = (float)pk.ABz;
+    const float ACx = (float)(pb.Ax - pk.Ax), ACy = (float)(pb.Ay - pk.Ay), ACz = (float)(pb.Az - pk.Az);
+    const PrimVals32 b0 = src.get(pb, 0);
+    PrimVals32 nk;
+    if (pk.n > 0) nk = src.get(pk, 0);
+    for (int ik = 0; ik < pk.n; ik++) {
+        const PrimVals32 kq = nk;
+        if (ik + 1 < pk.n) nk = src.get(pk, ik + 1);
+        if (SKIP && fabsf(b0.K * kq.K) < (float)GTF_PRIMQ_EPS) break;
+        const float q = kq.p, h2q = kq.h;
+        const float QCx = kq.PAx, QCy = kq.PAy, QCz = kq.PAz;
+        const float dx = ACx - QCx, dy = ACy - QCy, dz = ACz - QCz;
+        PrimVals32 nb = b0;
+        for (int ib = 0; ib < pb.n; ib++) {
+            const PrimVals32 bq = nb;
+            if (ib + 1 < pb.n) nb = src.get(pb, ib + 1);
+            if (SKIP && fabsf(bq.K * kq.K) < (float)GTF_PRIMQ_EPS) break;
+            const float p = bq.p, h2p = bq.h;
+            const float PAx = bq.PAx, PAy = bq.PAy, PAz = bq.PAz;
+            const float rpq = rsqrtf(p + q);
+            const float ipq = rpq * rpq;
+            const float PQx = PAx + dx, PQy = PAy + dy, PQz = PAz + dz;
+            const float rho = p * q * ipq;
+            const float T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
+            const float pref = bq.K * kq.K * rpq;
+            float u[NR], w[NR];
+            rys_roots<NR>(T, u, w, rtab);
+            const float qf = q * ipq, pf = p * ipq;
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                const float ur = u[r];
+                const float B00 = 0.5f * ur * ipq;
+                const float B10 = h2p * (1.0f - qf * ur);
+                const float B01 = h2q * (1.0f - pf * ur);
+                const float cq = qf * ur, cp = pf * ur;
+                float Gx[NI][NK], Gy[NI][NK], Gz[NI][NK];
+                rys_2d<NI, NK>(Gx, 1.0f, PAx - cq * PQx, QCx + cp * PQx, B10, B01, B00);
+                rys_2d<NI, NK>(Gy, 1.0f, PAy - cq * PQy, QCy + cp * PQy, B10, B01, B00);
+                rys_2d<NI, NK>(Gz, w[r] * pref, PAz - cq * PQz, QCz + cp * PQz, B10, B01, B00);
+                float Ix[LA + 1][LB + 1][LC + 1][LD + 1];
+                float Iy[LA + 1][LB + 1][LC + 1][LD + 1];
+                float Iz[LA + 1][LB + 1][LC + 1][LD + 1];
+                hrr_abcd<LA, LB, LC, LD>(Gx, Ix, ABx, CDx);
+                hrr_abcd<LA, LB, LC, LD>(Gy, Iy, ABy, CDy);
+                hrr_abcd<LA, LB, LC, LD>(Gz, Iz, ABz, CDz);
+#pragma unroll
+                for (int t = 0; t < N; t++) {
+                    const int ic = (CD0 + t) % NC, id = (CD0 + t) / NC;
+#pragma unroll
+                    for (int ibb = 0; ibb < NB; ibb++)
+#pragma unroll
+                        for (int ia = 0; ia < NA; ia++) {
+                            const float xy = Ix[cart_x(LA, ia)][cart_x(LB, ibb)][cart_x(LC, ic)][cart_x(LD, id)] *
+                                             Iy[cart_y(LA, ia)][cart_y(LB, ibb)][cart_y(LC, ic)][cart_y(LD, id)];
+                            float &dst = acc[ia + NA * (ibb + NB * t)];
+                            dst = fmaf(xy, Iz[cart_z(LA, ia)][cart_z(LB, ibb)][cart_z(LC, ic)][cart_z(LD, id)], dst);
+                        }
+                }
+            }
+        }
+    }
 }
 
 // the whole quartet: acc[ia + NA*(ib + NB*(ic + NC*id))]
