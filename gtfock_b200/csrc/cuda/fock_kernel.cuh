@@ -73,13 +73,15 @@ struct FockGrid {
 // ~54 accumulators in registers (the Rys roots and 2-D tables are
 // recomputed per slice, which costs less than spilling the accumulators).
 // FP32 values take one register each, so the FP32 kernels keep quartets of
-// up to 81 integrals in one pass and slices of up to ~72 accumulators (wider
-// FP32 slices spill, as FP64 slices wider than ~54 do).
+// up to 81 integrals in one pass and slices of up to ~72 accumulators.  FP64
+// (dd| classes also take 72 (2 ket components): their spills cost less than
+// recomputing the roots and 2-D tables for twice as many slices, which is not
+// so for the (dp| classes (measured on C54H18).
 __host__ __device__ constexpr int fock_slice(int LA, int LB, int LC, int LD, int fp32)
 {
     const int nab = ncart(LA) * ncart(LB), ncd = ncart(LC) * ncart(LD);
     if (nab * ncd <= (fp32 ? 81 : 64)) return ncd;
-    const int s = (fp32 ? 72 : 54) / nab;
+    const int s = (fp32 || nab >= 36 ? 72 : 54) / nab;
     return s < 1 ? 1 : (s > ncd ? ncd : s);
 }
 
