@@ -405,7 +405,8 @@ def run_served(args):
     items = workloads.served(args.count, args.seed, args.rate)
     reqs = [serve.Request(n, a, b, t, nb) for t, n, a, b, nb in items]
     cut = args.fp32_cutoff if args.fp32_cutoff is not None else 1e-6
-    srv = serve.SCFServer(slots=args.slots, precision=1, fp32_cutoff=cut, max_iters=30, etol=1e-6, tolscr=TOL)
+    srv = serve.SCFServer(slots=args.slots, precision=1, fp32_cutoff=cut, max_iters=30, etol=1e-6, tolscr=TOL,
+                          lanes=((400, None), (None, None)) if args.lanes == 2 else ((None, None),))
     done = serve.run_stream(reqs, srv)
     srv.close()
     seq = serve.run_sequential(reqs, max_iters=30, etol=1e-6, tolscr=TOL)
@@ -413,12 +414,16 @@ def run_served(args):
     # compared where both runs converged (|dE| < 1e-6 Ha before 30 iterations)
     conv = [r for r in done if len(r.energies) < 30 and len(by[r.name].energies) < 30]
     dE = max([abs(r.energies[-1] - by[r.name].energies[-1]) for r in conv] or [0.0])
+    worst = max(conv, key=lambda r: abs(r.energies[-1] - by[r.name].energies[-1])) if conv else None
     out = {"metric": "SCF solves/s and p50/p99 time-to-converged-energy, served (%d requests)" % args.count,
            "workload": "Poisson rate %.2f/s, seed %d, %d-%d bf" % (args.rate, args.seed,
                                                                  min(i[4] for i in items), max(i[4] for i in items)),
-           "fp32_cutoff": cut, "slots": args.slots,
+           "fp32_cutoff": cut, "slots_per_lane": args.slots, "lanes": args.lanes,
            "served_mixed": serve.latency_stats(done), "sequential_fp64": serve.latency_stats(seq),
-           "max_dE_served_vs_fp64": dE, "converged_requests": len(conv)}
+           "max_dE_served_vs_fp64": dE, "converged_requests": len(conv),
+           "worst_request": None if worst is None else {
+               "name": worst.name, "nbf": worst.nbf, "served_energies": [float(x) for x in worst.energies],
+               "fp64_energies": [float(x) for x in by[worst.name].energies]}}
     out["speedup_solves_per_s"] = out["served_mixed"]["solves_per_s"] / out["sequential_fp64"]["solves_per_s"]
     print(json.dumps(out), flush=True)
 
@@ -485,7 +490,9 @@ def main():
     ap.add_argument("--count", type=int, default=None, help="molecules (batched) or requests (served)")
     ap.add_argument("--seed", type=int, default=None)
     ap.add_argument("--rate", type=float, default=2.0, help="served: Poisson arrival rate (1/s)")
-    ap.add_argument("--slots", type=int, default=64, help="served: resident jobs at most")
+    ap.add_argument("--slots", type=int, default=64, help="served: resident jobs per lane at most")
+    ap.add_argument("--lanes", type=int, default=2, choices=[1, 2],
+                    help="served: size lanes (2: up to 400 functions, and the rest)")
     ap.add_argument("--seq-sample", type=int, default=256, help="batched: molecules timed on the one-job path")
     args = ap.parse_args()
     if args.workload == "batched":

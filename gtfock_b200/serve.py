@@ -1,11 +1,11 @@
 """SCF serving loop over the batched engine (continuous batching).
 
 A request is an SCF job (geometry + basis name).  The server keeps up to
-`slots` jobs resident on the device and advances all of them together, one
-SCF iteration per step (gtf_batch_step); a job leaves when its energy has
-converged (|E_k - E_k-1| < etol) or after max_iters iterations, and a waiting
-request is admitted as soon as a slot is free and its estimated device
-footprint fits the memory budget.  Requests that arrive while others are on
+`slots` jobs per size lane resident on the device and advances the jobs of a
+lane together, one SCF iteration per step (gtf_batch_step); a job leaves when
+its energy has converged (|E_k - E_k-1| < etol) or after max_iters
+iterations, and a waiting request is admitted as soon as a slot of its lane
+is free and its estimated device footprint fits the memory budget.  Requests that arrive while others are on
 the GPU therefore join the running batch between two steps, and their
 iterations overlap with those of the jobs already running.
 
@@ -45,52 +45,104 @@ def footprint_bytes(nbf):
     return Batch.job_bytes(nbf) + 8 * 64 * nbf * nbf
 
 
-class SCFServer:
-    def __init__(self, slots=64, mem_budget=64 << 30, precision=1, fp32_cutoff=1e-6, max_iters=30,
-                 etol=1e-6, tolscr=1e-10):
+class _Lane:
+    def __init__(self, max_nbf, slots):
+        self.max_nbf = max_nbf
         self.batch = Batch(slots)
         self.slots = slots
+        self.live = {}
+        self.ms = None          # moving average of a step's wall time
+
+    def fits(self, nbf):
+        return self.max_nbf is None or nbf <= self.max_nbf
+
+
+class SCFServer:
+    """Continuous-batching SCF server.
+
+    Requests are routed by size into lanes (default: up to 400 functions, and
+    the rest), each a batch stepped in lock-step.  Steps of the lanes share
+    the GPU: when several lanes have live jobs, the small-molecule lane runs
+    until its step time adds up to `share` times the large lane's step, then
+    the large lane takes one step -- so small jobs are not held to the pace of
+    a 1000-function molecule, while the large ones keep progressing."""
+
+    def __init__(self, slots=64, mem_budget=64 << 30, precision=1, fp32_cutoff=1e-6, max_iters=30,
+                 etol=1e-6, tolscr=1e-10, lanes=((400, None), (None, None)), share=0.5):
+        self.lanes = [_Lane(m, n if n else slots) for m, n in lanes]
         self.mem_budget = mem_budget
+        self.share = share
         self.kw = dict(tolscr=tolscr, precision=precision, fp32_cutoff=fp32_cutoff, max_iters=max_iters,
                        etol=etol)
-        self.live = {}
         self.mem_used = 0
+        self.credit = 0.0
         self.tmp = tempfile.mkdtemp(prefix="gtf_serve_")
+
+    @property
+    def live(self):
+        return {(k, s): r for k, ln in enumerate(self.lanes) for s, r in ln.live.items()}
 
     def _xyz(self, r):
         if r.xyz is None:
             r.xyz = mol.write_xyz(r.atoms, os.path.join(self.tmp, r.name + ".xyz"), r.name)
         return r.xyz
 
+    def _lane(self, r):
+        for ln in self.lanes:
+            if ln.fits(r.nbf or 1):
+                return ln
+        return self.lanes[-1]
+
     def can_admit(self, r):
-        need = footprint_bytes(r.nbf or 1)
-        return len(self.live) < self.slots and self.mem_used + need <= self.mem_budget
+        ln = self._lane(r)
+        return len(ln.live) < ln.slots and self.mem_used + footprint_bytes(r.nbf or 1) <= self.mem_budget
 
     def admit(self, r, now):
-        r.slot = self.batch.add(mol.basis_file(r.basis), self._xyz(r), **self.kw)
+        ln = self._lane(r)
+        r.slot = ln.batch.add(mol.basis_file(r.basis), self._xyz(r), **self.kw)
         r.admitted = now
-        self.live[r.slot] = r
+        ln.live[r.slot] = r
         self.mem_used += footprint_bytes(r.nbf or 1)
 
+    def _pick(self):
+        busy = [ln for ln in self.lanes if ln.live]
+        if len(busy) <= 1:
+            return busy[0] if busy else None
+        small, large = busy[0], busy[-1]
+        if large.ms is None or self.credit < self.share * large.ms:
+            return small
+        return large
+
     def step(self, now_fn):
-        """One SCF iteration of every live job; returns the requests that finished."""
-        if not self.live:
+        """One SCF iteration of every live job of one lane; returns the
+        requests that finished."""
+        ln = self._pick()
+        if ln is None:
             return []
-        self.batch.step()
+        t0 = time.perf_counter()
+        ln.batch.step()
+        dt = (time.perf_counter() - t0) * 1e3
+        ln.ms = dt if ln.ms is None else 0.7 * ln.ms + 0.3 * dt
+        busy = [x for x in self.lanes if x.live]
+        if ln is busy[-1] and len(busy) > 1:
+            self.credit = 0.0
+        else:
+            self.credit += dt
         done = []
-        for s in list(self.live):
-            e, fin = self.batch.result(s)
+        for s in list(ln.live):
+            e, fin = ln.batch.result(s)
             if fin:
-                r = self.live.pop(s)
+                r = ln.live.pop(s)
                 r.energies = e
                 r.finished = now_fn()
-                self.batch.remove(s)
+                ln.batch.remove(s)
                 self.mem_used -= footprint_bytes(r.nbf or 1)
                 done.append(r)
         return done
 
     def close(self):
-        self.batch.close()
+        for ln in self.lanes:
+            ln.batch.close()
 
 
 def run_stream(requests, server):
@@ -107,8 +159,12 @@ def run_stream(requests, server):
         t = now()
         while pending and pending[0].arrival <= t:
             waiting.append(pending.pop(0))
-        while waiting and server.can_admit(waiting[0]):
-            server.admit(waiting.pop(0), now())
+        # admit, in arrival order, every waiting request whose lane has room
+        # (a full lane does not hold back requests for the other lanes)
+        for r in list(waiting):
+            if server.can_admit(r):
+                waiting.remove(r)
+                server.admit(r, now())
         if server.live:
             finished += server.step(now)
         elif pending:
