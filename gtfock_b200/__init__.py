@@ -100,6 +100,8 @@ def load():
     _sig(L, "gtf_scf_nbf", [_vp])
     _sig(L, "gtf_scf_set_options", [_vp, _i, _d, _d])
     _sig(L, "gtf_scf_get_density", [_vp, _dp])
+    _sig(L, "gtf_scf_set_purification", [_vp, _i])
+    _sig(L, "gtf_scf_purification_iters", [_vp, _ip, _ip])
     _sig(L, "gtf_scf_destroy", [_vp], None)
     _sig(L, "gtf_launch_count", [], ctypes.c_ulonglong)
     _sig(L, "gtf_batch_create", [_i], _vp)
@@ -377,6 +379,18 @@ class SCFSolver:
         r = load().gtf_scf_set_options(self.h, precision, fp32_cutoff, etol)
         if r != 0:
             raise GtfError("gtf_scf_set_options failed (%d)" % r)
+
+    def set_purification(self, mode):
+        """0: FP64 products; 1: split-BF16 tensor-core products, FP64 finish."""
+        r = load().gtf_scf_set_purification(self.h, mode)
+        if r != 0:
+            raise GtfError("gtf_scf_set_purification failed (%d)" % r)
+
+    def purification_iters(self):
+        """(split-BF16, FP64) iterations of the last purification."""
+        a, b = ctypes.c_int(), ctypes.c_int()
+        load().gtf_scf_purification_iters(self.h, ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
 
     def density(self):
         """Density of the last solve (half density, AO basis)."""

@@ -98,6 +98,12 @@ int gtf_fock_class_stats(gtf_fock_dev_t *f, int *X, int *Y, double *ms, double *
 void *gtf_fock_stream(gtf_fock_dev_t *f);
 size_t gtf_fock_device_bytes(gtf_fock_dev_t *f);
 
+/* ---- split BF16 products on the tensor cores (purif_bf16.cu) ---- */
+typedef struct gtf_bf16x3 gtf_bf16x3_t;
+int gtf_bf16x3_create(int n, gtf_bf16x3_t **out);
+void gtf_bf16x3_destroy(gtf_bf16x3_t *g);
+int gtf_bf16x3_abt(gtf_bf16x3_t *g, const double *A, const double *B, double *C, void *stream);
+
 /* ---- purification / DIIS on the device (purif.cu) ---- */
 typedef struct gtf_purif_dev gtf_purif_dev_t;
 int gtf_purif_create(int nbf, int nocc, void *stream, gtf_purif_dev_t **out);
@@ -107,6 +113,11 @@ int gtf_purif_set_sx_dev(gtf_purif_dev_t *p, const double *S_dev, const double *
 /* canonical purification of F (orthogonal basis); D_AO returned; iterations */
 int gtf_purif_run(gtf_purif_dev_t *p, const double *F_host, double *D_host, int *iters);
 int gtf_purif_run_dev(gtf_purif_dev_t *p, const double *F_dev, double *D_dev, int *iters);
+/* 0: FP64 products (default); 1: split-BF16 tensor-core canonical steps until
+ * ||D - D^2||_F < 1e-2 or it stops falling, then FP64 canonical steps to 1e-11 */
+int gtf_purif_set_mode(gtf_purif_dev_t *p, int mode);
+/* iterations of the last purification: split-BF16 and FP64 */
+void gtf_purif_last_iters(gtf_purif_dev_t *p, int *bf16_iters, int *fp64_iters);
 /* one DIIS step: F (AO, host or device) in, extrapolated orthogonal F out */
 int gtf_diis_step(gtf_purif_dev_t *p, const double *D_host, double *F_host, int iter);
 int gtf_diis_step_dev(gtf_purif_dev_t *p, const double *D_dev, double *F_dev, int iter);

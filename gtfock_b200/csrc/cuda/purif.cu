@@ -56,6 +56,9 @@ struct gtf_purif_dev {
     int sx_set;
     cudaEvent_t e0, e1;
     double ms_gemm, ms_total, errnorm, idem, trerr;
+    int mode;                 // 0 FP64, 1 split-BF16 then FP64
+    gtf_bf16x3_t *bx;
+    int it_bf16, it_fp64;
 };
 
 // row-major C = A B^T (pdgemm3D_2) and C = A B, via column-major cuBLAS
@@ -204,6 +207,18 @@ __global__ void k_purif_update(double *__restrict__ D, const double *__restrict_
     else D[k] = ((1.0 + c) * D2[k] - D3[k]) / c;
 }
 
+// D = (D + D^T) / 2 (the split-BF16 products are symmetric only to FP32
+// rounding; the FP64 steps assume a symmetric D, as D D^T = D^2)
+__global__ void k_symmetrize(double *__restrict__ D, int n)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y;
+    if (j >= n || j <= i) return;
+    const double v = 0.5 * (D[(size_t)i * n + j] + D[(size_t)j * n + i]);
+    D[(size_t)i * n + j] = v;
+    D[(size_t)j * n + i] = v;
+}
+
 // cur = W - W^T (F D S - (F D S)^T, pscf/purif.c:553-558)
 __global__ void k_antisym(const double *__restrict__ W, double *__restrict__ cur, int n)
 {
@@ -277,10 +292,28 @@ extern "C" int gtf_purif_create(int nbf, int nocc, void *stream, gtf_purif_dev_t
     return GTF_OK;
 }
 
+extern "C" int gtf_purif_set_mode(gtf_purif_dev_t *p, int mode)
+{
+    if (mode != 0 && mode != 1) return GTF_ERR_INVALID;
+    if (mode == 1 && !p->bx) {
+        const int r = gtf_bf16x3_create(p->n, &p->bx);
+        if (r != GTF_OK) return r;
+    }
+    p->mode = mode;
+    return GTF_OK;
+}
+
+extern "C" void gtf_purif_last_iters(gtf_purif_dev_t *p, int *bf16_iters, int *fp64_iters)
+{
+    if (bf16_iters) *bf16_iters = p->it_bf16;
+    if (fp64_iters) *fp64_iters = p->it_fp64;
+}
+
 extern "C" void gtf_purif_destroy(gtf_purif_dev_t *p)
 {
     if (!p) return;
     cudaStreamSynchronize(p->st);
+    if (p->bx) gtf_bf16x3_destroy(p->bx);
     double *bufs[] = {p->S, p->X, p->D, p->D2, p->D3, p->F, p->W, p->W2, p->vecs, p->Fvecs, p->part, p->scal};
     for (double *b : bufs)
         if (b) cudaFree(b);
@@ -334,6 +367,37 @@ extern "C" int gtf_purif_run_dev(gtf_purif_dev_t *p, const double *F_dev, double
     gtf_note_launches(3);
     int it;
     double err = 0.0;
+    // split-BF16 phase: tensor-core products until the error stops falling
+    // (their rounding sets a floor near 2^-16 relative), then FP64 steps
+    p->it_bf16 = 0;
+    if (p->mode == 1 && p->bx) {
+        double best = 1e300;
+        int stall = 0;
+        for (int k = 0; k < PUR_MAX_ITERS; k++) {
+            if (gtf_bf16x3_abt(p->bx, p->D, p->D, p->D2, st)) return GTF_ERR_CUDA;
+            if (gtf_bf16x3_abt(p->bx, p->D, p->D2, p->D3, st)) return GTF_ERR_CUDA;
+            k_purif_stats<<<RED_BLOCKS, RED_THREADS, 0, st>>>(p->D, p->D2, p->D3, n, p->part);
+            k_purif_finish<<<1, 32, 0, st>>>(p->part, RED_BLOCKS, p->scal);
+            k_purif_update<<<ge, 256, 0, st>>>(p->D, p->D2, p->D3, nn, p->scal);
+            k_symmetrize<<<dim3((n + 127) / 128, n), 128, 0, st>>>(p->D, n);
+            CKP(cudaGetLastError());
+            gtf_note_launches(4);
+            CKP(cudaMemcpyAsync(p->h_scal + 6, p->scal + 6, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
+            CKP(cudaStreamSynchronize(st));
+            p->it_bf16++;
+            const double e = p->h_scal[6];
+            // hand over to FP64 once the error is small or stops falling
+            // (BF16 rounding floor)
+            if (!(e == e) || e < 1e-2) break;
+            if (e < 0.99 * best) {
+                best = e;
+                stall = 0;
+            } else if (++stall >= 3) {
+                break;
+            }
+        }
+    }
+    // FP64 canonical steps (from the split-BF16 state in mode 1)
     for (it = 0; it < PUR_MAX_ITERS; it++) {
         if (gemm_abt(p, p->D, p->D, p->D2)) return GTF_ERR_CUDA;
         if (gemm_ab(p, p->D, p->D2, p->D3)) return GTF_ERR_CUDA;
@@ -348,6 +412,8 @@ extern "C" int gtf_purif_run_dev(gtf_purif_dev_t *p, const double *F_dev, double
         if (err < 1e-11) break;
     }
     p->errnorm = err;
+    p->it_fp64 = (it < PUR_MAX_ITERS) ? it + 1 : PUR_MAX_ITERS;
+    it += p->it_bf16;
     // D_AO = X D X (pscf/purif.c:469-476)
     if (gemm_abt(p, p->X, p->D, p->W)) return GTF_ERR_CUDA;
     if (gemm_abt(p, p->W, p->X, D_dev)) return GTF_ERR_CUDA;

@@ -127,6 +127,19 @@ int gtf_scf_set_options(gtf_scf_t *s, int prec_mode, double fp32_cutoff, double 
     return 0;
 }
 
+int gtf_scf_set_purification(gtf_scf_t *s, int mode)
+{
+    if (!s || !s->pur) return -1;
+    return gtf_purif_set_mode((gtf_purif_dev_t *)s->pur->dev, mode) == GTF_OK ? 0 : -2;
+}
+
+int gtf_scf_purification_iters(gtf_scf_t *s, int *bf16_iters, int *fp64_iters)
+{
+    if (!s || !s->pur) return -1;
+    gtf_purif_last_iters((gtf_purif_dev_t *)s->pur->dev, bf16_iters, fp64_iters);
+    return 0;
+}
+
 int gtf_scf_get_density(gtf_scf_t *s, double *D)
 {
     if (!s || !D) return -1;

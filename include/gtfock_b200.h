@@ -92,6 +92,13 @@ int gtf_scf_nbf(gtf_scf_t *s);
  * convergence tolerance: a solve stops once |E_k - E_k-1| < etol (default
  * 1e-11).  0 on success. */
 int gtf_scf_set_options(gtf_scf_t *s, int prec_mode, double fp32_cutoff, double etol);
+/* Purification products: mode 0 FP64 (default); mode 1 split-BF16 products
+ * on the tensor cores (each FP64 factor as a sum of two BF16 matrices, FP32
+ * accumulation) until the idempotency error stops falling, then FP64 steps
+ * to ||D - D^2||_F < 1e-11.  0 on success. */
+int gtf_scf_set_purification(gtf_scf_t *s, int mode);
+/* Iterations of the last purification: split-BF16 and FP64 steps. */
+int gtf_scf_purification_iters(gtf_scf_t *s, int *bf16_iters, int *fp64_iters);
 /* Copy of the density (half density, AO basis, nbf x nbf) left by the last
  * solve.  0 on success. */
 int gtf_scf_get_density(gtf_scf_t *s, double *D);

@@ -92,3 +92,34 @@ def test_scf_energy_mixed(tmp_path):
     print("FP64 %.10f (%d it)  mixed 1e-6 %.10f (%d it)" % (e64[-1], len(e64), e32[-1], len(e32)))
     assert abs(e32[-1] - e64[-1]) < 1e-6, (e32[-1], e64[-1])
     s.close()
+
+
+@pytest.mark.parametrize("case", ["w8_631g", "c4h10_ccpvdz"])
+def test_bf16_split_purification(case, tmp_path):
+    """Purification with split-BF16 tensor-core products followed by FP64
+    steps: the converged SCF energy within 1e-6 Ha of the FP64 purification,
+    with both precisions of the ERIs, and an idempotent final density."""
+    g = load_golden(case)
+    gbs, xyz = golden_xyz(g, tmp_path)
+    s = gb.SCFSolver(gbs, xyz, tolscr=float(g["tol"]))
+    s.set_options(precision=0, etol=1e-9)
+    e64, _ = s.solve(niters=40)
+    s.set_purification(1)
+    e16, _ = s.solve(niters=40)
+    nb, n64 = s.purification_iters()
+    assert nb > 0 and n64 > 0
+    assert len(e64) < 40 and len(e16) < 40
+    assert abs(e16[-1] - e64[-1]) < 1e-6, (e16[-1], e64[-1])
+    s.set_options(precision=1, fp32_cutoff=1e-6, etol=1e-9)
+    em, _ = s.solve(niters=40)
+    assert abs(em[-1] - e64[-1]) < 1e-6, (em[-1], e64[-1])
+    b = gb.BasisSet(gbs, xyz)
+    pf = gb.PFock(b, tolscr=float(g["tol"]))
+    S, _, _ = pf.one_electron()
+    D = s.density()
+    assert np.linalg.norm(D @ S @ D - D) < 1e-8
+    assert abs(np.trace(D @ S) - b.nocc) < 1e-8
+    print("%s: FP64 %.10f, bf16-split purification %.10f (%d bf16 + %d fp64 steps)" %
+          (case, e64[-1], e16[-1], nb, n64))
+    pf.close()
+    s.close()
