@@ -465,13 +465,50 @@ def run_precision(args):
                          "dE": float(abs(e[-1] - e64[-1])), "idempotency_DSD_minus_D": float(
                              np.linalg.norm(D @ S @ D - D)), "trace_error": float(abs(np.trace(D @ S) - b.nocc)),
                          "fock_ms": msc, "scf_s": tc, "iterations": len(e)})
+        # split-BF16 purification products on the tensor cores (FP64 finish),
+        # with FP64 ERIs and with FP32 ERIs below 1e-6
+        bf = []
+        for prec, cut in ((0, 0.0), (1, 1e-6)):
+            s.set_options(precision=prec, fp32_cutoff=cut, etol=1e-10)
+            s.set_purification(1)
+            t0 = time.perf_counter()
+            e, tm = s.solve(niters=60)
+            tc = time.perf_counter() - t0
+            nb, n64 = s.purification_iters()
+            D = s.density()
+            bf.append({"eri": "fp64" if prec == 0 else "fp32 below %g" % cut, "dE": float(abs(e[-1] - e64[-1])),
+                       "idempotency_DSD_minus_D": float(np.linalg.norm(D @ S @ D - D)),
+                       "trace_error": float(abs(np.trace(D @ S) - b.nocc)), "scf_s": tc, "iterations": len(e),
+                       "purification_s_per_solve": tm["purif_s"],
+                       "last_purification_steps": {"bf16_split": nb, "fp64": n64}})
+            s.set_purification(0)
+        s.set_options(precision=0, etol=1e-10)
+        s.solve(niters=60)
+        nb0, n640 = s.purification_iters()
         pf.close()
         s.close()
     out = {"metric": "precision sweep, (H2O)64 / 6-31G (832 bf)", "fp64": {
         "energy": float(e64[-1]), "iterations": len(e64), "fock_ms": ms64, "scf_s": t64,
         "idempotency_DSD_minus_D": float(np.linalg.norm(D64 @ S @ D64 - D64)),
-        "trace_error": float(abs(np.trace(D64 @ S) - b.nocc))}, "mixed": rows}
+        "trace_error": float(abs(np.trace(D64 @ S) - b.nocc)),
+        "last_purification_steps": {"fp64": n640}}, "mixed": rows, "bf16_split_purification": bf}
     print(json.dumps(out), flush=True)
+
+
+def profile_purification(args):
+    """Two SCF iterations of (H2O)64 / 6-31G with the split-BF16 purification
+    (the small case profiled with ncu for the tensor-core products)."""
+    import gtfock_b200 as gb
+    from gtfock_b200 import molecules as mol
+    with tempfile.TemporaryDirectory() as td:
+        xyz = mol.write_xyz(mol.water_cluster(64, 2024), os.path.join(td, "w64.xyz"))
+        s = gb.SCFSolver(mol.basis_file("6-31g"), xyz, tolscr=TOL)
+        s.set_purification(1)
+        e, tm = s.solve(niters=2)
+        nb, n64 = s.purification_iters()
+        s.close()
+    print(json.dumps({"purification_s": tm["purif_s"], "bf16_split_steps": nb, "fp64_steps": n64,
+                      "energies": [float(x) for x in e]}), flush=True)
 
 
 def main():
@@ -483,6 +520,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-fock", choices=["c12h26", "c54h18", "c96h24", "w64"], default=None)
     ap.add_argument("--builds", type=int, default=2)
+    ap.add_argument("--profile-purif", action="store_true",
+                    help="two SCF iterations of (H2O)64 with the split-BF16 purification (ncu case)")
     ap.add_argument("--fp32-cutoff", type=float, default=None,
                     help="with --profile-fock: FP32 for quartets with Schwarz bound below this")
     ap.add_argument("--workload", choices=["default", "batched", "served", "precision"], default="default",
@@ -507,6 +546,9 @@ def main():
         return
     if args.workload == "precision":
         run_precision(args)
+        return
+    if args.profile_purif:
+        profile_purification(args)
         return
     if args.profile_fock:
         profile_fock(args)
