@@ -340,6 +340,10 @@ struct gtf_batch {
     gtf_fock_batch_t *fb;
     std::vector<int> fb_members;   // slots in the current Fock batch
     int dirty;
+    // the batched Fock build of the current membership, captured once as a
+    // CUDA graph and replayed every step (null: launch directly)
+    cudaGraphExec_t fock_exec;
+    int fock_launches;
     // device arrays (capacity-sized)
     JobDev *d_jobs;
     GemmDesc *d_gd;                // 10 call sets x capacity
@@ -390,6 +394,7 @@ extern "C" void gtf_batch_destroy(gtf_batch_t *b)
 {
     if (!b) return;
     cudaStreamSynchronize(b->st);
+    if (b->fock_exec) cudaGraphExecDestroy(b->fock_exec);
     if (b->fb) gtf_fock_batch_destroy(b->fb);
     for (auto &j : b->jobs)
         if (j.used) job_free(j);
@@ -681,9 +686,31 @@ extern "C" int gtf_batch_step(gtf_batch_t *b)
         }
         b->fb_members = run;
         b->dirty = 0;
+        // capture the build (one launch per class pair, part and slice, plus
+        // the transforms) for replay while the membership stays the same
+        if (b->fock_exec) cudaGraphExecDestroy(b->fock_exec);
+        b->fock_exec = nullptr;
+        b->fock_launches = 0;
+        cudaGraph_t graph = nullptr;
+        if (cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            const int nl = gtf_fock_batch_compute(b->fb);
+            const cudaError_t ce = cudaStreamEndCapture(b->st, &graph);
+            if (nl >= 0 && ce == cudaSuccess && graph &&
+                cudaGraphInstantiate(&b->fock_exec, graph, 0) == cudaSuccess) {
+                b->fock_launches = nl;
+                gtf_note_launches(-nl);   // counted when replayed, not when captured
+            } else {
+                b->fock_exec = nullptr;
+            }
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();
+        }
     }
     CKH(cudaEventRecord(b->e0, b->st));
-    if (gtf_fock_batch_compute(b->fb) < 0) {
+    if (b->fock_exec) {
+        CKH(cudaGraphLaunch(b->fock_exec, b->st));
+        gtf_note_launches(b->fock_launches);
+    } else if (gtf_fock_batch_compute(b->fb) < 0) {
         fprintf(stderr, "gtfock_b200: batched Fock build failed: %s\n", gtf_last_error());
         return -3;
     }
