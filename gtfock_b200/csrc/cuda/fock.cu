@@ -490,7 +490,7 @@ __global__ void k_build_pairs(const int *__restrict__ idx, const int *__restrict
 
 // Primitive pairs of each listed shell pair, compacted and sorted: pairs
 // whose prefactor |K| is below GTF_PRIM_EPS are dropped (their contribution
-// to any integral is below 1e-20 Hartree), the rest are stored in descending
+// to any integral is below ~1e-15 Hartree), the rest are stored in descending
 // |K| so that the quartet loop can stop once |K_ab K_cd| < GTF_PRIMQ_EPS.
 // pairs[s].n becomes the kept count (possibly 0); the slot keeps its size.
 // Records are {p, K, Px, Py, Pz, 1/(2p)} (PPRec).

