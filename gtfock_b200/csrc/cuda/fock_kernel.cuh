@@ -108,13 +108,8 @@ __global__ void __launch_bounds__(FOCK_THREADS,
     constexpr int NCD = ncart(LC) * ncart(LD);
     constexpr int S = fock_slice(LA, LB, LC, LD, sizeof(R) == 4 ? 1 : 0);
     constexpr int N = (NCD - CD0 < S) ? NCD - CD0 : S;
-    constexpr int TL = RysTab<R>::len(NR);
-    __shared__ __align__(16) R tab[TL];
-    {
-        const R *gt = RysTab<R>::ptr(NR);
-        for (int k = threadIdx.x; k < TL; k += blockDim.x) tab[k] = gt[k];
-        __syncthreads();
-    }
+    __shared__ __align__(16) R tab[RysTab<R>::slen(NR)];
+    rys_stage<R, NR>(tab);
     const int lane = threadIdx.x & 31;
     for (;;) {
         unsigned long long u = 0;
@@ -176,10 +171,10 @@ __global__ void __launch_bounds__(FOCK_THREADS,
         for (int k = 0; k < ncart(LA) * ncart(LB) * N; k++) acc[k] = (R)0;
         if constexpr (sizeof(R) == 4) {
             const PPRec32 src{GTF_FLD(pprec32)};
-            if (active) eri_accumulate_cd32<LA, LB, LC, LD, CD0, N, true>(src, pb, pk, acc, tab);
+            if (active) eri_accumulate_cd32<LA, LB, LC, LD, CD0, N, true, true>(src, pb, pk, acc, tab);
         } else {
             const PPRec src{GTF_FLD(pprec)};
-            if (active) eri_accumulate_cd<LA, LB, LC, LD, CD0, N, true>(src, pb, src, pk, acc, tab);
+            if (active) eri_accumulate_cd<LA, LB, LC, LD, CD0, N, true, true>(src, pb, src, pk, acc, tab);
         }
         digest_cd<LA, LB, LC, LD, CD0, N>(acc, active, pb, pk, same, GTF_FLD(D), GTF_FLD(Fj), GTF_FLD(Fk),
                                           GTF_FLD(ld), lane, GTF_FLD(konly) != 0);

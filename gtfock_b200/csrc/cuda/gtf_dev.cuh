@@ -124,31 +124,6 @@ __device__ __forceinline__ float grsqrt(float x) { return rsqrtf(x); }
 // ---------------------------------------------------------------------------
 // Rys roots and weights
 // ---------------------------------------------------------------------------
-// The N-root block of each table is [off(N), off(N+1)); its extent is known
-// at compile time so kernels can stage it in shared memory.
-template <typename R>
-struct RysTab;
-template <>
-struct RysTab<double> {
-    static __host__ __device__ constexpr int off(int n)
-    {
-        constexpr int o[] = {RYS_OFF_LIST, RYS_TABLE_LEN};
-        return o[n];
-    }
-    static __host__ __device__ constexpr int len(int n) { return off(n + 1) - off(n); }
-    static __device__ __forceinline__ const double *ptr(int n) { return RYS_TABLE + off(n); }
-};
-template <>
-struct RysTab<float> {
-    static __host__ __device__ constexpr int off(int n)
-    {
-        constexpr int o[] = {RYS32_OFF_LIST, RYS32_TABLE_LEN};
-        return o[n];
-    }
-    static __host__ __device__ constexpr int len(int n) { return off(n + 1) - off(n); }
-    static __device__ __forceinline__ const float *ptr(int n) { return RYS32_TABLE + off(n); }
-};
-
 // interval width and polynomial degree of the N-root FP64 table
 __host__ __device__ constexpr double rys_h(int n)
 {
@@ -161,8 +136,56 @@ __host__ __device__ constexpr int rys_deg(int n)
     return d[n];
 }
 
-// tab: the N-root block of RYS_TABLE (global or a shared-memory copy)
-template <int N>
+// The N-root block of each table is [off(N), off(N+1)); its extent is known
+// at compile time so kernels can stage it in shared memory.  rows(N) values
+// per interval; a lane reads one interval's row as 2-value vectors (16 bytes
+// FP64, 8 bytes FP32).  The lanes of a warp read different intervals, so the
+// shared-memory copy pads each interval to srows(N), an odd number of vectors:
+// consecutive intervals then start in different banks (unpadded, the FP64
+// 4-root rows are 48 vectors long and every interval starts in the same bank).
+template <typename R>
+struct RysTab;
+template <>
+struct RysTab<double> {
+    static __host__ __device__ constexpr int off(int n)
+    {
+        constexpr int o[] = {RYS_OFF_LIST, RYS_TABLE_LEN};
+        return o[n];
+    }
+    static __host__ __device__ constexpr int len(int n) { return off(n + 1) - off(n); }
+    static __host__ __device__ constexpr int rows(int n) { return (rys_deg(n) + 1) * 2 * n; }
+    static __host__ __device__ constexpr int srows(int n) { return (rows(n) / 2) % 2 == 0 ? rows(n) + 2 : rows(n); }
+    static __host__ __device__ constexpr int slen(int n) { return len(n) / rows(n) * srows(n); }
+    static __device__ __forceinline__ const double *ptr(int n) { return RYS_TABLE + off(n); }
+};
+template <>
+struct RysTab<float> {
+    static __host__ __device__ constexpr int off(int n)
+    {
+        constexpr int o[] = {RYS32_OFF_LIST, RYS32_TABLE_LEN};
+        return o[n];
+    }
+    static __host__ __device__ constexpr int len(int n) { return off(n + 1) - off(n); }
+    static __host__ __device__ constexpr int rows(int n) { return (RYS32_DEG + 1) * 2 * n; }
+    static __host__ __device__ constexpr int srows(int n) { return (rows(n) / 2) % 2 == 0 ? rows(n) + 2 : rows(n); }
+    static __host__ __device__ constexpr int slen(int n) { return len(n) / rows(n) * srows(n); }
+    static __device__ __forceinline__ const float *ptr(int n) { return RYS32_TABLE + off(n); }
+};
+
+// Stages the N-root block into shared memory with the padded row stride.
+template <typename R, int N>
+__device__ __forceinline__ void rys_stage(R *stab)
+{
+    constexpr int RW = RysTab<R>::rows(N), SR = RysTab<R>::srows(N), TL = RysTab<R>::len(N);
+    static_assert(TL % RW == 0, "whole intervals");
+    const R *gt = RysTab<R>::ptr(N);
+    for (int k = threadIdx.x; k < TL; k += blockDim.x) stab[(k / RW) * SR + k % RW] = __ldg(gt + k);
+    __syncthreads();
+}
+
+// tab: the N-root block of RYS_TABLE (global, STRIDE = rows) or its padded
+// shared-memory copy (STRIDE = srows)
+template <int N, int STRIDE = RysTab<double>::rows(N)>
 __device__ __forceinline__ void rys_roots(double T, double (&u)[N], double (&w)[N], const double *tab)
 {
     constexpr double H = rys_h(N), INV_H = 1.0 / rys_h(N);
@@ -179,7 +202,8 @@ __device__ __forceinline__ void rys_roots(double T, double (&u)[N], double (&w)[
     }
     const int k = (int)(T * INV_H);
     const double s = T - ((double)k * H + 0.5 * H);
-    const double *c = tab + k * (DEG + 1) * (2 * N);
+    static_assert(STRIDE % 2 == 0 && STRIDE >= (DEG + 1) * 2 * N, "interval stride");
+    const double *c = tab + k * STRIDE;
     // rows of 2N coefficients start on 16-byte boundaries (even offsets)
     const double2 *c2 = reinterpret_cast<const double2 *>(c);
     double a[2 * N];
@@ -207,7 +231,7 @@ __device__ __forceinline__ void rys_roots(double T, double (&u)[N], double (&w)[
 
 // FP32 form for quartets evaluated in single precision: degree-7 fit of the
 // same functions on the same intervals (RYS32_TABLE), same large-T form
-template <int N>
+template <int N, int STRIDE = RysTab<float>::rows(N)>
 __device__ __forceinline__ void rys_roots(float T, float (&u)[N], float (&w)[N], const float *tab)
 {
     if (T >= (float)RYS_TMAX[N]) {
@@ -222,7 +246,8 @@ __device__ __forceinline__ void rys_roots(float T, float (&u)[N], float (&w)[N],
     }
     const int k = (int)(T * RYS32_INV_H);
     const float s = T - ((float)k * (float)RYS32_H + 0.5f * (float)RYS32_H);
-    const float2 *c2 = reinterpret_cast<const float2 *>(tab + k * (RYS32_DEG + 1) * (2 * N));
+    static_assert(STRIDE % 2 == 0 && STRIDE >= (RYS32_DEG + 1) * 2 * N, "interval stride");
+    const float2 *c2 = reinterpret_cast<const float2 *>(tab + k * STRIDE);
     float a[2 * N];
 #pragma unroll
     for (int f = 0; f < N; f++) {
@@ -340,7 +365,8 @@ __device__ __forceinline__ void hrr_abcd(const R (&G)[LA + LB + 1][LC + LD + 1],
 // Loop order: ket primitive pairs outside (one per lane), bra primitive pairs
 // inside -- the bra is shared by the warp, so its records are warp-uniform
 // loads that stay in L1, and each lane reads its ket's records once.
-template <int LA, int LB, int LC, int LD, int CD0, int N, bool SKIP, class PPB, class PPK, typename R>
+template <int LA, int LB, int LC, int LD, int CD0, int N, bool SKIP, bool SPAD = false, class PPB, class PPK,
+          typename R>
 __device__ __forceinline__ void eri_accumulate_cd(const PPB &bra, const PairRec &pb, const PPK &ket,
                                                   const PairRec &pk, R (&acc)[ncart(LA) * ncart(LB) * N],
                                                   const R *rtab)
@@ -375,7 +401,7 @@ __device__ __forceinline__ void eri_accumulate_cd(const PPB &bra, const PairRec 
             const R T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
             const R pref = (R)(bq.K * kq.K) * rpq;
             R u[NR], w[NR];
-            rys_roots<NR>(T, u, w, rtab);
+            rys_roots<NR, SPAD ? RysTab<R>::srows(NR) : RysTab<R>::rows(NR)>(T, u, w, rtab);
             const R qf = q_ * ipq, pf = p_ * ipq;
 #pragma unroll
             for (int r = 0; r < NR; r++) {
@@ -417,7 +443,7 @@ __device__ __forceinline__ void eri_accumulate_cd(const PPB &bra, const PairRec 
 // FP32 quartets: everything in single precision, from the FP32 records (centres
 // relative to each pair's first shell; P - Q = PA - QC + (A - C) with A - C
 // formed in double once per quartet).  Same structure as eri_accumulate_cd.
-template <int LA, int LB, int LC, int LD, int CD0, int N, bool SKIP>
+template <int LA, int LB, int LC, int LD, int CD0, int N, bool SKIP, bool SPAD = false>
 __device__ __forceinline__ void eri_accumulate_cd32(const PPRec32 &src, const PairRec &pb, const PairRec &pk,
                                                     float (&acc)[ncart(LA) * ncart(LB) * N], const float *rtab)
 {
@@ -452,7 +478,7 @@ __device__ __forceinline__ void eri_accumulate_cd32(const PPRec32 &src, const Pa
             const float T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
             const float pref = bq.K * kq.K * rpq;
             float u[NR], w[NR];
-            rys_roots<NR>(T, u, w, rtab);
+            rys_roots<NR, SPAD ? RysTab<float>::srows(NR) : RysTab<float>::rows(NR)>(T, u, w, rtab);
             const float qf = q * ipq, pf = p * ipq;
 #pragma unroll
             for (int r = 0; r < NR; r++) {
