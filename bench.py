@@ -317,11 +317,17 @@ def profile_fock(args):
         if args.fp32_cutoff is not None:
             pf.set_precision(1, args.fp32_cutoff)
         D = np.eye(b.nbf) * 0.3
+        tune = None
+        if args.autotune:
+            pf.compute_fock(D)
+            t0 = time.perf_counter()
+            pf.autotune(2)
+            tune = {"seconds": time.perf_counter() - t0, "entries": gb.tune_entries()}
         for _ in range(args.builds):
             pf.compute_fock(D)
         tm = pf.timing()
         nq32, nq = pf.precision_stats()
-        out = {"molecule": args.profile_fock, "nbf": b.nbf, "counts": pf.counts(), "timing": tm,
+        out = {"molecule": args.profile_fock, "nbf": b.nbf, "counts": pf.counts(), "timing": tm, "autotune": tune,
                "fp32_cutoff": args.fp32_cutoff, "fp32_share": nq32 / nq if nq else 0.0,
                "classes": [{"bra": x, "ket": y, "ms": ms, "quartets": q, "gflop": w[0] / 1e9,
                             "primq": w[1], "tflops": w[0] / ms / 1e9 if ms > 0 else 0.0}
@@ -381,12 +387,19 @@ def run_batched(args):
             slots = [b.add(g, x, tolscr=TOL, precision=prec, fp32_cutoff=cut, max_iters=niter, etol=0.0)
                      for g, x in files]
             t1 = time.perf_counter()
+            setup_s = t1 - t0
+            tune_s = None
+            if args.autotune:
+                b.autotune(2)
+                tune_s = time.perf_counter() - t1
+                t1 = time.perf_counter()
             l0 = gb.launch_count()
             b.run()
             t2 = time.perf_counter()
             info = b.info()
             res[tag] = [b.result(s)[0] for s in slots]
-            out[tag] = {"solves_per_s": len(files) / (t2 - t1), "solve_s": t2 - t1, "setup_s": t1 - t0,
+            out[tag] = {"solves_per_s": len(files) / (t2 - t1), "solve_s": t2 - t1, "setup_s": setup_s,
+                        "autotune_s": tune_s,
                         "ms_fock": info["ms_fock"], "ms_energy": info["ms_energy"], "ms_diis": info["ms_diis"],
                         "ms_purification": info["ms_purification"],
                         "purification_steps": info["purification_steps"], "steps": info["steps"],
@@ -422,6 +435,8 @@ def run_batched(args):
         out["max_dE_mixed_vs_fp64"] = d_mix
         out["speedup_batched_mixed_vs_sequential_fp64"] = (out["batched_mixed"]["solves_per_s"] /
                                                            out["sequential_fp64"]["solves_per_s"])
+        if args.autotune:
+            out["tuned"] = [e for e in gb.tune_entries() if e["kind"] != "fock"]
     print(json.dumps(out), flush=True)
 
 
@@ -551,6 +566,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-fock", choices=["c12h26", "c54h18", "c96h24", "w64"], default=None)
     ap.add_argument("--builds", type=int, default=2)
+    ap.add_argument("--autotune", action="store_true",
+                    help="--profile-fock: tune the launch shapes before timing")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="--workload batched: keep the default launch shapes (tuned by default)")
     ap.add_argument("--profile-purif", action="store_true",
                     help="two SCF iterations of (H2O)64 with the split-BF16 purification (ncu case)")
     ap.add_argument("--fp32-cutoff", type=float, default=None,
@@ -567,6 +586,7 @@ def main():
     ap.add_argument("--seq-sample", type=int, default=256, help="batched: molecules timed on the one-job path")
     args = ap.parse_args()
     if args.workload == "batched":
+        args.autotune = not args.no_autotune
         args.count = args.count or 256
         args.seed = 2024 if args.seed is None else args.seed
         run_batched(args)

@@ -115,6 +115,14 @@ def load():
     _sig(L, "gtf_batch_job_bytes", [_i], ctypes.c_size_t)
     _sig(L, "gtf_batch_stats", [_vp, _dp, _i])
     _sig(L, "gtf_batch_destroy", [_vp], None)
+    _sig(L, "gtf_pfock_autotune", [_vp, _i])
+    _sig(L, "gtf_batch_autotune", [_vp, _i])
+    _sig(L, "gtf_tune_save", [_cp])
+    _sig(L, "gtf_tune_load", [_cp])
+    _sig(L, "gtf_tune_clear", [], None)
+    _sig(L, "gtf_tune_put", [_i, _i, _i, _i, _d, _i, _i, _d], None)
+    _sig(L, "gtf_tune_get", [_i, _i, _i, _i, _d, _ip, _ip])
+    _sig(L, "gtf_tune_entries", [_ip, _i])
     _sig(L, "gtf_fp64_peak", [_dp])
     _sig(L, "gtf_device_info", [_ip, _ip])
     _lib = L
@@ -259,6 +267,11 @@ class PFock:
         """mode 0: FP64; mode 1: FP32 for quartets with Schwarz bound < fp32_cutoff."""
         self._check(load().gtf_pfock_set_precision(self.h, mode, fp32_cutoff),
                     "gtf_pfock_set_precision")
+
+    def autotune(self, reps=2):
+        """Time candidate launch shapes of every Fock launch on the density last
+        put and record the fastest in the process-wide tuning table."""
+        self._check(load().gtf_pfock_autotune(self.h, reps), "gtf_pfock_autotune")
 
     def precision_stats(self):
         """(quartets evaluated in FP32, all quartets) under the current mode."""
@@ -473,6 +486,13 @@ class Batch:
                 "device_bytes": by.value, "ms_energy": st[1], "ms_diis": st[2], "ms_purification": st[3],
                 "purification_steps": st[4], "steps": st[5]}
 
+    def autotune(self, reps=2):
+        """Tune the Fock launch shapes and the product tile shape for the jobs
+        now in the batch (between steps)."""
+        r = load().gtf_batch_autotune(self.h, reps)
+        if r != 0:
+            raise GtfError("gtf_batch_autotune failed (%d)" % r)
+
     @staticmethod
     def job_bytes(nbf):
         return int(load().gtf_batch_job_bytes(nbf))
@@ -483,6 +503,47 @@ class Batch:
             self.h = None
 
     __del__ = close
+
+
+TUNE_KINDS = {0: "fock", 1: "fock-batch", 2: "products"}
+GEMM_SHAPES = {0: "64x64 (4x4)", 1: "32x32 (2x2)", 2: "32x64 (2x4)", 3: "128x64 (8x4)"}
+
+
+def tune_entries():
+    """The process-wide tuning table as a list of dicts."""
+    L = load()
+    n = L.gtf_tune_entries(None, 0)
+    rows = np.zeros(8 * max(n, 1), dtype=np.int32)
+    n = L.gtf_tune_entries(rows.ctypes.data_as(_ip), n)
+    out = []
+    for r in rows[:8 * n].reshape(n, 8):
+        kind = int(r[0])
+        e = {"kind": TUNE_KINDS.get(kind, kind), "X": int(r[1]), "Y": int(r[2]), "part": int(r[3]),
+             "bucket": int(r[4]), "ms": r[7] / 1000.0}
+        if kind == 2:
+            e["shape"] = GEMM_SHAPES.get(int(r[5]), int(r[5]))
+        else:
+            e["ctas_per_sm"] = int(r[5])
+            e["claim"] = int(r[6])
+        out.append(e)
+    return out
+
+
+def tune_save(path):
+    if load().gtf_tune_save(path.encode()) != 0:
+        raise GtfError("gtf_tune_save(%s) failed" % path)
+
+
+def tune_load(path):
+    """Merge a saved tuning table; raises GtfError for a missing file or one
+    written on another device model."""
+    r = load().gtf_tune_load(path.encode())
+    if r != 0:
+        raise GtfError("gtf_tune_load(%s) failed (%d)" % (path, r))
+
+
+def tune_clear():
+    load().gtf_tune_clear()
 
 
 def launch_count():

@@ -36,8 +36,6 @@ extern "C" const char *gtf_last_error(void);
 
 #define BJ_MAX_DIIS 10
 #define BJ_THREADS 256
-#define BJ_TILE 64
-#define BJ_KT 16
 #define BJ_PUR_MAX 200
 #define BJ_PUR_CHECK 8
 #define BJ_EBLOCKS 64   // blocks per job of the energy reduction
@@ -67,14 +65,24 @@ struct GemmDesc {
 };
 
 // C = A B^T (TB) or C = A B, row-major n x n.  Block t of the launch is tile
-// (ti, tj) of descriptor d, found in the exclusive tile prefix.
-template <bool TB>
-__global__ void __launch_bounds__(BJ_THREADS) k_bgemm(const GemmDesc *__restrict__ ds,
-                                                     const int *__restrict__ tile_prefix, int nd,
-                                                     const int *__restrict__ active)
+// (ti, tj) of descriptor d, found in the exclusive tile prefix.  BM x BN
+// output tiles, TM x TN per thread, KT-deep slabs of A and op(B) in
+// shared memory (column-major in the slab so a thread's TM / TN values are
+// contiguous 16-byte vectors), double-buffered: the next slab's global loads
+// are in flight while the current one is multiplied.  Rows of the
+// transposed slabs are padded by two doubles so the transposing stores of a
+// warp spread over the banks.
+template <bool TB, int BM, int BN, int TM, int TN, int KT>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN)) k_bgemm(const GemmDesc *__restrict__ ds,
+                                                               const int *__restrict__ tile_prefix, int nd,
+                                                               const int *__restrict__ active)
 {
-    __shared__ double As[BJ_KT][BJ_TILE];
-    __shared__ double Bs[BJ_KT][BJ_TILE];
+    constexpr int NT = (BM / TM) * (BN / TN);
+    constexpr int NA = BM * KT / NT, NB = BN * KT / NT;   // slab elements per thread
+    static_assert(BM * KT % NT == 0 && BN * KT % NT == 0 && TM % 2 == 0 && TN % 2 == 0, "tile shape");
+    constexpr int PA = BM + 2, PB = TB ? BN + 2 : BN;
+    __shared__ __align__(16) double As[2][KT][PA];
+    __shared__ __align__(16) double Bs[2][KT][PB];
     const int t = blockIdx.x;
     int lo = 0, hi = nd;
     while (hi - lo > 1) {
@@ -85,55 +93,111 @@ __global__ void __launch_bounds__(BJ_THREADS) k_bgemm(const GemmDesc *__restrict
     const GemmDesc g = ds[lo];
     if (g.job >= 0 && active && !active[g.job]) return;
     const int n = g.n;
-    const int nt = (n + BJ_TILE - 1) / BJ_TILE;
+    const int ntc = (n + BN - 1) / BN;
     const int local = t - tile_prefix[lo];
-    const int r0 = (local / nt) * BJ_TILE, c0 = (local % nt) * BJ_TILE;
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    double acc[4][4];
+    const int r0 = (local / ntc) * BM, c0 = (local % ntc) * BN;
+    const int tid = threadIdx.x;
+    const int tx = tid % (BN / TN), ty = tid / (BN / TN);
+    double ra[NA], rb[NB];
+    // slab k0 -> registers (zero outside the matrix)
+    auto load = [&](int k0) {
 #pragma unroll
-    for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
-    for (int k0 = 0; k0 < n; k0 += BJ_KT) {
-        // 64 x 16 tiles of A (rows r0..) and of op(B) (columns c0..)
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const int e = threadIdx.x + q * BJ_THREADS;  // 0..1023
-            const int kk = e & 15, rr = e >> 4;
+        for (int q = 0; q < NA; q++) {
+            const int e = tid + q * NT, kk = e % KT, rr = e / KT;
             const int ar = r0 + rr, ak = k0 + kk;
-            As[kk][rr] = (ar < n && ak < n) ? g.A[(size_t)ar * n + ak] : 0.0;
+            ra[q] = (ar < n && ak < n) ? __ldg(g.A + (size_t)ar * n + ak) : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < NB; q++) {
+            const int e = tid + q * NT;
             if (TB) {
-                const int bc = c0 + rr;
-                Bs[kk][rr] = (bc < n && ak < n) ? g.B[(size_t)bc * n + ak] : 0.0;
+                const int kk = e % KT, cc = e / KT, bc = c0 + cc, bk = k0 + kk;
+                rb[q] = (bc < n && bk < n) ? __ldg(g.B + (size_t)bc * n + bk) : 0.0;
             } else {
-                const int bk = k0 + (e >> 6), bc = c0 + (e & 63);
-                Bs[e >> 6][e & 63] = (bk < n && bc < n) ? g.B[(size_t)bk * n + bc] : 0.0;
+                const int cc = e % BN, kk = e / BN, bc = c0 + cc, bk = k0 + kk;
+                rb[q] = (bc < n && bk < n) ? __ldg(g.B + (size_t)bk * n + bc) : 0.0;
             }
         }
-        __syncthreads();
+    };
+    auto store = [&](int buf) {
 #pragma unroll
-        for (int kk = 0; kk < BJ_KT; kk++) {
-            double a[4], b[4];
-#pragma unroll
-            for (int i = 0; i < 4; i++) a[i] = As[kk][ty * 4 + i];
-#pragma unroll
-            for (int j = 0; j < 4; j++) b[j] = Bs[kk][tx * 4 + j];
-#pragma unroll
-            for (int i = 0; i < 4; i++)
-#pragma unroll
-                for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        for (int q = 0; q < NA; q++) {
+            const int e = tid + q * NT;
+            As[buf][e % KT][e / KT] = ra[q];
         }
+#pragma unroll
+        for (int q = 0; q < NB; q++) {
+            const int e = tid + q * NT;
+            if (TB) Bs[buf][e % KT][e / KT] = rb[q];
+            else Bs[buf][e / BN][e % BN] = rb[q];
+        }
+    };
+    double acc[TM][TN];
+#pragma unroll
+    for (int i = 0; i < TM; i++)
+#pragma unroll
+        for (int j = 0; j < TN; j++) acc[i][j] = 0.0;
+    load(0);
+    store(0);
+    __syncthreads();
+    int cur = 0;
+    for (int k0 = 0; k0 < n; k0 += KT) {
+        const bool more = k0 + KT < n;
+        if (more) load(k0 + KT);
+#pragma unroll
+        for (int kk = 0; kk < KT; kk++) {
+            double a[TM], b[TN];
+#pragma unroll
+            for (int i = 0; i < TM; i += 2) {
+                const double2 v = *reinterpret_cast<const double2 *>(&As[cur][kk][ty * TM + i]);
+                a[i] = v.x;
+                a[i + 1] = v.y;
+            }
+#pragma unroll
+            for (int j = 0; j < TN; j += 2) {
+                const double2 v = *reinterpret_cast<const double2 *>(&Bs[cur][kk][tx * TN + j]);
+                b[j] = v.x;
+                b[j + 1] = v.y;
+            }
+#pragma unroll
+            for (int i = 0; i < TM; i++)
+#pragma unroll
+                for (int j = 0; j < TN; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        }
+        if (more) store(cur ^ 1);
         __syncthreads();
+        cur ^= 1;
     }
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const int r = r0 + ty * 4 + i;
+    for (int i = 0; i < TM; i++) {
+        const int r = r0 + ty * TM + i;
         if (r >= n) continue;
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int c = c0 + tx * 4 + j;
+        for (int j = 0; j < TN; j++) {
+            const int c = c0 + tx * TN + j;
             if (c < n) g.C[(size_t)r * n + c] = acc[i][j];
         }
+    }
+}
+
+// Tile shapes the batched products can run with (the autotuner picks one per
+// batch; 0 is the default).
+struct BGemmShape {
+    int bm, bn, tm, tn, kt;
+};
+static const BGemmShape BG_SHAPES[] = {{64, 64, 4, 4, 16}, {32, 32, 2, 2, 16}, {32, 64, 2, 4, 16},
+                                       {128, 64, 8, 4, 8}};
+#define BG_NSHAPES 4
+
+template <bool TB>
+static void launch_bgemm_shape(int shape, int ntiles, cudaStream_t st, const GemmDesc *gd, const int *tp, int m,
+                               const int *active)
+{
+    switch (shape) {
+        case 1: k_bgemm<TB, 32, 32, 2, 2, 16><<<ntiles, 256, 0, st>>>(gd, tp, m, active); break;
+        case 2: k_bgemm<TB, 32, 64, 2, 4, 16><<<ntiles, 256, 0, st>>>(gd, tp, m, active); break;
+        case 3: k_bgemm<TB, 128, 64, 8, 4, 8><<<ntiles, 256, 0, st>>>(gd, tp, m, active); break;
+        default: k_bgemm<TB, 64, 64, 4, 4, 16><<<ntiles, 256, 0, st>>>(gd, tp, m, active); break;
     }
 }
 
@@ -344,6 +408,7 @@ struct gtf_batch {
     // CUDA graph and replayed every step (null: launch directly)
     cudaGraphExec_t fock_exec;
     int fock_launches;
+    int gshape;                    // tile shape of the batched products (BG_SHAPES)
     // device arrays (capacity-sized)
     JobDev *d_jobs;
     GemmDesc *d_gd;                // 10 call sets x capacity
@@ -423,6 +488,7 @@ extern "C" gtf_batch_t *gtf_batch_create(int capacity)
     b->jobs.resize(capacity);
     b->fb = nullptr;
     b->dirty = 1;
+    b->gshape = 0;
     b->ms_fock = b->ms_rest = b->ms_energy = b->ms_diis = b->ms_pur = b->pur_steps = b->nsteps = 0.0;
     bool ok = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) == cudaSuccess;
     ok = ok && cudaEventCreate(&b->e0) == cudaSuccess && cudaEventCreate(&b->e1) == cudaSuccess &&
@@ -593,8 +659,8 @@ static int run_gemm(gtf_batch *b, int s, int m, bool tb, const int *active, int 
     if (ntiles == 0) return GTF_OK;
     const GemmDesc *gd = b->d_gd + (size_t)s * b->capacity;
     const int *tp = b->d_tp + (size_t)s * (b->capacity + 1);
-    if (tb) k_bgemm<true><<<ntiles, BJ_THREADS, 0, b->st>>>(gd, tp, m, active);
-    else k_bgemm<false><<<ntiles, BJ_THREADS, 0, b->st>>>(gd, tp, m, active);
+    if (tb) launch_bgemm_shape<true>(b->gshape, ntiles, b->st, gd, tp, m, active);
+    else launch_bgemm_shape<false>(b->gshape, ntiles, b->st, gd, tp, m, active);
     CKH(cudaGetLastError());
     (*launches)++;
     return GTF_OK;
@@ -608,10 +674,11 @@ static void set_gemm(gtf_batch *b, int s, int k, const double *A, const double *
     g.C = C;
     g.n = n;
     g.job = job;
-    const int nt = (n + BJ_TILE - 1) / BJ_TILE;
+    const BGemmShape &sh = BG_SHAPES[b->gshape];
+    const int ntr = (n + sh.bm - 1) / sh.bm, ntc = (n + sh.bn - 1) / sh.bn;
     int *tp = b->h_tp + (size_t)s * (b->capacity + 1);
     if (k == 0) tp[0] = 0;
-    tp[k + 1] = tp[k] + nt * nt;
+    tp[k + 1] = tp[k] + ntr * ntc;
 }
 
 // inverse of the bordered DIIS matrix by Gauss-Jordan with partial pivoting;
@@ -666,6 +733,58 @@ static void diis_update(BJob &j, int cur_idx, const double *dots)
 
 // One SCF iteration of every running job.  Returns the number of jobs still
 // running afterwards, or a negative error.
+// sum of n^3 over the jobs whose dense products run batched (the size key of
+// the tile-shape tuning)
+static double batch_gemm_work(const gtf_batch *b, const std::vector<int> &run)
+{
+    double w = 0.0;
+    for (int s : run)
+        if (!b->jobs[s].pd) w += (double)b->jobs[s].n * b->jobs[s].n * b->jobs[s].n;
+    return w;
+}
+
+// (Re)creates the batched Fock build for the jobs in `run`, picks the tile
+// shape of the dense products from the tuning table, and captures the build
+// as a CUDA graph for replay while the membership stays the same.
+static int rebuild_fock_batch(gtf_batch *b, const std::vector<int> &run)
+{
+    if (b->fb) gtf_fock_batch_destroy(b->fb);
+    b->fb = nullptr;
+    std::vector<gtf_fock_dev_t *> eng;
+    for (int s : run) eng.push_back(b->jobs[s].eng);
+    if (gtf_fock_batch_create(eng.data(), (int)eng.size(), b->st, &b->fb) != GTF_OK) {
+        fprintf(stderr, "gtfock_b200: batched Fock set-up failed: %s\n", gtf_last_error());
+        return -2;
+    }
+    b->fb_members = run;
+    b->dirty = 0;
+    // capture the build (one launch per class pair, part and slice, plus
+    // the transforms) for replay while the membership stays the same
+    if (b->fock_exec) cudaGraphExecDestroy(b->fock_exec);
+    b->fock_exec = nullptr;
+    b->fock_launches = 0;
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        const int nl = gtf_fock_batch_compute(b->fb);
+        const cudaError_t ce = cudaStreamEndCapture(b->st, &graph);
+        if (nl >= 0 && ce == cudaSuccess && graph &&
+            cudaGraphInstantiate(&b->fock_exec, graph, 0) == cudaSuccess) {
+            b->fock_launches = nl;
+            gtf_note_launches(-nl);   // counted when replayed, not when captured
+        } else {
+            b->fock_exec = nullptr;
+        }
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+    }
+    // tile shape of the dense products: tuned for this size, else the default
+    b->gshape = 0;
+    int shape = 0;
+    if (gtf_tune_get(2, -1, -1, 0, batch_gemm_work(b, run), &shape, nullptr) && shape >= 0 && shape < BG_NSHAPES)
+        b->gshape = shape;
+    return 0;
+}
+
 extern "C" int gtf_batch_step(gtf_batch_t *b)
 {
     if (!b) return -1;
@@ -676,35 +795,8 @@ extern "C" int gtf_batch_step(gtf_batch_t *b)
     int launches = 0;
     // ---- Fock build of every running job ----
     if (b->dirty || run != b->fb_members) {
-        if (b->fb) gtf_fock_batch_destroy(b->fb);
-        b->fb = nullptr;
-        std::vector<gtf_fock_dev_t *> eng;
-        for (int s : run) eng.push_back(b->jobs[s].eng);
-        if (gtf_fock_batch_create(eng.data(), (int)eng.size(), b->st, &b->fb) != GTF_OK) {
-            fprintf(stderr, "gtfock_b200: batched Fock set-up failed: %s\n", gtf_last_error());
-            return -2;
-        }
-        b->fb_members = run;
-        b->dirty = 0;
-        // capture the build (one launch per class pair, part and slice, plus
-        // the transforms) for replay while the membership stays the same
-        if (b->fock_exec) cudaGraphExecDestroy(b->fock_exec);
-        b->fock_exec = nullptr;
-        b->fock_launches = 0;
-        cudaGraph_t graph = nullptr;
-        if (cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-            const int nl = gtf_fock_batch_compute(b->fb);
-            const cudaError_t ce = cudaStreamEndCapture(b->st, &graph);
-            if (nl >= 0 && ce == cudaSuccess && graph &&
-                cudaGraphInstantiate(&b->fock_exec, graph, 0) == cudaSuccess) {
-                b->fock_launches = nl;
-                gtf_note_launches(-nl);   // counted when replayed, not when captured
-            } else {
-                b->fock_exec = nullptr;
-            }
-            if (graph) cudaGraphDestroy(graph);
-            cudaGetLastError();
-        }
+        const int r = rebuild_fock_batch(b, run);
+        if (r) return r;
     }
     CKH(cudaEventRecord(b->e0, b->st));
     if (b->fock_exec) {
@@ -917,6 +1009,63 @@ extern "C" int gtf_batch_step(gtf_batch_t *b)
     for (int s = 0; s < b->capacity; s++)
         if (b->jobs[s].used && !b->jobs[s].done) left++;
     return left;
+}
+
+// Tunes the batch for its current jobs: the launch shapes of the batched
+// Fock build, then the tile shape of the dense products, timed on W = X X^T
+// of every job whose products run batched (W is scratch between steps).  The
+// next step re-captures the Fock graph with the tuned shapes.
+extern "C" int gtf_batch_autotune(gtf_batch_t *b, int reps)
+{
+    if (!b) return GTF_ERR_INVALID;
+    if (reps < 1) reps = 1;
+    std::vector<int> run;
+    for (int s = 0; s < b->capacity; s++)
+        if (b->jobs[s].used && !b->jobs[s].done) run.push_back(s);
+    if (run.empty()) return GTF_OK;
+    if ((b->dirty || run != b->fb_members) && rebuild_fock_batch(b, run) != 0) return GTF_ERR_CUDA;
+    const int rc = gtf_fock_batch_autotune(b->fb, reps);
+    if (rc != GTF_OK) return rc;
+    std::vector<int> small;
+    for (int s : run)
+        if (!b->jobs[s].pd) small.push_back(s);
+    if (!small.empty()) {
+        const int m = (int)small.size();
+        const size_t C1 = b->capacity + 1;
+        double best = -1.0;
+        int bs = 0;
+        for (int shape = 0; shape < BG_NSHAPES; shape++) {
+            b->gshape = shape;
+            for (int q = 0; q < m; q++) {
+                const BJob &j = b->jobs[small[q]];
+                set_gemm(b, 6, q, j.dv.X, j.dv.X, j.dv.W, j.n, -1);
+            }
+            CKH(cudaMemcpyAsync(b->d_gd + 6 * (size_t)b->capacity, b->h_gd + 6 * (size_t)b->capacity,
+                                sizeof(GemmDesc) * m, cudaMemcpyHostToDevice, b->st));
+            CKH(cudaMemcpyAsync(b->d_tp + 6 * C1, b->h_tp + 6 * C1, sizeof(int) * (m + 1), cudaMemcpyHostToDevice,
+                                b->st));
+            double tmin = 1e30;
+            int launches = 0;
+            for (int r = 0; r < reps + 1; r++) {   // the first run warms up
+                CKH(cudaEventRecord(b->e0, b->st));
+                if (run_gemm(b, 6, m, true, nullptr, &launches)) return GTF_ERR_CUDA;
+                CKH(cudaEventRecord(b->e1, b->st));
+                CKH(cudaEventSynchronize(b->e1));
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, b->e0, b->e1);
+                if (r > 0 && ms < tmin) tmin = ms;
+            }
+            gtf_note_launches(launches);
+            if (best < 0.0 || tmin < best) {
+                best = tmin;
+                bs = shape;
+            }
+        }
+        gtf_tune_put(2, -1, -1, 0, batch_gemm_work(b, run), bs, 0, best);
+        b->gshape = bs;
+    }
+    b->dirty = 1;
+    return GTF_OK;
 }
 
 extern "C" int gtf_batch_run(gtf_batch_t *b)

@@ -28,6 +28,9 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "gtf_cuda.h"
@@ -649,6 +652,197 @@ static int launch_fock(int X, int Y, const FockGrid &fg, cudaStream_t st)
         if (r != GTF_NOT_IN_GROUP) return r;  // launches, or -1 on error
     }
     return -1;
+}
+
+// ---------------------------------------------------------------------------
+// launch-shape autotuning
+// ---------------------------------------------------------------------------
+// Process-wide table: (kind, class X, class Y, precision part, size bucket)
+// -> (a, b).  Kind 0 / 1: a Fock launch of a single engine / of a batch,
+// a = persistent blocks per SM, b = units of 32 quartets a warp claims at
+// once; kind 2: the batched dense products, a = tile shape.  The size bucket
+// is floor(log2) of the launch's units (or of the products' n^3 sum).  The
+// tuners time candidate shapes on the live engine and record the fastest;
+// launches look their shape up here (absent: the defaults).
+struct TuneKey {
+    int kind, X, Y, part, bucket;
+    bool operator<(const TuneKey &o) const
+    {
+        return std::tie(kind, X, Y, part, bucket) < std::tie(o.kind, o.X, o.Y, o.part, o.bucket);
+    }
+};
+struct TuneVal {
+    int a, b;
+    double ms;
+};
+static std::map<TuneKey, TuneVal> g_tune;
+static std::mutex g_tune_mu;
+
+static int tune_bucket(double size)
+{
+    int b = 0;
+    while (b < 120 && ldexp(1.0, b + 1) <= size) b++;
+    return b;
+}
+
+extern "C" int gtf_tune_get(int kind, int X, int Y, int part, double size, int *a, int *b)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(TuneKey{kind, X, Y, part, tune_bucket(size)});
+    if (it == g_tune.end()) return 0;
+    if (a) *a = it->second.a;
+    if (b) *b = it->second.b;
+    return 1;
+}
+
+extern "C" void gtf_tune_put(int kind, int X, int Y, int part, double size, int a, int b, double ms)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[TuneKey{kind, X, Y, part, tune_bucket(size)}] = TuneVal{a, b, ms};
+}
+
+extern "C" void gtf_tune_clear(void)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune.clear();
+}
+
+// rows of 8 ints: kind, X, Y, part, bucket, a, b, ms x 1000 (rounded); returns the count
+extern "C" int gtf_tune_entries(int *rows, int max_rows)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    int n = 0;
+    for (const auto &kv : g_tune) {
+        if (rows && n < max_rows) {
+            int *r = rows + 8 * n;
+            r[0] = kv.first.kind;
+            r[1] = kv.first.X;
+            r[2] = kv.first.Y;
+            r[3] = kv.first.part;
+            r[4] = kv.first.bucket;
+            r[5] = kv.second.a;
+            r[6] = kv.second.b;
+            r[7] = (int)lrint(kv.second.ms * 1000.0);
+        }
+        n++;
+    }
+    return n;
+}
+
+static void device_name(char *out, size_t len)
+{
+    int dev = 0;
+    cudaDeviceProp p;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&p, dev) != cudaSuccess) {
+        snprintf(out, len, "unknown");
+        return;
+    }
+    snprintf(out, len, "%s sm_%d%d", p.name, p.major, p.minor);
+    for (char *c = out; *c; c++)
+        if (*c == ' ') *c = '_';
+}
+
+// Text file: "gtfock_b200-tune 1 <device>" then one entry per line
+// "kind X Y part bucket a b ms".
+extern "C" int gtf_tune_save(const char *path)
+{
+    char dev[256];
+    device_name(dev, sizeof(dev));
+    FILE *fp = fopen(path, "w");
+    if (!fp) return GTF_ERR_IO;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    fprintf(fp, "gtfock_b200-tune 1 %s\n", dev);
+    for (const auto &kv : g_tune)
+        fprintf(fp, "%d %d %d %d %d %d %d %.6f\n", kv.first.kind, kv.first.X, kv.first.Y, kv.first.part,
+                kv.first.bucket, kv.second.a, kv.second.b, kv.second.ms);
+    return fclose(fp) == 0 ? GTF_OK : GTF_ERR_IO;
+}
+
+// Merges a saved table; a file written on another device model is refused
+// (GTF_ERR_INVALID) and leaves the table unchanged.
+extern "C" int gtf_tune_load(const char *path)
+{
+    FILE *fp = fopen(path, "r");
+    if (!fp) return GTF_ERR_IO;
+    char magic[64], dev[256], here[256];
+    int ver = 0;
+    if (fscanf(fp, "%63s %d %255s", magic, &ver, dev) != 3 || strcmp(magic, "gtfock_b200-tune") != 0 || ver != 1) {
+        fclose(fp);
+        return GTF_ERR_INVALID;
+    }
+    device_name(here, sizeof(here));
+    if (strcmp(dev, here) != 0) {
+        fclose(fp);
+        return GTF_ERR_INVALID;
+    }
+    std::vector<std::pair<TuneKey, TuneVal>> rows;
+    TuneKey k;
+    TuneVal v;
+    int r;
+    while ((r = fscanf(fp, "%d %d %d %d %d %d %d %lf", &k.kind, &k.X, &k.Y, &k.part, &k.bucket, &v.a, &v.b, &v.ms)) == 8)
+        rows.push_back({k, v});
+    const bool ok = (r == EOF);
+    fclose(fp);
+    if (!ok) return GTF_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (const auto &kv : rows) g_tune[kv.first] = kv.second;
+    return GTF_OK;
+}
+
+static void tune_apply(int kind, int X, int Y, int part, FockGrid &g)
+{
+    int a = 0, b = 0;
+    if (gtf_tune_get(kind, X, Y, part, (double)g.nunits, &a, &b)) {
+        g.ctas_per_sm = a;
+        g.claim = b;
+    }
+}
+
+// Times launch_fock of one (class pair, part) under each candidate shape
+// (blocks per SM: the occupancy limit, one less, half; for batched launches
+// claims of 1, 2, 4 units) and records the fastest.  `counters` holds GTF_MAX_SLICES slots;
+// the launches accumulate into the grid's F buffers, which the next build
+// clears.  Returns the best time in ms, or a negative value on error.
+static double tune_launch(int kind, int X, int Y, int part, FockGrid g, cudaStream_t st, int reps,
+                          cudaEvent_t e0, cudaEvent_t e1)
+{
+    g.query = 1;
+    const int occ = launch_fock(X, Y, g, st);
+    g.query = 0;
+    if (occ < 1) return -1.0;
+    int ctas[3] = {occ, occ - 1, (occ + 1) / 2};
+    int nct = 1;
+    for (int i = 1; i < 3; i++) {
+        bool dup = ctas[i] < 1;
+        for (int j = 0; j < nct; j++) dup = dup || ctas[j] == ctas[i];
+        if (!dup) ctas[nct++] = ctas[i];
+    }
+    const int claims[3] = {1, 2, 4};
+    const int ncl = g.nmol > 1 ? 3 : 1;    // only the batched kernels claim several units
+    double best = -1.0;
+    int ba = occ, bb = 1;
+    for (int ci = 0; ci < nct; ci++)
+        for (int cl = 0; cl < ncl; cl++) {
+            g.ctas_per_sm = ctas[ci];
+            g.claim = claims[cl];
+            double tmin = 1e30;
+            for (int r = 0; r < reps + 1; r++) {   // the first run warms up
+                if (cudaMemsetAsync(g.counter, 0, sizeof(unsigned long long) * GTF_MAX_SLICES, st) != cudaSuccess ||
+                    cudaEventRecord(e0, st) != cudaSuccess || launch_fock(X, Y, g, st) < 0 ||
+                    cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess)
+                    return -1.0;
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (r > 0 && ms < tmin) tmin = ms;
+            }
+            if (best < 0.0 || tmin < best) {
+                best = tmin;
+                ba = ctas[ci];
+                bb = claims[cl];
+            }
+        }
+    gtf_tune_put(kind, X, Y, part, (double)g.nunits, ba, bb, best);
+    return best;
 }
 
 // Rys-model FLOPs of one quartet of a class (normalisation used for the roofline):
@@ -1273,6 +1467,7 @@ static int launch_class(const gtf_fock_dev *f, int c, const double *D, double *F
         g.counter = counters + (size_t)(2 * c + part) * GTF_MAX_SLICES;
         g.nsm = f->nsm;
         g.fp32 = part;
+        tune_apply(0, t.X, t.Y, part, g);
         const int r = launch_fock(t.X, t.Y, g, st);
         if (r < 0) {
             snprintf(g_errbuf, sizeof(g_errbuf), "Fock kernel launch for class pair (%d,%d)%s failed: %s", t.X, t.Y,
@@ -1369,6 +1564,41 @@ extern "C" int gtf_fock_compute(gtf_fock_dev_t *f, int numdmat)
     f->ms_total = tot;
     f->ms_eri = eri_ms_total;
     f->ms_other = tot - eri_ms_total;
+    return GTF_OK;
+}
+
+// Tunes the launch shapes of every class pair and precision part of this
+// engine on its current density (one build first, so the Cartesian density
+// is in place); the next build clears what the trial launches accumulated.
+extern "C" int gtf_fock_autotune(gtf_fock_dev_t *f, int reps)
+{
+    if (reps < 1) reps = 1;
+    if (f->nosymm) return GTF_ERR_INVALID;
+    int r = gtf_fock_compute(f, 1);
+    if (r != GTF_OK) return r;
+    cudaStream_t st = f->stream;
+    const bool need_tr = f->pure && f->nbf_cart != f->nbf;
+    const double *Dc = need_tr ? f->d_Dc : f->d_D;
+    for (int c = 0; c < NCLSPAIR; c++) {
+        const ClassPairTask &t = f->tasks[c];
+        for (int part = 0; part < 2; part++) {
+            const long long nu = part ? t.nunits32 : t.nunits;
+            if (nu == 0) continue;
+            FockGrid g;
+            memset(&g, 0, sizeof(g));
+            fill_launch(f, c, part, Dc, f->d_Fj, f->d_Fk, g.one);
+            g.nmol = 1;
+            g.nunits = nu;
+            g.counter = f->d_counters + (size_t)(2 * c + part) * GTF_MAX_SLICES;
+            g.nsm = f->nsm;
+            g.fp32 = part;
+            if (tune_launch(0, t.X, t.Y, part, g, st, reps, f->ev0, f->ev1) < 0.0) {
+                snprintf(g_errbuf, sizeof(g_errbuf), "autotuning class pair (%d,%d) failed: %s", t.X, t.Y,
+                         cudaGetErrorString(cudaGetLastError()));
+                return GTF_ERR_CUDA;
+            }
+        }
+    }
     return GTF_OK;
 }
 
@@ -1790,6 +2020,7 @@ extern "C" int gtf_fock_batch_compute(gtf_fock_batch_t *b)
             g.counter = b->d_counters + (size_t)(2 * c + p) * GTF_MAX_SLICES;
             g.nsm = b->nsm;
             g.fp32 = p;
+            tune_apply(1, t0.X, t0.Y, p, g);
             const int r = launch_fock(t0.X, t0.Y, g, st);
             if (r < 0) {
                 snprintf(g_errbuf, sizeof(g_errbuf), "batched Fock launch for class pair %d part %d failed: %s", c, p,
@@ -1807,4 +2038,42 @@ extern "C" int gtf_fock_batch_compute(gtf_fock_batch_t *b)
     }
     gtf_note_launches(launches);
     return launches;
+}
+
+// Tunes the shapes of the batched launches (all molecules per launch).
+extern "C" int gtf_fock_batch_autotune(gtf_fock_batch_t *b, int reps)
+{
+    if (reps < 1) reps = 1;
+    if (gtf_fock_batch_compute(b) < 0) return GTF_ERR_CUDA;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        if (e0) cudaEventDestroy(e0);
+        return GTF_ERR_CUDA;
+    }
+    int rc = GTF_OK;
+    for (int c = 0; c < NCLSPAIR && rc == GTF_OK; c++) {
+        const ClassPairTask &t0 = b->eng[0]->tasks[c];
+        for (int p = 0; p < 2; p++) {
+            if (b->total[c][p] == 0) continue;
+            FockGrid g;
+            memset(&g, 0, sizeof(g));
+            g.one = b->one[c][p];
+            g.mols = b->d_desc[c][p];
+            g.mol_prefix = b->d_prefix[c][p];
+            g.nmol = b->nmol[c][p];
+            g.nunits = b->total[c][p];
+            g.counter = b->d_counters + (size_t)(2 * c + p) * GTF_MAX_SLICES;
+            g.nsm = b->nsm;
+            g.fp32 = p;
+            if (tune_launch(1, t0.X, t0.Y, p, g, b->st, reps, e0, e1) < 0.0) {
+                snprintf(g_errbuf, sizeof(g_errbuf), "autotuning batched class pair %d part %d failed: %s", c, p,
+                         cudaGetErrorString(cudaGetLastError()));
+                rc = GTF_ERR_CUDA;
+                break;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
 }

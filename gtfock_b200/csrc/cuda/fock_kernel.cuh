@@ -63,6 +63,12 @@ struct FockGrid {
     unsigned long long *counter;    // GTF_MAX_SLICES zeroed counters, one per slice launch
     int nsm;
     int fp32;                       // evaluate the integrals in FP32 (digestion stays FP64)
+    // launch shape (autotuned; 0 = default): persistent blocks per SM (capped
+    // by the occupancy limit) and, in batched launches, units of 32 quartets
+    // a warp claims at once
+    int ctas_per_sm;
+    int claim;
+    int query;                      // launch nothing: return the first slice's occupancy limit
 };
 
 // ---------------------------------------------------------------------------
@@ -111,11 +117,27 @@ __global__ void __launch_bounds__(FOCK_THREADS,
     __shared__ __align__(16) R tab[RysTab<R>::slen(NR)];
     rys_stage<R, NR>(tab);
     const int lane = threadIdx.x & 31;
+    unsigned long long u = 0, uend = 0;   // batched launches: the claimed range of units
     for (;;) {
-        unsigned long long u = 0;
-        if (lane == 0) u = atomicAdd(counter, 1ULL);
-        u = __shfl_sync(GTF_FULL_MASK, u, 0);
-        if (u >= (unsigned long long)g.nunits) break;
+        unsigned long long uu;
+        if constexpr (BATCH) {
+            // a warp claims g.claim units at once (fewer atomics on the
+            // counter when the molecules' units are small)
+            if (u >= uend) {
+                const unsigned claim = g.claim > 1 ? (unsigned)g.claim : 1u;
+                unsigned long long c0 = 0;
+                if (lane == 0) c0 = atomicAdd(counter, (unsigned long long)claim);
+                u = __shfl_sync(GTF_FULL_MASK, c0, 0);
+                uend = u + claim;
+            }
+            if (u >= (unsigned long long)g.nunits) break;
+            uu = u++;
+        } else {
+            unsigned long long c0 = 0;
+            if (lane == 0) c0 = atomicAdd(counter, 1ULL);
+            uu = __shfl_sync(GTF_FULL_MASK, c0, 0);
+            if (uu >= (unsigned long long)g.nunits) break;
+        }
         // molecule of the unit (batched launches); the fields are read from
         // the kernel parameter (one molecule, no registers held for them) or
         // from the descriptor array
@@ -125,11 +147,11 @@ __global__ void __launch_bounds__(FOCK_THREADS,
             int lo = 0, hi = g.nmol;
             while (hi - lo > 1) {
                 const int mid = (lo + hi) >> 1;
-                if (__ldg(g.mol_prefix + mid) <= (long long)u) lo = mid;
+                if (__ldg(g.mol_prefix + mid) <= (long long)uu) lo = mid;
                 else hi = mid;
             }
             mp += lo;
-            u -= (unsigned long long)__ldg(g.mol_prefix + lo);
+            uu -= (unsigned long long)__ldg(g.mol_prefix + lo);
         }
 #define GTF_FLD(x) (bt ? mp->x : g.one.x)
         const long long *unit_prefix = GTF_FLD(unit_prefix);
@@ -141,11 +163,11 @@ __global__ void __launch_bounds__(FOCK_THREADS,
         int lo = 0, hi = nbra;
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
-            if (__ldg(unit_prefix + mid) <= (long long)u) lo = mid;
+            if (__ldg(unit_prefix + mid) <= (long long)uu) lo = mid;
             else hi = mid;
         }
         const int i = lo;
-        const int v = (int)((long long)u - __ldg(unit_prefix + i)) * 32 + lane;
+        const int v = (int)((long long)uu - __ldg(unit_prefix + i)) * 32 + lane;
         const int4 *cq = reinterpret_cast<const int4 *>(GTF_FLD(cum) + (size_t)i * GTF_CUM);
         const int4 c0 = __ldg(cq), c1 = __ldg(cq + 1), c2 = __ldg(cq + 2), c3 = __ldg(cq + 3);
         const int cum[GTF_CUM] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w,
@@ -201,6 +223,8 @@ int launch_fock_slices(const FockGrid &g, cudaStream_t st, int slice)
         int per_sm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k, FOCK_THREADS, 0);
         if (per_sm < 1) per_sm = 1;
+        if (g.query) return per_sm;
+        if (g.ctas_per_sm > 0 && g.ctas_per_sm < per_sm) per_sm = g.ctas_per_sm;
         long long want = (g.nunits + (FOCK_THREADS / 32) - 1) / (FOCK_THREADS / 32);
         long long grid = (long long)g.nsm * per_sm;
         if (want < grid) grid = want;

@@ -18,7 +18,8 @@ typedef enum {
     GTF_ERR_ALLOC = -2,      /* device or host allocation failed */
     GTF_ERR_INVALID = -3,    /* bad argument */
     GTF_ERR_NODEVICE = -4,   /* no CUDA device visible */
-    GTF_ERR_DEVICE_FLAG = -5 /* a kernel reported an error through its status word */
+    GTF_ERR_DEVICE_FLAG = -5,/* a kernel reported an error through its status word */
+    GTF_ERR_IO = -6          /* a file could not be opened, read or written */
 } gtf_err_t;
 
 /* read-only view of a loaded basis (gtf_basis.h fields) */
@@ -88,6 +89,18 @@ typedef struct gtf_fock_batch gtf_fock_batch_t;
 int gtf_fock_batch_create(gtf_fock_dev_t *const *engines, int M, void *stream, gtf_fock_batch_t **out);
 int gtf_fock_batch_compute(gtf_fock_batch_t *b);
 void gtf_fock_batch_destroy(gtf_fock_batch_t *b);
+
+/* launch-shape autotuning (process-wide table, see fock.cu): time candidate
+ * shapes of every Fock launch of an engine / a batch on its current density
+ * and record the fastest; the table can be saved and reloaded */
+int gtf_fock_autotune(gtf_fock_dev_t *f, int reps);
+int gtf_fock_batch_autotune(gtf_fock_batch_t *b, int reps);
+int gtf_tune_get(int kind, int X, int Y, int part, double size, int *a, int *b);
+void gtf_tune_put(int kind, int X, int Y, int part, double size, int a, int b, double ms);
+void gtf_tune_clear(void);
+int gtf_tune_entries(int *rows, int max_rows);
+int gtf_tune_save(const char *path);
+int gtf_tune_load(const char *path);
 /* per class pair: Rys-model FLOPs and primitive quartets of one build */
 int gtf_fock_class_work(gtf_fock_dev_t *f, double *flops, double *nprimq);
 /* quartets evaluated in FP32 under the current precision mode, and all */

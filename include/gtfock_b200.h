@@ -48,6 +48,25 @@ int gtf_pfock_class_work(PFock_t pfock, double *flops, double *nprimq);
  * accumulation into F stay FP64).  Rebuilds the task lists. */
 PFockStatus_t gtf_pfock_set_precision(PFock_t pfock, int mode, double fp32_cutoff);
 
+/* Launch-shape autotuning.  gtf_pfock_autotune times, for every class pair
+ * and precision part of this engine's Fock build (on the density last put),
+ * candidate shapes of the persistent kernels -- blocks per SM (the occupancy
+ * limit, one less, half), and in batched launches also the quartets a warp
+ * claims at once (32, 64, 128) -- and records the fastest in a process-wide table keyed by (single / batch,
+ * class pair, part, floor(log2(units of work))); later builds of any engine
+ * or batch of that size use it.  gtf_batch_autotune does the same for a
+ * batch's Fock launches and picks the tile shape of its batched dense
+ * products (64x64, 32x32, 32x64, 128x64 output tiles).  The table is saved /
+ * merged from a text file whose first line names the device model; a file
+ * from another model is refused.  gtf_tune_entries writes rows of 8 ints
+ * (kind 0 single / 1 batch / 2 products, class X, class Y, part, size bucket,
+ * blocks per SM or tile shape, claim, ms x 1000) and returns the count. */
+PFockStatus_t gtf_pfock_autotune(PFock_t pfock, int reps);
+int gtf_tune_save(const char *path);
+int gtf_tune_load(const char *path);
+void gtf_tune_clear(void);
+int gtf_tune_entries(int *rows, int max_rows);
+
 /* Quartets evaluated in FP32 under the current mode, and all quartets. */
 PFockStatus_t gtf_pfock_precision_stats(PFock_t pfock, double *nquart_fp32, double *nquart);
 
@@ -144,6 +163,9 @@ size_t gtf_batch_job_bytes(int nbf);
  * energies, [2] of DIIS, [3] of purification, [4] purification steps of the
  * batched jobs, [5] batch steps.  Writes min(n, 6) values, returns that count. */
 int gtf_batch_stats(gtf_batch_t *b, double *out, int n);
+/* Tunes the batch's launch shapes for its current jobs (see
+ * gtf_pfock_autotune); call between steps. */
+int gtf_batch_autotune(gtf_batch_t *b, int reps);
 void gtf_batch_destroy(gtf_batch_t *b);
 
 /* Number of this library's own kernel launches so far (all threads). */

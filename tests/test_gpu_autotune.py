@@ -1,0 +1,69 @@
+"""Launch-shape autotuning: tuned builds give the same Fock matrices and
+energies as the default shapes, and the table survives a save / load."""
+import os
+
+import numpy as np
+import pytest
+
+import gtfock_b200 as gb
+from gtfock_b200 import molecules as mol
+
+pytestmark = pytest.mark.gpu
+
+
+def _fock(xyz, basis, D=None):
+    b = gb.BasisSet(mol.basis_file(basis), xyz)
+    pf = gb.PFock(b, tolscr=1e-10)
+    if D is None:
+        D = np.eye(b.nbf) * 0.3
+    return b, pf, D
+
+
+def test_pfock_autotune_same_fock(tmp_path):
+    gb.tune_clear()
+    xyz = mol.write_xyz(mol.alkane(6), str(tmp_path / "c6.xyz"))
+    b, pf, D = _fock(xyz, "cc-pvdz")
+    F0 = pf.compute_fock(D).copy()
+    pf.autotune(1)
+    ent = [e for e in gb.tune_entries() if e["kind"] == "fock"]
+    assert ent, "no tuned launches recorded"
+    for e in ent:
+        assert e["ctas_per_sm"] >= 1 and e["claim"] in (1, 2, 4) and e["ms"] >= 0.0
+    F1 = pf.compute_fock(D)
+    assert np.max(np.abs(F1 - F0)) < 1e-11
+    # mixed precision parts are tuned separately
+    pf.set_precision(1, 1e-6)
+    pf.compute_fock(D)
+    pf.autotune(1)
+    assert any(e["part"] == 1 for e in gb.tune_entries() if e["kind"] == "fock")
+    pf.close()
+    del b
+    path = str(tmp_path / "tune.txt")
+    gb.tune_save(path)
+    n = len(gb.tune_entries())
+    gb.tune_clear()
+    assert gb.tune_entries() == []
+    gb.tune_load(path)
+    assert len(gb.tune_entries()) == n
+    gb.tune_clear()
+
+
+def test_batch_autotune_same_energies(tmp_path):
+    gb.tune_clear()
+    items = [(mol.water_cluster(4, 11), "6-31g"), (mol.alkane(5), "sto-3g"), (mol.water_cluster(9, 12), "sto-3g")]
+    files = [(mol.basis_file(bs), mol.write_xyz(a, str(tmp_path / ("m%d.xyz" % k)))) for k, (a, bs) in enumerate(items)]
+    res = []
+    for tune in (False, True):
+        bt = gb.Batch(len(files))
+        slots = [bt.add(g, x, tolscr=1e-10, max_iters=8, etol=0.0) for g, x in files]
+        if tune:
+            bt.autotune(1)
+        bt.run()
+        res.append([bt.result(s)[0] for s in slots])
+        bt.close()
+    kinds = {e["kind"] for e in gb.tune_entries()}
+    assert "fock-batch" in kinds and "products" in kinds
+    for e0, e1 in zip(*res):
+        assert len(e0) == len(e1) == 8
+        assert np.max(np.abs(e0 - e1)) < 1e-8
+    gb.tune_clear()

@@ -144,3 +144,47 @@ def test_pfock_create_without_device_fails_cleanly(tmp_path):
     h = ctypes.c_void_p()
     assert L.PFock_create(b.h, 1, 1, 4, 1e-10, 1, 1, ctypes.byref(h)) == 1  # INIT_FAILED
     assert gb.device_info()[0] == 0
+
+
+def test_tune_table_save_load(tmp_path):
+    """The launch-shape table: entries round-trip through the text file, a
+    file from another device model or a damaged one is refused and leaves
+    the table as it was."""
+    L = gb.load()
+    gb.tune_clear()
+    L.gtf_tune_put(0, 1, 0, 0, 3.0e5, 5, 2, 1.25)
+    L.gtf_tune_put(1, 4, 4, 1, 9.0e3, 2, 4, 0.5)
+    L.gtf_tune_put(2, -1, -1, 0, 2.0e9, 3, 0, 7.0)
+    before = gb.tune_entries()
+    assert len(before) == 3
+    fock = [e for e in before if e["kind"] == "fock"][0]
+    assert (fock["X"], fock["Y"], fock["ctas_per_sm"], fock["claim"], fock["bucket"]) == (1, 0, 5, 2, 18)
+    prod = [e for e in before if e["kind"] == "products"][0]
+    assert prod["shape"] == gb.GEMM_SHAPES[3] and prod["bucket"] == 30
+    path = str(tmp_path / "tune.txt")
+    gb.tune_save(path)
+    gb.tune_clear()
+    assert gb.tune_entries() == []
+    gb.tune_load(path)
+    assert gb.tune_entries() == before
+    # same bucket: a lookup for another size in [2^18, 2^19) finds the entry
+    a, b = ctypes.c_int(), ctypes.c_int()
+    assert L.gtf_tune_get(0, 1, 0, 0, 4.0e5, ctypes.byref(a), ctypes.byref(b)) == 1
+    assert (a.value, b.value) == (5, 2)
+    assert L.gtf_tune_get(0, 1, 0, 0, 6.0e5, ctypes.byref(a), ctypes.byref(b)) == 0
+    lines = open(path).read().splitlines()
+    other = str(tmp_path / "other.txt")
+    with open(other, "w") as f:
+        f.write("gtfock_b200-tune 1 Some_Other_GPU_sm_90\n" + "\n".join(lines[1:]) + "\n")
+    gb.tune_clear()
+    with pytest.raises(gb.GtfError):
+        gb.tune_load(other)
+    bad = str(tmp_path / "bad.txt")
+    with open(bad, "w") as f:
+        f.write(lines[0] + "\n0 1 0 0 18 5\n")
+    with pytest.raises(gb.GtfError):
+        gb.tune_load(bad)
+    assert gb.tune_entries() == []
+    with pytest.raises(gb.GtfError):
+        gb.tune_load(str(tmp_path / "missing.txt"))
+    gb.tune_clear()
