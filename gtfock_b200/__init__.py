@@ -116,6 +116,10 @@ def load():
     _sig(L, "gtf_batch_stats", [_vp, _dp, _i])
     _sig(L, "gtf_batch_destroy", [_vp], None)
     _sig(L, "gtf_pfock_autotune", [_vp, _i])
+    _sig(L, "gtf_pfock_set_shard", [_vp, _i, _i])
+    _sig(L, "gtf_shard_range", [ctypes.c_longlong, _i, _i, ctypes.POINTER(ctypes.c_longlong),
+                                ctypes.POINTER(ctypes.c_longlong)], None)
+    _sig(L, "gtf_pfock_compute_dev", [_vp, _vp, ctypes.POINTER(_vp)])
     _sig(L, "gtf_batch_autotune", [_vp, _i])
     _sig(L, "gtf_tune_save", [_cp])
     _sig(L, "gtf_tune_load", [_cp])
@@ -267,6 +271,19 @@ class PFock:
         """mode 0: FP64; mode 1: FP32 for quartets with Schwarz bound < fp32_cutoff."""
         self._check(load().gtf_pfock_set_precision(self.h, mode, fp32_cutoff),
                     "gtf_pfock_set_precision")
+
+    def set_shard(self, shard, nshards):
+        """Builds of this engine compute shard `shard` of `nshards` of every
+        class launch's quartet units (their F is that shard's part)."""
+        self._check(load().gtf_pfock_set_shard(self.h, shard, nshards), "gtf_pfock_set_shard")
+
+    def compute_dev(self, d_ptr):
+        """Fock build from a device density (pointer to nbf x nbf FP64);
+        returns the device pointer of F (library memory, valid until the
+        next build)."""
+        out = _vp()
+        self._check(load().gtf_pfock_compute_dev(self.h, _vp(d_ptr), ctypes.byref(out)), "gtf_pfock_compute_dev")
+        return out.value
 
     def autotune(self, reps=2):
         """Time candidate launch shapes of every Fock launch on the density last

@@ -128,6 +128,8 @@ struct gtf_fock_dev {
     // non-symmetric densities (PFock_create with symm = 0)
     int nosymm;
     double *d_Ds, *d_Da, *d_Dca, *d_Fka;
+    // sharded build: this engine computes shard `shard` of `nshards` (0: all)
+    int shard, nshards;
 };
 
 template <typename T>
@@ -1413,6 +1415,33 @@ extern "C" int gtf_fock_set_nosymm(gtf_fock_dev_t *f, int on)
     return GTF_OK;
 }
 
+// Units [lo, hi) of a class launch that shard r of n computes: contiguous,
+// sizes differing by at most one unit (units of one class launch are 32
+// quartets of equal class; the pre-sorted ket segments spread the heavy and
+// light bras over the range).
+extern "C" void gtf_shard_range(long long nunits, int r, int n, long long *lo, long long *hi)
+{
+    if (n <= 1) {
+        *lo = 0;
+        *hi = nunits;
+        return;
+    }
+    *lo = nunits * r / n;
+    *hi = nunits * (r + 1) / n;
+}
+
+// A sharded build: every class launch of this engine covers shard `shard` of
+// `nshards` of its units, so the F, J, K of the build are this shard's part;
+// the parts of all shards sum to the whole build.  nshards <= 1 restores
+// the whole build.
+extern "C" int gtf_fock_set_shard(gtf_fock_dev_t *f, int shard, int nshards)
+{
+    if (nshards < 0 || (nshards > 1 && (shard < 0 || shard >= nshards))) return GTF_ERR_INVALID;
+    f->shard = nshards > 1 ? shard : 0;
+    f->nshards = nshards > 1 ? nshards : 0;
+    return GTF_OK;
+}
+
 extern "C" int gtf_fock_set_precision(gtf_fock_dev_t *f, int prec, double fp32_cutoff)
 {
     if (prec != GTF_PREC_FP64 && prec != GTF_PREC_MIXED) return GTF_ERR_INVALID;
@@ -1463,7 +1492,11 @@ static int launch_class(const gtf_fock_dev *f, int c, const double *D, double *F
         memset(&g, 0, sizeof(g));
         fill_launch(f, c, part, D, Fj, Fk, g.one, konly);
         g.nmol = 1;
-        g.nunits = nu;
+        long long lo = 0, hi = nu;
+        gtf_shard_range(nu, f->shard, f->nshards, &lo, &hi);
+        if (hi <= lo) continue;
+        g.nunits = hi - lo;
+        g.unit_lo = lo;
         g.counter = counters + (size_t)(2 * c + part) * GTF_MAX_SLICES;
         g.nsm = f->nsm;
         g.fp32 = part;

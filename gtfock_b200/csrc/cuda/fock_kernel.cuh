@@ -69,6 +69,9 @@ struct FockGrid {
     int ctas_per_sm;
     int claim;
     int query;                      // launch nothing: return the first slice's occupancy limit
+    // single-molecule launches of a sharded build: this launch covers units
+    // [unit_lo, unit_lo + nunits) of the class's unit range
+    long long unit_lo;
 };
 
 // ---------------------------------------------------------------------------
@@ -137,6 +140,7 @@ __global__ void __launch_bounds__(FOCK_THREADS,
             if (lane == 0) c0 = atomicAdd(counter, 1ULL);
             uu = __shfl_sync(GTF_FULL_MASK, c0, 0);
             if (uu >= (unsigned long long)g.nunits) break;
+            uu += (unsigned long long)g.unit_lo;
         }
         // molecule of the unit (batched launches); the fields are read from
         // the kernel parameter (one molecule, no registers held for them) or

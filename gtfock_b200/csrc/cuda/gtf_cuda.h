@@ -90,6 +90,11 @@ int gtf_fock_batch_create(gtf_fock_dev_t *const *engines, int M, void *stream, g
 int gtf_fock_batch_compute(gtf_fock_batch_t *b);
 void gtf_fock_batch_destroy(gtf_fock_batch_t *b);
 
+/* sharded builds (one molecule over several GPUs): every class launch covers
+ * shard r of n of its units; the F of the shards sum to the whole build */
+int gtf_fock_set_shard(gtf_fock_dev_t *f, int shard, int nshards);
+void gtf_shard_range(long long nunits, int r, int n, long long *lo, long long *hi);
+
 /* launch-shape autotuning (process-wide table, see fock.cu): time candidate
  * shapes of every Fock launch of an engine / a batch on its current density
  * and record the fastest; the table can be saved and reloaded */

@@ -410,6 +410,12 @@ PFockStatus_t gtf_pfock_set_precision(PFock_t pf, int mode, double fp32_cutoff)
     return map_err(gtf_fock_set_precision(pf->dev, mode, fp32_cutoff));
 }
 
+PFockStatus_t gtf_pfock_set_shard(PFock_t pf, int shard, int nshards)
+{
+    if (pf == NULL) return PFOCK_STATUS_INVALID_VALUE;
+    return map_err(gtf_fock_set_shard(pf->dev, shard, nshards));
+}
+
 PFockStatus_t gtf_pfock_autotune(PFock_t pf, int reps)
 {
     if (pf == NULL) return PFOCK_STATUS_INVALID_VALUE;

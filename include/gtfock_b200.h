@@ -48,6 +48,17 @@ int gtf_pfock_class_work(PFock_t pfock, double *flops, double *nprimq);
  * accumulation into F stay FP64).  Rebuilds the task lists. */
 PFockStatus_t gtf_pfock_set_precision(PFock_t pfock, int mode, double fp32_cutoff);
 
+/* One molecule over several GPUs (one process per GPU): with
+ * gtf_pfock_set_shard(pf, r, n) every class launch of this engine's builds
+ * covers shard r of n of its quartet units (the 2-D task decomposition of
+ * pfock/pfock.c:22-154 becomes a split of each class's unit range), so
+ * PFock_getMat / gtf_pfock_compute_dev return this rank's part of F; the
+ * parts of the n ranks sum to the whole F (one all-reduce per build).
+ * n <= 1 restores the whole build.  gtf_shard_range gives the units
+ * [lo, hi) of shard r of n for a launch of `nunits`. */
+PFockStatus_t gtf_pfock_set_shard(PFock_t pfock, int shard, int nshards);
+void gtf_shard_range(long long nunits, int r, int n, long long *lo, long long *hi);
+
 /* Launch-shape autotuning.  gtf_pfock_autotune times, for every class pair
  * and precision part of this engine's Fock build (on the density last put),
  * candidate shapes of the persistent kernels -- blocks per SM (the occupancy

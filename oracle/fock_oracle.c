@@ -193,12 +193,30 @@ int or_fock_build(BasisSet_t basis, double tolscr, int nthreads,
                                 D, F, 1, 0, usq_o, uitl_o);
 }
 
+int or_fock_build_shard(BasisSet_t basis, double tolscr, int nthreads,
+                        const int *shellptr, const int *shellid, const int *shellrid,
+                        const double *shellvalue, const double *D, double *F,
+                        int stride, int offset, int count_only, double *usq_o, double *uitl_o);
+
 int or_fock_build_sample(BasisSet_t basis, double tolscr, int nthreads,
                          const int *shellptr, const int *shellid, const int *shellrid,
                          const double *shellvalue, const double *D, double *F,
                          int stride, int count_only, double *usq_o, double *uitl_o)
 {
+    return or_fock_build_shard(basis, tolscr, nthreads, shellptr, shellid, shellrid, shellvalue, D, F,
+                               stride, 0, count_only, usq_o, uitl_o);
+}
+
+/* The MN pairs i with (i - first) % stride == offset: with stride = n and
+ * offset = r, shard r of an n-way split of the build (the shards' F sum to
+ * the whole F, since the symmetrisation at the end is linear). */
+int or_fock_build_shard(BasisSet_t basis, double tolscr, int nthreads,
+                        const int *shellptr, const int *shellid, const int *shellrid,
+                        const double *shellvalue, const double *D, double *F,
+                        int stride, int offset, int count_only, double *usq_o, double *uitl_o)
+{
     if (stride < 1) stride = 1;
+    if (offset < 0 || offset >= stride) return -1;
     const int nbf = basis->nbf;
     const int nshells = basis->nshells;
     const double tolscr2 = tolscr * tolscr;
@@ -219,7 +237,7 @@ int or_fock_build_sample(BasisSet_t basis, double tolscr, int nthreads,
         double *K = Kt + nn * nt;
         #pragma omp for schedule(dynamic)
         for (int i = startMN; i < endMN; i++) {
-            if ((i - startMN) % stride != 0) continue;
+            if ((i - startMN) % stride != offset) continue;
             const int M = shellrid[i];
             const int N = shellid[i];
             const double value1 = shellvalue[i];

@@ -52,6 +52,7 @@ def lib():
                                    ctypes.POINTER(ip), ctypes.POINTER(dp), ip, dp]
         L.or_fock_build.argtypes = [vp, d, i, ip, ip, ip, dp, dp, dp, dp, dp]
         L.or_fock_build_sample.argtypes = [vp, d, i, ip, ip, ip, dp, dp, dp, i, i, dp, dp]
+        L.or_fock_build_shard.argtypes = [vp, d, i, ip, ip, ip, dp, dp, dp, i, i, i, dp, dp]
         L.or_diis_create.argtypes = [i]
         L.or_diis_create.restype = vp
         L.or_diis_destroy.argtypes = [vp]
@@ -186,6 +187,27 @@ def fock_build_sample(basis, tol, D, stride, count_only=False, scr=None, nthread
     if st != 0:
         raise RuntimeError("or_fock_build_sample failed")
     return usq.value, uitl.value, dt
+
+
+def fock_build_shard(basis, tol, D, nshards, shard, scr=None, nthreads=os.cpu_count()):
+    """Shard `shard` of an `nshards`-way split of one Fock build (every
+    nshards-th MN pair from `shard`): its part of F.  The parts sum to F."""
+    L = lib()
+    if scr is None:
+        scr = screening(basis, tol, nthreads)
+    shellptr, shellid, shellrid, shellvalue, _ = scr
+    D = np.ascontiguousarray(D, dtype=np.float64)
+    F = np.zeros_like(D)
+    usq = ctypes.c_double()
+    uitl = ctypes.c_double()
+    st = L.or_fock_build_shard(basis.h, tol, nthreads, _ip(np.ascontiguousarray(shellptr, dtype=np.int32)),
+                               _ip(np.ascontiguousarray(shellid, dtype=np.int32)),
+                               _ip(np.ascontiguousarray(shellrid, dtype=np.int32)),
+                               _dp(np.ascontiguousarray(shellvalue, dtype=np.float64)), _dp(D), _dp(F),
+                               nshards, shard, 0, ctypes.byref(usq), ctypes.byref(uitl))
+    if st != 0:
+        raise RuntimeError("or_fock_build_shard failed")
+    return F
 
 
 def diis_step_timed(X, S, D, F, it, state=None):

@@ -1,0 +1,85 @@
+"""Sharded Fock builds on the GPU: the parts of n shards built by the CUDA
+kernels sum to the whole F (FP64 and mixed precision), and the NCCL path of
+ShardedFock (device F all-reduced in place) gives the whole F on a one-rank
+group (the only group a one-GPU run can form)."""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+import gtfock_b200 as gb
+from gtfock_b200 import molecules as mol
+from conftest import golden_xyz, load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("nshards", [2, 3, 5])
+def test_shard_parts_sum_to_whole(tmp_path, nshards):
+    xyz = mol.write_xyz(mol.alkane(4), str(tmp_path / "c4.xyz"))
+    b = gb.BasisSet(mol.basis_file("cc-pvdz"), xyz)
+    pf = gb.PFock(b, tolscr=1e-10)
+    rng = np.random.default_rng(nshards)
+    A = rng.standard_normal((b.nbf, b.nbf)) * 0.05
+    D = A + A.T
+    for prec in (0, 1):
+        pf.set_shard(0, 1)
+        pf.set_precision(prec, 1e-6)
+        F = pf.compute_fock(D)
+        parts = []
+        for r in range(nshards):
+            pf.set_shard(r, nshards)
+            parts.append(pf.compute_fock(D))
+        assert all(np.max(np.abs(p)) > 0 for p in parts)
+        assert np.max(np.abs(sum(parts) - F)) < 1e-11
+    pf.close()
+
+
+def test_shard_against_oracle_fixture(tmp_path):
+    g = load_golden("c4h10_ccpvdz")
+    gbs, xyz = golden_xyz("c4h10_ccpvdz", tmp_path)
+    b = gb.BasisSet(gbs, xyz)
+    pf = gb.PFock(b, tolscr=float(g["tol"]))
+    parts = []
+    for r in range(4):
+        pf.set_shard(r, 4)
+        parts.append(pf.compute_fock(g["D"]))
+    assert np.max(np.abs(sum(parts) - g["F"])) < 1e-10
+    pf.close()
+
+
+def test_set_shard_rejects_bad_arguments(tmp_path):
+    xyz = mol.write_xyz(mol.alkane(2), str(tmp_path / "c2.xyz"))
+    b = gb.BasisSet(mol.basis_file("sto-3g"), xyz)
+    pf = gb.PFock(b, tolscr=1e-10)
+    for r, n in ((2, 2), (-1, 3), (0, -1)):
+        with pytest.raises(gb.GtfError):
+            pf.set_shard(r, n)
+    pf.close()
+
+
+def test_sharded_fock_nccl_one_rank(tmp_path):
+    import torch
+    import torch.distributed as dist
+    from gtfock_b200.shard import ShardedFock
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % port, rank=0, world_size=1)
+    try:
+        xyz = mol.write_xyz(mol.water_cluster(5, 9), str(tmp_path / "w5.xyz"))
+        b = gb.BasisSet(mol.basis_file("6-31g"), xyz)
+        ref = gb.PFock(b, tolscr=1e-10)
+        D = np.eye(b.nbf) * 0.2
+        F = ref.compute_fock(D)
+        ref.close()
+        sf = ShardedFock(b, tolscr=1e-10)
+        Fd = sf.compute_fock_dev(torch.from_numpy(D).cuda())
+        torch.cuda.synchronize()
+        assert np.max(np.abs(Fd.cpu().numpy() - F)) < 1e-11
+        Fh = sf.compute_fock(D)
+        assert np.max(np.abs(Fh - F)) < 1e-11
+        sf.close()
+    finally:
+        dist.destroy_process_group()
