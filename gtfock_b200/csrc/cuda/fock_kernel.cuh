@@ -148,29 +148,18 @@ __global__ void __launch_bounds__(FOCK_THREADS,
         constexpr bool bt = BATCH;
         const FockLaunch *mp = g.mols;
         if constexpr (BATCH) {
-            int lo = 0, hi = g.nmol;
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (__ldg(g.mol_prefix + mid) <= (long long)uu) lo = mid;
-                else hi = mid;
-            }
-            mp += lo;
-            uu -= (unsigned long long)__ldg(g.mol_prefix + lo);
+            const int m = warp_find_le(g.mol_prefix, g.nmol, (long long)uu, lane);
+            mp += m;
+            uu -= (unsigned long long)__ldg(g.mol_prefix + m);
         }
 #define GTF_FLD(x) (bt ? mp->x : g.one.x)
         const long long *unit_prefix = GTF_FLD(unit_prefix);
-        // unit u -> (bra i, chunk of 32 kets) by binary search of the unit
+        // unit u -> (bra i, chunk of 32 kets) by a warp search of the unit
         // prefix over bras; lane v of the chunk -> segment b and position in
         // it from the bra's segment prefix (the kets of consecutive segments
         // share a warp)
         const int nbra = GTF_FLD(nbra);
-        int lo = 0, hi = nbra;
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (__ldg(unit_prefix + mid) <= (long long)uu) lo = mid;
-            else hi = mid;
-        }
-        const int i = lo;
+        const int i = warp_find_le(unit_prefix, nbra, (long long)uu, lane);
         const int v = (int)((long long)uu - __ldg(unit_prefix + i)) * 32 + lane;
         const int4 *cq = reinterpret_cast<const int4 *>(GTF_FLD(cum) + (size_t)i * GTF_CUM);
         const int4 c0 = __ldg(cq), c1 = __ldg(cq + 1), c2 = __ldg(cq + 2), c3 = __ldg(cq + 3);

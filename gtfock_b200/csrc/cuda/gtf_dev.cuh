@@ -574,6 +574,28 @@ struct PPRec {
 __host__ __device__ constexpr int pow2_ceil(int m) { return m <= 1 ? 1 : 2 * pow2_ceil((m + 1) / 2); }
 __host__ __device__ constexpr int ilog2c(int m) { return m <= 1 ? 0 : 1 + ilog2c(m / 2); }
 
+// Last i in [0, n) with prefix[i] <= u, for a non-decreasing prefix with
+// prefix[0] = 0 <= u, searched by the whole warp (u and n warp-uniform, all
+// lanes active): each step probes 32 positions and keeps the sub-range after
+// the last probe that is <= u, so the search takes ceil(log32 n) dependent
+// loads instead of log2 n.
+__device__ __forceinline__ int warp_find_le(const long long *__restrict__ prefix, int n, long long u, int lane)
+{
+    int lo = 0, hi = n;
+    while (hi - lo > 32) {
+        const long long span = hi - lo;
+        const int p = lo + (int)(span * lane / 32);
+        const unsigned m = __ballot_sync(GTF_FULL_MASK, __ldg(prefix + p) <= u);
+        const int j = 31 - __clz(m);
+        const int nlo = lo + (int)(span * j / 32);
+        hi = (j == 31) ? hi : lo + (int)(span * (j + 1) / 32);
+        lo = nlo;
+    }
+    const bool le = (lane < hi - lo) && __ldg(prefix + lo + lane) <= u;
+    const unsigned m = __ballot_sync(GTF_FULL_MASK, le);
+    return lo + 31 - __clz(m);
+}
+
 template <int M, class Sink>
 __device__ __forceinline__ void warp_sum_values(const double *v, int lane, Sink &&sink)
 {
