@@ -43,7 +43,7 @@ NITER = 10
 MIXED_CUTOFF = 1e-6
 # DRAM bytes (read + write) of all k_fock launches of one C54H18 build, from one
 # ncu capture (profiles/fock_c54h18_dram_traffic.md); the kernels are FP64 bound
-FOCK_BUILD_DRAM_BYTES = 646.4e6 + 84.2e6
+FOCK_BUILD_DRAM_BYTES = 648.9e6 + 85.0e6
 METRIC = "SCF solves/s (C54H18 cc-pVDZ, 10 iterations, FP64)"
 WORKLOAD = "C54H18 graphene flake / cc-pVDZ (846 bf), Schwarz 1e-10, 10 SCF iterations, FP64"
 
