@@ -1213,7 +1213,7 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
             f->uitl += q * dims;
         }
     }
-    // Rys-model FLOPs per build (SURVEY-normalised work: every primitive
+    // Rys-model FLOPs per build (a fixed work normalisation: every primitive
     // quartet of every screened shell quartet, before primitive screening)
     {
         std::vector<int> hn(nnz > 0 ? nnz : 1);
@@ -1820,11 +1820,11 @@ static int fixed_scratch(int dev, double **out)
 
 extern "C" int gtf_fock_compute_fixed(gtf_fock_dev_t *f, const double *dev_D, double *dev_F)
 {
+    if (f == nullptr || dev_D == nullptr || dev_F == nullptr || f->max_numdmat <= 0) return GTF_ERR_INVALID;
     if (f->nosymm) {
         snprintf(g_errbuf, sizeof(g_errbuf), "allocation-free Fock build: non-symmetric densities are not supported");
         return GTF_ERR_INVALID;
     }
-    if (f == nullptr || dev_D == nullptr || dev_F == nullptr || f->max_numdmat <= 0) return GTF_ERR_INVALID;
     const int nbf = f->nbf, nbfc = f->nbf_cart;
     if (nbfc > GTF_FIXED_MAX_FUNCS || nbf > GTF_FIXED_MAX_FUNCS) {
         snprintf(g_errbuf, sizeof(g_errbuf),
