@@ -1924,8 +1924,34 @@ struct gtf_fock_batch {
     FockLaunch one[NCLSPAIR][2];
     int nmol[NCLSPAIR][2];
     long long total[NCLSPAIR][2];
+    // molecules with at least GTF_SOLO_UNITS units in a (class pair, part)
+    // run there as launches of their own with the single-molecule kernel
+    std::vector<FockLaunch> solo[NCLSPAIR][2];
+    std::vector<long long> solo_units[NCLSPAIR][2];
+    int solo_base[NCLSPAIR][2];     // first counter block of the part's solo launches
+    int ncounter_blocks;            // GTF_MAX_SLICES counters each
     unsigned long long *d_counters;
 };
+
+// A molecule whose units in one launch reach this many (32 quartets each)
+// fills the GPU by itself for ~70 rounds of its resident warps; it then runs
+// with the single-molecule kernel, which keeps its descriptor in the kernel
+// parameters (the batched kernel reads it from memory and holds the molecule
+// offset, at 50-60 more bytes of spills; measured 17% slower on 2-3 copies of
+// C54H18 or (H2O)64).  At 32768 units the tails and the serial order of many
+// medium solo launches cost more than that (256-molecule batch: -16%).  The
+// environment variable GTFOCK_SOLO_UNITS overrides the threshold (tests).
+#define GTF_SOLO_UNITS 262144
+
+static long long solo_units_threshold()
+{
+    const char *e = getenv("GTFOCK_SOLO_UNITS");
+    if (e && *e) {
+        const long long v = atoll(e);
+        if (v >= 1) return v;
+    }
+    return GTF_SOLO_UNITS;
+}
 
 extern "C" void gtf_fock_batch_destroy(gtf_fock_batch_t *b)
 {
@@ -1997,11 +2023,13 @@ extern "C" int gtf_fock_batch_create(gtf_fock_dev_t *const *engines, int M, void
     }
     CKB_(cudaMalloc(&b->d_xf, sizeof(XformDesc) * M));
     CKB_(cudaMemcpy(b->d_xf, xf.data(), sizeof(XformDesc) * M, cudaMemcpyHostToDevice));
-    CKB_(cudaMalloc(&b->d_counters, sizeof(unsigned long long) * 2 * NCLSPAIR * GTF_MAX_SLICES));
+    int nblocks = 2 * NCLSPAIR;
+    const long long solo_min = solo_units_threshold();
     for (int c = 0; c < NCLSPAIR; c++)
         for (int p = 0; p < 2; p++) {
             std::vector<FockLaunch> d;
             std::vector<long long> pre(1, 0);
+            b->solo_base[c][p] = nblocks;
             for (int m = 0; m < M; m++) {
                 gtf_fock_dev *f = engines[m];
                 const ClassPairTask &t = f->tasks[c];
@@ -2010,6 +2038,12 @@ extern "C" int gtf_fock_batch_create(gtf_fock_dev_t *const *engines, int M, void
                 const bool need_tr = f->pure && f->nbf_cart != f->nbf;
                 FockLaunch a;
                 fill_launch(f, c, p, need_tr ? f->d_Dc : f->d_D, f->d_Fj, f->d_Fk, a);
+                if (M > 1 && nu >= solo_min) {
+                    b->solo[c][p].push_back(a);
+                    b->solo_units[c][p].push_back(nu);
+                    nblocks++;
+                    continue;
+                }
                 d.push_back(a);
                 pre.push_back(pre.back() + nu);
             }
@@ -2022,6 +2056,8 @@ extern "C" int gtf_fock_batch_create(gtf_fock_dev_t *const *engines, int M, void
             CKB_(cudaMemcpy(b->d_desc[c][p], d.data(), sizeof(FockLaunch) * d.size(), cudaMemcpyHostToDevice));
             CKB_(cudaMemcpy(b->d_prefix[c][p], pre.data(), sizeof(long long) * pre.size(), cudaMemcpyHostToDevice));
         }
+    b->ncounter_blocks = nblocks;
+    CKB_(cudaMalloc(&b->d_counters, sizeof(unsigned long long) * (size_t)nblocks * GTF_MAX_SLICES));
     *out = b;
     return GTF_OK;
 }
@@ -2038,10 +2074,29 @@ extern "C" int gtf_fock_batch_compute(gtf_fock_batch_t *b)
         CK(cudaGetLastError());
         launches++;
     }
-    CK(cudaMemsetAsync(b->d_counters, 0, sizeof(unsigned long long) * 2 * NCLSPAIR * GTF_MAX_SLICES, st));
+    CK(cudaMemsetAsync(b->d_counters, 0, sizeof(unsigned long long) * (size_t)b->ncounter_blocks * GTF_MAX_SLICES,
+                       st));
     for (int c = 0; c < NCLSPAIR; c++) {
         const ClassPairTask &t0 = b->eng[0]->tasks[c];
         for (int p = 0; p < 2; p++) {
+            for (size_t k = 0; k < b->solo[c][p].size(); k++) {
+                FockGrid g;
+                memset(&g, 0, sizeof(g));
+                g.one = b->solo[c][p][k];
+                g.nmol = 1;
+                g.nunits = b->solo_units[c][p][k];
+                g.counter = b->d_counters + (size_t)(b->solo_base[c][p] + (int)k) * GTF_MAX_SLICES;
+                g.nsm = b->nsm;
+                g.fp32 = p;
+                tune_apply(0, t0.X, t0.Y, p, g);
+                const int r = launch_fock(t0.X, t0.Y, g, st);
+                if (r < 0) {
+                    snprintf(g_errbuf, sizeof(g_errbuf), "Fock launch for class pair %d part %d failed: %s", c, p,
+                             cudaGetErrorString(cudaGetLastError()));
+                    return GTF_ERR_CUDA;
+                }
+                launches += r;
+            }
             if (b->total[c][p] == 0) continue;
             FockGrid g;
             memset(&g, 0, sizeof(g));
@@ -2087,6 +2142,18 @@ extern "C" int gtf_fock_batch_autotune(gtf_fock_batch_t *b, int reps)
     for (int c = 0; c < NCLSPAIR && rc == GTF_OK; c++) {
         const ClassPairTask &t0 = b->eng[0]->tasks[c];
         for (int p = 0; p < 2; p++) {
+            for (size_t k = 0; k < b->solo[c][p].size() && rc == GTF_OK; k++) {
+                FockGrid g;
+                memset(&g, 0, sizeof(g));
+                g.one = b->solo[c][p][k];
+                g.nmol = 1;
+                g.nunits = b->solo_units[c][p][k];
+                g.counter = b->d_counters + (size_t)(b->solo_base[c][p] + (int)k) * GTF_MAX_SLICES;
+                g.nsm = b->nsm;
+                g.fp32 = p;
+                if (tune_launch(0, t0.X, t0.Y, p, g, b->st, reps, e0, e1) < 0.0) rc = GTF_ERR_CUDA;
+            }
+            if (rc != GTF_OK) break;
             if (b->total[c][p] == 0) continue;
             FockGrid g;
             memset(&g, 0, sizeof(g));

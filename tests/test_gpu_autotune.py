@@ -63,7 +63,11 @@ def test_batch_autotune_same_energies(tmp_path):
         bt.close()
     kinds = {e["kind"] for e in gb.tune_entries()}
     assert "fock-batch" in kinds and "products" in kinds
+    # other launch shapes sum F's atomics in another order (1e-14 relative);
+    # the unconverged early iterations amplify that, as between any two runs,
+    # so they are held to the 1e-6 Ha of the parity tests, the last to 1e-8
     for e0, e1 in zip(*res):
         assert len(e0) == len(e1) == 8
-        assert np.max(np.abs(e0 - e1)) < 1e-8
+        assert np.max(np.abs(e0 - e1)) < 1e-6
+        assert abs(e0[-1] - e1[-1]) < 1e-8
     gb.tune_clear()

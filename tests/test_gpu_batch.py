@@ -118,3 +118,26 @@ def test_batch_mixed_precision(tmp_path):
         assert d64 and d32 and len(e64) < 40
         assert abs(e32[-1] - e64[-1]) < 1e-6, (c, e32[-1], e64[-1])
     b.close()
+
+
+def test_solo_launches_in_a_batch(tmp_path, monkeypatch):
+    """Molecules with many units in a class pair run there with launches of
+    their own (the single-molecule kernel) beside the batched launch of the
+    rest.  With the threshold lowered to 2000 units, C12H26 / cc-pVDZ and
+    C4H10 / cc-pVDZ take that path in most class pairs; their energies still
+    match the pinned fixtures, and the small molecules' too."""
+    monkeypatch.setenv("GTFOCK_SOLO_UNITS", "2000")
+    cases = ["c12h26_ccpvdz", "c4h10_ccpvdz", "h2o_631g", "ch4_ccpvdz"]
+    b = gb.Batch(len(cases))
+    slots = {}
+    for c in cases:
+        g, gbs, xyz = _inputs(c, tmp_path)
+        slots[c] = (b.add(gbs, xyz, tolscr=float(g["tol"]), max_iters=len(g["energies"])), g)
+    b.run()
+    for c, (s, g) in slots.items():
+        e, done = b.result(s)
+        ref = g["energies"]
+        n = min(len(e), len(ref))
+        assert done and n >= 1
+        assert abs(e[n - 1] - ref[n - 1]) < 1e-9, (c, e[n - 1], ref[n - 1])
+    b.close()
