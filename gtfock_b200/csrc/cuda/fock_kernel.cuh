@@ -120,12 +120,27 @@ __global__ void __launch_bounds__(FOCK_THREADS,
     __shared__ __align__(16) R tab[RysTab<R>::slen(NR)];
     rys_stage<R, NR>(tab);
     const int lane = threadIdx.x & 31;
-    unsigned long long u = 0, uend = 0;   // batched launches: the claimed range of units
+    // batched launches: per-warp slots for the claimed range of units and the
+    // molecule of the current unit, so that neither holds registers across
+    // the integral loops
+    constexpr int NW = FOCK_THREADS / 32;
+    __shared__ unsigned long long s_claim[BATCH ? 2 * NW : 1];
+    __shared__ int s_mol[BATCH ? NW : 1];
+    const int wib = threadIdx.x >> 5;
+    if constexpr (BATCH) {
+        if (lane == 0) {
+            s_claim[2 * wib] = 0;
+            s_claim[2 * wib + 1] = 0;
+        }
+        __syncwarp();
+    }
     for (;;) {
         unsigned long long uu;
         if constexpr (BATCH) {
             // a warp claims g.claim units at once (fewer atomics on the
             // counter when the molecules' units are small)
+            volatile unsigned long long *sc = s_claim + 2 * wib;
+            unsigned long long u = sc[0], uend = sc[1];
             if (u >= uend) {
                 const unsigned claim = g.claim > 1 ? (unsigned)g.claim : 1u;
                 unsigned long long c0 = 0;
@@ -134,7 +149,13 @@ __global__ void __launch_bounds__(FOCK_THREADS,
                 uend = u + claim;
             }
             if (u >= (unsigned long long)g.nunits) break;
-            uu = u++;
+            uu = u;
+            __syncwarp();
+            if (lane == 0) {
+                sc[0] = u + 1;
+                sc[1] = uend;
+            }
+            __syncwarp();
         } else {
             unsigned long long c0 = 0;
             if (lane == 0) c0 = atomicAdd(counter, 1ULL);
@@ -146,11 +167,14 @@ __global__ void __launch_bounds__(FOCK_THREADS,
         // the kernel parameter (one molecule, no registers held for them) or
         // from the descriptor array
         constexpr bool bt = BATCH;
-        const FockLaunch *mp = g.mols;
+        const FockLaunch *mp = g.mols;   // reassigned after the integral loops (batched)
         if constexpr (BATCH) {
             const int m = warp_find_le(g.mol_prefix, g.nmol, (long long)uu, lane);
             mp += m;
             uu -= (unsigned long long)__ldg(g.mol_prefix + m);
+            __syncwarp();
+            if (lane == 0) s_mol[wib] = m;
+            __syncwarp();
         }
 #define GTF_FLD(x) (bt ? mp->x : g.one.x)
         const long long *unit_prefix = GTF_FLD(unit_prefix);
@@ -191,6 +215,7 @@ __global__ void __launch_bounds__(FOCK_THREADS,
             const PPRec src{GTF_FLD(pprec)};
             if (active) eri_accumulate_cd<LA, LB, LC, LD, CD0, N, true, true>(src, pb, src, pk, acc, tab);
         }
+        if constexpr (BATCH) mp = g.mols + ((volatile int *)s_mol)[wib];   // reloaded after the loops
         digest_cd<LA, LB, LC, LD, CD0, N>(acc, active, pb, pk, same, GTF_FLD(D), GTF_FLD(Fj), GTF_FLD(Fk),
                                           GTF_FLD(ld), lane, GTF_FLD(konly) != 0);
 #undef GTF_FLD
