@@ -1942,6 +1942,12 @@ struct gtf_fock_batch {
 // medium solo launches cost more than that (256-molecule batch: -16%).  The
 // environment variable GTFOCK_SOLO_UNITS overrides the threshold (tests).
 #define GTF_SOLO_UNITS 262144
+// A molecule with at least GTF_SOLO_MOL_UNITS units over all its launches
+// (C54H18 / cc-pVDZ: 13.4M; the molecules of the 256-molecule batch: below
+// 0.7M) is large enough that all its launches of at least GTF_SOLO_MIN_UNITS
+// run solo: it then runs as fast as a build of its own.
+#define GTF_SOLO_MOL_UNITS 2000000LL
+#define GTF_SOLO_MIN_UNITS 4096
 
 static long long solo_units_threshold()
 {
@@ -2025,6 +2031,12 @@ extern "C" int gtf_fock_batch_create(gtf_fock_dev_t *const *engines, int M, void
     CKB_(cudaMemcpy(b->d_xf, xf.data(), sizeof(XformDesc) * M, cudaMemcpyHostToDevice));
     int nblocks = 2 * NCLSPAIR;
     const long long solo_min = solo_units_threshold();
+    std::vector<char> big(M, 0);
+    for (int m = 0; m < M; m++) {
+        long long tot = 0;
+        for (int c = 0; c < NCLSPAIR; c++) tot += engines[m]->tasks[c].nunits + engines[m]->tasks[c].nunits32;
+        big[m] = tot >= GTF_SOLO_MOL_UNITS;
+    }
     for (int c = 0; c < NCLSPAIR; c++)
         for (int p = 0; p < 2; p++) {
             std::vector<FockLaunch> d;
@@ -2038,7 +2050,7 @@ extern "C" int gtf_fock_batch_create(gtf_fock_dev_t *const *engines, int M, void
                 const bool need_tr = f->pure && f->nbf_cart != f->nbf;
                 FockLaunch a;
                 fill_launch(f, c, p, need_tr ? f->d_Dc : f->d_D, f->d_Fj, f->d_Fk, a);
-                if (M > 1 && nu >= solo_min) {
+                if (M > 1 && (nu >= solo_min || (big[m] && nu >= GTF_SOLO_MIN_UNITS))) {
                     b->solo[c][p].push_back(a);
                     b->solo_units[c][p].push_back(nu);
                     nblocks++;
