@@ -366,6 +366,46 @@ def run_c12h26(args):
                       "energy_last_e2e": float(e2[-1])}), flush=True)
 
 
+def run_batch_scaling(args):
+    """Large molecules in one batch: the Fock time per step of 1, 2 and 3
+    copies of C54H18 / cc-pVDZ and of (H2O)64 / 6-31G against one build of
+    the molecule alone, with the default solo-launch rule and, with
+    GTFOCK_SOLO_UNITS set very high, with every launch batched."""
+    import numpy as np
+    import gtfock_b200 as gb
+    from gtfock_b200 import molecules as mol
+    out = {"workload": "1-3 copies of C54H18 / cc-pVDZ (846 bf) and (H2O)64 / 6-31G (832 bf) per batch, "
+                       "Fock ms per SCF step (2 steps after 1)"}
+    with tempfile.TemporaryDirectory() as td:
+        for name, atoms, basis in (("c54h18", mol.graphene_flake(2), "cc-pvdz"),
+                                   ("w64", mol.water_cluster(64, 2024), "6-31g")):
+            xyz = mol.write_xyz(atoms, os.path.join(td, name + ".xyz"))
+            gbs = mol.basis_file(basis)
+            b = gb.BasisSet(gbs, xyz)
+            pf = gb.PFock(b, tolscr=TOL)
+            D = np.eye(b.nbf) * 0.3
+            for _ in range(3):
+                pf.compute_fock(D)
+            out[name + "_single_ms"] = pf.timing()["ms_eri"]
+            pf.close()
+            for rule, env in (("solo_rule", None), ("all_batched", "1000000000000000")):
+                if env:
+                    os.environ["GTFOCK_SOLO_UNITS"] = env
+                for m in (2, 3):
+                    bt = gb.Batch(m)
+                    for _ in range(m):
+                        bt.add(gbs, xyz, tolscr=TOL, max_iters=4, etol=0.0)
+                    bt.step()
+                    i0 = bt.info()
+                    bt.step()
+                    bt.step()
+                    i1 = bt.info()
+                    out["%s_x%d_%s_ms" % (name, m, rule)] = (i1["ms_fock"] - i0["ms_fock"]) / 2
+                    bt.close()
+                os.environ.pop("GTFOCK_SOLO_UNITS", None)
+    print(json.dumps(out), flush=True)
+
+
 def run_batched(args):
     """Batched workload: `count` seeded molecules (water clusters of 2-24 and
     alkanes C2-C16, STO-3G or 6-31G), 15 SCF iterations each.  Solves/s of the
@@ -577,9 +617,10 @@ def main():
                     help="two SCF iterations of (H2O)64 with the split-BF16 purification (ncu case)")
     ap.add_argument("--fp32-cutoff", type=float, default=None,
                     help="with --profile-fock: FP32 for quartets with Schwarz bound below this")
-    ap.add_argument("--workload", choices=["default", "batched", "served", "precision", "c12h26"], default="default",
+    ap.add_argument("--workload", choices=["default", "batched", "served", "precision", "c12h26", "batch-scaling"], default="default",
                     help="batched / served / precision: the batched, served and precision-sweep workloads; "
-                         "c12h26: the 10-iteration C12H26 solve timed beside the reference driver")
+                         "c12h26: the 10-iteration C12H26 solve timed beside the reference driver; "
+                         "batch-scaling: large molecules in one batch against builds alone")
     ap.add_argument("--count", type=int, default=None, help="molecules (batched) or requests (served)")
     ap.add_argument("--seed", type=int, default=None)
     ap.add_argument("--rate", type=float, default=2.0, help="served: Poisson arrival rate (1/s)")
@@ -604,6 +645,9 @@ def main():
         return
     if args.workload == "c12h26":
         run_c12h26(args)
+        return
+    if args.workload == "batch-scaling":
+        run_batch_scaling(args)
         return
     if args.profile_purif:
         profile_purification(args)

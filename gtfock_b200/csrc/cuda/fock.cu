@@ -1940,7 +1940,8 @@ struct gtf_fock_batch {
 // offset, at 50-60 more bytes of spills; measured 17% slower on 2-3 copies of
 // C54H18 or (H2O)64).  At 32768 units the tails and the serial order of many
 // medium solo launches cost more than that (256-molecule batch: -16%).  The
-// environment variable GTFOCK_SOLO_UNITS overrides the threshold (tests).
+// environment variable GTFOCK_SOLO_UNITS replaces both rules by "solo when a
+// launch has at least that many units" (tests, measurements).
 #define GTF_SOLO_UNITS 262144
 // A molecule with at least GTF_SOLO_MOL_UNITS units over all its launches
 // (C54H18 / cc-pVDZ: 13.4M; the molecules of the 256-molecule batch: below
@@ -1949,12 +1950,18 @@ struct gtf_fock_batch {
 #define GTF_SOLO_MOL_UNITS 2000000LL
 #define GTF_SOLO_MIN_UNITS 4096
 
-static long long solo_units_threshold()
+// Returns the per-launch threshold; *overridden is set when the environment
+// variable gives it, which also turns off the per-molecule rule below.
+static long long solo_units_threshold(bool *overridden)
 {
+    *overridden = false;
     const char *e = getenv("GTFOCK_SOLO_UNITS");
     if (e && *e) {
         const long long v = atoll(e);
-        if (v >= 1) return v;
+        if (v >= 1) {
+            *overridden = true;
+            return v;
+        }
     }
     return GTF_SOLO_UNITS;
 }
@@ -2030,9 +2037,10 @@ extern "C" int gtf_fock_batch_create(gtf_fock_dev_t *const *engines, int M, void
     CKB_(cudaMalloc(&b->d_xf, sizeof(XformDesc) * M));
     CKB_(cudaMemcpy(b->d_xf, xf.data(), sizeof(XformDesc) * M, cudaMemcpyHostToDevice));
     int nblocks = 2 * NCLSPAIR;
-    const long long solo_min = solo_units_threshold();
+    bool solo_env = false;
+    const long long solo_min = solo_units_threshold(&solo_env);
     std::vector<char> big(M, 0);
-    for (int m = 0; m < M; m++) {
+    for (int m = 0; m < M && !solo_env; m++) {
         long long tot = 0;
         for (int c = 0; c < NCLSPAIR; c++) tot += engines[m]->tasks[c].nunits + engines[m]->tasks[c].nunits32;
         big[m] = tot >= GTF_SOLO_MOL_UNITS;
