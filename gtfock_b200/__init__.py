@@ -129,6 +129,18 @@ def load():
     _sig(L, "gtf_tune_entries", [_ip, _i])
     _sig(L, "gtf_fp64_peak", [_dp])
     _sig(L, "gtf_device_info", [_ip, _ip])
+    _sig(L, "gtf_pfock_set_incremental", [_vp, _i, _d, _i])
+    _sig(L, "gtf_pfock_incremental_stats", [_vp, _dp, _dp, _dp])
+    _sig(L, "gtf_scf_set_incremental", [_vp, _i, _d, _i])
+    _sig(L, "gtf_batch_set_incremental", [_vp, _i, _d, _i])
+    _sig(L, "gtf_batch_job_device_bytes", [_vp, _i], ctypes.c_size_t)
+    _sig(L, "gtf_device_memory", [ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)])
+    _sig(L, "gtf_debug_fail_alloc", [_i], None)
+    _sig(L, "gtf_debug_live_allocs", [], ctypes.c_longlong)
+    _sig(L, "gtf_pfock_compute_noalloc", [_vp, _vp, _vp])
+    _sig(L, "gtf_shard_split", [_dp, ctypes.c_longlong, _i, _i, ctypes.POINTER(ctypes.c_longlong),
+                                ctypes.POINTER(ctypes.c_longlong)], None)
+    _sig(L, "gtf_pfock_shard_work", [_vp, _dp])
     _lib = L
     return L
 
@@ -140,6 +152,14 @@ def device_info():
     cc = ctypes.c_int()
     L.gtf_device_info(ctypes.byref(n), ctypes.byref(cc))
     return n.value, cc.value
+
+
+def device_memory():
+    """(free bytes, total bytes) of the current CUDA device."""
+    fr, to = ctypes.c_size_t(), ctypes.c_size_t()
+    if load().gtf_device_memory(ctypes.byref(fr), ctypes.byref(to)) != 0:
+        raise GtfError("gtf_device_memory failed (no CUDA device?)")
+    return fr.value, to.value
 
 
 def _dptr(a):
@@ -272,10 +292,30 @@ class PFock:
         self._check(load().gtf_pfock_set_precision(self.h, mode, fp32_cutoff),
                     "gtf_pfock_set_precision")
 
+    def set_incremental(self, on=True, tau=0.0, period=8):
+        """Incremental builds: F_k = F_k-1 + G[D_k - D_k-1], quartets of the
+        change dropped below Schwarz bound x max|dD| < tau (tau <= 0: the
+        Schwarz threshold), a full build every `period` builds."""
+        self._check(load().gtf_pfock_set_incremental(self.h, 1 if on else 0, tau, period),
+                    "gtf_pfock_set_incremental")
+
+    def incremental_stats(self):
+        """(FP64 quartets, FP32 quartets, max|dD|) of the last incremental build."""
+        a, b, c = np.zeros(1), np.zeros(1), np.zeros(1)
+        self._check(load().gtf_pfock_incremental_stats(self.h, _dptr(a), _dptr(b), _dptr(c)),
+                    "gtf_pfock_incremental_stats")
+        return float(a[0]), float(b[0]), float(c[0])
+
     def set_shard(self, shard, nshards):
         """Builds of this engine compute shard `shard` of `nshards` of every
         class launch's quartet units (their F is that shard's part)."""
         self._check(load().gtf_pfock_set_shard(self.h, shard, nshards), "gtf_pfock_set_shard")
+
+    def shard_work(self):
+        """Model FLOPs of this engine's shard of a build (whole build if unsharded)."""
+        w = np.zeros(1)
+        self._check(load().gtf_pfock_shard_work(self.h, _dptr(w)), "gtf_pfock_shard_work")
+        return float(w[0])
 
     def compute_dev(self, d_ptr):
         """Fock build from a device density (pointer to nbf x nbf FP64);
@@ -410,6 +450,13 @@ class SCFSolver:
         if r != 0:
             raise GtfError("gtf_scf_set_options failed (%d)" % r)
 
+    def set_incremental(self, on=True, tau=0.0, period=8):
+        """Incremental Fock builds for this solver (see PFock.set_incremental);
+        every solve starts with a full build."""
+        r = load().gtf_scf_set_incremental(self.h, 1 if on else 0, tau, period)
+        if r != 0:
+            raise GtfError("gtf_scf_set_incremental failed (%d)" % r)
+
     def set_purification(self, mode):
         """0: FP64 products; 1: split-BF16 tensor-core products, FP64 finish."""
         r = load().gtf_scf_set_purification(self.h, mode)
@@ -451,6 +498,16 @@ class Batch:
             raise GtfError("gtf_batch_create failed")
         self.capacity = capacity
         self.max_iters = {}
+
+    def set_incremental(self, on=True, tau=0.0, period=8):
+        """Incremental Fock builds for every job (set before the first add)."""
+        r = load().gtf_batch_set_incremental(self.h, 1 if on else 0, tau, period)
+        if r != 0:
+            raise GtfError("gtf_batch_set_incremental failed (%d)" % r)
+
+    def job_device_bytes(self, slot):
+        """Device bytes a job holds (its batch buffers and its Fock engine)."""
+        return int(load().gtf_batch_job_device_bytes(self.h, slot))
 
     def add(self, gbs, xyz, tolscr=1e-10, precision=0, fp32_cutoff=0.0, max_iters=30, etol=1e-11):
         slot = load().gtf_batch_add(self.h, gbs.encode(), xyz.encode(), tolscr, precision, fp32_cutoff,

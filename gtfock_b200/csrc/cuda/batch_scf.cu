@@ -49,6 +49,10 @@ extern "C" const char *gtf_last_error(void);
 // ---------------------------------------------------------------------------
 struct JobDev {
     double *D, *F;                 // engine density (AO, input of the Fock build) and Fock matrix
+    // the Fock build's result: F itself, or for incremental builds the
+    // engine's running sum, which the step must leave intact (F is then the
+    // job's own copy that receives F + H and DIIS)
+    const double *Fe;
     const double *H, *S, *X;
     double *P, *P2, *P3, *W, *W2;  // purification (orthogonal basis) and scratch
     double *vecs, *Fvecs;          // DIIS error vectors and Fock matrices
@@ -223,7 +227,7 @@ __global__ void __launch_bounds__(BJ_THREADS) k_j_energy(const JobDev *__restric
     const size_t nn = (size_t)j.n * j.n;
     double e = 0.0;
     for (size_t k = (size_t)blockIdx.x * BJ_THREADS + threadIdx.x; k < nn; k += (size_t)BJ_EBLOCKS * BJ_THREADS) {
-        const double f = j.F[k] + j.H[k];
+        const double f = j.Fe[k] + j.H[k];
         j.F[k] = f;
         e += j.D[k] * (j.H[k] + f);
     }
@@ -360,8 +364,11 @@ __global__ void __launch_bounds__(BJ_THREADS) k_j_pur_step(const JobDev *__restr
     t = block_sum(t, sh);
     t2 = block_sum(t2, sh);
     const double c = t / t2;
-    const double err = isfinite(c) ? sqrt(e) : 0.0;   // 0/0 at an idempotent P: stop, as the one-job path
-    for (size_t k = threadIdx.x; k < nn && isfinite(c); k += BJ_THREADS) {
+    // 0/0 at an idempotent P, or c far outside [0, 1] (eigenvalues of P out
+    // of [0, 1], the update diverging): stop and keep P, as the one-job path
+    const bool ok = isfinite(c) && c >= -0.25 && c <= 1.25;
+    const double err = ok ? sqrt(e) : 0.0;
+    for (size_t k = threadIdx.x; k < nn && ok; k += BJ_THREADS) {
         if (c < 0.5) j.P[k] = ((1.0 - 2.0 * c) * j.P[k] + (1.0 + c) * j.P2[k] - j.P3[k]) / (1.0 - c);
         else j.P[k] = ((1.0 + c) * j.P2[k] - j.P3[k]) / c;
     }
@@ -384,6 +391,8 @@ struct BJob {
     gtf_fock_dev_t *eng;
     gtf_purif_dev_t *pd;           // jobs above BJ_BIG functions: single-job DIIS / purification
     double *mem;
+    double *fcopy;                 // incremental builds: the job's copy of F (see JobDev::Fe)
+    int inc_since;                 // builds since the last full one (incremental builds)
     size_t bytes;
     JobDev dv;
     // SCF state
@@ -423,6 +432,10 @@ struct gtf_batch {
     int *h_iters, *h_count, *h_act, *h_list;
     size_t dev_bytes_jobs;
     double ms_fock, ms_rest, ms_energy, ms_diis, ms_pur, pur_steps, nsteps;
+    // incremental Fock builds for the jobs added while on (gtf_batch_set_incremental)
+    int incr, incr_period;
+    double incr_tau;
+    std::vector<int> h_full;
     cudaEvent_t e0, e1, e2, e3, e4;
 };
 
@@ -445,6 +458,7 @@ extern "C" size_t gtf_batch_job_bytes(int nbf) { return job_buffer_bytes(nbf); }
 static void job_free(BJob &j)
 {
     if (j.mem) cudaFree(j.mem);
+    if (j.fcopy) cudaFree(j.fcopy);
     if (j.pd) gtf_purif_destroy(j.pd);
     if (j.pf) {
         PFock_destroyOvlMat(j.pf);
@@ -589,6 +603,18 @@ extern "C" int gtf_batch_add(gtf_batch_t *b, const char *bsfile, const char *xyz
     }
     d.D = const_cast<double *>(gtf_fock_mat_dev(j.eng, 0, 0));
     d.F = const_cast<double *>(gtf_fock_mat_dev(j.eng, 1, 0));
+    d.Fe = d.F;
+    if (b->incr) {
+        if (gtf_pfock_set_incremental(j.pf, 1, b->incr_tau, b->incr_period) != PFOCK_STATUS_SUCCESS ||
+            cudaMalloc(&j.fcopy, sizeof(double) * nn) != cudaSuccess) {
+            j.fcopy = nullptr;
+            job_free(j);
+            return -6;
+        }
+        j.bytes += sizeof(double) * nn;
+        d.F = j.fcopy;
+    }
+    j.inc_since = 0;
     d.H = gtf_fock_onee_dev(j.eng, 2);
     if (j.mem) {
         d.P = j.mem;
@@ -797,6 +823,20 @@ extern "C" int gtf_batch_step(gtf_batch_t *b)
     if (b->dirty || run != b->fb_members) {
         const int r = rebuild_fock_batch(b, run);
         if (r) return r;
+    }
+    if (b->incr) {
+        // full or incremental build, per member, before the (captured) build reads the flags
+        b->h_full.resize(run.size());
+        for (size_t k = 0; k < run.size(); k++) {
+            BJob &j = b->jobs[run[k]];
+            const int full = (j.inc_since == 0 || j.inc_since >= b->incr_period) ? 1 : 0;
+            b->h_full[k] = full;
+            j.inc_since = full ? 1 : j.inc_since + 1;
+        }
+        if (gtf_fock_batch_set_full(b->fb, b->h_full.data()) != GTF_OK) {
+            fprintf(stderr, "gtfock_b200: %s\n", gtf_last_error());
+            return -3;
+        }
     }
     CKH(cudaEventRecord(b->e0, b->st));
     if (b->fock_exec) {
@@ -1068,6 +1108,20 @@ extern "C" int gtf_batch_autotune(gtf_batch_t *b, int reps)
     return GTF_OK;
 }
 
+// Incremental Fock builds (gtf_pfock_set_incremental) for the jobs added from
+// now on (on = 0: plain builds).  A batch must not mix the two: set it before
+// the first job is added.
+extern "C" int gtf_batch_set_incremental(gtf_batch_t *b, int on, double tau, int period)
+{
+    if (!b || (on && period < 1)) return -1;
+    for (auto &j : b->jobs)
+        if (j.used) return -2;
+    b->incr = on ? 1 : 0;
+    b->incr_tau = tau;
+    b->incr_period = period;
+    return 0;
+}
+
 extern "C" int gtf_batch_run(gtf_batch_t *b)
 {
     int r;
@@ -1094,6 +1148,14 @@ extern "C" int gtf_batch_info(gtf_batch_t *b, int *nrunning, int *nused, double 
     if (ms_rest) *ms_rest = b->ms_rest;
     if (job_bytes) *job_bytes = by;
     return 0;
+}
+
+// device bytes held by the job in `slot` (batch buffers and Fock engine); 0 if empty
+extern "C" size_t gtf_batch_job_device_bytes(gtf_batch_t *b, int slot)
+{
+    if (!b || slot < 0 || slot >= b->capacity || !b->jobs[slot].used) return 0;
+    const BJob &j = b->jobs[slot];
+    return j.bytes + gtf_fock_device_bytes(j.eng);
 }
 
 // accumulated statistics: [0] ms of Fock builds, [1] energies, [2] DIIS,

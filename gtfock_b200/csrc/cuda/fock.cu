@@ -28,6 +28,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -68,12 +69,34 @@ __host__ __device__ inline int pair_class(int la, int lb)
 static const int k_cls_la[NCLS] = {0, 1, 1, 2, 2, 2};
 static const int k_cls_lb[NCLS] = {0, 0, 1, 0, 1, 2};
 
+struct UnitTask;
+
+static inline double __longlong_as_double_host(unsigned long long b)
+{
+    double d;
+    memcpy(&d, &b, sizeof(d));
+    return d;
+}
+
+// Device state of an engine for incremental builds: the largest |element| of
+// the density change of the current build (a non-negative double kept as its
+// bit pattern, so atomicMax orders it), the quartet thresholds derived from
+// it, whether the build adds to the previous result (acc) and the quartet
+// counts of the build's task lists (FP64, FP32).
+struct DynState {
+    unsigned long long dmax_bits;
+    double tol2, cut2;
+    int acc, pad;
+    unsigned long long nq64, nq32;
+};
+
 struct ClassPairTask {
     int X, Y;
     int bra_start, nbra;
     int ket_start, nketcls;
     int seg[GTF_NBKT + 1];  // ket segments (primitive-count buckets), relative to ket_start
     long long nunits, nunits32;  // units of the FP64 and the FP32 launch
+    long long nunits_bound;      // bound on either launch's units under any thresholds >= tol2
     double flops, nprimq;        // Rys-model FLOPs and primitive quartets (before primitive screening)
     double nquart, nquart32;     // quartets in all, of which evaluated in FP32
     int *d_nket;                 // [nbra][GTF_NBKT] kets per (bra, segment)
@@ -128,16 +151,112 @@ struct gtf_fock_dev {
     // non-symmetric densities (PFock_create with symm = 0)
     int nosymm;
     double *d_Ds, *d_Da, *d_Dca, *d_Fka;
-    // sharded build: this engine computes shard `shard` of `nshards` (0: all)
+    // sharded build: this engine computes shard `shard` of `nshards` (0: all);
+    // its units of every (class pair, part): [shard_lo, shard_hi), split by
+    // the work model (see shard_bounds)
     int shard, nshards;
+    long long shard_lo[NCLSPAIR][2], shard_hi[NCLSPAIR][2];
+    double shard_work;           // model FLOPs of this shard's units
+    std::vector<int> h_pair_n;   // primitive pairs per shell pair (pair list order)
+    // task lists on the device (UnitTask per class pair with work): static
+    // thresholds, and the same tasks reading the thresholds of d_dyn
+    std::vector<struct UnitTask> h_ut;
+    struct UnitTask *d_ut_static, *d_ut_dyn;
+    long long ut_nidx, ut_nbras;
+    // incremental builds (gtf_fock_set_incremental): F_k = F_k-1 + G[D_k -
+    // D_k-1], quartets screened against tau / max|D_k - D_k-1|
+    int incr, incr_period, incr_since;
+    double incr_tau;
+    double *d_Dprev, *d_Dd;
+    DynState *d_dyn;
+    // the task-list arrays hold an incremental build's lists (rebuilt from
+    // the static thresholds before a plain build uses them)
+    int lists_dyn;
 };
+
+// ---------------------------------------------------------------------------
+// Device allocations of an engine's set-up.  Every one goes through
+// dev_malloc, which a test can make fail: after gtf_debug_fail_alloc(n) the
+// n-th allocation from then on fails as an out-of-memory cudaMalloc would
+// (and the counter disarms), so each error path of PFock_create can be shown
+// to release what it had allocated.
+// ---------------------------------------------------------------------------
+static std::atomic<int> g_fail_alloc{0};
+static std::atomic<long long> g_live_allocs{0};   // dev_malloc'd and not yet dev_free'd
+
+extern "C" void gtf_debug_fail_alloc(int n) { g_fail_alloc.store(n > 0 ? n : 0); }
+extern "C" long long gtf_debug_live_allocs(void) { return g_live_allocs.load(); }
+
+static cudaError_t dev_malloc(void **p, size_t bytes)
+{
+    int n = g_fail_alloc.load();
+    while (n > 0 && !g_fail_alloc.compare_exchange_weak(n, n - 1)) {
+    }
+    if (n == 1) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
+    const cudaError_t e = cudaMalloc(p, bytes);
+    if (e == cudaSuccess) g_live_allocs++;
+    return e;
+}
+
+static void dev_free(void *p)
+{
+    if (!p) return;
+    cudaFree(p);
+    g_live_allocs--;
+}
+
+// Device temporaries of one set-up call: released when the call returns, on
+// success and on every error path alike.
+struct DevTemps {
+    std::vector<void *> p;
+    DevTemps() = default;
+    DevTemps(const DevTemps &) = delete;
+    DevTemps &operator=(const DevTemps &) = delete;
+    ~DevTemps()
+    {
+        for (void *q : p) dev_free(q);
+    }
+    template <typename T>
+    int get(T **out, size_t n)
+    {
+        *out = nullptr;
+        if (n == 0) n = 1;
+        void *q = nullptr;
+        cudaError_t e = dev_malloc(&q, n * sizeof(T));
+        if (e != cudaSuccess) {
+            snprintf(g_errbuf, sizeof(g_errbuf), "cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
+            return GTF_ERR_ALLOC;
+        }
+        p.push_back(q);
+        *out = (T *)q;
+        return GTF_OK;
+    }
+    void drop(void *q)
+    {
+        for (size_t k = 0; k < p.size(); k++)
+            if (p[k] == q) {
+                dev_free(q);
+                p.erase(p.begin() + (long)k);
+                return;
+            }
+    }
+};
+
+#define TALLOC(tmps, ptr, n)                        \
+    do {                                            \
+        int r_ = (tmps).get(&(ptr), (size_t)(n));   \
+        if (r_) return r_;                          \
+    } while (0)
 
 template <typename T>
 static int dalloc(gtf_fock_dev *f, T **p, size_t n)
 {
     *p = nullptr;
     if (n == 0) n = 1;
-    cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+    cudaError_t e = dev_malloc((void **)p, n * sizeof(T));
     if (e != cudaSuccess) {
         snprintf(g_errbuf, sizeof(g_errbuf), "cudaMalloc(%zu bytes): %s", n * sizeof(T),
                  cudaGetErrorString(e));
@@ -215,7 +334,7 @@ __device__ __forceinline__ void f_to_sph_elem(const double *__restrict__ Fj, con
                                               const int *__restrict__ sph2shell, const int *__restrict__ sh_L,
                                               const int *__restrict__ f_start, const int *__restrict__ fc_start,
                                               int nbf, int nbfc, int pure, int m, int n,
-                                              const double *__restrict__ Fka = nullptr)
+                                              const double *__restrict__ Fka = nullptr, bool acc = false)
 {
     const int sm = sph2shell[m], sn = sph2shell[n];
     const int cm = m - f_start[sm], cn = n - f_start[sn];
@@ -237,21 +356,89 @@ __device__ __forceinline__ void f_to_sph_elem(const double *__restrict__ Fj, con
         }
     }
     const size_t o = (size_t)m * nbf + n;
-    J[o] = j;
-    K[o] = k;
-    F[o] = j + k;
+    if (acc) {
+        // incremental build: this build's part is added to the previous result
+        J[o] += j;
+        K[o] += k;
+        F[o] += j + k;
+    } else {
+        J[o] = j;
+        K[o] = k;
+        F[o] = j + k;
+    }
 }
 
 __global__ void k_f_to_sph(const double *__restrict__ Fj, const double *__restrict__ Fk,
                            double *__restrict__ F, double *__restrict__ J, double *__restrict__ K,
                            const int *__restrict__ sph2shell, const int *__restrict__ sh_L,
                            const int *__restrict__ f_start, const int *__restrict__ fc_start,
-                           int nbf, int nbfc, int pure, const double *__restrict__ Fka = nullptr)
+                           int nbf, int nbfc, int pure, const double *__restrict__ Fka = nullptr,
+                           const int *__restrict__ acc_flag = nullptr)
 {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     const int m = blockIdx.y;
     if (n >= nbf) return;
-    f_to_sph_elem(Fj, Fk, F, J, K, sph2shell, sh_L, f_start, fc_start, nbf, nbfc, pure, m, n, Fka);
+    const bool acc = acc_flag != nullptr && *acc_flag != 0;
+    f_to_sph_elem(Fj, Fk, F, J, K, sph2shell, sh_L, f_start, fc_start, nbf, nbfc, pure, m, n, Fka, acc);
+}
+
+// ---------------------------------------------------------------------------
+// Incremental builds.  F is linear in D, so F[D_k] = F[D_k-1] + G[D_k -
+// D_k-1].  A quartet contributes at most its Schwarz bound times the largest
+// element of the density it digests, so with dmax = max |D_k - D_k-1| the
+// build of the change keeps the quartets with bound * dmax >= tau (tau the
+// Schwarz threshold by default: each dropped contribution is below what the
+// plain build's screening drops), and evaluates in FP32 those with bound *
+// dmax below the FP32 cutoff.  Every few builds a full one restarts the sum.
+// ---------------------------------------------------------------------------
+// Dd = D - Dprev (D itself on a full build), Dprev = D, and max |Dd| into the
+// state (its dmax_bits zeroed before the launch)
+__device__ __forceinline__ void delta_range(const double *__restrict__ D, double *__restrict__ Dprev,
+                                            double *__restrict__ Dd, size_t n, int full, DynState *dyn,
+                                            size_t i0, size_t step)
+{
+    double m = 0.0;
+    for (size_t i = i0; i < n; i += step) {
+        const double d = D[i];
+        const double dd = full ? d : d - Dprev[i];
+        Dd[i] = dd;
+        Dprev[i] = d;
+        m = fmax(m, fabs(dd));
+    }
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) m = fmax(m, __shfl_xor_sync(GTF_FULL_MASK, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0.0) atomicMax(&dyn->dmax_bits, (unsigned long long)__double_as_longlong(m));
+}
+
+__global__ void k_delta(const double *__restrict__ D, double *__restrict__ Dprev, double *__restrict__ Dd, size_t n,
+                        int full, DynState *dyn)
+{
+    delta_range(D, Dprev, Dd, n, full, dyn, (size_t)blockIdx.x * blockDim.x + threadIdx.x,
+                (size_t)gridDim.x * blockDim.x);
+}
+
+// the thresholds of the build from dmax (one thread per engine)
+__device__ __forceinline__ void dyn_thresholds(DynState *dyn, double tol2, double cut2, double tau2, double c2,
+                                               int full)
+{
+    dyn->nq64 = 0;
+    dyn->nq32 = 0;
+    if (full) {
+        dyn->tol2 = tol2;
+        dyn->cut2 = cut2;
+        dyn->acc = 0;
+        return;
+    }
+    const double dm = __longlong_as_double((long long)dyn->dmax_bits);
+    const double d2 = dm * dm;
+    dyn->tol2 = d2 > 0.0 ? fmax(tol2, tau2 / d2) : INFINITY;
+    dyn->cut2 = (c2 > 0.0 && d2 > 0.0) ? c2 / d2 : 0.0;
+    dyn->acc = 1;
+}
+
+__global__ void k_dyn_thresholds(DynState *dyn, double tol2, double cut2, double tau2, double c2, int full)
+{
+    dyn_thresholds(dyn, tol2, cut2, tau2, c2, full);
 }
 
 // non-symmetric D: Ds = (D + D^T) / 2, Da = (D - D^T) / 2
@@ -567,80 +754,183 @@ __global__ void k_fill_pp32(const PairRec *__restrict__ pairs, int npairs, const
     }
 }
 
-// number of ket pairs of segment b of the ket class that pass
-// v_bra * v_ket >= tol2 (pfock/fock_task.c:192): each segment is sorted by
-// value, descending, so they form a prefix.  For bra class == ket class only
-// kets at or before the bra in the class order count, so every unordered
-// pair of pairs is visited once.  Thread (i, b); segment 0 holds pairs whose
-// primitive pairs were all screened out: counted, but given no units.
-struct SegStarts {
-    int s[GTF_NBKT + 1];
+// ---------------------------------------------------------------------------
+// Task lists, built on the device.
+//
+// For every (engine, class pair) and bra pair i of class X: the number of ket
+// pairs of each segment b of class Y that pass the quartet Schwarz test
+// v_i v_j >= tol2 (pfock/fock_task.c:192).  Each segment is sorted by value,
+// descending, so these kets are a prefix, found by binary search.  For X == Y
+// only kets at or before the bra in the class order count, so every unordered
+// pair of pairs is visited once.  Segment 0 holds pairs whose primitive pairs
+// were all screened out: counted, but given no units.
+//
+// cut2 > 0 (mixed precision): the kets with v_i v_j < cut2, i.e. a Schwarz
+// bound sqrt(v_i v_j) below the FP32 cutoff, form the tail of each prefix and
+// go to the FP32 launch; n64 counts the FP64 head.
+//
+// Per bra, the kets of all segments (in segment order, segment 0 left out)
+// form one list per launch part, so a warp's 32 lanes are filled across
+// segment boundaries: cum[i][b] is the exclusive prefix of the segment counts
+// and the bra has ceil(total / 32) units; the unit prefixes over the bras
+// close the lists.
+//
+// The thresholds are an engine's static ones, or, for incremental builds,
+// read from the engine's device state, where they were scaled by the largest
+// element of the density change.  Three launches rebuild the lists of every
+// engine of a build (one engine, or all the molecules of a batch) with no
+// host round trip, so a rebuild can sit inside a captured graph.
+// ---------------------------------------------------------------------------
+struct UnitTask {
+    const double *pair_v;
+    int *nket, *n64, *cum64, *cum32;
+    long long *up64, *up32;      // unit prefixes, [nbra + 1] each
+    DynState *dyn;               // null: the static thresholds below
+    double tol2, cut2;
+    long long idx0;              // first (bra, segment) index of this task, over all tasks
+    long long bra0;              // first bra index of this task, over all tasks
+    int bra_start, nbra, ket_start, same;
+    int seg[GTF_NBKT + 1];
 };
 
-// cut2 > 0 (mixed precision): the kets with v_bra * v_ket < cut2, i.e. a
-// Schwarz bound sqrt(v_bra v_ket) below the FP32 cutoff, form the tail of each
-// prefix and go to the FP32 launch; n64 counts the FP64 head.
-__global__ void k_count_kets(const double *__restrict__ pair_v, int bra_start, int nbra, int ket_start,
-                             SegStarts seg, int same, double tol2, double cut2, int *__restrict__ nket,
-                             int *__restrict__ n64)
+// last task k with key(k) <= v (key non-decreasing, key(0) = 0 <= v)
+template <typename Key>
+__device__ __forceinline__ int task_of(const UnitTask *__restrict__ t, int nt, long long v, Key key)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int nidx = nbra * GTF_NBKT;
-    if (t >= nidx) return;
-    const int i = t / GTF_NBKT, b = t - i * GTF_NBKT;
-    const double v = pair_v[bra_start + i];
-    const int s0 = seg.s[b], s1 = seg.s[b + 1];
-    int lo = s0, hi = s1;  // first index failing the Schwarz test
+    int lo = 0, hi = nt - 1;
     while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (fabs(v * pair_v[ket_start + mid]) >= tol2) lo = mid + 1;
-        else hi = mid;
+        const int mid = (lo + hi + 1) >> 1;
+        if (key(t[mid]) <= v) lo = mid;
+        else hi = mid - 1;
     }
-    int c = lo - s0;
-    int lo2 = s0, hi2 = s0 + c;  // first index below the FP32 cutoff
-    while (lo2 < hi2) {
-        const int mid = (lo2 + hi2) >> 1;
-        if (fabs(v * pair_v[ket_start + mid]) >= cut2) lo2 = mid + 1;
-        else hi2 = mid;
-    }
-    int c64 = lo2 - s0;
-    if (same) {
-        const int lim = i - s0 + 1;  // kets j <= i
-        c = lim < 0 ? 0 : (c < lim ? c : lim);
-        c64 = c64 < c ? c64 : c;
-    }
-    nket[t] = c;
-    n64[t] = c64;
+    return lo;
 }
 
-// Per bra: the kets of all segments (in segment order, segment 0 left out)
-// form one list per launch part, so a warp's 32 lanes are filled across
-// segment boundaries.  cum[i][b] is the exclusive prefix of the segment
-// counts (cum[i][GTF_NBKT] = the bra's total); units[i] = ceil(total / 32).
-__global__ void k_pack_units(int nbra, const int *__restrict__ nket, const int *__restrict__ n64,
-                             int *__restrict__ cum64, int *__restrict__ cum32, long long *__restrict__ units64,
-                             long long *__restrict__ units32)
+// phase 1: one thread per (task, bra, segment)
+__global__ void k_units_count(const UnitTask *__restrict__ tasks, int nt, long long total)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i > nbra) return;
-    if (i == nbra) {
-        units64[nbra] = 0;
-        units32[nbra] = 0;
-        return;
+    for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < total;
+         x += (long long)gridDim.x * blockDim.x) {
+        const int k = task_of(tasks, nt, x, [](const UnitTask &t) { return t.idx0; });
+        const UnitTask &t = tasks[k];
+        const int r = (int)(x - t.idx0);
+        const int i = r / GTF_NBKT, b = r - i * GTF_NBKT;
+        double tol2 = t.tol2, cut2 = t.cut2;
+        if (t.dyn) {
+            tol2 = t.dyn->tol2;
+            cut2 = t.dyn->cut2;
+        }
+        const double *pv = t.pair_v + t.ket_start;
+        const double v = t.pair_v[t.bra_start + i];
+        const int s0 = t.seg[b], s1 = t.seg[b + 1];
+        int lo = s0, hi = s1;  // first index failing the Schwarz test
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (fabs(v * pv[mid]) >= tol2) lo = mid + 1;
+            else hi = mid;
+        }
+        int c = lo - s0;
+        int lo2 = s0, hi2 = s0 + c;  // first index below the FP32 cutoff
+        while (lo2 < hi2) {
+            const int mid = (lo2 + hi2) >> 1;
+            if (fabs(v * pv[mid]) >= cut2) lo2 = mid + 1;
+            else hi2 = mid;
+        }
+        int c64 = lo2 - s0;
+        if (t.same) {
+            const int lim = i - s0 + 1;  // kets j <= i
+            c = lim < 0 ? 0 : (c < lim ? c : lim);
+            c64 = c64 < c ? c64 : c;
+        }
+        t.nket[r] = c;
+        t.n64[r] = c64;
+        if (t.dyn) {
+            // quartets of this build (FP64, FP32), for the statistics
+            unsigned long long q64 = (unsigned long long)c64, q32 = (unsigned long long)(c - c64);
+            atomicAdd(&t.dyn->nq64, q64);
+            atomicAdd(&t.dyn->nq32, q32);
+        }
     }
-    int a = 0, c = 0;
-    for (int b = 0; b < GTF_NBKT; b++) {
-        cum64[i * GTF_CUM + b] = a;
-        cum32[i * GTF_CUM + b] = c;
-        if (b == 0) continue;  // pairs whose primitive pairs were all screened out
-        const int n = nket[i * GTF_NBKT + b], h = n64[i * GTF_NBKT + b];
-        a += h;
-        c += n - h;
+}
+
+// phase 2: one thread per (task, bra): segment prefixes and units per bra
+// (the unit counts go into the prefix arrays, scanned in place by phase 3)
+__global__ void k_units_pack(const UnitTask *__restrict__ tasks, int nt, long long total)
+{
+    for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < total;
+         x += (long long)gridDim.x * blockDim.x) {
+        const int k = task_of(tasks, nt, x, [](const UnitTask &t) { return t.bra0; });
+        const UnitTask &t = tasks[k];
+        const int i = (int)(x - t.bra0);
+        int a = 0, c = 0;
+        for (int b = 0; b < GTF_NBKT; b++) {
+            t.cum64[i * GTF_CUM + b] = a;
+            t.cum32[i * GTF_CUM + b] = c;
+            if (b == 0) continue;  // pairs whose primitive pairs were all screened out
+            const int n = t.nket[i * GTF_NBKT + b], h = t.n64[i * GTF_NBKT + b];
+            a += h;
+            c += n - h;
+        }
+        t.cum64[i * GTF_CUM + GTF_NBKT] = a;
+        t.cum32[i * GTF_CUM + GTF_NBKT] = c;
+        t.up64[i] = (a + 31) / 32;
+        t.up32[i] = (c + 31) / 32;
     }
-    cum64[i * GTF_CUM + GTF_NBKT] = a;
-    cum32[i * GTF_CUM + GTF_NBKT] = c;
-    units64[i] = (a + 31) / 32;
-    units32[i] = (c + 31) / 32;
+}
+
+// phase 3: block (task, part) turns the per-bra units into the exclusive
+// prefix [nbra + 1] in place
+#define UNIT_SCAN_THREADS 256
+#define UNIT_SCAN_ITEMS 4
+__global__ void __launch_bounds__(UNIT_SCAN_THREADS) k_units_scan(const UnitTask *__restrict__ tasks)
+{
+    typedef cub::BlockScan<long long, UNIT_SCAN_THREADS> Scan;
+    __shared__ typename Scan::TempStorage tmp;
+    __shared__ long long s_carry;
+    const UnitTask &t = tasks[blockIdx.x >> 1];
+    long long *u = (blockIdx.x & 1) ? t.up32 : t.up64;
+    const int n = t.nbra;
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    constexpr int CH = UNIT_SCAN_THREADS * UNIT_SCAN_ITEMS;
+    for (int base = 0; base < n; base += CH) {
+        long long v[UNIT_SCAN_ITEMS];
+#pragma unroll
+        for (int q = 0; q < UNIT_SCAN_ITEMS; q++) {
+            const int i = base + threadIdx.x * UNIT_SCAN_ITEMS + q;
+            v[q] = i < n ? u[i] : 0;
+        }
+        long long agg;
+        Scan(tmp).ExclusiveSum(v, v, agg);
+        const long long carry = s_carry;
+#pragma unroll
+        for (int q = 0; q < UNIT_SCAN_ITEMS; q++) {
+            const int i = base + threadIdx.x * UNIT_SCAN_ITEMS + q;
+            if (i < n) u[i] = v[q] + carry;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_carry = carry + agg;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) u[n] = s_carry;
+}
+
+// Launches the three phases over `nt` tasks (device array) whose flattened
+// (bra, segment) and bra counts are nidx and nbras.
+static int run_units(const UnitTask *d_tasks, int nt, long long nidx, long long nbras, int nsm, cudaStream_t st)
+{
+    if (nt == 0) return GTF_OK;
+    auto grid = [&](long long n) {
+        long long g = (n + 255) / 256, cap = (long long)nsm * 8;
+        return (unsigned)(g < 1 ? 1 : (g > cap ? cap : g));
+    };
+    k_units_count<<<grid(nidx), 256, 0, st>>>(d_tasks, nt, nidx);
+    CK(cudaGetLastError());
+    k_units_pack<<<grid(nbras), 256, 0, st>>>(d_tasks, nt, nbras);
+    CK(cudaGetLastError());
+    k_units_scan<<<2 * nt, UNIT_SCAN_THREADS, 0, st>>>(d_tasks);
+    CK(cudaGetLastError());
+    return GTF_OK;
 }
 
 typedef int (*fock_group_launch_t)(int la, int lb, int lc, int ld, const FockGrid &g, cudaStream_t st);
@@ -937,59 +1227,123 @@ extern "C" int gtf_basis_dev_create(const gtf_basis_view_t *b, gtf_fock_dev_t **
     return upload_basis(f, b);
 }
 
+// The engine's task set: one UnitTask per class pair with work, static and
+// dynamic copies on the device (called once, after the per-task arrays exist).
+static int make_unit_tasks(gtf_fock_dev *f)
+{
+    f->h_ut.clear();
+    long long nidx = 0, nbras = 0;
+    for (int c = 0; c < NCLSPAIR; c++) {
+        ClassPairTask &t = f->tasks[c];
+        if (t.nbra == 0 || t.nketcls == 0) continue;
+        UnitTask u;
+        memset(&u, 0, sizeof(u));
+        u.pair_v = f->d_pair_v;
+        u.nket = t.d_nket;
+        u.n64 = t.d_n64;
+        u.cum64 = t.d_cum64;
+        u.cum32 = t.d_cum32;
+        u.up64 = t.d_unit_prefix;
+        u.up32 = t.d_unit_prefix32;
+        u.idx0 = nidx;
+        u.bra0 = nbras;
+        u.bra_start = t.bra_start;
+        u.nbra = t.nbra;
+        u.ket_start = t.ket_start;
+        u.same = t.X == t.Y;
+        for (int bk = 0; bk <= GTF_NBKT; bk++) u.seg[bk] = t.seg[bk];
+        f->h_ut.push_back(u);
+        nidx += (long long)t.nbra * GTF_NBKT;
+        nbras += t.nbra;
+    }
+    f->ut_nidx = nidx;
+    f->ut_nbras = nbras;
+    const size_t nt = f->h_ut.size();
+    DALLOC(f->d_ut_static, nt);
+    DALLOC(f->d_ut_dyn, nt);
+    DALLOC(f->d_dyn, 1);
+    std::vector<UnitTask> dyn(f->h_ut);
+    for (auto &u : dyn) u.dyn = f->d_dyn;
+    if (nt) CK(cudaMemcpyAsync(f->d_ut_dyn, dyn.data(), sizeof(UnitTask) * nt, cudaMemcpyHostToDevice, f->stream));
+    CK(cudaMemsetAsync(f->d_dyn, 0, sizeof(DynState), f->stream));
+    CK(cudaStreamSynchronize(f->stream));
+    return GTF_OK;
+}
+
+static int shard_bounds(gtf_fock_dev *f, int c, const std::vector<int> &nk, const std::vector<int> &n64);
+
 // Per class pair and (bra, segment): ket counts, the FP64 / FP32 split for
-// the current precision mode and the unit prefixes of both launches.
+// the current precision mode and the unit prefixes of both launches, under
+// the engine's static thresholds; the unit totals and quartet counts come
+// back to the host.
 static int build_units(gtf_fock_dev *f)
 {
     cudaStream_t st = f->stream;
     const double cut2 = f->prec == GTF_PREC_MIXED ? f->fp32_cutoff * f->fp32_cutoff : 0.0;
-    void *d_tmp = nullptr;
-    size_t tmp_cap = 0;
+    const int nt = (int)f->h_ut.size();
+    for (auto &u : f->h_ut) {
+        u.tol2 = f->tolscr2;
+        u.cut2 = cut2;
+    }
     for (int c = 0; c < NCLSPAIR; c++) {
         ClassPairTask &t = f->tasks[c];
         t.nunits = t.nunits32 = 0;
         t.nquart = t.nquart32 = 0.0;
+    }
+    f->lists_dyn = 0;
+    if (nt == 0) return GTF_OK;
+    CK(cudaMemcpyAsync(f->d_ut_static, f->h_ut.data(), sizeof(UnitTask) * nt, cudaMemcpyHostToDevice, st));
+    int r = run_units(f->d_ut_static, nt, f->ut_nidx, f->ut_nbras, f->nsm, st);
+    if (r) return r;
+    gtf_note_launches(3);
+    std::vector<std::vector<int>> nk(NCLSPAIR), n64(NCLSPAIR);
+    for (int c = 0; c < NCLSPAIR; c++) {
+        ClassPairTask &t = f->tasks[c];
         if (t.nbra == 0 || t.nketcls == 0) continue;
         const int nidx = t.nbra * GTF_NBKT;
-        SegStarts seg;
-        for (int bk = 0; bk <= GTF_NBKT; bk++) seg.s[bk] = t.seg[bk];
-        const int nb1 = t.nbra + 1;
-        long long *d_units;
-        CK(cudaMalloc(&d_units, sizeof(long long) * 2 * nb1));
-        k_count_kets<<<(nidx + 255) / 256, 256, 0, st>>>(f->d_pair_v, t.bra_start, t.nbra, t.ket_start, seg,
-                                                        t.X == t.Y, f->tolscr2, cut2, t.d_nket, t.d_n64);
-        CK(cudaGetLastError());
-        k_pack_units<<<(nb1 + 255) / 256, 256, 0, st>>>(t.nbra, t.d_nket, t.d_n64, t.d_cum64, t.d_cum32, d_units,
-                                                       d_units + nb1);
-        CK(cudaGetLastError());
-        size_t b4 = 0;
-        CK(cub::DeviceScan::ExclusiveSum(nullptr, b4, d_units, t.d_unit_prefix, nb1, st));
-        if (b4 > tmp_cap) {
-            if (d_tmp) cudaFree(d_tmp);
-            tmp_cap = b4;
-            CK(cudaMalloc(&d_tmp, tmp_cap));
-        }
-        b4 = tmp_cap;
-        CK(cub::DeviceScan::ExclusiveSum(d_tmp, b4, d_units, t.d_unit_prefix, nb1, st));
-        b4 = tmp_cap;
-        CK(cub::DeviceScan::ExclusiveSum(d_tmp, b4, d_units + nb1, t.d_unit_prefix32, nb1, st));
-        std::vector<int> nk(nidx), n64(nidx);
+        nk[c].resize(nidx);
+        n64[c].resize(nidx);
         CK(cudaMemcpyAsync(&t.nunits, t.d_unit_prefix + t.nbra, sizeof(long long), cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(&t.nunits32, t.d_unit_prefix32 + t.nbra, sizeof(long long), cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(nk.data(), t.d_nket, sizeof(int) * nidx, cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(n64.data(), t.d_n64, sizeof(int) * nidx, cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        cudaFree(d_units);
+        CK(cudaMemcpyAsync(nk[c].data(), t.d_nket, sizeof(int) * nidx, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(n64[c].data(), t.d_n64, sizeof(int) * nidx, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    for (int c = 0; c < NCLSPAIR; c++) {
+        ClassPairTask &t = f->tasks[c];
+        if (t.nbra == 0 || t.nketcls == 0) continue;
         double q = 0.0, q32 = 0.0;
-        for (int i = 0; i < nidx; i++) {
-            q += nk[i];
-            q32 += nk[i] - n64[i];
+        long long bound = 0;
+        for (int i = 0; i < t.nbra; i++) {
+            long long all = 0;
+            for (int b = 0; b < GTF_NBKT; b++) {
+                const int k = i * GTF_NBKT + b;
+                q += nk[c][k];
+                q32 += nk[c][k] - n64[c][k];
+                if (b > 0) all += nk[c][k];
+            }
+            bound += (all + 31) / 32;
         }
         t.nquart = q;
         t.nquart32 = q32;
+        // thresholds at or above tol2 select a subset of these kets, in one
+        // launch or split between two (one more unit per bra at most)
+        t.nunits_bound = bound + t.nbra;
     }
-    if (d_tmp) cudaFree(d_tmp);
+    // the units of this engine's shard (all of them when not sharded)
+    f->shard_work = 0.0;
+    for (int c = 0; c < NCLSPAIR; c++) {
+        const int r2 = shard_bounds(f, c, nk[c], n64[c]);
+        if (r2) return r2;
+    }
     return GTF_OK;
+}
+
+// Plain builds use the static task lists: restore them after incremental
+// builds overwrote the arrays (no allocation; one host wait).
+static int static_lists(gtf_fock_dev *f)
+{
+    return f->lists_dyn ? build_units(f) : GTF_OK;
 }
 
 extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max_numdmat,
@@ -1013,9 +1367,10 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
 
     // ---- Schwarz values of every shell pair (M >= N), one class at a time ----
     const size_t n2 = (size_t)ns * ns;
+    DevTemps tmps;
     DALLOC(f->d_sq, n2);
     unsigned long long *d_gmax;
-    DALLOC(d_gmax, 1);
+    TALLOC(tmps, d_gmax, 1);
     CK(cudaMemsetAsync(d_gmax, 0, sizeof(unsigned long long), st));
     {
         std::vector<int2> mn[NCLS];
@@ -1036,10 +1391,10 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
             int *d_off;
             PairRec *d_pr;
             double *d_pp;
-            CK(cudaMalloc(&d_mn, sizeof(int2) * n));
-            CK(cudaMalloc(&d_off, sizeof(int) * n));
-            CK(cudaMalloc(&d_pr, sizeof(PairRec) * n));
-            CK(cudaMalloc(&d_pp, sizeof(double) * 5 * npp_cls[c]));
+            TALLOC(tmps, d_mn, n);
+            TALLOC(tmps, d_off, n);
+            TALLOC(tmps, d_pr, n);
+            TALLOC(tmps, d_pp, 5 * npp_cls[c]);
             CK(cudaMemcpyAsync(d_mn, mn[c].data(), sizeof(int2) * n, cudaMemcpyHostToDevice, st));
             CK(cudaMemcpyAsync(d_off, off[c].data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
             k_screen_prep<<<(n + 127) / 128, 128, 0, st>>>(bd, d_mn, d_off, n, d_pr, d_pp, npp_cls[c]);
@@ -1049,32 +1404,31 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
             if (launch_screen(c, d_pr, pps, d_mn, n, ns, b->pure, f->d_sq, d_gmax, st) != 0)
                 CK(cudaGetLastError());
             CK(cudaStreamSynchronize(st));
-            cudaFree(d_mn);
-            cudaFree(d_off);
-            cudaFree(d_pr);
-            cudaFree(d_pp);
+            tmps.drop(d_mn);
+            tmps.drop(d_off);
+            tmps.drop(d_pr);
+            tmps.drop(d_pp);
         }
     }
     unsigned long long hmax = 0;
     CK(cudaMemcpyAsync(&hmax, d_gmax, sizeof(hmax), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     memcpy(&f->maxvalue, &hmax, sizeof(double));
-    cudaFree(d_gmax);
-    f->dev_bytes -= sizeof(unsigned long long);
+    tmps.drop(d_gmax);
     const double eta = f->tolscr2 / f->maxvalue;
 
     // ---- reference CSR list (row-major scan + scatter) ----
     int *d_flags, *d_pos;
-    DALLOC(d_flags, n2);
-    DALLOC(d_pos, n2);
+    TALLOC(tmps, d_flags, n2);
+    TALLOC(tmps, d_pos, n2);
     const unsigned g2 = (unsigned)((n2 + 255) / 256);
     k_csr_flags<<<g2, 256, 0, st>>>(f->d_sq, ns, eta, d_flags);
     CK(cudaGetLastError());
     size_t tmp_bytes = 0;
     CK(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, d_flags, d_pos, (int)n2, st));
-    void *d_tmp = nullptr;
+    char *d_tmp = nullptr;
     size_t tmp_cap = tmp_bytes;
-    CK(cudaMalloc(&d_tmp, tmp_cap));
+    TALLOC(tmps, d_tmp, tmp_cap);
     CK(cub::DeviceScan::ExclusiveSum(d_tmp, tmp_bytes, d_flags, d_pos, (int)n2, st));
     int last_pos = 0, last_flag = 0;
     CK(cudaMemcpyAsync(&last_pos, d_pos + n2 - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1094,15 +1448,15 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
     f->npairs = nnz;
     unsigned long long *d_kval, *d_kval2;
     int *d_kcls, *d_kcls2, *d_idx, *d_idx2, *d_pair_n, *d_pair_off, *d_kept;
-    DALLOC(d_kval, nnz);
-    DALLOC(d_kval2, nnz);
-    DALLOC(d_kcls, nnz);
-    DALLOC(d_kcls2, nnz);
-    DALLOC(d_idx, nnz);
-    DALLOC(d_idx2, nnz);
-    DALLOC(d_pair_n, nnz + 1);
-    DALLOC(d_pair_off, nnz + 1);
-    DALLOC(d_kept, nnz);
+    TALLOC(tmps, d_kval, nnz);
+    TALLOC(tmps, d_kval2, nnz);
+    TALLOC(tmps, d_kcls, nnz);
+    TALLOC(tmps, d_kcls2, nnz);
+    TALLOC(tmps, d_idx, nnz);
+    TALLOC(tmps, d_idx2, nnz);
+    TALLOC(tmps, d_pair_n, nnz + 1);
+    TALLOC(tmps, d_pair_off, nnz + 1);
+    TALLOC(tmps, d_kept, nnz);
     const unsigned gp = (unsigned)((nnz + 255) / 256 > 0 ? (nnz + 255) / 256 : 1);
     if (nnz > 0) {
         k_sort_keys<<<gp, 256, 0, st>>>(f->d_shellvalue, f->d_shellid, f->d_shellrid, f->d_sh_L, nnz,
@@ -1115,9 +1469,9 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
         CK(cub::DeviceRadixSort::SortPairs(nullptr, b2, d_kcls, d_kcls2, d_idx2, d_idx, nnz, 0, 7, st));
         size_t need = b1 > b2 ? b1 : b2;
         if (need > tmp_cap) {
-            cudaFree(d_tmp);
+            tmps.drop(d_tmp);
             tmp_cap = need;
-            CK(cudaMalloc(&d_tmp, tmp_cap));
+            TALLOC(tmps, d_tmp, tmp_cap);
         }
         b1 = tmp_cap;
         CK(cub::DeviceRadixSort::SortPairs(d_tmp, b1, d_kval, d_kval2, d_idx, d_idx2, nnz, 0, 64, st));
@@ -1137,9 +1491,9 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
     size_t b3 = 0;
     CK(cub::DeviceScan::ExclusiveSum(nullptr, b3, d_pair_n, d_pair_off, nnz + 1, st));
     if (b3 > tmp_cap) {
-        cudaFree(d_tmp);
+        tmps.drop(d_tmp);
         tmp_cap = b3;
-        CK(cudaMalloc(&d_tmp, tmp_cap));
+        TALLOC(tmps, d_tmp, tmp_cap);
     }
     b3 = tmp_cap;
     CK(cub::DeviceScan::ExclusiveSum(d_tmp, b3, d_pair_n, d_pair_off, nnz + 1, st));
@@ -1195,7 +1549,8 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
         }
     }
     {
-        const int r = build_units(f);
+        int r = make_unit_tasks(f);
+        if (r == GTF_OK) r = build_units(f);
         if (r != GTF_OK) return r;
     }
     cp = 0;
@@ -1251,20 +1606,9 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
             flops += cf;
         }
         f->eri_flops = flops;
+        f->h_pair_n.assign(hn.begin(), hn.begin() + nnz);
     }
-    cudaFree(d_tmp);
-    cudaFree(d_flags);
-    cudaFree(d_pos);
-    cudaFree(d_kval);
-    cudaFree(d_kval2);
-    cudaFree(d_kcls);
-    cudaFree(d_kcls2);
-    cudaFree(d_idx2);
-    cudaFree(d_pair_n);
-    cudaFree(d_pair_off);
-    cudaFree(d_kept);
-    cudaFree(d_idx);
-    f->dev_bytes -= n2 * 2 * sizeof(int) + (size_t)nnz * (2 * 8 + 4 * 4) + (size_t)(nnz + 1) * 8;
+    // the set-up temporaries are released here (tmps) and on every error return
 
     // ---- matrices ----
     const size_t nn = (size_t)b->nbf * b->nbf, nnc = (size_t)b->nbf_cart * b->nbf_cart;
@@ -1293,25 +1637,30 @@ extern "C" void gtf_fock_destroy(gtf_fock_dev_t *f)
                     f->d_cart2shell, f->d_Z, f->d_sh_xyz, f->d_alpha, f->d_coef, f->d_atom_xyz, f->d_sq,
                     f->d_shellptr, f->d_shellid, f->d_shellrid, f->d_shellvalue, f->d_pairs, f->d_pair_v,
                     f->d_pp, f->d_pp32, f->d_counters, f->d_D, f->d_Dc, f->d_Fj, f->d_Fk, f->d_F, f->d_J, f->d_K,
-                    f->d_S, f->d_X, f->d_H, f->d_Ds, f->d_Da, f->d_Dca, f->d_Fka};
-    for (void *p : ptrs)
-        if (p) cudaFree(p);
+                    f->d_Ds, f->d_Da, f->d_Dca, f->d_Fka, f->d_ut_static, f->d_ut_dyn, f->d_Dprev, f->d_Dd,
+                    f->d_dyn};
+    for (void *p : ptrs) dev_free(p);   // all from dalloc
     for (int c = 0; c < NCLSPAIR; c++) {
-        if (f->tasks[c].d_nket) cudaFree(f->tasks[c].d_nket);
-        if (f->tasks[c].d_unit_prefix) cudaFree(f->tasks[c].d_unit_prefix);
-        if (f->tasks[c].d_n64) cudaFree(f->tasks[c].d_n64);
-        if (f->tasks[c].d_cum64) cudaFree(f->tasks[c].d_cum64);
-        if (f->tasks[c].d_cum32) cudaFree(f->tasks[c].d_cum32);
-        if (f->tasks[c].d_unit_prefix32) cudaFree(f->tasks[c].d_unit_prefix32);
+        dev_free(f->tasks[c].d_nket);
+        dev_free(f->tasks[c].d_unit_prefix);
+        dev_free(f->tasks[c].d_n64);
+        dev_free(f->tasks[c].d_cum64);
+        dev_free(f->tasks[c].d_cum32);
+        dev_free(f->tasks[c].d_unit_prefix32);
     }
+    // the one-electron matrices come from onee.cu's own allocations
+    void *onee[] = {f->d_S, f->d_X, f->d_H};
+    for (void *p : onee)
+        if (p) cudaFree(p);
     if (f->d_host_stage) cudaFreeHost(f->d_host_stage);
-    cudaEventDestroy(f->ev0);
-    cudaEventDestroy(f->ev1);
-    cudaEventDestroy(f->ev2);
-    cudaEventDestroy(f->ev3);
+    // a partly created engine has some of these unset: destroying a null
+    // handle would leave a stale error for the next cudaGetLastError
+    cudaEvent_t evs[] = {f->ev0, f->ev1, f->ev2, f->ev3};
+    for (cudaEvent_t e : evs)
+        if (e) cudaEventDestroy(e);
     for (int c = 0; c <= NCLSPAIR; c++)
         if (f->ev_cls[c]) cudaEventDestroy(f->ev_cls[c]);
-    cudaStreamDestroy(f->stream);
+    if (f->stream) cudaStreamDestroy(f->stream);
     delete f;
 }
 
@@ -1345,8 +1694,9 @@ extern "C" int gtf_fock_get_csr(gtf_fock_dev_t *f, int *shellptr, int *shellid, 
 static int put_block(gtf_fock_dev *f, double *dmat, int n, int r0, int r1, int c0, int c1, int stride,
                      const double *host)
 {
-    if (r0 < 0 || c0 < 0 || r1 >= n || c1 >= n || r1 < r0 || c1 < c0) return GTF_ERR_INVALID;
+    if (r0 < 0 || c0 < 0 || r1 >= n || c1 >= n || r1 < r0 || c1 < c0 || !host) return GTF_ERR_INVALID;
     const int nr = r1 - r0 + 1, nc = c1 - c0 + 1;
+    if (stride < nc) return GTF_ERR_INVALID;   // rows of the host block would overlap
     CK(cudaMemcpy2DAsync(dmat + (size_t)r0 * n + c0, sizeof(double) * n, host, sizeof(double) * stride,
                          sizeof(double) * nc, nr, cudaMemcpyHostToDevice, f->stream));
     CK(cudaStreamSynchronize(f->stream));
@@ -1356,8 +1706,9 @@ static int put_block(gtf_fock_dev *f, double *dmat, int n, int r0, int r1, int c
 static int get_block(gtf_fock_dev *f, const double *dmat, int n, int r0, int r1, int c0, int c1, int stride,
                      double *host)
 {
-    if (r0 < 0 || c0 < 0 || r1 >= n || c1 >= n || r1 < r0 || c1 < c0) return GTF_ERR_INVALID;
+    if (r0 < 0 || c0 < 0 || r1 >= n || c1 >= n || r1 < r0 || c1 < c0 || !host) return GTF_ERR_INVALID;
     const int nr = r1 - r0 + 1, nc = c1 - c0 + 1;
+    if (stride < nc) return GTF_ERR_INVALID;   // rows of the host block would overlap
     CK(cudaMemcpy2DAsync(host, sizeof(double) * stride, dmat + (size_t)r0 * n + c0, sizeof(double) * n,
                          sizeof(double) * nc, nr, cudaMemcpyDeviceToHost, f->stream));
     CK(cudaStreamSynchronize(f->stream));
@@ -1430,15 +1781,110 @@ extern "C" void gtf_shard_range(long long nunits, int r, int n, long long *lo, l
     *hi = nunits * (r + 1) / n;
 }
 
+// Contiguous split of n weighted items (w[i] >= 0) into nshards: shard r
+// gets [lo, hi), lo the first item whose preceding weight reaches W r /
+// nshards (W the total).  The shards tile [0, n) in order, each within one
+// item's weight of W / nshards; every rank computes the same split from the
+// same weights.
+extern "C" void gtf_shard_split(const double *w, long long n, int r, int nshards, long long *lo, long long *hi)
+{
+    if (n <= 0) {
+        *lo = *hi = 0;
+        return;
+    }
+    if (nshards <= 1) {
+        *lo = 0;
+        *hi = n;
+        return;
+    }
+    double W = 0.0;
+    for (long long i = 0; i < n; i++) W += w[i];
+    const double t0 = W * (double)r / nshards, t1 = W * (double)(r + 1) / nshards;
+    long long a = -1, b = -1;
+    double pre = 0.0;
+    for (long long i = 0; i <= n; i++) {
+        if (a < 0 && (r == 0 || pre >= t0)) a = i;
+        if (b < 0 && r + 1 < nshards && pre >= t1) b = i;
+        if (i < n) pre += w[i];
+    }
+    *lo = a < 0 ? n : a;
+    *hi = (r + 1 == nshards || b < 0) ? n : b;
+    if (*hi < *lo) *hi = *lo;
+}
+
+// Unit ranges of this engine's shard, per (class pair, part): the bras of
+// the launch are split by the work model (primitive quartets x FLOPs per
+// primitive quartet + per-quartet contraction and digestion FLOPs), so the
+// shards get equal work rather than equal unit counts (a d-class bra with
+// 8 primitive pairs costs tens of times an s-class one).  nk / n64: the
+// launch's ket counts per (bra, segment) for the current thresholds.
+static int shard_bounds(gtf_fock_dev *f, int c, const std::vector<int> &nk, const std::vector<int> &n64)
+{
+    ClassPairTask &t = f->tasks[c];
+    for (int p = 0; p < 2; p++) {
+        f->shard_lo[c][p] = 0;
+        f->shard_hi[c][p] = p ? t.nunits32 : t.nunits;
+    }
+    if (t.nbra == 0 || t.nketcls == 0) return GTF_OK;
+    if (f->nshards <= 1) {
+        f->shard_work += t.flops;
+        return GTF_OK;
+    }
+    const int la = k_cls_la[t.X], lb = k_cls_lb[t.X], lc = k_cls_la[t.Y], ld = k_cls_lb[t.Y];
+    double cpart;
+    const double per_prim = class_flops_per_prim(t.X, t.Y, &cpart);
+    const double ns_ = (double)(f->pure && la == 2 ? 5 : ncart(la)) * (f->pure && lb == 2 ? 5 : ncart(lb)) *
+                       (f->pure && lc == 2 ? 5 : ncart(lc)) * (f->pure && ld == 2 ? 5 : ncart(ld));
+    std::vector<double> kpre(t.nketcls + 1, 0.0);
+    for (int j = 0; j < t.nketcls; j++) kpre[j + 1] = kpre[j] + f->h_pair_n[t.ket_start + j];
+    std::vector<long long> up(t.nbra + 1);
+    std::vector<double> w(t.nbra);
+    for (int p = 0; p < 2; p++) {
+        const long long nu = p ? t.nunits32 : t.nunits;
+        if (nu == 0) continue;
+        CK(cudaMemcpy(up.data(), p ? t.d_unit_prefix32 : t.d_unit_prefix, sizeof(long long) * (t.nbra + 1),
+                      cudaMemcpyDeviceToHost));
+        for (int i = 0; i < t.nbra; i++) {
+            const double kb = f->h_pair_n[t.bra_start + i];
+            double wi = 0.0;
+            for (int b = 1; b < GTF_NBKT; b++) {   // segment 0 has no units
+                const int k = i * GTF_NBKT + b;
+                const int j0 = t.seg[b] + (p ? n64[k] : 0), j1 = t.seg[b] + (p ? nk[k] : n64[k]);
+                wi += kb * (kpre[j1] - kpre[j0]) * per_prim + (cpart + 12.0 * ns_) * (j1 - j0);
+            }
+            w[i] = wi;
+        }
+        long long blo = 0, bhi = 0;
+        gtf_shard_split(w.data(), t.nbra, f->shard, f->nshards, &blo, &bhi);
+        f->shard_lo[c][p] = up[blo];
+        f->shard_hi[c][p] = up[bhi];
+        for (long long i = blo; i < bhi; i++) f->shard_work += w[i];
+    }
+    return GTF_OK;
+}
+
 // A sharded build: every class launch of this engine covers shard `shard` of
-// `nshards` of its units, so the F, J, K of the build are this shard's part;
-// the parts of all shards sum to the whole build.  nshards <= 1 restores
-// the whole build.
+// `nshards` of its units (contiguous, split by the work model), so the F, J,
+// K of the build are this shard's part; the parts of all shards sum to the
+// whole build.  nshards <= 1 restores the whole build.
 extern "C" int gtf_fock_set_shard(gtf_fock_dev_t *f, int shard, int nshards)
 {
     if (nshards < 0 || (nshards > 1 && (shard < 0 || shard >= nshards))) return GTF_ERR_INVALID;
+    if (nshards > 1 && f->incr) {
+        snprintf(g_errbuf, sizeof(g_errbuf), "a sharded engine cannot use incremental builds");
+        return GTF_ERR_INVALID;
+    }
     f->shard = nshards > 1 ? shard : 0;
     f->nshards = nshards > 1 ? nshards : 0;
+    return build_units(f);   // recomputes the shard's unit ranges
+}
+
+// Model FLOPs of this engine's shard of a build (the whole build when not
+// sharded): the work the shard split balances.
+extern "C" int gtf_fock_shard_work(gtf_fock_dev_t *f, double *work)
+{
+    if (!f || !work) return GTF_ERR_INVALID;
+    *work = f->nshards > 1 ? f->shard_work : f->eri_flops;
     return GTF_OK;
 }
 
@@ -1480,21 +1926,30 @@ static void fill_launch(const gtf_fock_dev *f, int c, int part, const double *D,
 // range, then (mixed precision) the FP32 tail.  counters holds
 // GTF_MAX_SLICES zeroed slots per (class pair, part), one per slice launch.
 // Returns the number of launches, or -1 on a launch error.
+// dyn: the task lists were rebuilt on the device for this build (incremental
+// builds): every part that can have work is launched, with its unit count
+// read by the kernel and its grid sized for the bound.
 static int launch_class(const gtf_fock_dev *f, int c, const double *D, double *Fj, double *Fk,
-                        unsigned long long *counters, cudaStream_t st, int konly = 0)
+                        unsigned long long *counters, cudaStream_t st, int konly = 0, bool dyn = false)
 {
     const ClassPairTask &t = f->tasks[c];
     int n = 0;
     for (int part = 0; part < 2; part++) {
-        const long long nu = part ? t.nunits32 : t.nunits;
-        if (nu == 0) continue;
+        const long long nu = dyn ? ((part == 0 || f->prec == GTF_PREC_MIXED) ? t.nunits_bound : 0)
+                                 : (part ? t.nunits32 : t.nunits);
+        if (nu == 0 || t.nbra == 0 || t.nketcls == 0) continue;
         FockGrid g;
         memset(&g, 0, sizeof(g));
         fill_launch(f, c, part, D, Fj, Fk, g.one, konly);
         g.nmol = 1;
         long long lo = 0, hi = nu;
-        gtf_shard_range(nu, f->shard, f->nshards, &lo, &hi);
-        if (hi <= lo) continue;
+        if (dyn) {
+            g.nunits_dev = (part ? t.d_unit_prefix32 : t.d_unit_prefix) + t.nbra;
+        } else if (f->nshards > 1) {
+            lo = f->shard_lo[c][part];
+            hi = f->shard_hi[c][part];
+            if (hi <= lo) continue;
+        }
         g.nunits = hi - lo;
         g.unit_lo = lo;
         g.counter = counters + (size_t)(2 * c + part) * GTF_MAX_SLICES;
@@ -1512,9 +1967,125 @@ static int launch_class(const gtf_fock_dev *f, int c, const double *D, double *F
     return n;
 }
 
+// One incremental build of density 0 (see k_delta): the change of D since
+// the previous build goes through device-rebuilt task lists, and F, J, K
+// receive its part (or are overwritten on a full build).
+static int fock_compute_incremental(gtf_fock_dev *f)
+{
+    cudaStream_t st = f->stream;
+    const int nbf = f->nbf, nbfc = f->nbf_cart;
+    const size_t nn = (size_t)nbf * nbf, nnc = (size_t)nbfc * nbfc;
+    const bool need_tr = f->pure && nbfc != nbf;
+    const int full = (f->incr_since == 0 || f->incr_since >= f->incr_period) ? 1 : 0;
+    const double cut2 = f->prec == GTF_PREC_MIXED ? f->fp32_cutoff * f->fp32_cutoff : 0.0;
+    f->lists_dyn = 1;
+    CK(cudaEventRecord(f->ev0, st));
+    CK(cudaMemsetAsync(&f->d_dyn->dmax_bits, 0, sizeof(unsigned long long), st));
+    {
+        const size_t nb = (nn + 255) / 256;
+        const unsigned g = (unsigned)(nb < (size_t)f->nsm * 8 ? (nb < 1 ? 1 : nb) : (size_t)f->nsm * 8);
+        k_delta<<<g, 256, 0, st>>>(f->d_D, f->d_Dprev, f->d_Dd, nn, full, f->d_dyn);
+        CK(cudaGetLastError());
+    }
+    k_dyn_thresholds<<<1, 1, 0, st>>>(f->d_dyn, f->tolscr2, cut2, f->incr_tau * f->incr_tau,
+                                      f->prec == GTF_PREC_MIXED ? f->fp32_cutoff * f->fp32_cutoff : 0.0, full);
+    CK(cudaGetLastError());
+    int r = run_units(f->d_ut_dyn, (int)f->h_ut.size(), f->ut_nidx, f->ut_nbras, f->nsm, st);
+    if (r) return r;
+    gtf_note_launches(5);
+    const double *Dc = f->d_Dd;
+    if (need_tr) {
+        dim3 g((nbfc + 127) / 128, nbfc);
+        k_d_to_cart<<<g, 128, 0, st>>>(f->d_Dd, f->d_Dc, f->d_cart2shell, f->d_sh_L, f->d_f_start, f->d_fc_start,
+                                       nbf, nbfc, f->pure);
+        CK(cudaGetLastError());
+        Dc = f->d_Dc;
+        gtf_note_launches(1);
+    }
+    CK(cudaMemsetAsync(f->d_Fj, 0, sizeof(double) * nnc, st));
+    CK(cudaMemsetAsync(f->d_Fk, 0, sizeof(double) * nnc, st));
+    CK(cudaMemsetAsync(f->d_counters, 0, sizeof(unsigned long long) * 2 * NCLSPAIR * GTF_MAX_SLICES, st));
+    CK(cudaEventRecord(f->ev1, st));
+    for (int c = 0; c < NCLSPAIR; c++) {
+        CK(cudaEventRecord(f->ev_cls[c], st));
+        const int n = launch_class(f, c, Dc, f->d_Fj, f->d_Fk, f->d_counters, st, 0, true);
+        if (n < 0) return GTF_ERR_CUDA;
+        gtf_note_launches(n);
+    }
+    CK(cudaEventRecord(f->ev_cls[NCLSPAIR], st));
+    CK(cudaEventRecord(f->ev2, st));
+    dim3 g2((nbf + 127) / 128, nbf);
+    k_f_to_sph<<<g2, 128, 0, st>>>(f->d_Fj, f->d_Fk, f->d_F, f->d_J, f->d_K, f->d_sph2shell, f->d_sh_L,
+                                   f->d_f_start, f->d_fc_start, nbf, nbfc, f->pure, nullptr, &f->d_dyn->acc);
+    CK(cudaGetLastError());
+    gtf_note_launches(1);
+    CK(cudaEventRecord(f->ev3, st));
+    CK(cudaEventSynchronize(f->ev3));
+    float tot = 0.0f, eri = 0.0f;
+    CK(cudaEventElapsedTime(&tot, f->ev0, f->ev3));
+    CK(cudaEventElapsedTime(&eri, f->ev1, f->ev2));
+    for (int c = 0; c < NCLSPAIR; c++) {
+        float mc = 0.0f;
+        CK(cudaEventElapsedTime(&mc, f->ev_cls[c], f->ev_cls[c + 1]));
+        f->ms_cls[c] = mc;
+    }
+    f->ms_total = tot;
+    f->ms_eri = eri;
+    f->ms_other = tot - eri;
+    f->incr_since = full ? 1 : f->incr_since + 1;
+    return GTF_OK;
+}
+
+// Incremental builds on (on = 1) or off: tau is the threshold on Schwarz
+// bound x max |D_k - D_k-1| below which a quartet of the change is dropped
+// (<= 0: the engine's Schwarz threshold), period the number of builds
+// between full ones (>= 1; 1 = every build full).  Density 0 only, symmetric
+// densities, unsharded engines.  The next build is a full one.
+extern "C" int gtf_fock_set_incremental(gtf_fock_dev_t *f, int on, double tau, int period)
+{
+    if (!f || f->max_numdmat < 1) return GTF_ERR_INVALID;
+    if (!on) {
+        f->incr = 0;
+        return GTF_OK;
+    }
+    if (f->nosymm || f->nshards > 1 || period < 1) {
+        snprintf(g_errbuf, sizeof(g_errbuf), "incremental builds need a symmetric, unsharded engine and period >= 1");
+        return GTF_ERR_INVALID;
+    }
+    if (!f->d_Dprev) {
+        const size_t nn = (size_t)f->nbf * f->nbf;
+        DALLOC(f->d_Dprev, nn);
+        DALLOC(f->d_Dd, nn);
+    }
+    f->incr = 1;
+    f->incr_tau = tau > 0.0 ? tau : f->tolscr;
+    f->incr_period = period;
+    f->incr_since = 0;
+    return GTF_OK;
+}
+
+// Statistics of the last incremental build: quartets evaluated in FP64 and in
+// FP32, and max |D_k - D_k-1| (0 on a full build).
+extern "C" int gtf_fock_incremental_stats(gtf_fock_dev_t *f, double *nq64, double *nq32, double *dmax)
+{
+    if (!f || !f->d_dyn) return GTF_ERR_INVALID;
+    DynState h;
+    CK(cudaMemcpyAsync(&h, f->d_dyn, sizeof(h), cudaMemcpyDeviceToHost, f->stream));
+    CK(cudaStreamSynchronize(f->stream));
+    if (nq64) *nq64 = (double)h.nq64;
+    if (nq32) *nq32 = (double)h.nq32;
+    if (dmax) *dmax = h.acc ? __longlong_as_double_host(h.dmax_bits) : 0.0;
+    return GTF_OK;
+}
+
 extern "C" int gtf_fock_compute(gtf_fock_dev_t *f, int numdmat)
 {
     if (numdmat <= 0 || numdmat > f->max_numdmat) return GTF_ERR_INVALID;
+    if (f->incr && numdmat == 1 && !f->nosymm && f->nshards <= 1) return fock_compute_incremental(f);
+    {
+        const int r = static_lists(f);
+        if (r) return r;
+    }
     cudaStream_t st = f->stream;
     const int nbf = f->nbf, nbfc = f->nbf_cart;
     const size_t nn = (size_t)nbf * nbf, nnc = (size_t)nbfc * nbfc;
@@ -1607,7 +2178,11 @@ extern "C" int gtf_fock_autotune(gtf_fock_dev_t *f, int reps)
 {
     if (reps < 1) reps = 1;
     if (f->nosymm) return GTF_ERR_INVALID;
+    const int incr = f->incr;
+    f->incr = 0;   // tune on a plain build (static task lists)
     int r = gtf_fock_compute(f, 1);
+    f->incr = incr;
+    if (incr) f->incr_since = 0;   // the plain build replaced F: restart the sum
     if (r != GTF_OK) return r;
     cudaStream_t st = f->stream;
     const bool need_tr = f->pure && f->nbf_cart != f->nbf;
@@ -1825,6 +2400,13 @@ extern "C" int gtf_fock_compute_fixed(gtf_fock_dev_t *f, const double *dev_D, do
         snprintf(g_errbuf, sizeof(g_errbuf), "allocation-free Fock build: non-symmetric densities are not supported");
         return GTF_ERR_INVALID;
     }
+    if (f->nshards > 1) {
+        // the launches of a sharded engine cover one shard's units only; this
+        // entry point promises the whole F
+        snprintf(g_errbuf, sizeof(g_errbuf), "allocation-free Fock build: engine is sharded (%d of %d)", f->shard,
+                 f->nshards);
+        return GTF_ERR_INVALID;
+    }
     const int nbf = f->nbf, nbfc = f->nbf_cart;
     if (nbfc > GTF_FIXED_MAX_FUNCS || nbf > GTF_FIXED_MAX_FUNCS) {
         snprintf(g_errbuf, sizeof(g_errbuf),
@@ -1841,6 +2423,7 @@ extern "C" int gtf_fock_compute_fixed(gtf_fock_dev_t *f, const double *dev_D, do
     }
     double *scr = nullptr;
     int r = fixed_scratch(dev, &scr);
+    if (r == GTF_OK) r = static_lists(f);
     if (r) return r;
     cudaStream_t st = f->stream;
     const size_t nn = (size_t)nbf * nbf, nnc = (size_t)nbfc * nbfc;
@@ -1884,8 +2467,61 @@ struct XformDesc {
     const double *D;
     double *Dc, *Fj, *Fk, *F, *J, *K;
     const int *cart2shell, *sph2shell, *sh_L, *f_start, *fc_start;
+    const int *acc;   // incremental builds: add to the previous result when *acc (null: overwrite)
     int nbf, nbfc, pure, need_tr;
 };
+
+// Incremental builds of a batch: per molecule, the density change and the
+// thresholds (see k_delta); full[m] (written by the host before each build)
+// selects a full build of molecule m.
+struct DeltaDesc {
+    const double *D;
+    double *Dprev, *Dd;
+    DynState *dyn;
+    size_t n;
+    double tol2, cut2, tau2, c2;
+};
+
+__global__ void k_b_dzero(const DeltaDesc *__restrict__ ds, int M)
+{
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m < M) ds[m].dyn->dmax_bits = 0ULL;
+}
+
+// molecule blockIdx.y
+__global__ void k_b_delta(const DeltaDesc *__restrict__ ds, const int *__restrict__ full)
+{
+    const DeltaDesc &d = ds[blockIdx.y];
+    delta_range(d.D, d.Dprev, d.Dd, d.n, full[blockIdx.y], d.dyn, (size_t)blockIdx.x * blockDim.x + threadIdx.x,
+                (size_t)gridDim.x * blockDim.x);
+}
+
+__global__ void k_b_thresholds(const DeltaDesc *__restrict__ ds, const int *__restrict__ full, int M)
+{
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m < M) dyn_thresholds(ds[m].dyn, ds[m].tol2, ds[m].cut2, ds[m].tau2, ds[m].c2, full[m]);
+}
+
+// The unit prefix over the molecules of each batched launch, from the
+// molecules' unit totals of this build (one thread per launch).
+struct PrefixDesc {
+    const long long *const *tot;   // [n] pointers to the members' totals
+    long long *prefix;             // [n + 1]
+    int n;
+};
+
+__global__ void k_b_molprefix(const PrefixDesc *__restrict__ ps, int np)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= np) return;
+    const PrefixDesc p = ps[k];
+    long long a = 0;
+    p.prefix[0] = 0;
+    for (int m = 0; m < p.n; m++) {
+        a += *p.tot[m];
+        p.prefix[m + 1] = a;
+    }
+}
 
 // molecule blockIdx.z: Dc = T D T^T (when spherical), Fj = Fk = 0
 __global__ void k_b_prep(const XformDesc *__restrict__ xs)
@@ -1909,7 +2545,7 @@ __global__ void k_b_post(const XformDesc *__restrict__ xs)
     for (int m = blockIdx.y; m < x.nbf; m += gridDim.y) {
         if (n >= x.nbf) continue;
         f_to_sph_elem(x.Fj, x.Fk, x.F, x.J, x.K, x.sph2shell, x.sh_L, x.f_start, x.fc_start, x.nbf, x.nbfc, x.pure,
-                      m, n);
+                      m, n, nullptr, x.acc != nullptr && *x.acc != 0);
     }
 }
 
@@ -1931,6 +2567,19 @@ struct gtf_fock_batch {
     int solo_base[NCLSPAIR][2];     // first counter block of the part's solo launches
     int ncounter_blocks;            // GTF_MAX_SLICES counters each
     unsigned long long *d_counters;
+    // incremental builds (every engine has them on): task lists rebuilt on
+    // the device each build, unit counts read by the kernels
+    int dyn;
+    DeltaDesc *d_delta;
+    int *d_full, *h_full;
+    UnitTask *d_ut;
+    int ut_n;
+    long long ut_nidx, ut_nbras;
+    PrefixDesc *d_pdesc;
+    const long long **d_ptot;
+    int npdesc;
+    size_t maxnn;
+    std::vector<const long long *> solo_tot[NCLSPAIR][2];
 };
 
 // A molecule whose units in one launch reach this many (32 quartets each)
@@ -1972,6 +2621,12 @@ extern "C" void gtf_fock_batch_destroy(gtf_fock_batch_t *b)
     cudaStreamSynchronize(b->st);
     cudaFree(b->d_xf);
     cudaFree(b->d_counters);
+    if (b->d_delta) cudaFree(b->d_delta);
+    if (b->d_full) cudaFree(b->d_full);
+    if (b->h_full) cudaFreeHost(b->h_full);
+    if (b->d_ut) cudaFree(b->d_ut);
+    if (b->d_pdesc) cudaFree(b->d_pdesc);
+    if (b->d_ptot) cudaFree(b->d_ptot);
     for (int c = 0; c < NCLSPAIR; c++)
         for (int p = 0; p < 2; p++) {
             cudaFree(b->d_desc[c][p]);
@@ -2002,7 +2657,36 @@ extern "C" int gtf_fock_batch_create(gtf_fock_dev_t *const *engines, int M, void
     memset(b->d_prefix, 0, sizeof(b->d_prefix));
     b->d_xf = nullptr;
     b->d_counters = nullptr;
+    b->dyn = 0;
+    b->d_delta = nullptr;
+    b->d_full = b->h_full = nullptr;
+    b->d_ut = nullptr;
+    b->d_pdesc = nullptr;
+    b->d_ptot = nullptr;
+    b->npdesc = 0;
+    b->ut_n = 0;
+    b->maxnn = 0;
     b->M = M;
+    // incremental builds are all or nothing in a batch
+    {
+        int ninc = 0;
+        for (int m = 0; m < M; m++) ninc += (engines[m] && engines[m]->incr) ? 1 : 0;
+        if (ninc != 0 && ninc != M) {
+            snprintf(g_errbuf, sizeof(g_errbuf), "batch mixes engines with and without incremental builds");
+            delete b;
+            return GTF_ERR_INVALID;
+        }
+        b->dyn = ninc == M;
+        for (int m = 0; m < M; m++) {
+            if (!engines[m]) continue;
+            if (b->dyn) {
+                engines[m]->lists_dyn = 1;
+            } else if (static_lists(engines[m]) != GTF_OK) {
+                delete b;
+                return GTF_ERR_CUDA;
+            }
+        }
+    }
     b->eng.assign(engines, engines + M);
     b->st = (cudaStream_t)stream;
     b->nsm = engines[0]->nsm;
@@ -2015,7 +2699,9 @@ extern "C" int gtf_fock_batch_create(gtf_fock_dev_t *const *engines, int M, void
             return GTF_ERR_INVALID;
         }
         XformDesc &x = xf[m];
-        x.D = f->d_D;
+        memset(&x, 0, sizeof(x));
+        x.D = b->dyn ? f->d_Dd : f->d_D;
+        x.acc = b->dyn ? &f->d_dyn->acc : nullptr;
         x.Dc = f->d_Dc;
         x.Fj = f->d_Fj;
         x.Fk = f->d_Fk;
@@ -2045,27 +2731,37 @@ extern "C" int gtf_fock_batch_create(gtf_fock_dev_t *const *engines, int M, void
         for (int c = 0; c < NCLSPAIR; c++) tot += engines[m]->tasks[c].nunits + engines[m]->tasks[c].nunits32;
         big[m] = tot >= GTF_SOLO_MOL_UNITS;
     }
+    // (incremental batches) the members' unit totals, per batched launch
+    std::vector<PrefixDesc> pdesc;
+    std::vector<std::vector<const long long *>> ptot;
+    std::vector<int> pdesc_cp;
     for (int c = 0; c < NCLSPAIR; c++)
         for (int p = 0; p < 2; p++) {
             std::vector<FockLaunch> d;
             std::vector<long long> pre(1, 0);
+            std::vector<const long long *> tots;
             b->solo_base[c][p] = nblocks;
             for (int m = 0; m < M; m++) {
                 gtf_fock_dev *f = engines[m];
                 const ClassPairTask &t = f->tasks[c];
-                const long long nu = p ? t.nunits32 : t.nunits;
-                if (nu == 0) continue;
+                // incremental: every part that can have work, sized by its bound
+                const long long nu = b->dyn ? ((p == 0 || f->prec == GTF_PREC_MIXED) ? t.nunits_bound : 0)
+                                            : (p ? t.nunits32 : t.nunits);
+                if (nu == 0 || t.nbra == 0 || t.nketcls == 0) continue;
                 const bool need_tr = f->pure && f->nbf_cart != f->nbf;
                 FockLaunch a;
-                fill_launch(f, c, p, need_tr ? f->d_Dc : f->d_D, f->d_Fj, f->d_Fk, a);
+                fill_launch(f, c, p, need_tr ? f->d_Dc : (b->dyn ? f->d_Dd : f->d_D), f->d_Fj, f->d_Fk, a);
+                const long long *tot = (p ? t.d_unit_prefix32 : t.d_unit_prefix) + t.nbra;
                 if (M > 1 && (nu >= solo_min || (big[m] && nu >= GTF_SOLO_MIN_UNITS))) {
                     b->solo[c][p].push_back(a);
                     b->solo_units[c][p].push_back(nu);
+                    b->solo_tot[c][p].push_back(tot);
                     nblocks++;
                     continue;
                 }
                 d.push_back(a);
                 pre.push_back(pre.back() + nu);
+                tots.push_back(tot);
             }
             b->nmol[c][p] = (int)d.size();
             b->total[c][p] = pre.back();
@@ -2075,7 +2771,73 @@ extern "C" int gtf_fock_batch_create(gtf_fock_dev_t *const *engines, int M, void
             CKB_(cudaMalloc(&b->d_prefix[c][p], sizeof(long long) * pre.size()));
             CKB_(cudaMemcpy(b->d_desc[c][p], d.data(), sizeof(FockLaunch) * d.size(), cudaMemcpyHostToDevice));
             CKB_(cudaMemcpy(b->d_prefix[c][p], pre.data(), sizeof(long long) * pre.size(), cudaMemcpyHostToDevice));
+            if (b->dyn) {
+                PrefixDesc q;
+                q.tot = nullptr;
+                q.prefix = b->d_prefix[c][p];
+                q.n = (int)tots.size();
+                pdesc.push_back(q);
+                ptot.push_back(tots);
+            }
         }
+    if (b->dyn) {
+        // per-molecule delta descriptors and the concatenated task set
+        std::vector<DeltaDesc> dd(M);
+        std::vector<UnitTask> ut;
+        long long nidx = 0, nbras = 0;
+        for (int m = 0; m < M; m++) {
+            gtf_fock_dev *f = engines[m];
+            DeltaDesc &x = dd[m];
+            x.D = f->d_D;
+            x.Dprev = f->d_Dprev;
+            x.Dd = f->d_Dd;
+            x.dyn = f->d_dyn;
+            x.n = (size_t)f->nbf * f->nbf;
+            x.tol2 = f->tolscr2;
+            x.cut2 = f->prec == GTF_PREC_MIXED ? f->fp32_cutoff * f->fp32_cutoff : 0.0;
+            x.tau2 = f->incr_tau * f->incr_tau;
+            x.c2 = x.cut2;
+            if (x.n > b->maxnn) b->maxnn = x.n;
+            for (const UnitTask &u0 : f->h_ut) {
+                UnitTask u = u0;
+                u.dyn = f->d_dyn;
+                u.idx0 = nidx;
+                u.bra0 = nbras;
+                nidx += (long long)u.nbra * GTF_NBKT;
+                nbras += u.nbra;
+                ut.push_back(u);
+            }
+        }
+        b->ut_n = (int)ut.size();
+        b->ut_nidx = nidx;
+        b->ut_nbras = nbras;
+        CKB_(cudaMalloc(&b->d_delta, sizeof(DeltaDesc) * M));
+        CKB_(cudaMemcpy(b->d_delta, dd.data(), sizeof(DeltaDesc) * M, cudaMemcpyHostToDevice));
+        CKB_(cudaMalloc(&b->d_full, sizeof(int) * M));
+        CKB_(cudaMallocHost(&b->h_full, sizeof(int) * M));
+        for (int m = 0; m < M; m++) b->h_full[m] = 1;
+        CKB_(cudaMemcpy(b->d_full, b->h_full, sizeof(int) * M, cudaMemcpyHostToDevice));
+        if (!ut.empty()) {
+            CKB_(cudaMalloc(&b->d_ut, sizeof(UnitTask) * ut.size()));
+            CKB_(cudaMemcpy(b->d_ut, ut.data(), sizeof(UnitTask) * ut.size(), cudaMemcpyHostToDevice));
+        }
+        size_t ntot = 0;
+        for (auto &v : ptot) ntot += v.size();
+        b->npdesc = (int)pdesc.size();
+        if (ntot > 0) {
+            CKB_(cudaMalloc(&b->d_ptot, sizeof(const long long *) * ntot));
+            std::vector<const long long *> flat;
+            for (size_t k = 0; k < ptot.size(); k++) {
+                pdesc[k].tot = b->d_ptot + flat.size();
+                flat.insert(flat.end(), ptot[k].begin(), ptot[k].end());
+            }
+            CKB_(cudaMemcpy(b->d_ptot, flat.data(), sizeof(const long long *) * ntot, cudaMemcpyHostToDevice));
+        }
+        if (b->npdesc > 0) {
+            CKB_(cudaMalloc(&b->d_pdesc, sizeof(PrefixDesc) * pdesc.size()));
+            CKB_(cudaMemcpy(b->d_pdesc, pdesc.data(), sizeof(PrefixDesc) * pdesc.size(), cudaMemcpyHostToDevice));
+        }
+    }
     b->ncounter_blocks = nblocks;
     CKB_(cudaMalloc(&b->d_counters, sizeof(unsigned long long) * (size_t)nblocks * GTF_MAX_SLICES));
     *out = b;
@@ -2084,10 +2846,43 @@ extern "C" int gtf_fock_batch_create(gtf_fock_dev_t *const *engines, int M, void
 
 // One Fock build of every engine of the batch; returns the number of kernels
 // launched (>= 0) or a negative error.  Stream-ordered: no host wait.
+// Incremental batches: full[m] != 0 makes molecule m's next build a full one
+// (copied to the device on the batch's stream, so a captured build replayed
+// afterwards reads it).
+extern "C" int gtf_fock_batch_set_full(gtf_fock_batch_t *b, const int *full)
+{
+    if (!b || !b->dyn || !full) return GTF_ERR_INVALID;
+    CK(cudaStreamSynchronize(b->st));   // the pinned flags may still be in flight
+    for (int m = 0; m < b->M; m++) b->h_full[m] = full[m] ? 1 : 0;
+    CK(cudaMemcpyAsync(b->d_full, b->h_full, sizeof(int) * b->M, cudaMemcpyHostToDevice, b->st));
+    return GTF_OK;
+}
+
 extern "C" int gtf_fock_batch_compute(gtf_fock_batch_t *b)
 {
     cudaStream_t st = b->st;
     int launches = 0;
+    if (b->dyn) {
+        // density changes, thresholds, task lists and launch prefixes of
+        // every molecule, all on the device
+        k_b_dzero<<<(b->M + 127) / 128, 128, 0, st>>>(b->d_delta, b->M);
+        CK(cudaGetLastError());
+        const size_t nb = (b->maxnn + 255) / 256;
+        dim3 g((unsigned)(nb < 64 ? (nb < 1 ? 1 : nb) : 64), b->M);
+        k_b_delta<<<g, 256, 0, st>>>(b->d_delta, b->d_full);
+        CK(cudaGetLastError());
+        k_b_thresholds<<<(b->M + 127) / 128, 128, 0, st>>>(b->d_delta, b->d_full, b->M);
+        CK(cudaGetLastError());
+        launches += 3;
+        const int r = run_units(b->d_ut, b->ut_n, b->ut_nidx, b->ut_nbras, b->nsm, st);
+        if (r) return r;
+        launches += 3;
+        if (b->npdesc > 0) {
+            k_b_molprefix<<<(b->npdesc + 127) / 128, 128, 0, st>>>(b->d_pdesc, b->npdesc);
+            CK(cudaGetLastError());
+            launches++;
+        }
+    }
     {
         dim3 g((b->maxnc + 127) / 128, b->maxnc < 1024 ? b->maxnc : 1024, b->M);
         k_b_prep<<<g, 128, 0, st>>>(b->d_xf);
@@ -2105,6 +2900,7 @@ extern "C" int gtf_fock_batch_compute(gtf_fock_batch_t *b)
                 g.one = b->solo[c][p][k];
                 g.nmol = 1;
                 g.nunits = b->solo_units[c][p][k];
+                if (b->dyn) g.nunits_dev = b->solo_tot[c][p][k];
                 g.counter = b->d_counters + (size_t)(b->solo_base[c][p] + (int)k) * GTF_MAX_SLICES;
                 g.nsm = b->nsm;
                 g.fp32 = p;
@@ -2125,6 +2921,7 @@ extern "C" int gtf_fock_batch_compute(gtf_fock_batch_t *b)
             g.mol_prefix = b->d_prefix[c][p];
             g.nmol = b->nmol[c][p];
             g.nunits = b->total[c][p];
+            if (b->dyn) g.nunits_dev = b->d_prefix[c][p] + b->nmol[c][p];
             g.counter = b->d_counters + (size_t)(2 * c + p) * GTF_MAX_SLICES;
             g.nsm = b->nsm;
             g.fp32 = p;
@@ -2168,6 +2965,7 @@ extern "C" int gtf_fock_batch_autotune(gtf_fock_batch_t *b, int reps)
                 g.one = b->solo[c][p][k];
                 g.nmol = 1;
                 g.nunits = b->solo_units[c][p][k];
+                if (b->dyn) g.nunits_dev = b->solo_tot[c][p][k];
                 g.counter = b->d_counters + (size_t)(b->solo_base[c][p] + (int)k) * GTF_MAX_SLICES;
                 g.nsm = b->nsm;
                 g.fp32 = p;
@@ -2182,6 +2980,7 @@ extern "C" int gtf_fock_batch_autotune(gtf_fock_batch_t *b, int reps)
             g.mol_prefix = b->d_prefix[c][p];
             g.nmol = b->nmol[c][p];
             g.nunits = b->total[c][p];
+            if (b->dyn) g.nunits_dev = b->d_prefix[c][p] + b->nmol[c][p];
             g.counter = b->d_counters + (size_t)(2 * c + p) * GTF_MAX_SLICES;
             g.nsm = b->nsm;
             g.fp32 = p;

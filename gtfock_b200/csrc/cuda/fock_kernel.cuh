@@ -59,7 +59,10 @@ struct FockGrid {
     const FockLaunch *mols;         // device array, nmol > 1
     const long long *mol_prefix;    // device, [nmol + 1] exclusive prefix of units
     int nmol;
-    long long nunits;               // all units of the launch
+    long long nunits;               // all units of the launch (with nunits_dev: an upper bound)
+    // task lists rebuilt on the device (incremental builds): the launch's
+    // unit count is read here when the kernel starts; null: nunits
+    const long long *nunits_dev;
     unsigned long long *counter;    // GTF_MAX_SLICES zeroed counters, one per slice launch
     int nsm;
     int fp32;                       // evaluate the integrals in FP32 (digestion stays FP64)
@@ -118,6 +121,10 @@ __global__ void __launch_bounds__(FOCK_THREADS,
     constexpr int S = fock_slice(LA, LB, LC, LD, sizeof(R) == 4 ? 1 : 0);
     constexpr int N = (NCD - CD0 < S) ? NCD - CD0 : S;
     __shared__ __align__(16) R tab[RysTab<R>::slen(NR)];
+    // the launch's unit count, kept in shared memory rather than a register
+    // across the integral loops (visible after the staging's barrier)
+    __shared__ unsigned long long s_nunits;
+    if (threadIdx.x == 0) s_nunits = (unsigned long long)(g.nunits_dev ? *g.nunits_dev : g.nunits);
     rys_stage<R, NR>(tab);
     const int lane = threadIdx.x & 31;
     // batched launches: per-warp slots for the claimed range of units and the
@@ -148,7 +155,7 @@ __global__ void __launch_bounds__(FOCK_THREADS,
                 u = __shfl_sync(GTF_FULL_MASK, c0, 0);
                 uend = u + claim;
             }
-            if (u >= (unsigned long long)g.nunits) break;
+            if (u >= *(volatile unsigned long long *)&s_nunits) break;
             uu = u;
             __syncwarp();
             if (lane == 0) {
@@ -160,7 +167,7 @@ __global__ void __launch_bounds__(FOCK_THREADS,
             unsigned long long c0 = 0;
             if (lane == 0) c0 = atomicAdd(counter, 1ULL);
             uu = __shfl_sync(GTF_FULL_MASK, c0, 0);
-            if (uu >= (unsigned long long)g.nunits) break;
+            if (uu >= *(volatile unsigned long long *)&s_nunits) break;
             uu += (unsigned long long)g.unit_lo;
         }
         // molecule of the unit (batched launches); the fields are read from

@@ -78,6 +78,11 @@ void gtf_fock_release_onee(gtf_fock_dev_t *f, int which);
 
 /* precision control and statistics */
 int gtf_fock_set_precision(gtf_fock_dev_t *f, int prec, double fp32_cutoff);
+/* incremental builds: F_k = F_k-1 + G[D_k - D_k-1], quartets of the change
+ * screened against tau / max |D_k - D_k-1|, a full build every `period`
+ * builds (density 0, symmetric, unsharded); statistics of the last build */
+int gtf_fock_set_incremental(gtf_fock_dev_t *f, int on, double tau, int period);
+int gtf_fock_incremental_stats(gtf_fock_dev_t *f, double *nq64, double *nq32, double *dmax);
 /* non-symmetric densities: F = 2 J[D] - K[D] exactly for a general D */
 int gtf_fock_set_nosymm(gtf_fock_dev_t *f, int on);
 int gtf_fock_last_timing(gtf_fock_dev_t *f, double *ms_total, double *ms_eri, double *ms_other);
@@ -88,12 +93,16 @@ int gtf_fock_eri_flops(gtf_fock_dev_t *f, double *flops);
 typedef struct gtf_fock_batch gtf_fock_batch_t;
 int gtf_fock_batch_create(gtf_fock_dev_t *const *engines, int M, void *stream, gtf_fock_batch_t **out);
 int gtf_fock_batch_compute(gtf_fock_batch_t *b);
+/* incremental batches: full[m] != 0 makes member m's next build a full one */
+int gtf_fock_batch_set_full(gtf_fock_batch_t *b, const int *full);
 void gtf_fock_batch_destroy(gtf_fock_batch_t *b);
 
 /* sharded builds (one molecule over several GPUs): every class launch covers
  * shard r of n of its units; the F of the shards sum to the whole build */
 int gtf_fock_set_shard(gtf_fock_dev_t *f, int shard, int nshards);
 void gtf_shard_range(long long nunits, int r, int n, long long *lo, long long *hi);
+void gtf_shard_split(const double *w, long long n, int r, int nshards, long long *lo, long long *hi);
+int gtf_fock_shard_work(gtf_fock_dev_t *f, double *work);
 
 /* launch-shape autotuning (process-wide table, see fock.cu): time candidate
  * shapes of every Fock launch of an engine / a batch on its current density

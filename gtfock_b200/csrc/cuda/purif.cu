@@ -180,7 +180,12 @@ __global__ void k_purif_stats(const double *__restrict__ D, const double *__rest
 // scal[6] = errnorm, scal[7] = c = tr(D2-D3)/tr(D-D2) (pscf/purif.c:394-440).
 // Where the reference would divide 0/0 (an exactly idempotent D) and write NaN
 // into D, the iteration stops instead: errnorm is reported as 0 and the
-// update below is skipped.
+// update below is skipped (c set to NaN).  It stops the same way when c is
+// far outside [0, 1]: with every eigenvalue of D in [0, 1], c lies in [0, 1];
+// far outside it the eigenvalues have left that interval and the cubic
+// update diverges (in the reference, to Inf and NaN within a few steps).
+#define PURIF_C_LO (-0.25)
+#define PURIF_C_HI 1.25
 __global__ void k_purif_finish(const double *__restrict__ part, int nblk, double *scal)
 {
     if (threadIdx.x != 0) return;
@@ -191,8 +196,9 @@ __global__ void k_purif_finish(const double *__restrict__ part, int nblk, double
         t2 += part[3 * b + 2];
     }
     const double c = t / t2;
-    scal[6] = isfinite(c) ? sqrt(e) : 0.0;
-    scal[7] = c;
+    const bool ok = isfinite(c) && c >= PURIF_C_LO && c <= PURIF_C_HI;
+    scal[6] = ok ? sqrt(e) : 0.0;
+    scal[7] = ok ? c : __longlong_as_double(0x7ff8000000000000LL);
 }
 
 // D update (pscf/purif.c:441-455)

@@ -92,6 +92,18 @@ extern "C" void gtf_note_launches(int n) { g_launches += (unsigned long long)n; 
 
 extern "C" unsigned long long gtf_launch_count(void) { return g_launches.load(); }
 
+extern "C" int gtf_device_memory(size_t *free_bytes, size_t *total_bytes)
+{
+    size_t fr = 0, to = 0;
+    if (cudaMemGetInfo(&fr, &to) != cudaSuccess) {
+        cudaGetLastError();
+        return GTF_ERR_CUDA;
+    }
+    if (free_bytes) *free_bytes = fr;
+    if (total_bytes) *total_bytes = to;
+    return GTF_OK;
+}
+
 // FP64 FMA throughput probe: FP64_CHAINS independent dependency chains per
 // thread keep the FP64 pipe busy; every FMA is 2 flops
 #define FP64_CHAINS 8

@@ -444,5 +444,25 @@ PFockStatus_t gtf_pfock_compute_noalloc(PFock_t pf, const double *dev_D, double 
     return map_err(e);
 }
 
+PFockStatus_t gtf_pfock_set_incremental(PFock_t pf, int on, double tau, int period)
+{
+    if (pf == NULL) return PFOCK_STATUS_INVALID_VALUE;
+    int e = gtf_fock_set_incremental(pf->dev, on, tau, period);
+    if (e != GTF_OK) PFOCK_PRINTF(1, "%s\n", gtf_last_error());
+    return map_err(e);
+}
+
+PFockStatus_t gtf_pfock_incremental_stats(PFock_t pf, double *nquart_fp64, double *nquart_fp32, double *dmax)
+{
+    if (pf == NULL) return PFOCK_STATUS_INVALID_VALUE;
+    return map_err(gtf_fock_incremental_stats(pf->dev, nquart_fp64, nquart_fp32, dmax));
+}
+
+PFockStatus_t gtf_pfock_shard_work(PFock_t pf, double *work)
+{
+    if (pf == NULL) return PFOCK_STATUS_INVALID_VALUE;
+    return map_err(gtf_fock_shard_work(pf->dev, work));
+}
+
 /* internal accessors for scf_driver.c */
 gtf_fock_dev_t *gtf_pfock_device(PFock_t pf) { return pf->dev; }

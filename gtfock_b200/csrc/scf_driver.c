@@ -34,6 +34,8 @@ struct gtf_scf {
     double *D0;          /* initial guess (host) */
     double *dD, *dF;     /* device-resident D and F (mode 1) */
     double etol;         /* stop when |E_k - E_k-1| < etol */
+    int incr, incr_period;   /* incremental Fock builds (restarted by every solve) */
+    double incr_tau;
     int last_mode;       /* where the last solve left D: 0 host, 1 device */
 };
 
@@ -127,6 +129,16 @@ int gtf_scf_set_options(gtf_scf_t *s, int prec_mode, double fp32_cutoff, double 
     return 0;
 }
 
+int gtf_scf_set_incremental(gtf_scf_t *s, int on, double tau, int period)
+{
+    if (!s) return -1;
+    if (gtf_pfock_set_incremental(s->pf, on, tau, period) != PFOCK_STATUS_SUCCESS) return -2;
+    s->incr = on ? 1 : 0;
+    s->incr_tau = tau;
+    s->incr_period = period;
+    return 0;
+}
+
 int gtf_scf_set_purification(gtf_scf_t *s, int mode)
 {
     if (!s || !s->pur) return -1;
@@ -164,6 +176,9 @@ int gtf_scf_solve(gtf_scf_t *s, int niters, int mode, double *energies, double *
     gtf_purif_dev_t *pd = (gtf_purif_dev_t *)pur->dev;
     gtf_purif_reset(pd);
     pur->len_diis = 0;
+    /* an incremental sum never carries over from the previous solve */
+    if (s->incr && gtf_pfock_set_incremental(s->pf, 1, s->incr_tau, s->incr_period) != PFOCK_STATUS_SUCCESS)
+        return -7;
     double t_fock = 0.0, t_diis = 0.0, t_pur = 0.0, h2d = 0.0, d2h = 0.0;
     const unsigned long long l0 = gtf_launch_count();
     const double t_start = wall();

@@ -5,8 +5,10 @@ data/; the GPU machines do not have that tree, so the element blocks needed by
 the synthetic molecules (alkanes, graphene flakes, water clusters) are copied
 here verbatim, header line ("spherical"/"cartesian") included.
 
-Run in a checkout that has the reference tree:
-    python gtfock_b200/data/extract_basis.py /root/reference/data
+Run with the reference tree's data/ directory as the argument (default: the
+data/ of $GTFOCK_REFERENCE, else of a checkout named `reference` beside this
+repository):
+    python gtfock_b200/data/extract_basis.py <reference>/data
 """
 import os
 import sys
@@ -36,8 +38,10 @@ def extract(src, dst):
 
 
 if __name__ == "__main__":
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/data"
     here = os.path.dirname(os.path.abspath(__file__))
+    repo = os.path.dirname(os.path.dirname(here))
+    default = os.environ.get("GTFOCK_REFERENCE") or os.path.join(os.path.dirname(repo), "reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.path.join(default, "data")
     for name in FILES:
         extract(os.path.join(ref, name), os.path.join(here, name))
         print("wrote", name)

@@ -11,8 +11,13 @@ iterations overlap with those of the jobs already running.
 
 run_stream() replays an arrival stream against the wall clock and returns,
 per request, its arrival, admission and completion times and its energies.
-run_sequential() serves the same stream one job at a time on the plain
-single-job GPU path (gtf_scf_*), FIFO, for comparison.
+run_sequential() serves the same stream one job at a time on the
+single-job GPU path (gtf_scf_*), FIFO -- by default the plain FP64 path, for
+comparison.
+
+Admission is by HBM footprint (Admission): the estimated bytes of a waiting
+request must fit the budget left by the jobs on the device, each counted at
+its measured size, and the device's free memory at that moment.
 """
 import os
 import tempfile
@@ -20,7 +25,7 @@ import time
 
 import numpy as np
 
-from . import Batch, SCFSolver
+from . import BasisSet, Batch, SCFSolver, device_memory
 from . import molecules as mol
 
 
@@ -36,13 +41,46 @@ class Request:
         self.finished = None
         self.energies = None
         self.slot = None
+        self.cancelled = False
 
 
-def footprint_bytes(nbf):
-    """Device bytes of one job: batch buffers plus the Fock engine's matrices
-    (D, F, J, K, S, X, H, Cartesian scratch) and pair data (bounded by 64 nbf^2
-    doubles for the bases used here)."""
-    return Batch.job_bytes(nbf) + 8 * 64 * nbf * nbf
+def footprint_bytes(nbf, incremental=False):
+    """Estimated device bytes of one job before it is set up: batch buffers
+    plus the Fock engine's matrices (D, F, J, K, S, X, H, Cartesian scratch),
+    pair data and task lists (bounded by 64 nbf^2 doubles for the bases used
+    here), plus the previous density and the density change of incremental
+    builds.  Once a job runs, the server holds its measured bytes instead."""
+    return Batch.job_bytes(nbf) + 8 * (64 + (3 if incremental else 0)) * nbf * nbf
+
+
+class Admission:
+    """HBM-footprint admission.
+
+    A request is admitted when its footprint fits the budget left (what the
+    admitted jobs hold counted against `budget`) and, at that moment, the
+    device's free memory less `reserve` (room for the set-up's temporaries).
+    The budget defaults to the device's free memory when the server starts,
+    less the reserve.  `free_fn` returns the device's free bytes (default:
+    cudaMemGetInfo through gtf_device_memory)."""
+
+    def __init__(self, budget=None, reserve=2 << 30, free_fn=None):
+        self.free_fn = free_fn or (lambda: device_memory()[0])
+        self.reserve = int(reserve)
+        self.budget = int(self.free_fn() - self.reserve) if budget is None else int(budget)
+        self.held = {}
+
+    @property
+    def used(self):
+        return sum(self.held.values())
+
+    def fits(self, nbytes):
+        return self.used + nbytes <= self.budget and nbytes + self.reserve <= self.free_fn()
+
+    def hold(self, key, nbytes):
+        self.held[key] = int(nbytes)
+
+    def release(self, key):
+        self.held.pop(key, None)
 
 
 class _Lane:
@@ -67,16 +105,24 @@ class SCFServer:
     the large lane takes one step -- so small jobs are not held to the pace of
     a 1000-function molecule, while the large ones keep progressing."""
 
-    def __init__(self, slots=64, mem_budget=64 << 30, precision=1, fp32_cutoff=1e-6, max_iters=30,
-                 etol=1e-6, tolscr=1e-10, lanes=((400, None), (None, None)), share=0.5):
+    def __init__(self, slots=64, mem_budget=None, precision=1, fp32_cutoff=1e-6, max_iters=30,
+                 etol=1e-6, tolscr=1e-10, lanes=((400, None), (None, None)), share=0.5,
+                 incremental=False, incr_tau=0.0, incr_period=8, reserve=2 << 30, free_fn=None):
+        self.admission = Admission(mem_budget, reserve, free_fn)
         self.lanes = [_Lane(m, n if n else slots) for m, n in lanes]
-        self.mem_budget = mem_budget
+        self.incremental = bool(incremental)
+        if self.incremental:
+            for ln in self.lanes:
+                ln.batch.set_incremental(True, incr_tau, incr_period)
         self.share = share
         self.kw = dict(tolscr=tolscr, precision=precision, fp32_cutoff=fp32_cutoff, max_iters=max_iters,
                        etol=etol)
-        self.mem_used = 0
         self.credit = 0.0
         self.tmp = tempfile.mkdtemp(prefix="gtf_serve_")
+
+    @property
+    def mem_used(self):
+        return self.admission.used
 
     @property
     def live(self):
@@ -87,22 +133,45 @@ class SCFServer:
             r.xyz = mol.write_xyz(r.atoms, os.path.join(self.tmp, r.name + ".xyz"), r.name)
         return r.xyz
 
+    def _nbf(self, r):
+        """The request's basis size (from its basis and geometry when not given)."""
+        if r.nbf is None:
+            b = BasisSet(mol.basis_file(r.basis), self._xyz(r))
+            r.nbf = b.nbf
+        return r.nbf
+
     def _lane(self, r):
         for ln in self.lanes:
-            if ln.fits(r.nbf or 1):
+            if ln.fits(self._nbf(r)):
                 return ln
         return self.lanes[-1]
 
+    def footprint(self, r):
+        return footprint_bytes(self._nbf(r), self.incremental)
+
     def can_admit(self, r):
         ln = self._lane(r)
-        return len(ln.live) < ln.slots and self.mem_used + footprint_bytes(r.nbf or 1) <= self.mem_budget
+        return len(ln.live) < ln.slots and self.admission.fits(self.footprint(r))
 
     def admit(self, r, now):
         ln = self._lane(r)
         r.slot = ln.batch.add(mol.basis_file(r.basis), self._xyz(r), **self.kw)
         r.admitted = now
         ln.live[r.slot] = r
-        self.mem_used += footprint_bytes(r.nbf or 1)
+        # the job's measured device bytes replace the estimate
+        self.admission.hold(id(r), ln.batch.job_device_bytes(r.slot))
+
+    def cancel(self, r):
+        """Withdraw a live request between steps: its slot and memory are
+        freed; the other jobs continue unaffected."""
+        for ln in self.lanes:
+            if ln.live.get(r.slot) is r:
+                ln.live.pop(r.slot)
+                ln.batch.remove(r.slot)
+                self.admission.release(id(r))
+                r.cancelled = True
+                return True
+        return False
 
     def _pick(self):
         busy = [ln for ln in self.lanes if ln.live]
@@ -136,7 +205,7 @@ class SCFServer:
                 r.energies = e
                 r.finished = now_fn()
                 ln.batch.remove(s)
-                self.mem_used -= footprint_bytes(r.nbf or 1)
+                self.admission.release(id(r))
                 done.append(r)
         return done
 
@@ -170,11 +239,15 @@ def run_stream(requests, server):
         elif pending:
             time.sleep(max(0.0, min(0.01, pending[0].arrival - now())))
         elif waiting:
-            raise RuntimeError("request %s does not fit the server" % waiting[0].name)
+            raise RuntimeError("request %s (%d functions, %.2f GB estimated) does not fit the device memory "
+                               "budget of %.2f GB" % (waiting[0].name, waiting[0].nbf or 0,
+                                                      server.footprint(waiting[0]) / 1e9,
+                                                      server.admission.budget / 1e9))
     return finished
 
 
-def run_sequential(requests, max_iters=30, etol=1e-6, tolscr=1e-10):
+def run_sequential(requests, max_iters=30, etol=1e-6, tolscr=1e-10, precision=0, fp32_cutoff=0.0,
+                   incremental=False, incr_tau=0.0, incr_period=8):
     """The same stream on the plain FP64 single-job GPU path, FIFO: each job's
     service time (set-up + solve) is measured alone; its completion time is
     max(arrival, previous completion) + service."""
@@ -185,7 +258,9 @@ def run_sequential(requests, max_iters=30, etol=1e-6, tolscr=1e-10):
         xyz = r.xyz or mol.write_xyz(r.atoms, os.path.join(tmp, r.name + ".xyz"), r.name)
         t1 = time.perf_counter()
         s = SCFSolver(mol.basis_file(r.basis), xyz, tolscr=tolscr)
-        s.set_options(precision=0, etol=etol)
+        s.set_options(precision=precision, fp32_cutoff=fp32_cutoff, etol=etol)
+        if incremental:
+            s.set_incremental(True, incr_tau, incr_period)
         e, _ = s.solve(niters=max_iters)
         s.close()
         service = time.perf_counter() - t1

@@ -4,7 +4,8 @@ The reference splits the quartet task space of a build over MPI ranks in a
 2-D (M-block x P-block) grid, accumulates F in Global Arrays and reduces it
 (pfock/pfock.c:22-154, 1373-1669).  Here every rank builds one shard of
 every class launch's quartet units on its own GPU (PFock.set_shard: a
-contiguous slice of each launch's unit range, gtf_shard_range), and one
+contiguous slice of each launch's unit range, its bras split by their work
+model with gtf_shard_split), and one
 all-reduce over the ranks' torch.distributed group sums the parts into F
 -- NCCL over NVLink for device matrices, gloo for host arrays.  D is the
 same on every rank (the SCF state is replicated, as in the reference where
@@ -22,9 +23,21 @@ from . import PFock, load
 
 
 def shard_range(nunits, shard, nshards):
-    """Units [lo, hi) of shard `shard` of `nshards` of a launch of `nunits`."""
+    """Units [lo, hi) of shard `shard` of `nshards` of a launch of `nunits`
+    equal units."""
     lo, hi = ctypes.c_longlong(), ctypes.c_longlong()
     load().gtf_shard_range(int(nunits), int(shard), int(nshards), ctypes.byref(lo), ctypes.byref(hi))
+    return lo.value, hi.value
+
+
+def shard_split(weights, shard, nshards):
+    """Items [lo, hi) of shard `shard` of `nshards` for items of the given
+    weights: the library's contiguous weighted split (gtf_shard_split), the
+    one a sharded engine applies to each launch's bras."""
+    w = np.ascontiguousarray(weights, dtype=np.float64)
+    lo, hi = ctypes.c_longlong(), ctypes.c_longlong()
+    load().gtf_shard_split(w.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), int(w.size), int(shard),
+                           int(nshards), ctypes.byref(lo), ctypes.byref(hi))
     return lo.value, hi.value
 
 
@@ -80,6 +93,9 @@ class ShardedFock:
         import torch
         if not (D.is_cuda and D.dtype == torch.float64 and D.is_contiguous() and D.shape == (self.nbf, self.nbf)):
             raise ValueError("D must be a contiguous float64 CUDA tensor of shape (nbf, nbf)")
+        # the engine reads D on its own stream, which is not ordered after
+        # torch's: D must be complete before the build starts
+        torch.cuda.current_stream(D.device).synchronize()
         ptr = self.pf.compute_dev(D.data_ptr())
         F = torch.as_tensor(_DeviceMatrix(ptr, self.nbf), device=D.device)
         return allreduce_fock(F, self.group)

@@ -54,10 +54,19 @@ PFockStatus_t gtf_pfock_set_precision(PFock_t pfock, int mode, double fp32_cutof
  * pfock/pfock.c:22-154 becomes a split of each class's unit range), so
  * PFock_getMat / gtf_pfock_compute_dev return this rank's part of F; the
  * parts of the n ranks sum to the whole F (one all-reduce per build).
- * n <= 1 restores the whole build.  gtf_shard_range gives the units
- * [lo, hi) of shard r of n for a launch of `nunits`. */
+ * n <= 1 restores the whole build.  The split is contiguous and weighted:
+ * each launch's bras are divided by gtf_shard_split on their work model
+ * (primitive quartets x Rys-model FLOPs per primitive quartet, plus the
+ * per-quartet contraction and digestion), so the shards get equal work.
+ * gtf_shard_split: items [lo, hi) of shard r of nshards for n items of
+ * weights w (contiguous, in order, each shard within one item's weight of
+ * the mean).  gtf_shard_range: the same for equal weights (units [lo, hi)
+ * of a launch of `nunits`).  gtf_pfock_shard_work: model FLOPs of this
+ * engine's shard of a build (the whole build when not sharded). */
 PFockStatus_t gtf_pfock_set_shard(PFock_t pfock, int shard, int nshards);
+void gtf_shard_split(const double *w, long long n, int r, int nshards, long long *lo, long long *hi);
 void gtf_shard_range(long long nunits, int r, int n, long long *lo, long long *hi);
+PFockStatus_t gtf_pfock_shard_work(PFock_t pfock, double *work);
 
 /* Launch-shape autotuning.  gtf_pfock_autotune times, for every class pair
  * and precision part of this engine's Fock build (on the density last put),
@@ -78,12 +87,33 @@ int gtf_tune_load(const char *path);
 void gtf_tune_clear(void);
 int gtf_tune_entries(int *rows, int max_rows);
 
+/* Incremental Fock builds (no counterpart in the reference, whose builds
+ * always start from zero).  F is linear in D, so with on = 1 each build of
+ * density 0 computes only the change: F_k = F_k-1 + G[D_k - D_k-1].  A
+ * quartet of the change is dropped when its Schwarz bound times
+ * dmax = max |D_k - D_k-1| is below tau (tau <= 0: the engine's Schwarz
+ * threshold, so each dropped contribution is below what the plain build's
+ * screening drops), and evaluated in FP32 (mixed precision mode) when that
+ * product is below the FP32 cutoff.  The task lists are rebuilt on the device
+ * for every build.  Every `period` builds (and the first after this call) is
+ * a full one, which restarts the sum.  Symmetric densities on an unsharded
+ * engine only; on = 0 returns to plain builds.
+ * gtf_pfock_incremental_stats: quartets of the last build in FP64 and FP32,
+ * and its dmax (0 for a full build). */
+PFockStatus_t gtf_pfock_set_incremental(PFock_t pfock, int on, double tau, int period);
+PFockStatus_t gtf_pfock_incremental_stats(PFock_t pfock, double *nquart_fp64, double *nquart_fp32,
+                                          double *dmax);
+
 /* Quartets evaluated in FP32 under the current mode, and all quartets. */
 PFockStatus_t gtf_pfock_precision_stats(PFock_t pfock, double *nquart_fp32, double *nquart);
 
 /* Device-resident Fock build for callers that keep D on the GPU: dev_D is a
  * device pointer to the nbf x nbf density; the result stays on the device
- * (returned through *dev_F, valid until the next build). */
+ * (returned through *dev_F, valid until the next build).  The engine reads
+ * dev_D on its own stream, which is not ordered after the caller's streams:
+ * the kernels or copies that write dev_D must have completed before the call
+ * (synchronize the stream that produced it).  The call returns once F is
+ * complete. */
 PFockStatus_t gtf_pfock_compute_dev(PFock_t pfock, const double *dev_D,
                                     const double **dev_F);
 
@@ -96,11 +126,14 @@ PFockStatus_t gtf_pfock_compute_dev(PFock_t pfock, const double *dev_D,
  * F = J + K, both device pointers owned by the caller.  The scratch lives in
  * one static device array of about 5.9 MB that every GPU loading the library
  * keeps until exit; bases above 384 Cartesian functions are rejected with
- * PFOCK_STATUS_INVALID_VALUE.  All calls on a GPU share that array: calls
- * whose work overlaps on the GPU race and must be ordered by the caller.
- * The first call on a device looks up the array's address; make it before
- * any stream capture.  The engine must have been created on the current
- * device. */
+ * PFOCK_STATUS_INVALID_VALUE, and so are engines built with symm = 0 or
+ * sharded with gtf_pfock_set_shard (this call returns the whole F).  All
+ * calls on a GPU share that array: calls whose work overlaps on the GPU race
+ * and must be ordered by the caller.  As for gtf_pfock_compute_dev, dev_D
+ * must be complete on the device before the call, which returns once dev_F
+ * holds F.  The first call on a device looks up the array's address; make it
+ * before any stream capture.  The engine must have been created on the
+ * current device. */
 PFockStatus_t gtf_pfock_compute_noalloc(PFock_t pfock, const double *dev_D, double *dev_F);
 
 /* Native SCF driver: the loop of pscf/scf.c:329-459 (Fock build, energy,
@@ -122,6 +155,9 @@ int gtf_scf_nbf(gtf_scf_t *s);
  * convergence tolerance: a solve stops once |E_k - E_k-1| < etol (default
  * 1e-11).  0 on success. */
 int gtf_scf_set_options(gtf_scf_t *s, int prec_mode, double fp32_cutoff, double etol);
+/* Incremental Fock builds for this solver's engine (gtf_pfock_set_incremental);
+ * every solve starts with a full build.  0 on success. */
+int gtf_scf_set_incremental(gtf_scf_t *s, int on, double tau, int period);
 /* Purification products: mode 0 FP64 (default); mode 1 split-BF16 products
  * on the tensor cores (each FP64 factor as a sum of two BF16 matrices, FP32
  * accumulation) until the idempotency error stops falling, then FP64 steps
@@ -170,14 +206,31 @@ int gtf_batch_remove(gtf_batch_t *b, int slot);
 int gtf_batch_info(gtf_batch_t *b, int *nrunning, int *nused, double *ms_fock, double *ms_rest,
                    size_t *job_bytes);
 size_t gtf_batch_job_bytes(int nbf);
+/* Device bytes held by the job in `slot` (its batch buffers and its Fock
+ * engine); 0 for an empty slot. */
+size_t gtf_batch_job_device_bytes(gtf_batch_t *b, int slot);
 /* Accumulated statistics of a batch: [0] ms of the Fock builds, [1] of the
  * energies, [2] of DIIS, [3] of purification, [4] purification steps of the
  * batched jobs, [5] batch steps.  Writes min(n, 6) values, returns that count. */
 int gtf_batch_stats(gtf_batch_t *b, double *out, int n);
+/* Incremental Fock builds (gtf_pfock_set_incremental) for every job of the
+ * batch; set before the first gtf_batch_add (-2 otherwise).  0 on success. */
+int gtf_batch_set_incremental(gtf_batch_t *b, int on, double tau, int period);
 /* Tunes the batch's launch shapes for its current jobs (see
  * gtf_pfock_autotune); call between steps. */
 int gtf_batch_autotune(gtf_batch_t *b, int reps);
 void gtf_batch_destroy(gtf_batch_t *b);
+
+/* Free and total bytes of the current device (cudaMemGetInfo); 0 on success. */
+int gtf_device_memory(size_t *free_bytes, size_t *total_bytes);
+
+/* Test hook: the n-th device allocation of an engine's set-up from now on
+ * fails as an out-of-memory cudaMalloc would (n <= 0 disarms), so that the
+ * error paths of PFock_create can be checked for leaks. */
+void gtf_debug_fail_alloc(int n);
+/* Device allocations made through that hook's allocator (engine set-up and
+ * engine buffers) that have not been freed yet. */
+long long gtf_debug_live_allocs(void);
 
 /* Number of this library's own kernel launches so far (all threads). */
 unsigned long long gtf_launch_count(void);

@@ -207,6 +207,11 @@ int or_fock_build_sample(BasisSet_t basis, double tolscr, int nthreads,
                                stride, 0, count_only, usq_o, uitl_o);
 }
 
+static int fock_build_sel(BasisSet_t basis, double tolscr, int nthreads, const int *shellptr,
+                          const int *shellid, const int *shellrid, const double *shellvalue,
+                          const double *D, double *F, int stride, int offset, int lo, int hi,
+                          int count_only, double *usq_o, double *uitl_o, double *pair_cost);
+
 /* The MN pairs i with (i - first) % stride == offset: with stride = n and
  * offset = r, shard r of an n-way split of the build (the shards' F sum to
  * the whole F, since the symmetrisation at the end is linear). */
@@ -215,8 +220,40 @@ int or_fock_build_shard(BasisSet_t basis, double tolscr, int nthreads,
                         const double *shellvalue, const double *D, double *F,
                         int stride, int offset, int count_only, double *usq_o, double *uitl_o)
 {
+    return fock_build_sel(basis, tolscr, nthreads, shellptr, shellid, shellrid, shellvalue, D, F, stride,
+                          offset, 0, 1 << 30, count_only, usq_o, uitl_o, NULL);
+}
+
+/* The MN pairs lo <= i - first < hi: a contiguous shard of the build, as a
+ * partition of the MN-pair range into ranks' slices produces. */
+int or_fock_build_range(BasisSet_t basis, double tolscr, int nthreads,
+                        const int *shellptr, const int *shellid, const int *shellrid,
+                        const double *shellvalue, const double *D, double *F, int lo, int hi,
+                        double *usq_o, double *uitl_o)
+{
+    return fock_build_sel(basis, tolscr, nthreads, shellptr, shellid, shellrid, shellvalue, D, F, 1, 0, lo,
+                          hi, 0, usq_o, uitl_o, NULL);
+}
+
+/* Work of every MN pair of the build: the integrals of its screened quartets
+ * (sum of dM dN dP dQ, the uitl counter of pfock/fock_task.c:195-196 per
+ * pair), into cost[nnz]; no integrals are evaluated. */
+int or_fock_pair_cost(BasisSet_t basis, double tolscr, int nthreads,
+                      const int *shellptr, const int *shellid, const int *shellrid,
+                      const double *shellvalue, double *cost)
+{
+    return fock_build_sel(basis, tolscr, nthreads, shellptr, shellid, shellrid, shellvalue, NULL, NULL, 1,
+                          0, 0, 1 << 30, 1, NULL, NULL, cost);
+}
+
+static int fock_build_sel(BasisSet_t basis, double tolscr, int nthreads, const int *shellptr,
+                          const int *shellid, const int *shellrid, const double *shellvalue,
+                          const double *D, double *F, int stride, int offset, int lo, int hi,
+                          int count_only, double *usq_o, double *uitl_o, double *pair_cost)
+{
     if (stride < 1) stride = 1;
     if (offset < 0 || offset >= stride) return -1;
+    if (!count_only && (!D || !F)) return -1;
     const int nbf = basis->nbf;
     const int nshells = basis->nshells;
     const double tolscr2 = tolscr * tolscr;
@@ -238,6 +275,8 @@ int or_fock_build_shard(BasisSet_t basis, double tolscr, int nthreads,
         #pragma omp for schedule(dynamic)
         for (int i = startMN; i < endMN; i++) {
             if ((i - startMN) % stride != offset) continue;
+            if (i - startMN < lo || i - startMN >= hi) continue;
+            double cost_i = 0.0;
             const int M = shellrid[i];
             const int N = shellid[i];
             const double value1 = shellvalue[i];
@@ -260,6 +299,7 @@ int or_fock_build_shard(BasisSet_t basis, double tolscr, int nthreads,
                     double *ints;
                     usq += 1.0;
                     uitl += dimM * dimN * dimP * dimQ;
+                    cost_i += dimM * dimN * dimP * dimQ;
                     if (count_only) continue;
                     CInt_computeShellQuartet(basis, erd, nt, M, N, P, Q, &ints, &nints);
                     if (nints != 0) {
@@ -269,9 +309,17 @@ int or_fock_build_shard(BasisSet_t basis, double tolscr, int nthreads,
                     }
                 }
             }
+            if (pair_cost) pair_cost[i - startMN] = cost_i;
         }
     }
     CInt_destroyERD(erd);
+    if (count_only && !F) {
+        free(Jt);
+        free(Kt);
+        if (usq_o) *usq_o = usq;
+        if (uitl_o) *uitl_o = uitl;
+        return 0;
+    }
     /* reduce the per-thread copies (reduce_F, pfock/fock_task.c:257-324) */
     for (int t = 1; t < nthreads; t++) {
         for (size_t k = 0; k < nn; k++) {

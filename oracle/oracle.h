@@ -45,6 +45,13 @@ int or_fock_build_shard(BasisSet_t basis, double tolscr, int nthreads,
                         const int *shellptr, const int *shellid, const int *shellrid,
                         const double *shellvalue, const double *D, double *F,
                         int stride, int offset, int count_only, double *usq_o, double *uitl_o);
+int or_fock_build_range(BasisSet_t basis, double tolscr, int nthreads,
+                        const int *shellptr, const int *shellid, const int *shellrid,
+                        const double *shellvalue, const double *D, double *F, int lo, int hi,
+                        double *usq_o, double *uitl_o);
+int or_fock_pair_cost(BasisSet_t basis, double tolscr, int nthreads,
+                      const int *shellptr, const int *shellid, const int *shellrid,
+                      const double *shellvalue, double *cost);
 
 /* S, H_core and X = U diag(1/sqrt(lambda)) U^T
  * (pfock/one_electron.c:28-119, pfock/pfock.c:1782-1867). */

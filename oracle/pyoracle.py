@@ -53,6 +53,8 @@ def lib():
         L.or_fock_build.argtypes = [vp, d, i, ip, ip, ip, dp, dp, dp, dp, dp]
         L.or_fock_build_sample.argtypes = [vp, d, i, ip, ip, ip, dp, dp, dp, i, i, dp, dp]
         L.or_fock_build_shard.argtypes = [vp, d, i, ip, ip, ip, dp, dp, dp, i, i, i, dp, dp]
+        L.or_fock_build_range.argtypes = [vp, d, i, ip, ip, ip, dp, dp, dp, i, i, dp, dp]
+        L.or_fock_pair_cost.argtypes = [vp, d, i, ip, ip, ip, dp, dp]
         L.or_diis_create.argtypes = [i]
         L.or_diis_create.restype = vp
         L.or_diis_destroy.argtypes = [vp]
@@ -250,3 +252,34 @@ def scf(basis, tol, niters, nthreads=os.cpu_count()):
     if it < 0:
         raise RuntimeError("or_scf failed")
     return e[:it], F, D
+
+
+def _csr(basis, tol, scr, nthreads):
+    if scr is None:
+        scr = screening(basis, tol, nthreads)
+    shellptr, shellid, shellrid, shellvalue, _ = scr
+    return (np.ascontiguousarray(shellptr, dtype=np.int32), np.ascontiguousarray(shellid, dtype=np.int32),
+            np.ascontiguousarray(shellrid, dtype=np.int32), np.ascontiguousarray(shellvalue, dtype=np.float64))
+
+
+def pair_cost(basis, tol, scr=None, nthreads=os.cpu_count()):
+    """Integrals of the screened quartets of every MN pair of the build (the
+    pair's share of uitl), in the CSR order; no integrals evaluated."""
+    sptr, sid, srid, sval = _csr(basis, tol, scr, nthreads)
+    cost = np.zeros(max(sid.size, 1))
+    if lib().or_fock_pair_cost(basis.h, tol, nthreads, _ip(sptr), _ip(sid), _ip(srid), _dp(sval), _dp(cost)) != 0:
+        raise RuntimeError("or_fock_pair_cost failed")
+    return cost[:sid.size]
+
+
+def fock_build_range(basis, tol, D, lo, hi, scr=None, nthreads=os.cpu_count()):
+    """The part of F from the MN pairs lo <= i < hi (CSR order); the parts of a
+    partition of [0, nnz) sum to F."""
+    sptr, sid, srid, sval = _csr(basis, tol, scr, nthreads)
+    D = np.ascontiguousarray(D, dtype=np.float64)
+    F = np.zeros_like(D)
+    usq, uitl = ctypes.c_double(), ctypes.c_double()
+    if lib().or_fock_build_range(basis.h, tol, nthreads, _ip(sptr), _ip(sid), _ip(srid), _dp(sval), _dp(D), _dp(F),
+                                 int(lo), int(hi), ctypes.byref(usq), ctypes.byref(uitl)) != 0:
+        raise RuntimeError("or_fock_build_range failed")
+    return F

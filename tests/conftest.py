@@ -23,6 +23,27 @@ def load_golden(name):
     return dict(np.load(os.path.join(GOLDEN, name + ".npz"), allow_pickle=False))
 
 
+def large_density(n, seed):
+    """Seeded symmetric density-like matrix of the large-molecule fixtures
+    (tests/golden/make_large.py): diagonal 0.3, off-diagonal N(0, 0.05^2)
+    damped by exp(-|i-j|/20), symmetrised.  numpy's PCG64 stream is the same
+    on every machine, so the fixtures store the seed, not the matrix."""
+    rng = np.random.default_rng(seed)
+    A = rng.standard_normal((n, n)) * 0.05
+    idx = np.arange(n)
+    A *= np.exp(-np.abs(idx[:, None] - idx[None, :]) / 20.0)
+    return 0.5 * (A + A.T) + np.eye(n) * 0.3
+
+
+def unpack_upper(v, n):
+    """Symmetric n x n matrix from its row-major upper triangle."""
+    F = np.zeros((n, n))
+    iu = np.triu_indices(n)
+    F[iu] = v
+    F.T[iu] = v
+    return F
+
+
 def golden_xyz(case, tmpdir):
     """Write the fixture's geometry to an .xyz file; returns (gbs path, xyz path)."""
     from gtfock_b200 import molecules as mol

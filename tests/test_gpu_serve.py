@@ -1,0 +1,139 @@
+"""The serving loop (gtfock_b200/serve.py) on the GPU.
+
+* A seeded stream with fewer slots than requests: requests wait, join the
+  running batch as slots free up, and every result equals the same job run
+  alone (1e-9 Ha) -- the continuous-batching guarantee.
+* HBM-footprint admission: with a budget that holds one job, the jobs run
+  one after another; a request that can never fit is reported.
+* Cancellation: a request withdrawn between steps frees its slot and memory;
+  the others finish as they would without it.
+* Incremental builds in the server give the plain path's energies."""
+import numpy as np
+import pytest
+
+import gtfock_b200 as gb
+from gtfock_b200 import molecules as mol
+from gtfock_b200 import serve
+
+pytestmark = pytest.mark.gpu
+
+ETOL = 1e-8
+MAXIT = 40
+
+
+def _stream(gap=0.0):
+    """Six small requests, arriving `gap` seconds apart."""
+    items = [("w2", mol.water_cluster(2, 31), "6-31g"), ("c2", mol.alkane(2), "sto-3g"),
+             ("w3", mol.water_cluster(3, 32), "6-31g"), ("c3", mol.alkane(3), "6-31g"),
+             ("w4", mol.water_cluster(4, 33), "sto-3g"), ("c4", mol.alkane(4), "sto-3g")]
+    return [serve.Request(n, a, b, arrival=gap * k) for k, (n, a, b) in enumerate(items)]
+
+
+def _alone(r, tmp_path, incremental=False):
+    xyz = mol.write_xyz(r.atoms, str(tmp_path / (r.name + "_alone.xyz")))
+    bt = gb.Batch(1)
+    if incremental:
+        bt.set_incremental(True, 0.0, 8)
+    s = bt.add(mol.basis_file(r.basis), xyz, precision=0, max_iters=MAXIT, etol=ETOL)
+    bt.run()
+    e = bt.result(s)[0]
+    bt.close()
+    return e
+
+
+def _server(**kw):
+    args = dict(slots=2, precision=0, max_iters=MAXIT, etol=ETOL, lanes=((None, None),))
+    args.update(kw)
+    return serve.SCFServer(**args)
+
+
+def test_stream_results_equal_alone(tmp_path):
+    reqs = _stream()
+    srv = _server()
+    try:
+        done = serve.run_stream(reqs, srv)
+    finally:
+        srv.close()
+    assert sorted(r.name for r in done) == sorted(r.name for r in reqs)
+    # all arrive at once and two slots serve them: four wait for a slot, and
+    # two jobs are on the device together throughout
+    waited = [r for r in done if r.admitted > r.arrival]
+    assert len(waited) >= 4
+    overlaps = sum(1 for a in done for b in done if a is not b and a.admitted <= b.admitted < a.finished)
+    assert overlaps > 0
+    for r in done:
+        e_ref = _alone(r, tmp_path)
+        assert len(r.energies) == len(e_ref), r.name
+        assert np.abs(r.energies - e_ref).max() < 1e-9, r.name
+
+
+def test_admission_by_memory_budget(tmp_path):
+    # three requests of one size: a budget of one footprint holds one job
+    reqs = [serve.Request("w3_%d" % k, mol.water_cluster(3, 32), "6-31g", arrival=0.0) for k in range(3)]
+    probe = _server()
+    one = max(probe.footprint(r) for r in reqs)
+    probe.close()
+    srv = _server(slots=8, mem_budget=one)
+    try:
+        done = serve.run_stream(reqs, srv)
+    finally:
+        srv.close()
+    spans = sorted((r.admitted, r.finished) for r in done)
+    for (a0, f0), (a1, f1) in zip(spans, spans[1:]):
+        assert a1 >= f0 - 1e-6, "two jobs held memory at once under a one-job budget"
+    # a request larger than the whole budget is refused, not admitted
+    big = serve.Request("w40", mol.water_cluster(40, 7), "6-31g")
+    srv = _server(mem_budget=one)
+    assert one < srv.footprint(big)
+    try:
+        assert not srv.can_admit(big)
+        with pytest.raises(RuntimeError, match="does not fit"):
+            serve.run_stream([big], srv)
+    finally:
+        srv.close()
+
+
+def test_admission_uses_device_memory():
+    srv = _server()
+    try:
+        free, total = gb.device_memory()
+        assert 0 < srv.admission.budget <= free
+        assert total > free > 0
+    finally:
+        srv.close()
+
+
+def test_cancel_between_steps(tmp_path):
+    reqs = _stream()[:3]
+    srv = _server(slots=3)
+    try:
+        for r in reqs:
+            assert srv.can_admit(r)
+            srv.admit(r, 0.0)
+        held = srv.mem_used
+        srv.step(lambda: 0.0)
+        assert srv.cancel(reqs[1])
+        assert reqs[1].cancelled and srv.mem_used < held
+        assert len(srv.lanes[0].live) == 2
+        done = []
+        while srv.live:
+            done += srv.step(lambda: 1.0)
+        assert sorted(r.name for r in done) == sorted([reqs[0].name, reqs[2].name])
+        for r in done:
+            e_ref = _alone(r, tmp_path)
+            assert np.abs(r.energies - e_ref).max() < 1e-9
+        assert srv.mem_used == 0
+    finally:
+        srv.close()
+
+
+def test_incremental_server_matches_plain(tmp_path):
+    reqs = _stream()[:4]
+    srv = _server(incremental=True)
+    try:
+        done = serve.run_stream(reqs, srv)
+    finally:
+        srv.close()
+    for r in done:
+        e_ref = _alone(r, tmp_path)
+        assert abs(r.energies[-1] - e_ref[-1]) < 1e-8, r.name

@@ -1,5 +1,6 @@
 """Sharded Fock builds on the GPU: the parts of n shards built by the CUDA
-kernels sum to the whole F (FP64 and mixed precision), and the NCCL path of
+kernels sum to the whole F (FP64 and mixed precision), the shards' work is
+balanced by the weighted split, and the NCCL path of
 ShardedFock (device F all-reduced in place) gives the whole F on a one-rank
 group (the only group a one-GPU run can form)."""
 import os
@@ -46,6 +47,24 @@ def test_shard_against_oracle_fixture(tmp_path):
         pf.set_shard(r, 4)
         parts.append(pf.compute_fock(g["D"]))
     assert np.max(np.abs(sum(parts) - g["F"])) < 1e-10
+    pf.close()
+
+
+def test_shards_balanced_by_work(tmp_path):
+    """The shards of a launch are split by the work model, so their model
+    FLOPs sum to the whole build's and are within a few percent of each
+    other (a split by unit counts leaves d-heavy and s-heavy ranges)."""
+    xyz = mol.write_xyz(mol.alkane(12), str(tmp_path / "c12.xyz"))
+    b = gb.BasisSet(mol.basis_file("cc-pvdz"), xyz)
+    pf = gb.PFock(b, tolscr=1e-10)
+    whole = pf.shard_work()
+    for n in (2, 4):
+        work = []
+        for r in range(n):
+            pf.set_shard(r, n)
+            work.append(pf.shard_work())
+        assert abs(sum(work) - whole) < 1e-6 * whole
+        assert max(work) / min(work) < 1.05, work
     pf.close()
 
 

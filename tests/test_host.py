@@ -188,3 +188,30 @@ def test_tune_table_save_load(tmp_path):
     with pytest.raises(gb.GtfError):
         gb.tune_load(str(tmp_path / "missing.txt"))
     gb.tune_clear()
+
+
+def test_admission_by_footprint():
+    """HBM-footprint admission (gtfock_b200/serve.py): a request fits when its
+    footprint fits the budget left and the device's free memory less the
+    reserve; released jobs give their bytes back."""
+    from gtfock_b200.serve import Admission, footprint_bytes
+    free = [10 << 30]
+    a = Admission(budget=None, reserve=1 << 30, free_fn=lambda: free[0])
+    assert a.budget == 9 << 30
+    assert a.fits(9 << 30) and not a.fits((9 << 30) + 1)
+    a.hold("x", 6 << 30)
+    free[0] -= 6 << 30
+    assert a.used == 6 << 30
+    assert a.fits(3 << 30)
+    assert not a.fits((3 << 30) + 1)          # budget left
+    free[0] = 2 << 30                          # another process took memory
+    assert not a.fits(2 << 30)                 # free memory less the reserve
+    assert a.fits(1 << 30)
+    a.release("x")
+    a.release("x")                             # idempotent
+    assert a.used == 0
+    b = Admission(budget=5 << 30, reserve=0, free_fn=lambda: 100 << 30)
+    assert b.budget == 5 << 30 and not b.fits((5 << 30) + 1)
+    # the estimate grows with the basis and with incremental builds
+    assert footprint_bytes(800) > footprint_bytes(400) > 0
+    assert footprint_bytes(800, incremental=True) > footprint_bytes(800)
