@@ -590,8 +590,10 @@ extern "C" int gtf_batch_add(gtf_batch_t *b, const char *bsfile, const char *xyz
     d.S = gtf_fock_onee_dev(j.eng, 0);
     d.X = gtf_fock_onee_dev(j.eng, 1);
     if (j.n > BJ_BIG) {
+        // mixed precision: split-BF16 tensor-core purification products too
         if (gtf_purif_create(j.n, j.nocc, b->st, &j.pd) != GTF_OK ||
-            gtf_purif_set_sx_dev(j.pd, d.S, d.X) != GTF_OK) {
+            gtf_purif_set_sx_dev(j.pd, d.S, d.X) != GTF_OK ||
+            (prec_mode == 1 && gtf_purif_set_mode(j.pd, 1) != GTF_OK)) {
             j.pd = nullptr;
             job_free(j);
             return -6;

@@ -184,11 +184,21 @@ __global__ void k_purif_stats(const double *__restrict__ D, const double *__rest
 // far outside [0, 1]: with every eigenvalue of D in [0, 1], c lies in [0, 1];
 // far outside it the eigenvalues have left that interval and the cubic
 // update diverges (in the reference, to Inf and NaN within a few steps).
+// The loop's stop is kept on the device, so the host need not wait for every
+// step: scal[8] != 0 once a step found ||D - D2||_F < 1e-11 (that step's
+// update still applies, as in pscf/purif.c:394-455) or stopped as above;
+// later steps then change nothing.  scal[9] counts the steps that ran.
 #define PURIF_C_LO (-0.25)
 #define PURIF_C_HI 1.25
+#define PURIF_TOL 1e-11
 __global__ void k_purif_finish(const double *__restrict__ part, int nblk, double *scal)
 {
     if (threadIdx.x != 0) return;
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    if (scal[8] != 0.0) {
+        scal[7] = nan;   // stopped: no update
+        return;
+    }
     double e = 0.0, t = 0.0, t2 = 0.0;
     for (int b = 0; b < nblk; b++) {
         e += part[3 * b];
@@ -198,8 +208,13 @@ __global__ void k_purif_finish(const double *__restrict__ part, int nblk, double
     const double c = t / t2;
     const bool ok = isfinite(c) && c >= PURIF_C_LO && c <= PURIF_C_HI;
     scal[6] = ok ? sqrt(e) : 0.0;
-    scal[7] = ok ? c : __longlong_as_double(0x7ff8000000000000LL);
+    scal[7] = ok ? c : nan;
+    scal[9] += 1.0;
+    if (!ok || scal[6] < PURIF_TOL) scal[8] = 1.0;
 }
+
+// steps between two host reads of the stop flag (FP64 phase)
+#define PURIF_CHECK 4
 
 // D update (pscf/purif.c:441-455)
 __global__ void k_purif_update(double *__restrict__ D, const double *__restrict__ D2, const double *__restrict__ D3,
@@ -377,6 +392,7 @@ extern "C" int gtf_purif_run_dev(gtf_purif_dev_t *p, const double *F_dev, double
     // (their rounding sets a floor near 2^-16 relative), then FP64 steps
     p->it_bf16 = 0;
     if (p->mode == 1 && p->bx) {
+        CKP(cudaMemsetAsync(p->scal + 8, 0, sizeof(double) * 2, st));
         double best = 1e300;
         int stall = 0;
         for (int k = 0; k < PUR_MAX_ITERS; k++) {
@@ -403,23 +419,32 @@ extern "C" int gtf_purif_run_dev(gtf_purif_dev_t *p, const double *F_dev, double
             }
         }
     }
-    // FP64 canonical steps (from the split-BF16 state in mode 1)
-    for (it = 0; it < PUR_MAX_ITERS; it++) {
-        if (gemm_abt(p, p->D, p->D, p->D2)) return GTF_ERR_CUDA;
-        if (gemm_ab(p, p->D, p->D2, p->D3)) return GTF_ERR_CUDA;
-        k_purif_stats<<<RED_BLOCKS, RED_THREADS, 0, st>>>(p->D, p->D2, p->D3, n, p->part);
-        k_purif_finish<<<1, 32, 0, st>>>(p->part, RED_BLOCKS, p->scal);
-        k_purif_update<<<ge, 256, 0, st>>>(p->D, p->D2, p->D3, nn, p->scal);
-        CKP(cudaGetLastError());
-        gtf_note_launches(3);
-        CKP(cudaMemcpyAsync(p->h_scal + 6, p->scal + 6, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
+    // FP64 canonical steps (from the split-BF16 state in mode 1), PURIF_CHECK
+    // launched per host read of the device-side stop flag
+    CKP(cudaMemsetAsync(p->scal + 8, 0, sizeof(double) * 2, st));
+    int steps = 0;
+    bool stopped = false;
+    for (it = 0; it < PUR_MAX_ITERS && !stopped;) {
+        for (int k = 0; k < PURIF_CHECK && it < PUR_MAX_ITERS; k++, it++) {
+            if (gemm_abt(p, p->D, p->D, p->D2)) return GTF_ERR_CUDA;
+            if (gemm_ab(p, p->D, p->D2, p->D3)) return GTF_ERR_CUDA;
+            k_purif_stats<<<RED_BLOCKS, RED_THREADS, 0, st>>>(p->D, p->D2, p->D3, n, p->part);
+            k_purif_finish<<<1, 32, 0, st>>>(p->part, RED_BLOCKS, p->scal);
+            k_purif_update<<<ge, 256, 0, st>>>(p->D, p->D2, p->D3, nn, p->scal);
+            CKP(cudaGetLastError());
+            gtf_note_launches(3);
+        }
+        CKP(cudaMemcpyAsync(p->h_scal + 6, p->scal + 6, sizeof(double) * 4, cudaMemcpyDeviceToHost, st));
         CKP(cudaStreamSynchronize(st));
         err = p->h_scal[6];
-        if (err < 1e-11) break;
+        steps = (int)p->h_scal[9];
+        stopped = p->h_scal[8] != 0.0;
     }
     p->errnorm = err;
-    p->it_fp64 = (it < PUR_MAX_ITERS) ? it + 1 : PUR_MAX_ITERS;
-    it += p->it_bf16;
+    // the counts of the reference's loop: steps run, and the index of the
+    // step that met the tolerance
+    p->it_fp64 = stopped ? steps : PUR_MAX_ITERS;
+    it = (stopped ? steps - 1 : PUR_MAX_ITERS) + p->it_bf16;
     // D_AO = X D X (pscf/purif.c:469-476)
     if (gemm_abt(p, p->X, p->D, p->W)) return GTF_ERR_CUDA;
     if (gemm_abt(p, p->W, p->X, D_dev)) return GTF_ERR_CUDA;

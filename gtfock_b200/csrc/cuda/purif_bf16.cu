@@ -7,11 +7,14 @@
 // operand is split into two BF16 matrices, X = X_hi + X_lo with
 // X_hi = bf16(X) and X_lo = bf16(X - X_hi), and
 //     C ~= A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T
-// is one BF16 GEMM with FP32 accumulation over the stacked inner dimension
-// (K = 3 n): A' = [A_hi | A_hi | A_lo], B' = [B_hi | B_lo | B_hi] row by row.
-// The dropped A_lo B_lo^T term and the BF16 rounding of the low parts leave a
-// relative error near 2^-16 per product, which is why the purification
-// finishes with FP64 steps.
+// is one batched BF16 GEMM (batch L = 3, one term each) with FP32
+// accumulation: A' = [A_hi | A_hi | A_lo], B' = [B_hi | B_lo | B_hi] row by
+// row, batch l reading column block l of both; the three FP32 products are
+// summed in FP64.  Three batches of (n / 128)^2 output tiles keep the SMs
+// busy at n ~ 830 (147 CTAs for 148 SMs, against 49 for one GEMM over the
+// stacked K = 3 n).  The dropped A_lo B_lo^T term and the BF16 rounding of
+// the low parts leave a relative error near 2^-16 per product, which is why
+// the purification finishes with FP64 steps.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -22,6 +25,8 @@
 #include <cutlass/gemm/device/gemm_universal_adapter.h>
 #include <cutlass/gemm/kernel/gemm_universal.hpp>
 #include <cutlass/util/packed_stride.hpp>
+
+#include <type_traits>
 
 #include "gtf_cuda.h"
 
@@ -67,13 +72,14 @@ __global__ void k_split_bf16(const double *__restrict__ X, int n, int np, int ro
     row[2 * np + j] = role == 0 ? lo : hi;
 }
 
-// C (n x np FP32) -> n x n FP64
-__global__ void k_f32_to_f64(const float *__restrict__ C, int n, int np, double *__restrict__ out)
+// C_0 + C_1 + C_2 (three n x np FP32 batches) -> n x n FP64
+__global__ void k_sum3_f64(const float *__restrict__ C, int n, int np, double *__restrict__ out)
 {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = blockIdx.y;
     if (j >= n) return;
-    out[(size_t)i * n + j] = (double)C[(size_t)i * np + j];
+    const size_t o = (size_t)i * np + j, b = (size_t)n * np;
+    out[(size_t)i * n + j] = (double)C[o] + (double)C[o + b] + (double)C[o + 2 * b];
 }
 
 struct gtf_bf16x3 {
@@ -94,7 +100,7 @@ extern "C" int gtf_bf16x3_create(int n, gtf_bf16x3_t **out)
     g->np = (n + 7) / 8 * 8;
     const size_t ab = sizeof(__nv_bfloat16) * (size_t)g->np * 3 * g->np;
     if (cudaMalloc(&g->A, ab) != cudaSuccess || cudaMalloc(&g->B, ab) != cudaSuccess ||
-        cudaMalloc(&g->C, sizeof(float) * (size_t)n * g->np) != cudaSuccess ||
+        cudaMalloc(&g->C, sizeof(float) * 3 * (size_t)n * g->np) != cudaSuccess ||
         cudaMemset(g->B, 0, ab) != cudaSuccess) {
         gtf_bf16x3_destroy(g);
         return GTF_ERR_ALLOC;
@@ -127,12 +133,17 @@ extern "C" int gtf_bf16x3_abt(gtf_bf16x3_t *g, const double *A, const double *B,
     using StrideA = typename Gemm::GemmKernel::StrideA;
     using StrideB = typename Gemm::GemmKernel::StrideB;
     using StrideC = typename Gemm::GemmKernel::StrideC;
-    const int M = n, N = np, K = 3 * np;
-    StrideA sa = cutlass::make_cute_packed_stride(StrideA{}, cute::make_shape(M, K, 1));
-    StrideB sb = cutlass::make_cute_packed_stride(StrideB{}, cute::make_shape(N, K, 1));
-    StrideC sc = cutlass::make_cute_packed_stride(StrideC{}, cute::make_shape(M, np, 1));
-    typename Gemm::Arguments args{cutlass::gemm::GemmUniversalMode::kGemm,
-                                  {M, N, K, 1},
+    // batch l: columns [l np, (l + 1) np) of the stacked rows (leading
+    // dimension 3 np) for A' and B'; its own n x np FP32 output
+    const int M = n, N = np, K = np, L = 3;
+    StrideA sa = cute::make_stride(int64_t(3 * np), cute::Int<1>{}, int64_t(np));
+    StrideB sb = cute::make_stride(int64_t(3 * np), cute::Int<1>{}, int64_t(np));
+    StrideC sc = cute::make_stride(int64_t(np), cute::Int<1>{}, int64_t(n) * np);
+    static_assert(std::is_same<StrideA, cute::Stride<int64_t, cute::Int<1>, int64_t>>::value, "row-major A");
+    static_assert(std::is_same<StrideB, cute::Stride<int64_t, cute::Int<1>, int64_t>>::value, "K-major B");
+    static_assert(std::is_same<StrideC, cute::Stride<int64_t, cute::Int<1>, int64_t>>::value, "row-major C");
+    typename Gemm::Arguments args{cutlass::gemm::GemmUniversalMode::kBatched,
+                                  {M, N, K, L},
                                   {reinterpret_cast<const ElementIn *>(g->A), sa,
                                    reinterpret_cast<const ElementIn *>(g->B), sb},
                                   {{1.0f, 0.0f}, g->C, sc, g->C, sc}};
@@ -148,7 +159,7 @@ extern "C" int gtf_bf16x3_abt(gtf_bf16x3_t *g, const double *A, const double *B,
     if (gemm.initialize(args, g->ws, st) != cutlass::Status::kSuccess) return GTF_ERR_CUDA;
     if (gemm.run(st) != cutlass::Status::kSuccess) return GTF_ERR_CUDA;
     dim3 grd2((n + 127) / 128, n);
-    k_f32_to_f64<<<grd2, blk, 0, st>>>(g->C, n, np, C);
+    k_sum3_f64<<<grd2, blk, 0, st>>>(g->C, n, np, C);
     if (cudaGetLastError() != cudaSuccess) return GTF_ERR_CUDA;
     gtf_note_launches(4);
     return GTF_OK;

@@ -35,6 +35,7 @@ struct gtf_scf {
     double *dD, *dF;     /* device-resident D and F (mode 1) */
     double etol;         /* stop when |E_k - E_k-1| < etol */
     int incr, incr_period;   /* incremental Fock builds (restarted by every solve) */
+    int pur_mode_set;        /* purification mode chosen by gtf_scf_set_purification */
     double incr_tau;
     int last_mode;       /* where the last solve left D: 0 host, 1 device */
 };
@@ -126,6 +127,10 @@ int gtf_scf_set_options(gtf_scf_t *s, int prec_mode, double fp32_cutoff, double 
     if (!s || !(etol >= 0.0)) return -1;
     if (gtf_pfock_set_precision(s->pf, prec_mode, fp32_cutoff) != PFOCK_STATUS_SUCCESS) return -2;
     s->etol = etol;
+    /* mixed precision takes the split-BF16 tensor-core purification products
+     * too, unless a mode was chosen explicitly */
+    if (!s->pur_mode_set && gtf_purif_set_mode((gtf_purif_dev_t *)s->pur->dev, prec_mode == 1 ? 1 : 0) != GTF_OK)
+        return -3;
     return 0;
 }
 
@@ -142,6 +147,7 @@ int gtf_scf_set_incremental(gtf_scf_t *s, int on, double tau, int period)
 int gtf_scf_set_purification(gtf_scf_t *s, int mode)
 {
     if (!s || !s->pur) return -1;
+    s->pur_mode_set = 1;
     return gtf_purif_set_mode((gtf_purif_dev_t *)s->pur->dev, mode) == GTF_OK ? 0 : -2;
 }
 

@@ -153,7 +153,9 @@ int gtf_scf_solve(gtf_scf_t *s, int niters, int mode, double *energies, double *
 int gtf_scf_nbf(gtf_scf_t *s);
 /* ERI precision of the engine (as gtf_pfock_set_precision) and the energy
  * convergence tolerance: a solve stops once |E_k - E_k-1| < etol (default
- * 1e-11).  0 on success. */
+ * 1e-11).  Mixed precision (prec_mode 1) also selects the split-BF16
+ * purification products (gtf_scf_set_purification mode 1) unless a mode was
+ * set explicitly.  0 on success. */
 int gtf_scf_set_options(gtf_scf_t *s, int prec_mode, double fp32_cutoff, double etol);
 /* Incremental Fock builds for this solver's engine (gtf_pfock_set_incremental);
  * every solve starts with a full build.  0 on success. */
@@ -182,8 +184,10 @@ int gtf_scf_run(const char *bsfile, const char *xyzfile, double tolscr,
  * request as soon as a slot and device memory are free.
  *   gtf_batch_create(capacity): at most `capacity` jobs at a time.
  *   gtf_batch_add: set-up of one job (basis, screening, S, X, H_core,
- *     initial guess) with its ERI precision (as gtf_pfock_set_precision),
- *     at most max_iters iterations, stopping once |E_k - E_k-1| < etol;
+ *     initial guess) with its ERI precision (as gtf_pfock_set_precision;
+ *     jobs above 640 functions in mixed precision also purify with the
+ *     split-BF16 products), at most max_iters iterations, stopping once
+ *     |E_k - E_k-1| < etol;
  *     returns the job's slot (>= 0) or a negative error (-2: no free slot).
  *   gtf_batch_step: returns the number of jobs still running, or < 0.
  *   gtf_batch_run: steps until every job is done.
