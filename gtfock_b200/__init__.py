@@ -141,6 +141,7 @@ def load():
     _sig(L, "gtf_shard_split", [_dp, ctypes.c_longlong, _i, _i, ctypes.POINTER(ctypes.c_longlong),
                                 ctypes.POINTER(ctypes.c_longlong)], None)
     _sig(L, "gtf_pfock_shard_work", [_vp, _dp])
+    _sig(L, "gtf_pfock_class_work_screened", [_vp, _dp, _dp])
     _lib = L
     return L
 
@@ -286,6 +287,16 @@ class PFock:
         npq = np.zeros(32)
         n = load().gtf_pfock_class_work(self.h, _dptr(fl), _dptr(npq))
         return [(float(fl[i]), float(npq[i])) for i in range(n)]
+
+    def class_work_screened(self):
+        """[(Rys-model FLOPs, primitive quartets)] per class pair after
+        primitive screening (what the kernels evaluate), same order."""
+        f = np.zeros(21)
+        q = np.zeros(21)
+        n = load().gtf_pfock_class_work_screened(self.h, _dptr(f), _dptr(q))
+        if n < 0:
+            raise GtfError("gtf_pfock_class_work_screened failed (%d)" % n)
+        return list(zip(f[:n], q[:n]))
 
     def set_precision(self, mode, fp32_cutoff=0.0):
         """mode 0: FP64; mode 1: FP32 for quartets with Schwarz bound < fp32_cutoff."""

@@ -915,6 +915,42 @@ __global__ void __launch_bounds__(UNIT_SCAN_THREADS) k_units_scan(const UnitTask
     if (threadIdx.x == 0) u[n] = s_carry;
 }
 
+// Primitive quartets the Fock kernels evaluate after primitive screening: the
+// loops stop at |K_ab K_cd| < GTF_PRIMQ_EPS with both lists in descending
+// |K| (the ket loop once the largest bra primitive fails), so a quartet
+// evaluates, per ket primitive that passes with the first bra primitive, the
+// prefix of bra primitives that pass with it.  One thread per (task, bra,
+// segment) walks its kets; out[k] receives task k's total.  Statistics only.
+__global__ void k_count_primq(const UnitTask *__restrict__ tasks, int nt, long long total,
+                              const PairRec *__restrict__ pairs, const double *__restrict__ pp,
+                              double *__restrict__ out)
+{
+    for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < total;
+         x += (long long)gridDim.x * blockDim.x) {
+        const int k = task_of(tasks, nt, x, [](const UnitTask &t) { return t.idx0; });
+        const UnitTask &t = tasks[k];
+        const int r = (int)(x - t.idx0);
+        const int i = r / GTF_NBKT, b = r - i * GTF_NBKT;
+        if (b == 0) continue;   // segment 0 gets no units
+        const int n = t.nket[r];
+        const PairRec pb = pairs[t.bra_start + i];
+        if (n == 0 || pb.n <= 0) continue;
+        const double kb0 = fabs(pp[(size_t)2 * GTF_PPREC_D2 * pb.off + 1]);
+        double cnt = 0.0;
+        for (int q = 0; q < n; q++) {
+            const PairRec pk = pairs[t.ket_start + t.seg[b] + q];
+            for (int ik = 0; ik < pk.n; ik++) {
+                const double kk = fabs(pp[(size_t)2 * GTF_PPREC_D2 * (pk.off + ik) + 1]);
+                if (kb0 * kk < GTF_PRIMQ_EPS) break;
+                int nb = 0;
+                while (nb < pb.n && fabs(pp[(size_t)2 * GTF_PPREC_D2 * (pb.off + nb) + 1]) * kk >= GTF_PRIMQ_EPS) nb++;
+                cnt += nb;
+            }
+        }
+        atomicAdd(out + k, cnt);
+    }
+}
+
 // Launches the three phases over `nt` tasks (device array) whose flattened
 // (bra, segment) and bra counts are nidx and nbras.
 static int run_units(const UnitTask *d_tasks, int nt, long long nidx, long long nbras, int nsm, cudaStream_t st)
@@ -2247,6 +2283,48 @@ extern "C" int gtf_fock_class_stats(gtf_fock_dev_t *f, int *X, int *Y, double *m
         if (Y) Y[c] = f->tasks[c].Y;
         if (ms) ms[c] = f->ms_cls[c];
         if (nquart) nquart[c] = f->tasks[c].nquart;
+    }
+    return NCLSPAIR;
+}
+
+// Per class pair: Rys-model FLOPs and primitive quartets of one build after
+// primitive screening (the primitive quartets the kernels evaluate, counted
+// by k_count_primq on the static task lists; the per-quartet contraction and
+// digestion terms as in gtf_fock_class_work).
+extern "C" int gtf_fock_class_work_screened(gtf_fock_dev_t *f, double *flops, double *nprimq)
+{
+    int r = static_lists(f);
+    if (r) return r;
+    const int nt = (int)f->h_ut.size();
+    std::vector<double> cnt(nt > 0 ? nt : 1, 0.0);
+    if (nt > 0) {
+        DevTemps tmps;
+        double *d_out;
+        TALLOC(tmps, d_out, nt);
+        CK(cudaMemsetAsync(d_out, 0, sizeof(double) * nt, f->stream));
+        const long long g = (f->ut_nidx + 255) / 256;
+        const unsigned grid = (unsigned)(g < (long long)f->nsm * 16 ? (g < 1 ? 1 : g) : (long long)f->nsm * 16);
+        k_count_primq<<<grid, 256, 0, f->stream>>>(f->d_ut_static, nt, f->ut_nidx, f->d_pairs, f->d_pp, d_out);
+        CK(cudaGetLastError());
+        gtf_note_launches(1);
+        CK(cudaMemcpyAsync(cnt.data(), d_out, sizeof(double) * nt, cudaMemcpyDeviceToHost, f->stream));
+        CK(cudaStreamSynchronize(f->stream));
+    }
+    int k = 0;
+    for (int c = 0; c < NCLSPAIR; c++) {
+        const ClassPairTask &t = f->tasks[c];
+        double q = 0.0, fl = 0.0;
+        if (t.nbra > 0 && t.nketcls > 0) {
+            q = cnt[k++];
+            double cpart;
+            const double per_prim = class_flops_per_prim(t.X, t.Y, &cpart);
+            const int la = k_cls_la[t.X], lb = k_cls_lb[t.X], lc = k_cls_la[t.Y], ld = k_cls_lb[t.Y];
+            const double ns_ = (double)(f->pure && la == 2 ? 5 : ncart(la)) * (f->pure && lb == 2 ? 5 : ncart(lb)) *
+                               (f->pure && lc == 2 ? 5 : ncart(lc)) * (f->pure && ld == 2 ? 5 : ncart(ld));
+            fl = q * per_prim + (cpart + 12.0 * ns_) * t.nquart;
+        }
+        if (flops) flops[c] = fl;
+        if (nprimq) nprimq[c] = q;
     }
     return NCLSPAIR;
 }

@@ -117,6 +117,8 @@ int gtf_tune_save(const char *path);
 int gtf_tune_load(const char *path);
 /* per class pair: Rys-model FLOPs and primitive quartets of one build */
 int gtf_fock_class_work(gtf_fock_dev_t *f, double *flops, double *nprimq);
+/* the same after primitive screening (primitive quartets the kernels evaluate) */
+int gtf_fock_class_work_screened(gtf_fock_dev_t *f, double *flops, double *nprimq);
 /* quartets evaluated in FP32 under the current precision mode, and all */
 int gtf_fock_fp32_quartets(gtf_fock_dev_t *f, double *nq32, double *nq);
 /* per angular class pair (21 of them for s/p/d): classes, ms of the last

@@ -458,6 +458,12 @@ PFockStatus_t gtf_pfock_incremental_stats(PFock_t pf, double *nquart_fp64, doubl
     return map_err(gtf_fock_incremental_stats(pf->dev, nquart_fp64, nquart_fp32, dmax));
 }
 
+int gtf_pfock_class_work_screened(PFock_t pf, double *flops, double *nprimq)
+{
+    if (pf == NULL) return -1;
+    return gtf_fock_class_work_screened(pf->dev, flops, nprimq);
+}
+
 PFockStatus_t gtf_pfock_shard_work(PFock_t pf, double *work)
 {
     if (pf == NULL) return PFOCK_STATUS_INVALID_VALUE;

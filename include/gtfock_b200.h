@@ -41,6 +41,10 @@ int gtf_pfock_class_stats(PFock_t pfock, int *X, int *Y, double *ms, double *nqu
 /* Per class pair (same order): Rys-model FLOPs of one build and the number of
  * primitive quartets before primitive screening.  Returns the pair count. */
 int gtf_pfock_class_work(PFock_t pfock, double *flops, double *nprimq);
+/* The same after primitive screening: the primitive quartets the kernels
+ * evaluate (their loops stop at |K_ab K_cd| < 1e-17) and the Rys-model FLOPs
+ * of those.  Returns the pair count, or < 0 on error. */
+int gtf_pfock_class_work_screened(PFock_t pfock, double *flops, double *nprimq);
 
 /* Precision of the ERI kernels: 0 = FP64 (default), 1 = FP32 for quartets
  * whose Schwarz bound sqrt(v1 v2) is below fp32_cutoff (Rys roots, 2-D

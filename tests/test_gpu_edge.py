@@ -10,6 +10,8 @@ and size-independent properties at the largest size of the benchmarks.
 import numpy as np
 import pytest
 
+from conftest import golden_xyz, load_golden
+
 import gtfock_b200 as gb
 from gtfock_b200 import molecules as mol
 from oracle import pyoracle as po
@@ -103,4 +105,31 @@ def test_largest_size_properties(tmp_path):
     # FP32 quartets have Schwarz bounds below 1e-6; their rounding moves F
     # by far less than 1e-6 per element
     assert np.abs(F2m - F2).max() < 1e-6
+    pf.close()
+
+
+def test_primitive_quartets_after_screening(tmp_path):
+    """The count of primitive quartets the kernels evaluate (after the
+    |K_ab K_cd| < 1e-17 cut) is at most the model's count before it, for
+    every class, and smaller in total on C12H26 / cc-pVDZ, whose contracted
+    s shells have tight, small-coefficient primitives; for water / STO-3G
+    the (ss|ss) count is the product of the pairs' primitive counts less
+    the few cut quartets."""
+    g = load_golden("h2o_sto3g")
+    gbs, xyz = golden_xyz(g, tmp_path)
+    pf = gb.PFock(gb.BasisSet(gbs, xyz), tolscr=1e-10)
+    before = pf.class_work()
+    after = pf.class_work_screened()
+    for (fb, qb), (fa, qa) in zip(before, after):
+        assert 0.5 * qb <= qa <= qb
+    pf.close()
+    g = load_golden("c12h26_ccpvdz")
+    gbs, xyz = golden_xyz(g, tmp_path)
+    pf = gb.PFock(gb.BasisSet(gbs, xyz), tolscr=1e-10)
+    before = pf.class_work()
+    after = pf.class_work_screened()
+    for (fb, qb), (fa, qa) in zip(before, after):
+        assert 0 <= qa <= qb and fa <= fb * (1 + 1e-12)
+    assert sum(q for _, q in after) < sum(q for _, q in before)
+    assert sum(q for _, q in after) > 0.1 * sum(q for _, q in before)
     pf.close()
