@@ -134,6 +134,7 @@ def load():
     _sig(L, "gtf_scf_set_incremental", [_vp, _i, _d, _i])
     _sig(L, "gtf_batch_set_incremental", [_vp, _i, _d, _i])
     _sig(L, "gtf_batch_job_device_bytes", [_vp, _i], ctypes.c_size_t)
+    _sig(L, "gtf_batch_job_stats", [_vp, _i, _dp, _i])
     _sig(L, "gtf_device_memory", [ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)])
     _sig(L, "gtf_debug_fail_alloc", [_i], None)
     _sig(L, "gtf_debug_live_allocs", [], ctypes.c_longlong)
@@ -515,6 +516,13 @@ class Batch:
         r = load().gtf_batch_set_incremental(self.h, 1 if on else 0, tau, period)
         if r != 0:
             raise GtfError("gtf_batch_set_incremental failed (%d)" % r)
+
+    def job_stats(self, slot):
+        """(basis functions, SCF iterations, purification iterations of the
+        last step, purification iterations in all) of the job in `slot`."""
+        out = np.zeros(4)
+        n = load().gtf_batch_job_stats(self.h, slot, _dptr(out), 4)
+        return tuple(int(x) for x in out[:n])
 
     def job_device_bytes(self, slot):
         """Device bytes a job holds (its batch buffers and its Fock engine)."""

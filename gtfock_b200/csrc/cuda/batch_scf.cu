@@ -326,6 +326,8 @@ __global__ void __launch_bounds__(BJ_THREADS) k_j_pur_init(const JobDev *__restr
         c01[1] = lambda * mu_bar / (double)n + (double)j.nocc / n;
         scal[blockIdx.x * 8 + 0] = c01[0];
         scal[blockIdx.x * 8 + 1] = c01[1];
+        scal[blockIdx.x * 8 + 3] = 0.0;   // best error so far (0: none yet)
+        scal[blockIdx.x * 8 + 4] = 0.0;   // steps since it last fell by 1%
         active[blockIdx.x] = 1;
     }
     __syncthreads();
@@ -338,7 +340,10 @@ __global__ void __launch_bounds__(BJ_THREADS) k_j_pur_init(const JobDev *__restr
 }
 
 // ||P - P2||_F, c = tr(P2 - P3) / tr(P - P2), then the trace-conserving
-// update (pscf/purif.c:394-455); a job stops once ||P - P2||_F < 1e-11
+// update (pscf/purif.c:394-455); a job stops once ||P - P2||_F < 1e-11, or
+// once that error, already below 1e-8, has not fallen by 1% in 8 steps
+// (rounding above the tolerance: the reference's loop would run to its cap
+// without changing P), as the one-job path does.
 // Block b serves job list[b] (the jobs still purifying).
 __global__ void __launch_bounds__(BJ_THREADS) k_j_pur_step(const JobDev *__restrict__ jobs, const int *__restrict__ list,
                                                           double *__restrict__ scal, int *__restrict__ active,
@@ -375,7 +380,16 @@ __global__ void __launch_bounds__(BJ_THREADS) k_j_pur_step(const JobDev *__restr
     if (threadIdx.x == 0) {
         scal[q * 8 + 2] = err;
         iters[q] += 1;
-        if (err < 1e-11) active[q] = 0;
+        double &best = scal[q * 8 + 3], &stall = scal[q * 8 + 4];
+        if (ok) {
+            if (best == 0.0 || err < 0.99 * best) {
+                best = err;
+                stall = 0.0;
+            } else {
+                stall += 1.0;
+            }
+        }
+        if (err < 1e-11 || (best < 1e-8 && stall >= 8.0)) active[q] = 0;
     }
 }
 
@@ -404,6 +418,7 @@ struct BJob {
     double bmax;
     double b[BJ_MAX_DIIS + 1][BJ_MAX_DIIS + 1];
     int pur_iters;
+    long long pur_total;           // purification iterations over all steps
 };
 
 struct gtf_batch {
@@ -1031,10 +1046,15 @@ extern "C" int gtf_batch_step(gtf_batch_t *b)
             j.done = 1;
         }
         j.pur_iters = it;
+        j.pur_total += it;
     }
     CKH(cudaEventRecord(b->e2, b->st));
     CKH(cudaStreamSynchronize(b->st));
-    for (int q = 0; q < C; q++) b->jobs[run[cont[q]]].pur_iters = b->h_iters[q];
+    for (int q = 0; q < C; q++) {
+        BJob &j = b->jobs[run[cont[q]]];
+        j.pur_iters = b->h_iters[q];
+        j.pur_total += j.pur_iters;
+    }
     float ms1 = 0.0f, ms2 = 0.0f, ms3 = 0.0f, ms4 = 0.0f;
     cudaEventElapsedTime(&ms1, b->e0, b->e1);
     cudaEventElapsedTime(&ms2, b->e1, b->e2);
@@ -1150,6 +1170,19 @@ extern "C" int gtf_batch_info(gtf_batch_t *b, int *nrunning, int *nused, double 
     if (ms_rest) *ms_rest = b->ms_rest;
     if (job_bytes) *job_bytes = by;
     return 0;
+}
+
+// per-job statistics: [0] basis functions, [1] SCF iterations run, [2]
+// purification iterations of the last step, [3] over all steps; returns the
+// count written (0 for an empty slot)
+extern "C" int gtf_batch_job_stats(gtf_batch_t *b, int slot, double *out, int n)
+{
+    if (!b || !out || slot < 0 || slot >= b->capacity || !b->jobs[slot].used) return 0;
+    const BJob &j = b->jobs[slot];
+    const double v[4] = {(double)j.n, (double)j.iter, (double)j.pur_iters, (double)j.pur_total};
+    const int m = n < 4 ? n : 4;
+    for (int k = 0; k < m; k++) out[k] = v[k];
+    return m;
 }
 
 // device bytes held by the job in `slot` (batch buffers and Fock engine); 0 if empty

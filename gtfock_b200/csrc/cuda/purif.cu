@@ -188,9 +188,17 @@ __global__ void k_purif_stats(const double *__restrict__ D, const double *__rest
 // step: scal[8] != 0 once a step found ||D - D2||_F < 1e-11 (that step's
 // update still applies, as in pscf/purif.c:394-455) or stopped as above;
 // later steps then change nothing.  scal[9] counts the steps that ran.
+// It also stops once the error, already below PURIF_FLOOR, has not fallen by
+// 1% in PURIF_STALL steps (scal[10] the best error so far, 0 before the first
+// step; scal[11] the steps since): rounding that holds the error just above
+// the 1e-11 tolerance keeps the reference's loop running to its cap without
+// changing D.  Above the floor the early steps of a purification can move
+// the error by less than 1% for many steps, so no such stop applies there.
 #define PURIF_C_LO (-0.25)
 #define PURIF_C_HI 1.25
 #define PURIF_TOL 1e-11
+#define PURIF_STALL 8
+#define PURIF_FLOOR 1e-8
 __global__ void k_purif_finish(const double *__restrict__ part, int nblk, double *scal)
 {
     if (threadIdx.x != 0) return;
@@ -210,7 +218,15 @@ __global__ void k_purif_finish(const double *__restrict__ part, int nblk, double
     scal[6] = ok ? sqrt(e) : 0.0;
     scal[7] = ok ? c : nan;
     scal[9] += 1.0;
-    if (!ok || scal[6] < PURIF_TOL) scal[8] = 1.0;
+    if (ok) {
+        if (scal[10] == 0.0 || scal[6] < 0.99 * scal[10]) {
+            scal[10] = scal[6];
+            scal[11] = 0.0;
+        } else {
+            scal[11] += 1.0;
+        }
+    }
+    if (!ok || scal[6] < PURIF_TOL || (scal[10] < PURIF_FLOOR && scal[11] >= PURIF_STALL)) scal[8] = 1.0;
 }
 
 // steps between two host reads of the stop flag (FP64 phase)
@@ -392,7 +408,7 @@ extern "C" int gtf_purif_run_dev(gtf_purif_dev_t *p, const double *F_dev, double
     // (their rounding sets a floor near 2^-16 relative), then FP64 steps
     p->it_bf16 = 0;
     if (p->mode == 1 && p->bx) {
-        CKP(cudaMemsetAsync(p->scal + 8, 0, sizeof(double) * 2, st));
+        CKP(cudaMemsetAsync(p->scal + 8, 0, sizeof(double) * 4, st));
         double best = 1e300;
         int stall = 0;
         for (int k = 0; k < PUR_MAX_ITERS; k++) {
@@ -421,7 +437,7 @@ extern "C" int gtf_purif_run_dev(gtf_purif_dev_t *p, const double *F_dev, double
     }
     // FP64 canonical steps (from the split-BF16 state in mode 1), PURIF_CHECK
     // launched per host read of the device-side stop flag
-    CKP(cudaMemsetAsync(p->scal + 8, 0, sizeof(double) * 2, st));
+    CKP(cudaMemsetAsync(p->scal + 8, 0, sizeof(double) * 4, st));
     int steps = 0;
     bool stopped = false;
     for (it = 0; it < PUR_MAX_ITERS && !stopped;) {

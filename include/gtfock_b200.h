@@ -217,6 +217,11 @@ size_t gtf_batch_job_bytes(int nbf);
 /* Device bytes held by the job in `slot` (its batch buffers and its Fock
  * engine); 0 for an empty slot. */
 size_t gtf_batch_job_device_bytes(gtf_batch_t *b, int slot);
+/* Per-job statistics of the job in `slot`: [0] basis functions, [1] SCF
+ * iterations run, [2] purification iterations of its last step, [3] its
+ * purification iterations over all steps.  Writes min(n, 4) values and
+ * returns that count (0 for an empty slot). */
+int gtf_batch_job_stats(gtf_batch_t *b, int slot, double *out, int n);
 /* Accumulated statistics of a batch: [0] ms of the Fock builds, [1] of the
  * energies, [2] of DIIS, [3] of purification, [4] purification steps of the
  * batched jobs, [5] batch steps.  Writes min(n, 6) values, returns that count. */
