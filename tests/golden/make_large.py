@@ -21,7 +21,7 @@ built by oracle/ref/Makefile) and --pin is given, the probe's screening list,
 counters and F for the same density are compared with the oracle's and the
 fixture records ref_pinned = 1 and the largest |dF|.
 
-Run:  python tests/golden/make_large.py [--pin] [--threads N] [case ...]
+Run:  python tests/golden/make_large.py [--pin | --pin-existing] [--threads N] [case ...]
 """
 import argparse
 import os
@@ -102,14 +102,53 @@ def make(name, pin, nthreads):
         np.savez_compressed(os.path.join(OUT, name + ".npz"), **out)
 
 
+def pin_existing(name):
+    """Check an existing fixture against oracle/_ref/ref_probe (the
+    reference's own sources) without recomputing the oracle's F."""
+    path = os.path.join(OUT, name + ".npz")
+    out = dict(np.load(path, allow_pickle=False))
+    atoms = [(str(sy),) + tuple(float(v) for v in x) for sy, x in zip(out["atoms_sym"], out["atoms_xyz"])]
+    gbs = mol.basis_file(str(out["basis"]))
+    tol = float(out["tol"])
+    n = int(out["nbf"])
+    F = np.zeros((n, n))
+    iu = np.triu_indices(n)
+    F[iu] = out["F_upper"]
+    F.T[iu] = out["F_upper"]
+    with tempfile.TemporaryDirectory() as td:
+        xyz = mol.write_xyz(atoms, os.path.join(td, name + ".xyz"), name)
+        t0 = time.time()
+        ref = ref_probe(gbs, xyz, tol, density(n, int(out["density_seed"])))
+        if ref is None:
+            raise RuntimeError("oracle/_ref/ref_probe is not built (make -C oracle/ref)")
+        for k in ("shellptr", "shellid", "shellrid"):
+            assert np.array_equal(ref[k], out[k]), (name, k)
+        assert np.array_equal(ref["shellvalue"], out["shellvalue"]), name
+        assert ref["maxvalue"] == float(out["maxvalue"]), name
+        assert ref["usq"] == float(out["usq"]) and ref["uitl"] == float(out["uitl"]), name
+        err = float(np.abs(ref["F"] - F).max())
+        assert err < 1e-11, (name, err)
+        out["ref_pinned"] = np.array(1)
+        out["ref_max_dF"] = np.array(err)
+        out["ref_seconds"] = np.array(time.time() - t0)
+        print("%s: pinned to the reference build (max |dF| %.2e, %.0f s)" % (name, err, time.time() - t0),
+              flush=True)
+    np.savez_compressed(path, **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("cases", nargs="*")
     ap.add_argument("--pin", action="store_true", help="check against oracle/_ref/ref_probe")
+    ap.add_argument("--pin-existing", action="store_true",
+                    help="pin the stored fixtures to oracle/_ref/ref_probe without recomputing them")
     ap.add_argument("--threads", type=int, default=os.cpu_count())
     a = ap.parse_args()
     for n in a.cases or list(CASES):
-        make(n, a.pin, a.threads)
+        if a.pin_existing:
+            pin_existing(n)
+        else:
+            make(n, a.pin, a.threads)
 
 
 if __name__ == "__main__":

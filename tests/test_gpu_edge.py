@@ -133,3 +133,25 @@ def test_primitive_quartets_after_screening(tmp_path):
     assert sum(q for _, q in after) < sum(q for _, q in before)
     assert sum(q for _, q in after) > 0.1 * sum(q for _, q in before)
     pf.close()
+
+
+def test_short_stride_rejected(tmp_path):
+    """A row stride shorter than the block (the rows would overlap) is an
+    argument error in PFock_getMat and PFock_putDenMat, before any copy."""
+    import ctypes
+    L = gb.load()
+    g = load_golden("h2o_631g")
+    gbs, xyz = golden_xyz(g, tmp_path)
+    b = gb.BasisSet(gbs, xyz)
+    pf = gb.PFock(b, tolscr=1e-10)
+    n = b.nbf
+    buf = np.zeros((n, n))
+    ptr = buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    INVALID = 3
+    assert L.PFock_getMat(pf.h, gb.MAT_F, 0, 0, n - 1, 0, n - 1, n - 1, ptr) == INVALID
+    assert L.PFock_getMat(pf.h, gb.MAT_F, 0, 0, n - 1, 2, 5, 3, ptr) == INVALID
+    assert L.PFock_getMat(pf.h, gb.MAT_F, 0, 0, n - 1, 2, 5, 4, ptr) == 0
+    assert L.PFock_putDenMat(0, n - 1, 0, n - 1, n - 1, ptr, 0, pf.h) == INVALID
+    F = pf.compute_fock(g["D"])
+    assert np.abs(F - g["F"]).max() < 1e-10
+    pf.close()
