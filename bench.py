@@ -575,11 +575,11 @@ def batched_measure(count, seed, cut, autotune, seq_sample):
 def run_served(args):
     """Served workload (--workload served): see served_measure."""
     out = served_measure(args.count, args.seed, args.rate, args.fp32_cutoff if args.fp32_cutoff is not None
-                         else 1e-6, args.slots, args.lanes, not args.no_incremental)
+                         else 1e-6, args.slots, args.lanes, not args.no_incremental, not args.turns)
     print(json.dumps(out), flush=True)
 
 
-def served_measure(count, seed, rate, cut, slots, lanes, incremental):
+def served_measure(count, seed, rate, cut, slots, lanes, incremental, concurrent=True, with_sequential=True):
     """Served workload: a seeded Poisson stream of SCF requests, sizes
     log-uniform over 20-1500 bf (water clusters in 6-31G, alkanes C4-C40 in
     cc-pVDZ), each iterated until |dE| < 1e-6 Ha (max 30 iterations).  The
@@ -592,10 +592,13 @@ def served_measure(count, seed, rate, cut, slots, lanes, incremental):
     reqs = [serve.Request(n, a, b, t, nb) for t, n, a, b, nb in items]
     srv = serve.SCFServer(slots=slots, precision=1, fp32_cutoff=cut, max_iters=30, etol=1e-6, tolscr=TOL,
                           lanes=((400, None), (None, None)) if lanes == 2 else ((None, None),),
-                          incremental=incremental, incr_period=INCR_PERIOD)
+                          incremental=incremental, incr_period=INCR_PERIOD, concurrent=concurrent)
     done = serve.run_stream(reqs, srv)
     budget = srv.admission.budget
     srv.close()
+    if not with_sequential:
+        return {"served_mixed": serve.latency_stats(done), "energies": {r.name: float(r.energies[-1]) for r in done},
+                "iterations": {r.name: len(r.energies) for r in done}}
     seq = serve.run_sequential(reqs, max_iters=30, etol=1e-6, tolscr=TOL)
     by = {r.name: r for r in seq}
     # compared where both runs converged (|dE| < 1e-6 Ha before 30 iterations)
@@ -606,7 +609,8 @@ def served_measure(count, seed, rate, cut, slots, lanes, incremental):
     out = {"metric": "SCF solves/s and p50/p99 time-to-converged-energy, served (%d requests)" % count,
            "workload": "Poisson rate %.2f/s, seed %d, %d-%d bf" % (rate, seed,
                                                                  min(i[4] for i in items), max(i[4] for i in items)),
-           "served_form": "continuous batching, FP32 quartets below %g%s" % (
+           "served_form": "continuous batching%s, FP32 quartets below %g%s" % (
+               ", size lanes stepped concurrently on their own streams" if concurrent else "",
                cut, ", incremental Fock builds (full every %d)" % INCR_PERIOD if incremental else ""),
            "fp32_cutoff": cut, "slots_per_lane": slots, "lanes": lanes,
            "hbm_budget_gb": budget / 1e9,
@@ -734,6 +738,8 @@ def main():
                     help="served: size lanes (2: up to 400 functions, and the rest)")
     ap.add_argument("--seq-sample", type=int, default=256, help="batched: molecules timed on the one-job path")
     ap.add_argument("--no-incremental", action="store_true", help="served: plain (not incremental) Fock builds")
+    ap.add_argument("--turns", action="store_true",
+                    help="served: the lanes take turns on one thread instead of stepping concurrently")
     ap.add_argument("--quick", action="store_true",
                     help="default workload only: leave out the served, batched and C12H26 blocks")
     args = ap.parse_args()

@@ -50,6 +50,7 @@ struct gtf_purif_dev {
     double *part;     // [RED_BLOCKS * 16] block partials
     double *scal;     // device scalars
     double *h_scal;   // pinned mirror
+    double *h_part;   // host copy of the DIIS dot-product partials
     int len_diis, bmax_id;
     double bmax;
     double b[PUR_LDB * PUR_LDB];
@@ -319,6 +320,7 @@ extern "C" int gtf_purif_create(int nbf, int nocc, void *stream, gtf_purif_dev_t
     CKP(cudaMalloc((void **)&p->part, sizeof(double) * RED_BLOCKS * 16));
     CKP(cudaMalloc((void **)&p->scal, sizeof(double) * 16));
     CKP(cudaMallocHost((void **)&p->h_scal, sizeof(double) * 16));
+    CKP(cudaMallocHost((void **)&p->h_part, sizeof(double) * RED_BLOCKS * PUR_MAX_DIIS));
     CKP(cudaEventCreate(&p->e0));
     CKP(cudaEventCreate(&p->e1));
     p->bmax = DBL_MIN;
@@ -355,6 +357,7 @@ extern "C" void gtf_purif_destroy(gtf_purif_dev_t *p)
     for (double *b : bufs)
         if (b) cudaFree(b);
     if (p->h_scal) cudaFreeHost(p->h_scal);
+    if (p->h_part) cudaFreeHost(p->h_part);
     cublasDestroy(p->blas);
     cudaEventDestroy(p->e0);
     cudaEventDestroy(p->e1);
@@ -542,7 +545,7 @@ extern "C" int gtf_diis_step_dev(gtf_purif_dev_t *p, const double *D_dev, double
         k_dots<<<RED_BLOCKS, RED_THREADS, 0, st>>>(cur, p->vecs, nn, p->len_diis, p->part);
         CKP(cudaGetLastError());
         gtf_note_launches(2);
-        static double hpart[RED_BLOCKS * PUR_MAX_DIIS];
+        double *hpart = p->h_part;   // per object: engines may run on several host threads
         CKP(cudaMemcpyAsync(hpart, p->part, sizeof(double) * RED_BLOCKS * PUR_MAX_DIIS, cudaMemcpyDeviceToHost, st));
         CKP(cudaStreamSynchronize(st));
         for (int i = 0; i < p->len_diis; i++) {

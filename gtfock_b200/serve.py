@@ -21,6 +21,7 @@ its measured size, and the device's free memory at that moment.
 """
 import os
 import tempfile
+import threading
 import time
 
 import numpy as np
@@ -90,6 +91,9 @@ class _Lane:
         self.slots = slots
         self.live = {}
         self.ms = None          # moving average of a step's wall time
+        # serialises this lane's batch calls (admission from the serving
+        # thread, steps from the lane's own thread in concurrent mode)
+        self.lock = threading.Lock()
 
     def fits(self, nbf):
         return self.max_nbf is None or nbf <= self.max_nbf
@@ -107,8 +111,14 @@ class SCFServer:
 
     def __init__(self, slots=64, mem_budget=None, precision=1, fp32_cutoff=1e-6, max_iters=30,
                  etol=1e-6, tolscr=1e-10, lanes=((400, None), (None, None)), share=0.5,
-                 incremental=False, incr_tau=0.0, incr_period=8, reserve=2 << 30, free_fn=None):
+                 incremental=False, incr_tau=0.0, incr_period=8, reserve=2 << 30, free_fn=None,
+                 concurrent=False):
         self.admission = Admission(mem_budget, reserve, free_fn)
+        self._mu = threading.Lock()   # admission state
+        # concurrent: run_stream steps every lane from a thread of its own,
+        # so the lanes' launches (each batch has its own CUDA stream) overlap
+        # on the GPU instead of taking turns
+        self.concurrent = bool(concurrent)
         self.lanes = [_Lane(m, n if n else slots) for m, n in lanes]
         self.incremental = bool(incremental)
         if self.incremental:
@@ -126,7 +136,10 @@ class SCFServer:
 
     @property
     def live(self):
-        return {(k, s): r for k, ln in enumerate(self.lanes) for s, r in ln.live.items()}
+        return {(k, s): r for k, ln in enumerate(self.lanes) for s, r in list(ln.live.items())}
+
+    def has_live(self):
+        return any(len(ln.live) for ln in self.lanes)
 
     def _xyz(self, r):
         if r.xyz is None:
@@ -151,26 +164,32 @@ class SCFServer:
 
     def can_admit(self, r):
         ln = self._lane(r)
-        return len(ln.live) < ln.slots and self.admission.fits(self.footprint(r))
+        with self._mu:
+            return len(ln.live) < ln.slots and self.admission.fits(self.footprint(r))
 
     def admit(self, r, now):
         ln = self._lane(r)
-        r.slot = ln.batch.add(mol.basis_file(r.basis), self._xyz(r), **self.kw)
-        r.admitted = now
-        ln.live[r.slot] = r
+        with ln.lock:
+            r.slot = ln.batch.add(mol.basis_file(r.basis), self._xyz(r), **self.kw)
+            r.admitted = now
+            ln.live[r.slot] = r
+            nbytes = ln.batch.job_device_bytes(r.slot)
         # the job's measured device bytes replace the estimate
-        self.admission.hold(id(r), ln.batch.job_device_bytes(r.slot))
+        with self._mu:
+            self.admission.hold(id(r), nbytes)
 
     def cancel(self, r):
         """Withdraw a live request between steps: its slot and memory are
         freed; the other jobs continue unaffected."""
         for ln in self.lanes:
-            if ln.live.get(r.slot) is r:
-                ln.live.pop(r.slot)
-                ln.batch.remove(r.slot)
-                self.admission.release(id(r))
-                r.cancelled = True
-                return True
+            with ln.lock:
+                if ln.live.get(r.slot) is r:
+                    ln.live.pop(r.slot)
+                    ln.batch.remove(r.slot)
+                    with self._mu:
+                        self.admission.release(id(r))
+                    r.cancelled = True
+                    return True
         return False
 
     def _pick(self):
@@ -183,30 +202,39 @@ class SCFServer:
         return large
 
     def step(self, now_fn):
-        """One SCF iteration of every live job of one lane; returns the
-        requests that finished."""
+        """One SCF iteration of every live job of one lane (the lanes take
+        turns); returns the requests that finished."""
         ln = self._pick()
         if ln is None:
             return []
+        busy = [x for x in self.lanes if x.live]   # before this step's jobs leave
         t0 = time.perf_counter()
-        ln.batch.step()
+        done = self.step_lane(ln, now_fn)
         dt = (time.perf_counter() - t0) * 1e3
         ln.ms = dt if ln.ms is None else 0.7 * ln.ms + 0.3 * dt
-        busy = [x for x in self.lanes if x.live]
         if ln is busy[-1] and len(busy) > 1:
             self.credit = 0.0
         else:
             self.credit += dt
+        return done
+
+    def step_lane(self, ln, now_fn):
+        """One SCF iteration of every live job of lane `ln`."""
         done = []
-        for s in list(ln.live):
-            e, fin = ln.batch.result(s)
-            if fin:
-                r = ln.live.pop(s)
-                r.energies = e
-                r.finished = now_fn()
-                ln.batch.remove(s)
-                self.admission.release(id(r))
-                done.append(r)
+        with ln.lock:
+            if not ln.live:
+                return done
+            ln.batch.step()
+            for s in list(ln.live):
+                e, fin = ln.batch.result(s)
+                if fin:
+                    r = ln.live.pop(s)
+                    r.energies = e
+                    r.finished = now_fn()
+                    ln.batch.remove(s)
+                    with self._mu:
+                        self.admission.release(id(r))
+                    done.append(r)
         return done
 
     def close(self):
@@ -217,6 +245,8 @@ class SCFServer:
 def run_stream(requests, server):
     """Replay `requests` (sorted by arrival, seconds from start) against the
     wall clock through `server`; returns the finished requests."""
+    if server.concurrent:
+        return _run_stream_concurrent(requests, server)
     pending = sorted(requests, key=lambda r: r.arrival)
     for r in pending:
         server._xyz(r)
@@ -243,6 +273,64 @@ def run_stream(requests, server):
                                "budget of %.2f GB" % (waiting[0].name, waiting[0].nbf or 0,
                                                       server.footprint(waiting[0]) / 1e9,
                                                       server.admission.budget / 1e9))
+    return finished
+
+
+def _run_stream_concurrent(requests, server):
+    """run_stream with one stepping thread per lane: the serving thread
+    admits arriving requests; each lane's thread steps its batch while it has
+    live jobs.  The library's calls release the GIL, so the lanes' CUDA
+    streams run at the same time."""
+    pending = sorted(requests, key=lambda r: r.arrival)
+    for r in pending:
+        server._xyz(r)
+        server._nbf(r)
+    t0 = time.perf_counter()
+    now = lambda: time.perf_counter() - t0  # noqa: E731
+    finished = []
+    fin_mu = threading.Lock()
+    stop = threading.Event()
+    errors = []
+
+    def lane_loop(ln):
+        try:
+            while not stop.is_set():
+                if ln.live:
+                    done = server.step_lane(ln, now)
+                    if done:
+                        with fin_mu:
+                            finished.extend(done)
+                else:
+                    time.sleep(0.0005)
+        except Exception as e:  # surfaced by the serving thread
+            errors.append(e)
+            stop.set()
+
+    threads = [threading.Thread(target=lane_loop, args=(ln,), daemon=True) for ln in server.lanes]
+    for th in threads:
+        th.start()
+    waiting = []
+    try:
+        while (pending or waiting or server.has_live()) and not errors:
+            t = now()
+            while pending and pending[0].arrival <= t:
+                waiting.append(pending.pop(0))
+            for r in list(waiting):
+                if server.can_admit(r):
+                    waiting.remove(r)
+                    server.admit(r, now())
+            if waiting and not pending and not server.has_live():
+                raise RuntimeError("request %s (%d functions, %.2f GB estimated) does not fit the device "
+                                   "memory budget of %.2f GB" % (waiting[0].name, waiting[0].nbf or 0,
+                                                                 server.footprint(waiting[0]) / 1e9,
+                                                                 server.admission.budget / 1e9))
+            time.sleep(0.0005)
+    finally:
+        stop.set()
+        for th in threads:
+            th.join()
+    if errors:
+        raise errors[0]
     return finished
 
 

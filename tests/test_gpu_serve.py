@@ -47,18 +47,21 @@ def _server(**kw):
     return serve.SCFServer(**args)
 
 
-def test_stream_results_equal_alone(tmp_path):
+@pytest.mark.parametrize("concurrent", [False, True])
+def test_stream_results_equal_alone(tmp_path, concurrent):
+    """Also with concurrent lanes (one stepping thread per lane, the lanes'
+    streams overlapping on the GPU): a small and a large lane here."""
     reqs = _stream()
-    srv = _server()
+    srv = _server(concurrent=concurrent, lanes=((30, 1), (None, None))) if concurrent else _server()
     try:
         done = serve.run_stream(reqs, srv)
     finally:
         srv.close()
     assert sorted(r.name for r in done) == sorted(r.name for r in reqs)
-    # all arrive at once and two slots serve them: four wait for a slot, and
-    # two jobs are on the device together throughout
+    # all arrive at once and fewer slots serve them: some wait for a slot,
+    # and jobs are on the device together
     waited = [r for r in done if r.admitted > r.arrival]
-    assert len(waited) >= 4
+    assert len(waited) >= 2
     overlaps = sum(1 for a in done for b in done if a is not b and a.admitted <= b.admitted < a.finished)
     assert overlaps > 0
     for r in done:
