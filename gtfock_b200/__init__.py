@@ -91,6 +91,7 @@ def load():
     _sig(L, "gtf_pfock_screening", [_vp, _ip, _ip, _ip, _dp])
     _sig(L, "gtf_pfock_timing", [_vp, _dp, _dp, _dp])
     _sig(L, "gtf_pfock_set_precision", [_vp, _i, _d])
+    _sig(L, "gtf_pfock_set_nosymm_mode", [_vp, _i])
     _sig(L, "gtf_pfock_precision_stats", [_vp, _dp, _dp])
     _sig(L, "gtf_pfock_class_stats", [_vp, _ip, _ip, _dp, _dp])
     _sig(L, "gtf_pfock_class_work", [_vp, _dp, _dp])
@@ -298,6 +299,15 @@ class PFock:
         if n < 0:
             raise GtfError("gtf_pfock_class_work_screened failed (%d)" % n)
         return list(zip(f[:n], q[:n]))
+
+    NOSYMM_MODES = {"reference": 1, "exact": 2}
+
+    def set_nosymm_mode(self, mode):
+        """Engines created with symm=0: "reference" (default) returns the
+        reference's own symm = 0 result, (F[D] + F[D^T]^T) / 2 of its
+        unique-quartet digestion; "exact" returns F = 2 J[D] - K[D]."""
+        self._check(load().gtf_pfock_set_nosymm_mode(self.h, self.NOSYMM_MODES[mode]),
+                    "gtf_pfock_set_nosymm_mode")
 
     def set_precision(self, mode, fp32_cutoff=0.0):
         """mode 0: FP64; mode 1: FP32 for quartets with Schwarz bound < fp32_cutoff."""

@@ -148,9 +148,13 @@ struct gtf_fock_dev {
     int prec;
     double fp32_cutoff;
     size_t dev_bytes;
-    // non-symmetric densities (PFock_create with symm = 0)
+    // non-symmetric densities (PFock_create with symm = 0): GTF_NOSYMM_*
     int nosymm;
     double *d_Ds, *d_Da, *d_Dca, *d_Fka;
+    // the reference's own symm = 0 output: sign-adjusted antisymmetric part
+    // (spherical, Cartesian), its Coulomb accumulator and a scratch exchange
+    // accumulator
+    double *d_Dta, *d_Dcta, *d_Fja, *d_Fscr;
     // sharded build: this engine computes shard `shard` of `nshards` (0: all);
     // its units of every (class pair, part): [shard_lo, shard_hi), split by
     // the work model (see shard_bounds)
@@ -326,6 +330,23 @@ __global__ void k_d_to_cart(const double *__restrict__ D, double *__restrict__ D
     d_to_cart_elem(D, Dc, cart2shell, sh_L, f_start, fc_start, nbf, nbfc, pure, i, j);
 }
 
+// Orientation of shell pair {A, B} in the reference's pair list
+// (pfock/screening.c:146-163 keeps (A, B) for A > B with A + B even, A < B
+// with A + B odd, and A == B): +1 for that orientation, -1 for the other.
+// The reference digests each unique quartet once, in the orientation of its
+// bra and ket pairs, with the update_F formulas written for a symmetric D
+// (pfock/fock_task.c:29-117); with a non-symmetric D its Coulomb terms keep
+// the part of the antisymmetric density Da that these orientations select.
+// With Dta = s(M, N) Da the usual Coulomb digestion over any fixed pair
+// orientations gives Fja, and the reference's symm = 0 result
+// (F[D] + F[D^T]^T) / 2 (pfock/pfock.c:1704-1718) is the exact
+// 2 J[D] - K[D] plus (S.Fja - (S.Fja)^T) / 2, S the block signs s(M, N).
+__host__ __device__ __forceinline__ double ref_pair_sign(int A, int B)
+{
+    if (A == B) return 1.0;
+    return ((A > B) == (((A + B) & 1) == 0)) ? 1.0 : -1.0;
+}
+
 // J = T sym(Fj) T^T, K = T sym(Fk) T^T, F = J + K (pfock/pfock.c:1719-1726, 1161-1185)
 // Fka (non-symmetric densities only, else null): exchange accumulator of the
 // antisymmetric part of D, whose full contribution is (Fka - Fka^T) / 2
@@ -334,13 +355,16 @@ __device__ __forceinline__ void f_to_sph_elem(const double *__restrict__ Fj, con
                                               const int *__restrict__ sph2shell, const int *__restrict__ sh_L,
                                               const int *__restrict__ f_start, const int *__restrict__ fc_start,
                                               int nbf, int nbfc, int pure, int m, int n,
-                                              const double *__restrict__ Fka = nullptr, bool acc = false)
+                                              const double *__restrict__ Fka = nullptr, bool acc = false,
+                                              const double *__restrict__ Fja = nullptr)
 {
     const int sm = sph2shell[m], sn = sph2shell[n];
     const int cm = m - f_start[sm], cn = n - f_start[sn];
     const int Lm = sh_L[sm], Ln = sh_L[sn];
     const int fm = fc_start[sm], fn = fc_start[sn];
     const int nm = ncart(Lm), nn = ncart(Ln);
+    // Fja: sign of the shell block in the reference's pair orientation
+    const double smn = Fja ? ref_pair_sign(sm, sn) : 0.0, snm = Fja ? ref_pair_sign(sn, sm) : 0.0;
     double j = 0.0, k = 0.0;
     for (int a = 0; a < nm; a++) {
         const double ta = sph_coef(Lm, pure, cm, a);
@@ -353,6 +377,7 @@ __device__ __forceinline__ void f_to_sph_elem(const double *__restrict__ Fj, con
             j += ta * tb * (0.5 * (Fj[ab] + Fj[ba]));
             k += ta * tb * (0.5 * (Fk[ab] + Fk[ba]));
             if (Fka) k += ta * tb * (0.5 * (Fka[ab] - Fka[ba]));
+            if (Fja) j += ta * tb * (0.5 * (smn * Fja[ab] - snm * Fja[ba]));
         }
     }
     const size_t o = (size_t)m * nbf + n;
@@ -373,13 +398,13 @@ __global__ void k_f_to_sph(const double *__restrict__ Fj, const double *__restri
                            const int *__restrict__ sph2shell, const int *__restrict__ sh_L,
                            const int *__restrict__ f_start, const int *__restrict__ fc_start,
                            int nbf, int nbfc, int pure, const double *__restrict__ Fka = nullptr,
-                           const int *__restrict__ acc_flag = nullptr)
+                           const int *__restrict__ acc_flag = nullptr, const double *__restrict__ Fja = nullptr)
 {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     const int m = blockIdx.y;
     if (n >= nbf) return;
     const bool acc = acc_flag != nullptr && *acc_flag != 0;
-    f_to_sph_elem(Fj, Fk, F, J, K, sph2shell, sh_L, f_start, fc_start, nbf, nbfc, pure, m, n, Fka, acc);
+    f_to_sph_elem(Fj, Fk, F, J, K, sph2shell, sh_L, f_start, fc_start, nbf, nbfc, pure, m, n, Fka, acc, Fja);
 }
 
 // ---------------------------------------------------------------------------
@@ -441,8 +466,11 @@ __global__ void k_dyn_thresholds(DynState *dyn, double tol2, double cut2, double
     dyn_thresholds(dyn, tol2, cut2, tau2, c2, full);
 }
 
-// non-symmetric D: Ds = (D + D^T) / 2, Da = (D - D^T) / 2
-__global__ void k_split_density(const double *__restrict__ D, double *__restrict__ Ds, double *__restrict__ Da, int n)
+// non-symmetric D: Ds = (D + D^T) / 2, Da = (D - D^T) / 2 and, for the
+// reference's symm = 0 output (Dta non-null), Dta = s(M, N) Da with M, N the
+// shells of the element (ref_pair_sign)
+__global__ void k_split_density(const double *__restrict__ D, double *__restrict__ Ds, double *__restrict__ Da, int n,
+                                double *__restrict__ Dta = nullptr, const int *__restrict__ sph2shell = nullptr)
 {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = blockIdx.y;
@@ -450,6 +478,7 @@ __global__ void k_split_density(const double *__restrict__ D, double *__restrict
     const double a = D[(size_t)i * n + j], t = D[(size_t)j * n + i];
     Ds[(size_t)i * n + j] = 0.5 * (a + t);
     Da[(size_t)i * n + j] = 0.5 * (a - t);
+    if (Dta) Dta[(size_t)i * n + j] = ref_pair_sign(sph2shell[i], sph2shell[j]) * 0.5 * (a - t);
 }
 
 // ---------------------------------------------------------------------------
@@ -1674,7 +1703,7 @@ extern "C" void gtf_fock_destroy(gtf_fock_dev_t *f)
                     f->d_shellptr, f->d_shellid, f->d_shellrid, f->d_shellvalue, f->d_pairs, f->d_pair_v,
                     f->d_pp, f->d_pp32, f->d_counters, f->d_D, f->d_Dc, f->d_Fj, f->d_Fk, f->d_F, f->d_J, f->d_K,
                     f->d_Ds, f->d_Da, f->d_Dca, f->d_Fka, f->d_ut_static, f->d_ut_dyn, f->d_Dprev, f->d_Dd,
-                    f->d_dyn};
+                    f->d_dyn, f->d_Dta, f->d_Dcta, f->d_Fja, f->d_Fscr};
     for (void *p : ptrs) dev_free(p);   // all from dalloc
     for (int c = 0; c < NCLSPAIR; c++) {
         dev_free(f->tasks[c].d_nket);
@@ -1784,21 +1813,37 @@ extern "C" int gtf_fock_put_density_dev(gtf_fock_dev_t *f, int index, const doub
 }
 
 // Non-symmetric densities (PFock_create with symm = 0): buffers for the
-// symmetric and antisymmetric parts and the second exchange accumulator.
-extern "C" int gtf_fock_set_nosymm(gtf_fock_dev_t *f, int on)
+// symmetric and antisymmetric parts and the second exchange accumulator, and
+// for the reference's own output the sign-adjusted density and its Coulomb
+// accumulator (GTF_NOSYMM_REFERENCE / GTF_NOSYMM_EXACT / off).
+extern "C" int gtf_fock_set_nosymm(gtf_fock_dev_t *f, int mode)
 {
-    if (!on) {
+    if (mode != GTF_NOSYMM_OFF && mode != GTF_NOSYMM_REFERENCE && mode != GTF_NOSYMM_EXACT) {
+        snprintf(g_errbuf, sizeof(g_errbuf), "unknown non-symmetric density mode %d", mode);
+        return GTF_ERR_INVALID;
+    }
+    if (mode == GTF_NOSYMM_OFF) {
         f->nosymm = 0;
         return GTF_OK;
     }
+    if (f->incr) {
+        snprintf(g_errbuf, sizeof(g_errbuf), "non-symmetric densities: incremental builds are on");
+        return GTF_ERR_INVALID;
+    }
+    const size_t nn = (size_t)f->nbf * f->nbf, nnc = (size_t)f->nbf_cart * f->nbf_cart;
     if (!f->d_Fka) {
-        const size_t nn = (size_t)f->nbf * f->nbf, nnc = (size_t)f->nbf_cart * f->nbf_cart;
         DALLOC(f->d_Ds, nn);
         DALLOC(f->d_Da, nn);
         DALLOC(f->d_Dca, nnc);
         DALLOC(f->d_Fka, nnc);
     }
-    f->nosymm = 1;
+    if (mode == GTF_NOSYMM_REFERENCE && !f->d_Fja) {
+        DALLOC(f->d_Dta, nn);
+        DALLOC(f->d_Dcta, nnc);
+        DALLOC(f->d_Fja, nnc);
+        DALLOC(f->d_Fscr, nnc);
+    }
+    f->nosymm = mode;
     return GTF_OK;
 }
 
@@ -2135,7 +2180,9 @@ extern "C" int gtf_fock_compute(gtf_fock_dev_t *f, int numdmat)
             // through the usual build, the antisymmetric part only through
             // the exchange terms (it has no Coulomb contribution)
             dim3 g((nbf + 127) / 128, nbf);
-            k_split_density<<<g, 128, 0, st>>>(D, f->d_Ds, f->d_Da, nbf);
+            const bool ref = f->nosymm == GTF_NOSYMM_REFERENCE;
+            k_split_density<<<g, 128, 0, st>>>(D, f->d_Ds, f->d_Da, nbf, ref ? f->d_Dta : nullptr,
+                                               f->d_sph2shell);
             CK(cudaGetLastError());
             gtf_note_launches(1);
             D = f->d_Ds;
@@ -2179,12 +2226,35 @@ extern "C" int gtf_fock_compute(gtf_fock_dev_t *f, int numdmat)
                 gtf_note_launches(r);
             }
         }
+        if (f->nosymm == GTF_NOSYMM_REFERENCE) {
+            // the reference's orientation-dependent Coulomb part: a plain
+            // build of the sign-adjusted Dta, whose exchange part (into the
+            // scratch accumulator) is not used
+            const double *Dcta = f->d_Dta;
+            if (need_tr) {
+                dim3 g((nbfc + 127) / 128, nbfc);
+                k_d_to_cart<<<g, 128, 0, st>>>(f->d_Dta, f->d_Dcta, f->d_cart2shell, f->d_sh_L, f->d_f_start,
+                                               f->d_fc_start, nbf, nbfc, f->pure);
+                CK(cudaGetLastError());
+                gtf_note_launches(1);
+                Dcta = f->d_Dcta;
+            }
+            CK(cudaMemsetAsync(f->d_Fja, 0, sizeof(double) * nnc, st));
+            CK(cudaMemsetAsync(f->d_Fscr, 0, sizeof(double) * nnc, st));
+            CK(cudaMemsetAsync(f->d_counters, 0, sizeof(unsigned long long) * 2 * NCLSPAIR * GTF_MAX_SLICES, st));
+            for (int c = 0; c < NCLSPAIR; c++) {
+                const int r = launch_class(f, c, Dcta, f->d_Fja, f->d_Fscr, f->d_counters, st);
+                if (r < 0) return GTF_ERR_CUDA;
+                gtf_note_launches(r);
+            }
+        }
         CK(cudaEventRecord(f->ev_cls[NCLSPAIR], st));
         CK(cudaEventRecord(f->ev2, st));
         dim3 g2((nbf + 127) / 128, nbf);
         k_f_to_sph<<<g2, 128, 0, st>>>(f->d_Fj, f->d_Fk, f->d_F + nn * d, f->d_J + nn * d, f->d_K + nn * d,
                                        f->d_sph2shell, f->d_sh_L, f->d_f_start, f->d_fc_start, nbf, nbfc,
-                                       f->pure, f->nosymm ? f->d_Fka : nullptr);
+                                       f->pure, f->nosymm ? f->d_Fka : nullptr, nullptr,
+                                       f->nosymm == GTF_NOSYMM_REFERENCE ? f->d_Fja : nullptr);
         CK(cudaGetLastError());
         gtf_note_launches(1);
         CK(cudaEventSynchronize(f->ev2));

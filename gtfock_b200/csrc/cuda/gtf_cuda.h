@@ -83,8 +83,12 @@ int gtf_fock_set_precision(gtf_fock_dev_t *f, int prec, double fp32_cutoff);
  * builds (density 0, symmetric, unsharded); statistics of the last build */
 int gtf_fock_set_incremental(gtf_fock_dev_t *f, int on, double tau, int period);
 int gtf_fock_incremental_stats(gtf_fock_dev_t *f, double *nq64, double *nq32, double *dmax);
-/* non-symmetric densities: F = 2 J[D] - K[D] exactly for a general D */
-int gtf_fock_set_nosymm(gtf_fock_dev_t *f, int on);
+/* non-symmetric densities (PFock_create with symm = 0): the reference's own
+ * symm = 0 output, or F = 2 J[D] - K[D] exactly for a general D; off */
+#define GTF_NOSYMM_OFF 0
+#define GTF_NOSYMM_REFERENCE 1
+#define GTF_NOSYMM_EXACT 2
+int gtf_fock_set_nosymm(gtf_fock_dev_t *f, int mode);
 int gtf_fock_last_timing(gtf_fock_dev_t *f, double *ms_total, double *ms_eri, double *ms_other);
 int gtf_fock_eri_flops(gtf_fock_dev_t *f, double *flops);
 /* batched Fock builds over many engines (molecules): one launch per class

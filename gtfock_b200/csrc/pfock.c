@@ -128,11 +128,12 @@ PFockStatus_t PFock_create(BasisSet_t basis, int nprow, int npcol, int ntasks,
         return map_err(e);
     }
     /* symm = 0 (pfock/pfock.c:828): densities may be non-symmetric.  The
-     * engine forms F = 2 J[D] - K[D] exactly for a general D: the symmetric
-     * part of D through the usual build, the antisymmetric part through the
-     * exchange terms only.  For a symmetric D this is the symm = 1 result. */
+     * engine returns what the reference returns, (F[D] + F[D^T]^T) / 2 with
+     * its unique-quartet digestion (pfock/pfock.c:1704-1718);
+     * gtf_pfock_set_nosymm_mode selects the exact F = 2 J[D] - K[D] instead.
+     * For a symmetric D both are the symm = 1 result. */
     if (symm == 0) {
-        e = gtf_fock_set_nosymm(pf->dev, 1);
+        e = gtf_fock_set_nosymm(pf->dev, GTF_NOSYMM_REFERENCE);
         if (e != GTF_OK) {
             gtf_fock_destroy(pf->dev);
             free(pf);
@@ -408,6 +409,18 @@ int gtf_pfock_class_work(PFock_t pf, double *flops, double *nprimq)
 PFockStatus_t gtf_pfock_set_precision(PFock_t pf, int mode, double fp32_cutoff)
 {
     return map_err(gtf_fock_set_precision(pf->dev, mode, fp32_cutoff));
+}
+
+PFockStatus_t gtf_pfock_set_nosymm_mode(PFock_t pf, int mode)
+{
+    if (pf == NULL) return PFOCK_STATUS_INVALID_VALUE;
+    if (!pf->nosymm || (mode != GTF_NOSYMM_REFERENCE && mode != GTF_NOSYMM_EXACT)) {
+        PFOCK_PRINTF(1, "non-symmetric density mode: engine created with symm = 1, or mode not 1 or 2\n");
+        return PFOCK_STATUS_INVALID_VALUE;
+    }
+    int e = gtf_fock_set_nosymm(pf->dev, mode);
+    if (e != GTF_OK) PFOCK_PRINTF(1, "%s\n", gtf_last_error());
+    return map_err(e);
 }
 
 PFockStatus_t gtf_pfock_set_shard(PFock_t pf, int shard, int nshards)

@@ -52,6 +52,16 @@ int gtf_pfock_class_work_screened(PFock_t pfock, double *flops, double *nprimq);
  * accumulation into F stay FP64).  Rebuilds the task lists. */
 PFockStatus_t gtf_pfock_set_precision(PFock_t pfock, int mode, double fp32_cutoff);
 
+/* Engines created with symm = 0 (non-symmetric densities):
+ *   mode 1 (default): the reference's own result, (F[D] + F[D^T]^T) / 2 of
+ *     its unique-quartet digestion (pfock/pfock.c:1704-1718), which for a
+ *     non-symmetric D depends on the orientation of its shell-pair lists;
+ *   mode 2: the exact F = 2 J[D] - K[D], J_ab = sum_cd (ab|cd) D_cd,
+ *     K_ab = sum_cd (ac|bd) D_cd.
+ * Both equal the symm = 1 result for a symmetric D.  Returns
+ * PFOCK_STATUS_INVALID_VALUE on an engine created with symm = 1. */
+PFockStatus_t gtf_pfock_set_nosymm_mode(PFock_t pfock, int mode);
+
 /* One molecule over several GPUs (one process per GPU): with
  * gtf_pfock_set_shard(pf, r, n) every class launch of this engine's builds
  * covers shard r of n of its quartet units (the 2-D task decomposition of

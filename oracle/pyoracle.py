@@ -283,3 +283,72 @@ def fock_build_range(basis, tol, D, lo, hi, scr=None, nthreads=os.cpu_count()):
                                  int(lo), int(hi), ctypes.byref(usq), ctypes.byref(uitl)) != 0:
         raise RuntimeError("or_fock_build_range failed")
     return F
+
+
+def eri_tensor(basis):
+    """Full (ab|cd) tensor from the oracle engine, for small bases only."""
+    n, ns = basis.nbf, basis.nshells
+    eri = np.zeros((n, n, n, n))
+    for A in range(ns):
+        for B in range(ns):
+            for C in range(ns):
+                for D in range(ns):
+                    fa, fb, fc, fd = [basis.func_start(s) for s in (A, B, C, D)]
+                    da, db, dc, dd = [basis.shell_dim(s) for s in (A, B, C, D)]
+                    try:
+                        blk = shell_quartet(basis, A, B, C, D)
+                    except ValueError:   # screened out inside the engine: zero block
+                        continue
+                    eri[fa:fa + da, fb:fb + db, fc:fc + dc, fd:fd + dd] = blk
+    return eri
+
+
+def fock_nosymm_reference(basis, tol, eri, D, scr=None):
+    """The reference's symm = 0 Fock matrix for a (non-symmetric) D, restated
+    in numpy for small bases: G[X] is fock_task's digestion of every unique
+    quartet over the screened pair lists, in the orientation the lists give
+    its bra and ket (pfock/fock_task.c:121-219, update_F at
+    pfock/fock_task.c:29-117, J and K terms into one F as with __SCF__), and
+    the result is (G[D] + G[D^T]^T) / 2 (PFock_commitDenMats transposes D,
+    pfock/pfock.c:1113-1121; the correction step pfock/pfock.c:1704-1718)."""
+    if scr is None:
+        scr = screening(basis, tol)
+    shellptr, shellid, shellrid, shellvalue, _ = scr
+    ns, n = basis.nshells, basis.nbf
+    fs = [basis.func_start(s) for s in range(ns)]
+    dm = [basis.shell_dim(s) for s in range(ns)]
+
+    def sl(s):
+        return slice(fs[s], fs[s] + dm[s])
+
+    tol2 = tol * tol
+
+    def G(Dm):
+        X = np.zeros((n, n))
+        pairs = range(int(shellptr[0]), int(shellptr[ns]))
+        for i in pairs:
+            M, N, v1 = int(shellrid[i]), int(shellid[i]), float(shellvalue[i])
+            f1 = 1 if v1 < 0.0 else 0
+            for j in pairs:
+                P, Q, v2 = int(shellrid[j]), int(shellid[j]), float(shellvalue[j])
+                if (M > P and (M + P) % 2 == 1) or (M < P and (M + P) % 2 == 0):
+                    continue
+                if M == P and ((N > Q and (N + Q) % 2 == 1) or (N < Q and (N + Q) % 2 == 0)):
+                    continue
+                if abs(v1 * v2) < tol2:
+                    continue
+                f2 = 1 if v2 < 0.0 else 0
+                f3 = 0 if (M == P and N == Q) else 1
+                f4, f5, f6 = f1 & f2, f1 & f3, f2 & f3
+                f7 = f4 & f3
+                I = eri[sl(M), sl(N), sl(P), sl(Q)]
+                X[sl(M), sl(N)] += 2.0 * (1 + f1 + f2 + f4) * np.einsum("mnpq,pq->mn", I, Dm[sl(P), sl(Q)])
+                X[sl(P), sl(Q)] += 2.0 * (f3 + f5 + f6 + f7) * np.einsum("mnpq,mn->pq", I, Dm[sl(M), sl(N)])
+                X[sl(M), sl(P)] -= (1 + f3) * np.einsum("mnpq,nq->mp", I, Dm[sl(N), sl(Q)])
+                X[sl(N), sl(P)] -= (f1 + f5) * np.einsum("mnpq,mq->np", I, Dm[sl(M), sl(Q)])
+                X[sl(M), sl(Q)] -= (f2 + f6) * np.einsum("mnpq,np->mq", I, Dm[sl(N), sl(P)])
+                X[sl(N), sl(Q)] -= (f4 + f7) * np.einsum("mnpq,mp->nq", I, Dm[sl(M), sl(P)])
+        return X
+
+    D = np.asarray(D, dtype=np.float64)
+    return 0.5 * (G(D) + G(np.ascontiguousarray(D.T)).T)

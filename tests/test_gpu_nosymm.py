@@ -1,10 +1,13 @@
 """Non-symmetric densities (PFock_create with symm = 0), through the C ABI.
 
-The engine forms F = 2 J[D] - K[D] exactly for a general D (symmetric part
-through the usual build, antisymmetric part through the exchange terms only).
-Fixtures (tests/golden/nosymm/, made by tests/golden/make_nosymm.py) hold a
-seeded non-symmetric D and that F from the oracle's full ERI tensor; the
-formula itself reproduces the reference's symmetric-density F to 1e-14.
+By default the engine returns the reference's own symm = 0 result
+(pfock/pfock.c:1704-1718): (F[D] + F[D^T]^T) / 2 of its unique-quartet
+digestion, which for a non-symmetric D depends on the orientation of the
+shell-pair lists.  Mode "exact" returns F = 2 J[D] - K[D].  Fixtures
+(tests/golden/nosymm/, made by tests/golden/make_nosymm.py) hold a seeded
+non-symmetric D, the reference build's output for it (F_ns_ref) and, for the
+cases small enough for the oracle's full ERI tensor, the exact F (F_ns) and
+the oracle's restatement of the reference's digestion (F_ns_port).
 """
 import os
 
@@ -18,7 +21,7 @@ import gtfock_b200 as gb
 pytestmark = pytest.mark.gpu
 
 F_TOL = 1e-10
-CASES = ["h2o_631g", "h2o_ccpvdz"]
+CASES = ["h2o_631g", "h2o_ccpvdz", "ch4_ccpvdz", "c4h10_ccpvdz"]
 
 
 def _ns(case):
@@ -26,16 +29,47 @@ def _ns(case):
 
 
 @pytest.mark.parametrize("case", CASES)
-def test_nosymm_matches_exact(case, tmp_path):
+def test_nosymm_matches_reference(case, tmp_path):
     g = load_golden(case)
     ns = _ns(case)
     gbs, xyz = golden_xyz(g, tmp_path)
     b = gb.BasisSet(gbs, xyz)
     pf = gb.PFock(b, tolscr=float(g["tol"]), symm=0)
     F = pf.compute_fock(ns["D_ns"])
-    assert np.abs(F - ns["F_ns"]).max() < F_TOL
+    assert np.abs(F - ns["F_ns_ref"]).max() < F_TOL
+    if "F_ns_port" in ns:
+        assert np.abs(F - ns["F_ns_port"]).max() < F_TOL
     assert np.abs(F - F.T).max() > 1e-3          # the result is not symmetric
     # a symmetric D gives the symm = 1 result
     F2 = pf.compute_fock(g["D"])
     assert np.abs(F2 - g["F"]).max() < F_TOL
+    pf.close()
+
+
+@pytest.mark.parametrize("case", [c for c in CASES if c != "c4h10_ccpvdz"])
+def test_nosymm_exact(case, tmp_path):
+    g = load_golden(case)
+    ns = _ns(case)
+    gbs, xyz = golden_xyz(g, tmp_path)
+    b = gb.BasisSet(gbs, xyz)
+    pf = gb.PFock(b, tolscr=float(g["tol"]), symm=0)
+    pf.set_nosymm_mode("exact")
+    F = pf.compute_fock(ns["D_ns"])
+    assert np.abs(F - ns["F_ns"]).max() < F_TOL
+    F2 = pf.compute_fock(g["D"])
+    assert np.abs(F2 - g["F"]).max() < F_TOL
+    # and back to the reference's result on the same engine
+    pf.set_nosymm_mode("reference")
+    F3 = pf.compute_fock(ns["D_ns"])
+    assert np.abs(F3 - ns["F_ns_ref"]).max() < F_TOL
+    pf.close()
+
+
+def test_nosymm_mode_needs_symm0(tmp_path):
+    g = load_golden("h2o_631g")
+    gbs, xyz = golden_xyz(g, tmp_path)
+    b = gb.BasisSet(gbs, xyz)
+    pf = gb.PFock(b, tolscr=float(g["tol"]), symm=1)
+    with pytest.raises(gb.GtfError):
+        pf.set_nosymm_mode("exact")
     pf.close()
