@@ -26,6 +26,7 @@
 
 #include <vector>
 
+#include "diis_dev.cuh"
 #include "gtf_cuda.h"
 #include "gtfock_b200.h"
 
@@ -34,7 +35,7 @@ extern "C" int gtf_initial_density(BasisSet_t basis, double *D, int n);
 extern "C" void gtf_note_launches(int n);
 extern "C" const char *gtf_last_error(void);
 
-#define BJ_MAX_DIIS 10
+#define BJ_MAX_DIIS GTF_MAX_DIIS
 #define BJ_THREADS 256
 #define BJ_PUR_MAX 200
 #define BJ_PUR_CHECK 8
@@ -56,9 +57,9 @@ struct JobDev {
     const double *H, *S, *X;
     double *P, *P2, *P3, *W, *W2;  // purification (orthogonal basis) and scratch
     double *vecs, *Fvecs;          // DIIS error vectors and Fock matrices
+    DiisState *ds;                 // the job's DIIS bookkeeping (device)
     int n, nocc;
-    int cur;                       // DIIS slot of this iteration (-1: no DIIS)
-    int len;                       // DIIS vectors in use
+    int diis;                      // DIIS this iteration (else F = X F X only)
 };
 
 struct GemmDesc {
@@ -235,46 +236,77 @@ __global__ void __launch_bounds__(BJ_THREADS) k_j_energy(const JobDev *__restric
     if (threadIdx.x == 0) part[blockIdx.y * BJ_EBLOCKS + blockIdx.x] = e;
 }
 
-// cur = W2 - W2^T into the DIIS slot (pscf/purif.c:553-558); jobs with cur < 0 skip
+__global__ void k_j_diis_reset(DiisState *ds) { diis_reset(ds, threadIdx.x, blockDim.x); }
+
+// slot of this iteration's vectors, per DIIS job
+__global__ void k_j_diis_slot(const JobDev *__restrict__ jobs, int m)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < m && jobs[q].diis) diis_slot(jobs[q].ds);
+}
+
+// P2 = W2 - W2^T, the commutator of the error vector (pscf/purif.c:553-558);
+// P2 and P3 are free until the purification starts
 __global__ void k_j_antisym(const JobDev *__restrict__ jobs)
 {
     const JobDev j = jobs[blockIdx.y];
-    if (j.cur < 0) return;
+    if (!j.diis) return;
     const size_t nn = (size_t)j.n * j.n;
-    double *cur = j.vecs + nn * j.cur;
     for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += (size_t)gridDim.x * blockDim.x) {
         const int r = (int)(k / j.n), c = (int)(k % j.n);
-        cur[k] = j.W2[k] - j.W2[(size_t)c * j.n + r];
+        j.P2[k] = j.W2[k] - j.W2[(size_t)c * j.n + r];
     }
 }
 
-// dots[job][i] = <vecs[cur], vecs[i]>, i < len
+// dots[job][i] = <e, vecs[i]>, i < len, with e = P2 the error vector in the
+// orthogonal basis; slot cur stands for e, which is stored into it on the way
 __global__ void __launch_bounds__(BJ_THREADS) k_j_dots(const JobDev *__restrict__ jobs, double *__restrict__ dots)
 {
     __shared__ double sh[BJ_THREADS];
     const JobDev j = jobs[blockIdx.x];
-    if (j.cur < 0) return;
+    if (!j.diis) return;
     const size_t nn = (size_t)j.n * j.n;
-    const double *a = j.vecs + nn * j.cur;
-    for (int i = 0; i < j.len; i++) {
-        const double *b = j.vecs + nn * i;
+    const double *a = j.P2;
+    const int len = j.ds->len, cur = j.ds->cur;
+    for (int i = 0; i < len; i++) {
+        double *b = j.vecs + nn * i;
         double v = 0.0;
-        for (size_t k = threadIdx.x; k < nn; k += BJ_THREADS) v += a[k] * b[k];
+        if (i == cur) {
+            for (size_t k = threadIdx.x; k < nn; k += BJ_THREADS) {
+                const double x = a[k];
+                b[k] = x;
+                v += x * x;
+            }
+        } else {
+            for (size_t k = threadIdx.x; k < nn; k += BJ_THREADS) v += a[k] * b[k];
+        }
         v = block_sum(v, sh);
         if (threadIdx.x == 0) dots[blockIdx.x * BJ_MAX_DIIS + i] = v;
     }
 }
 
-// F = sum_i c_i Fvecs_i
-__global__ void k_j_combine(const JobDev *__restrict__ jobs, const double *__restrict__ coef)
+// new row and column of the bordered matrix, then the coefficients: one warp per job
+__global__ void k_j_diis_solve(const JobDev *__restrict__ jobs, const double *__restrict__ dots)
+{
+    const JobDev j = jobs[blockIdx.x];
+    if (!j.diis) return;
+    diis_update_solve(j.ds, dots + blockIdx.x * BJ_MAX_DIIS, threadIdx.x);
+}
+
+// F = sum_i c_i Fvecs_i, slot cur standing for this iteration's X F X (P3),
+// which is stored into it on the way
+__global__ void k_j_combine(const JobDev *__restrict__ jobs)
 {
     const JobDev j = jobs[blockIdx.y];
-    if (j.cur < 0) return;
+    if (!j.diis) return;
     const size_t nn = (size_t)j.n * j.n;
-    const double *c = coef + blockIdx.y * BJ_MAX_DIIS;
+    const int len = j.ds->len, cur = j.ds->cur;
+    const double *c = j.ds->co;
     for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += (size_t)gridDim.x * blockDim.x) {
+        const double fx = j.P3[k];
+        j.Fvecs[nn * cur + k] = fx;
         double v = 0.0;
-        for (int i = 0; i < j.len; i++) v += c[i] * j.Fvecs[nn * i + k];
+        for (int i = 0; i < len; i++) v += c[i] * (i == cur ? fx : j.Fvecs[nn * i + k]);
         j.F[k] = v;
     }
 }
@@ -413,10 +445,6 @@ struct BJob {
     int iter, max_iters, done, failed;
     double etol, e_prev;
     std::vector<double> energies;
-    // DIIS state (pscf/purif.c:491-641)
-    int len_diis, bmax_id;
-    double bmax;
-    double b[BJ_MAX_DIIS + 1][BJ_MAX_DIIS + 1];
     int pur_iters;
     long long pur_total;           // purification iterations over all steps
 };
@@ -437,13 +465,14 @@ struct gtf_batch {
     JobDev *d_jobs;
     GemmDesc *d_gd;                // 10 call sets x capacity
     int *d_tp;                     // 10 call sets x (capacity + 1)
-    double *d_energy, *d_dots, *d_coef, *d_scal;
+    double *d_energy, *d_dots, *d_scal;
+    DiisState *d_diis;             // per slot: the job's DIIS bookkeeping
     int *d_active, *d_iters, *d_count, *d_list;
     // pinned mirrors
     JobDev *h_jobs;
     GemmDesc *h_gd;
     int *h_tp;
-    double *h_energy, *h_dots, *h_coef;
+    double *h_energy;
     int *h_iters, *h_count, *h_act, *h_list;
     size_t dev_bytes_jobs;
     double ms_fock, ms_rest, ms_energy, ms_diis, ms_pur, pur_steps, nsteps;
@@ -492,12 +521,11 @@ extern "C" void gtf_batch_destroy(gtf_batch_t *b)
     if (b->fb) gtf_fock_batch_destroy(b->fb);
     for (auto &j : b->jobs)
         if (j.used) job_free(j);
-    void *dp[] = {b->d_jobs, b->d_gd, b->d_tp, b->d_energy, b->d_dots, b->d_coef, b->d_scal, b->d_active,
+    void *dp[] = {b->d_jobs, b->d_gd, b->d_tp, b->d_energy, b->d_dots, b->d_diis, b->d_scal, b->d_active,
                   b->d_iters, b->d_count, b->d_list};
     for (void *p : dp)
         if (p) cudaFree(p);
-    void *hp[] = {b->h_jobs, b->h_gd, b->h_tp, b->h_energy, b->h_dots, b->h_coef, b->h_iters, b->h_count,
-                  b->h_act, b->h_list};
+    void *hp[] = {b->h_jobs, b->h_gd, b->h_tp, b->h_energy, b->h_iters, b->h_count, b->h_act, b->h_list};
     for (void *p : hp)
         if (p) cudaFreeHost(p);
     cudaEventDestroy(b->e0);
@@ -529,7 +557,7 @@ extern "C" gtf_batch_t *gtf_batch_create(int capacity)
     ok = ok && cudaMalloc(&b->d_tp, sizeof(int) * (C + 1) * NSETS) == cudaSuccess;
     ok = ok && cudaMalloc(&b->d_energy, sizeof(double) * C * BJ_EBLOCKS) == cudaSuccess;
     ok = ok && cudaMalloc(&b->d_dots, sizeof(double) * C * BJ_MAX_DIIS) == cudaSuccess;
-    ok = ok && cudaMalloc(&b->d_coef, sizeof(double) * C * BJ_MAX_DIIS) == cudaSuccess;
+    ok = ok && cudaMalloc(&b->d_diis, sizeof(DiisState) * C) == cudaSuccess;
     ok = ok && cudaMalloc(&b->d_scal, sizeof(double) * C * 8) == cudaSuccess;
     ok = ok && cudaMalloc(&b->d_active, sizeof(int) * C) == cudaSuccess;
     ok = ok && cudaMalloc(&b->d_iters, sizeof(int) * C) == cudaSuccess;
@@ -541,8 +569,6 @@ extern "C" gtf_batch_t *gtf_batch_create(int capacity)
     ok = ok && cudaMallocHost(&b->h_gd, sizeof(GemmDesc) * C * NSETS) == cudaSuccess;
     ok = ok && cudaMallocHost(&b->h_tp, sizeof(int) * (C + 1) * NSETS) == cudaSuccess;
     ok = ok && cudaMallocHost(&b->h_energy, sizeof(double) * C * BJ_EBLOCKS) == cudaSuccess;
-    ok = ok && cudaMallocHost(&b->h_dots, sizeof(double) * C * BJ_MAX_DIIS) == cudaSuccess;
-    ok = ok && cudaMallocHost(&b->h_coef, sizeof(double) * C * BJ_MAX_DIIS) == cudaSuccess;
     ok = ok && cudaMallocHost(&b->h_iters, sizeof(int) * C) == cudaSuccess;
     ok = ok && cudaMallocHost(&b->h_count, sizeof(int)) == cudaSuccess;
     if (!ok) {
@@ -551,15 +577,6 @@ extern "C" gtf_batch_t *gtf_batch_create(int capacity)
         return nullptr;
     }
     return b;
-}
-
-static void diis_reset(BJob &j)
-{
-    j.len_diis = 0;
-    j.bmax = DBL_MIN;
-    j.bmax_id = -1;
-    for (int r = 0; r <= BJ_MAX_DIIS; r++)
-        for (int c = 0; c <= BJ_MAX_DIIS; c++) j.b[r][c] = (r != c) ? -1.0 : 0.0;
 }
 
 // Set-up of one SCF job (pscf/scf.c:298-314, init_oedmat pscf/scf.c:131-185)
@@ -644,8 +661,9 @@ extern "C" int gtf_batch_add(gtf_batch_t *b, const char *bsfile, const char *xyz
     }
     d.n = j.n;
     d.nocc = j.nocc;
-    d.cur = -1;
-    d.len = 0;
+    d.diis = 0;
+    d.ds = b->d_diis + slot;
+    k_j_diis_reset<<<1, 128, 0, b->st>>>(d.ds);
     // initial guess (pscf/scf.c:34-76) into the engine's density buffer
     std::vector<double> D0(nn);
     gtf_initial_density(j.basis, D0.data(), j.n);
@@ -660,7 +678,6 @@ extern "C" int gtf_batch_add(gtf_batch_t *b, const char *bsfile, const char *xyz
     j.e_prev = 0.0;
     j.done = 0;
     j.failed = 0;
-    diis_reset(j);
     b->dirty = 1;
     return slot;
 }
@@ -722,56 +739,6 @@ static void set_gemm(gtf_batch *b, int s, int k, const double *A, const double *
     int *tp = b->h_tp + (size_t)s * (b->capacity + 1);
     if (k == 0) tp[0] = 0;
     tp[k + 1] = tp[k] + ntr * ntc;
-}
-
-// inverse of the bordered DIIS matrix by Gauss-Jordan with partial pivoting;
-// coeffs[i] = -inv[i][m] (as the single-job path)
-static void diis_coeffs(const double (&bm)[BJ_MAX_DIIS + 1][BJ_MAX_DIIS + 1], int m, double *coeffs)
-{
-    const int s = m + 1;
-    double a[BJ_MAX_DIIS + 1][2 * (BJ_MAX_DIIS + 1)];
-    for (int i = 0; i < s; i++)
-        for (int j = 0; j < s; j++) {
-            a[i][j] = bm[i][j];
-            a[i][s + j] = (i == j) ? 1.0 : 0.0;
-        }
-    for (int c = 0; c < s; c++) {
-        int piv = c;
-        for (int r = c + 1; r < s; r++)
-            if (fabs(a[r][c]) > fabs(a[piv][c])) piv = r;
-        if (piv != c)
-            for (int j = 0; j < 2 * s; j++) {
-                const double t = a[c][j];
-                a[c][j] = a[piv][j];
-                a[piv][j] = t;
-            }
-        const double d = a[c][c];
-        for (int j = 0; j < 2 * s; j++) a[c][j] /= d;
-        for (int r = 0; r < s; r++) {
-            if (r == c) continue;
-            const double f = a[r][c];
-            if (f == 0.0) continue;
-            for (int j = 0; j < 2 * s; j++) a[r][j] -= f * a[c][j];
-        }
-    }
-    for (int i = 0; i < s; i++) coeffs[i] = -a[i][s + s - 1];
-}
-
-// The bordered matrix lives in the top-left (len+1) x (len+1) block with the
-// border in row/column len (pscf/purif.c:600-620).  The single-job path keeps
-// it the same way: entries b[i][j] for i, j < len are error dot products,
-// the rest -1 off the diagonal and 0 on it.
-static void diis_update(BJob &j, int cur_idx, const double *dots)
-{
-    for (int i = 0; i < j.len_diis; i++) j.b[cur_idx][i] = dots[i];
-    j.bmax = -DBL_MAX;
-    for (int i = 0; i < j.len_diis; i++) {
-        j.b[i][cur_idx] = j.b[cur_idx][i];
-        if (j.bmax < j.b[i][i]) {
-            j.bmax = j.b[i][i];
-            j.bmax_id = i;
-        }
-    }
 }
 
 // One SCF iteration of every running job.  Returns the number of jobs still
@@ -868,8 +835,7 @@ extern "C" int gtf_batch_step(gtf_batch_t *b)
     const int M = (int)run.size();
     for (int k = 0; k < M; k++) {
         BJob &j = b->jobs[run[k]];
-        j.dv.cur = -1;
-        j.dv.len = j.len_diis;
+        j.dv.diis = 0;
         b->h_jobs[k] = j.dv;
     }
     CKH(cudaMemcpyAsync(b->d_jobs, b->h_jobs, sizeof(JobDev) * M, cudaMemcpyHostToDevice, b->st));
@@ -907,27 +873,18 @@ extern "C" int gtf_batch_step(gtf_batch_t *b)
             BJob &j = b->jobs[run[cont[q]]];
             JobDev &d = j.dv;
             const int it = j.iter - 1;   // this iteration's index
-            const size_t nn = (size_t)j.n * j.n;
-            d.cur = -1;
+            // DIIS jobs: the error vector and X F X go through P2 and P3,
+            // and the device bookkeeping stores them into the job's slot
+            d.diis = it > 1;
             double *target = d.F;
-            if (it > 1) {
-                int cur_idx;
-                if (j.len_diis < BJ_MAX_DIIS) {
-                    cur_idx = j.len_diis;
-                    j.len_diis++;
-                } else {
-                    cur_idx = j.bmax_id;
-                }
-                d.cur = cur_idx;
-                double *cur = d.vecs + nn * cur_idx;
-                target = d.Fvecs + nn * cur_idx;
+            if (d.diis) {
+                target = d.P3;
                 set_gemm(b, 0, nd, d.F, d.D, d.W, j.n, -1);
                 set_gemm(b, 1, nd, d.W, d.S, d.W2, j.n, -1);
-                set_gemm(b, 2, nd, d.X, cur, d.W, j.n, -1);
-                set_gemm(b, 3, nd, d.W, d.X, cur, j.n, -1);
+                set_gemm(b, 2, nd, d.X, d.P2, d.W, j.n, -1);
+                set_gemm(b, 3, nd, d.W, d.X, d.P2, j.n, -1);
                 nd++;
             }
-            d.len = j.len_diis;
             set_gemm(b, 4, q, d.X, d.F, d.W, j.n, -1);
             set_gemm(b, 5, q, d.W, d.X, target, j.n, -1);
             set_gemm(b, 6, q, d.P, d.P, d.P2, j.n, q);
@@ -936,8 +893,8 @@ extern "C" int gtf_batch_step(gtf_batch_t *b)
             set_gemm(b, 9, q, d.W, d.X, d.D, j.n, -1);
             b->h_jobs[q] = d;
         }
-        // DIIS-set descriptors come first in `cont` order: remap antisym /
-        // dots / combine through JobDev.cur (jobs without DIIS have cur < 0)
+        // DIIS-set descriptors come first in `cont` order; the slot, antisym,
+        // dots, solve and combine kernels skip the jobs without DIIS
         const size_t C1 = b->capacity + 1;
         CKH(cudaMemcpyAsync(b->d_jobs, b->h_jobs, sizeof(JobDev) * C, cudaMemcpyHostToDevice, b->st));
         CKH(cudaMemcpyAsync(b->d_gd, b->h_gd, sizeof(GemmDesc) * b->capacity * NSETS, cudaMemcpyHostToDevice, b->st));
@@ -946,6 +903,9 @@ extern "C" int gtf_batch_step(gtf_batch_t *b)
         for (int q = 0; q < C; q++) maxn = b->h_jobs[q].n > maxn ? b->h_jobs[q].n : maxn;
         const unsigned ge = (unsigned)(((size_t)maxn * maxn + 255) / 256 < 1024 ? ((size_t)maxn * maxn + 255) / 256 : 1024);
         if (nd > 0) {
+            k_j_diis_slot<<<(C + 127) / 128, 128, 0, b->st>>>(b->d_jobs, C);
+            CKH(cudaGetLastError());
+            launches++;
             if (run_gemm(b, 0, nd, true, nullptr, &launches) || run_gemm(b, 1, nd, true, nullptr, &launches))
                 return -4;
             k_j_antisym<<<dim3(ge, C), 256, 0, b->st>>>(b->d_jobs);
@@ -954,37 +914,14 @@ extern "C" int gtf_batch_step(gtf_batch_t *b)
             if (run_gemm(b, 2, nd, true, nullptr, &launches) || run_gemm(b, 3, nd, true, nullptr, &launches))
                 return -4;
             k_j_dots<<<C, BJ_THREADS, 0, b->st>>>(b->d_jobs, b->d_dots);
+            k_j_diis_solve<<<C, 32, 0, b->st>>>(b->d_jobs, b->d_dots);
             CKH(cudaGetLastError());
-            launches++;
-            CKH(cudaMemcpyAsync(b->h_dots, b->d_dots, sizeof(double) * C * BJ_MAX_DIIS, cudaMemcpyDeviceToHost,
-                                b->st));
+            launches += 2;
         }
         // F' = X F X^T (pscf/purif.c:620-636)
         if (run_gemm(b, 4, C, true, nullptr, &launches) || run_gemm(b, 5, C, true, nullptr, &launches)) return -4;
         if (nd > 0) {
-            CKH(cudaStreamSynchronize(b->st));
-            for (int q = 0; q < C; q++) {
-                BJob &j = b->jobs[run[cont[q]]];
-                const int cur_idx = b->h_jobs[q].cur;
-                double *co = b->h_coef + q * BJ_MAX_DIIS;
-                for (int i = 0; i < BJ_MAX_DIIS; i++) co[i] = 0.0;
-                if (cur_idx < 0) continue;
-                diis_update(j, cur_idx, b->h_dots + q * BJ_MAX_DIIS);
-                double cf[BJ_MAX_DIIS + 1];
-                // the bordered system: copy with the border at index len
-                double bm[BJ_MAX_DIIS + 1][BJ_MAX_DIIS + 1];
-                const int L = j.len_diis;
-                for (int r = 0; r <= L; r++)
-                    for (int c = 0; c <= L; c++)
-                        bm[r][c] = (r < L && c < L) ? j.b[r][c] : ((r == c) ? 0.0 : -1.0);
-                diis_coeffs(bm, L, cf);
-                bool finite = true;
-                for (int i = 0; i < L; i++) finite = finite && isfinite(cf[i]);
-                for (int i = 0; i < L; i++) co[i] = finite ? cf[i] : (i == cur_idx ? 1.0 : 0.0);
-            }
-            CKH(cudaMemcpyAsync(b->d_coef, b->h_coef, sizeof(double) * C * BJ_MAX_DIIS, cudaMemcpyHostToDevice,
-                                b->st));
-            k_j_combine<<<dim3(ge, C), 256, 0, b->st>>>(b->d_jobs, b->d_coef);
+            k_j_combine<<<dim3(ge, C), 256, 0, b->st>>>(b->d_jobs);
             CKH(cudaGetLastError());
             launches++;
         }

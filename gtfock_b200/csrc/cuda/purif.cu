@@ -15,11 +15,11 @@
 #include <stdio.h>
 #include <string.h>
 
+#include "diis_dev.cuh"
 #include "gtf_cuda.h"
 
 #define PUR_MAX_ITERS 200
-#define PUR_MAX_DIIS 10
-#define PUR_LDB 128
+#define PUR_MAX_DIIS GTF_MAX_DIIS
 #define RED_BLOCKS 148
 #define RED_THREADS 256
 
@@ -50,10 +50,8 @@ struct gtf_purif_dev {
     double *part;     // [RED_BLOCKS * 16] block partials
     double *scal;     // device scalars
     double *h_scal;   // pinned mirror
-    double *h_part;   // host copy of the DIIS dot-product partials
-    int len_diis, bmax_id;
-    double bmax;
-    double b[PUR_LDB * PUR_LDB];
+    double *E;        // this iteration's DIIS error vector, before it enters its slot
+    struct DiisState *ds;   // device: DIIS bookkeeping and coefficients
     int sx_set;
     cudaEvent_t e0, e1;
     double ms_gemm, ms_total, errnorm, idem, trerr;
@@ -266,16 +264,30 @@ __global__ void k_antisym(const double *__restrict__ W, double *__restrict__ cur
     cur[(size_t)i * n + j] = W[(size_t)i * n + j] - W[(size_t)j * n + i];
 }
 
-// block partials of <a, b_k> for k < m
-__global__ void k_dots(const double *__restrict__ a, const double *__restrict__ vecs, size_t nn, int m,
+__global__ void k_diis_reset(DiisState *ds) { diis_reset(ds, threadIdx.x, blockDim.x); }
+
+// slot of this iteration: the next free one, else the largest-error one
+__global__ void k_diis_slot(DiisState *ds) { diis_slot(ds); }
+
+// block partials of <e, e_k> for the stored vectors k < len, slot `cur`
+// standing for e itself, which is stored into it on the way
+__global__ void k_dots(const double *__restrict__ e, double *__restrict__ vecs, size_t nn, const DiisState *ds,
                        double *__restrict__ part)
 {
     __shared__ double s[RED_THREADS];
+    const int m = ds->len, cur = ds->cur;
     for (int k = 0; k < m; k++) {
-        const double *b = vecs + nn * k;
+        double *b = vecs + nn * k;
         double v = 0.0;
-        for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += (size_t)gridDim.x * blockDim.x)
-            v += a[i] * b[i];
+        for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += (size_t)gridDim.x * blockDim.x) {
+            const double a = e[i];
+            if (k == cur) {
+                b[i] = a;
+                v += a * a;
+            } else {
+                v += a * b[i];
+            }
+        }
         s[threadIdx.x] = v;
         __syncthreads();
         for (int st = RED_THREADS / 2; st > 0; st >>= 1) {
@@ -287,16 +299,34 @@ __global__ void k_dots(const double *__restrict__ a, const double *__restrict__ 
     }
 }
 
-struct Coeffs {
-    double c[PUR_MAX_DIIS];
-};
+// New row and column of b from the block partials, then the largest-error
+// slot and the coefficients (diis_coefficients).  One warp: lane i sums the
+// partials of column i in block order.
+__global__ void k_diis_solve(const double *__restrict__ part, DiisState *ds)
+{
+    __shared__ double dots[PUR_MAX_DIIS];
+    const int lane = threadIdx.x;
+    if (lane < ds->len) {
+        double v = 0.0;
+        for (int bk = 0; bk < RED_BLOCKS; bk++) v += part[bk * PUR_MAX_DIIS + lane];
+        dots[lane] = v;
+    }
+    __syncwarp();
+    diis_update_solve(ds, dots, lane);
+}
 
-__global__ void k_combine(double *__restrict__ F, const double *__restrict__ Fvecs, size_t nn, int m, Coeffs co)
+// F = sum_i c_i F_i over the stored Fock matrices, slot `cur` standing for
+// this iteration's X F X (Fx), which is stored into it on the way
+__global__ void k_combine(double *__restrict__ F, double *__restrict__ Fvecs, const double *__restrict__ Fx, size_t nn,
+                          const DiisState *ds)
 {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nn) return;
+    const int m = ds->len, cur = ds->cur;
+    const double fx = Fx[k];
+    Fvecs[nn * cur + k] = fx;
     double v = 0.0;
-    for (int i = 0; i < m; i++) v += co.c[i] * Fvecs[nn * i + k];
+    for (int i = 0; i < m; i++) v += ds->co[i] * (i == cur ? fx : Fvecs[nn * i + k]);
     F[k] = v;
 }
 
@@ -313,20 +343,18 @@ extern "C" int gtf_purif_create(int nbf, int nocc, void *stream, gtf_purif_dev_t
     CKB(cublasCreate(&p->blas));
     CKB(cublasSetStream(p->blas, p->st));
     const size_t nn = (size_t)nbf * nbf;
-    double **bufs[] = {&p->S, &p->X, &p->D, &p->D2, &p->D3, &p->F, &p->W, &p->W2};
+    double **bufs[] = {&p->S, &p->X, &p->D, &p->D2, &p->D3, &p->F, &p->W, &p->W2, &p->E};
     for (double **b : bufs) CKP(cudaMalloc((void **)b, sizeof(double) * nn));
     CKP(cudaMalloc((void **)&p->vecs, sizeof(double) * nn * PUR_MAX_DIIS));
     CKP(cudaMalloc((void **)&p->Fvecs, sizeof(double) * nn * PUR_MAX_DIIS));
     CKP(cudaMalloc((void **)&p->part, sizeof(double) * RED_BLOCKS * 16));
     CKP(cudaMalloc((void **)&p->scal, sizeof(double) * 16));
     CKP(cudaMallocHost((void **)&p->h_scal, sizeof(double) * 16));
-    CKP(cudaMallocHost((void **)&p->h_part, sizeof(double) * RED_BLOCKS * PUR_MAX_DIIS));
+    CKP(cudaMalloc((void **)&p->ds, sizeof(DiisState)));
     CKP(cudaEventCreate(&p->e0));
     CKP(cudaEventCreate(&p->e1));
-    p->bmax = DBL_MIN;
-    p->bmax_id = -1;
-    for (int i = 0; i < PUR_LDB; i++)
-        for (int j = 0; j < PUR_LDB; j++) p->b[i * PUR_LDB + j] = (i != j) ? -1.0 : 0.0;
+    k_diis_reset<<<1, 128, 0, p->st>>>(p->ds);
+    CKP(cudaGetLastError());
     *out = p;
     return GTF_OK;
 }
@@ -353,25 +381,22 @@ extern "C" void gtf_purif_destroy(gtf_purif_dev_t *p)
     if (!p) return;
     cudaStreamSynchronize(p->st);
     if (p->bx) gtf_bf16x3_destroy(p->bx);
-    double *bufs[] = {p->S, p->X, p->D, p->D2, p->D3, p->F, p->W, p->W2, p->vecs, p->Fvecs, p->part, p->scal};
+    double *bufs[] = {p->S, p->X, p->D, p->D2, p->D3, p->F, p->W, p->W2, p->E, p->vecs, p->Fvecs, p->part, p->scal};
     for (double *b : bufs)
         if (b) cudaFree(b);
+    if (p->ds) cudaFree(p->ds);
     if (p->h_scal) cudaFreeHost(p->h_scal);
-    if (p->h_part) cudaFreeHost(p->h_part);
     cublasDestroy(p->blas);
     cudaEventDestroy(p->e0);
     cudaEventDestroy(p->e1);
     delete p;
 }
 
-// forget the DIIS history (a new SCF solve starts)
+// forget the DIIS history (a new SCF solve starts); stream-ordered
 extern "C" void gtf_purif_reset(gtf_purif_dev_t *p)
 {
-    p->len_diis = 0;
-    p->bmax = DBL_MIN;
-    p->bmax_id = -1;
-    for (int i = 0; i < PUR_LDB; i++)
-        for (int j = 0; j < PUR_LDB; j++) p->b[i * PUR_LDB + j] = (i != j) ? -1.0 : 0.0;
+    k_diis_reset<<<1, 128, 0, p->st>>>(p->ds);
+    gtf_note_launches(1);
 }
 
 extern "C" int gtf_purif_set_sx(gtf_purif_dev_t *p, const double *S_host, const double *X_host)
@@ -487,99 +512,35 @@ extern "C" int gtf_purif_run(gtf_purif_dev_t *p, const double *F_host, double *D
     return GTF_OK;
 }
 
-// inverse of the bordered DIIS matrix (symmetric, order <= 11) by Gauss-Jordan
-// elimination with partial pivoting; returns coeffs[i] = -inv[i][m]
-static void diis_coeffs(const double *b, int m, double *coeffs)
-{
-    const int s = m + 1;
-    double a[PUR_MAX_DIIS + 1][2 * (PUR_MAX_DIIS + 1)];
-    for (int i = 0; i < s; i++)
-        for (int j = 0; j < s; j++) {
-            a[i][j] = b[i * PUR_LDB + j];
-            a[i][s + j] = (i == j) ? 1.0 : 0.0;
-        }
-    for (int c = 0; c < s; c++) {
-        int piv = c;
-        for (int r = c + 1; r < s; r++)
-            if (fabs(a[r][c]) > fabs(a[piv][c])) piv = r;
-        if (piv != c)
-            for (int j = 0; j < 2 * s; j++) {
-                double t = a[c][j];
-                a[c][j] = a[piv][j];
-                a[piv][j] = t;
-            }
-        const double d = a[c][c];
-        for (int j = 0; j < 2 * s; j++) a[c][j] /= d;
-        for (int r = 0; r < s; r++) {
-            if (r == c) continue;
-            const double f = a[r][c];
-            if (f == 0.0) continue;
-            for (int j = 0; j < 2 * s; j++) a[r][j] -= f * a[c][j];
-        }
-    }
-    for (int i = 0; i < s; i++) coeffs[i] = -a[i][s + s - 1];
-}
-
+// One DIIS step (pscf/purif.c:491-641) with its bookkeeping on the device:
+// no host synchronisation.  iter <= 1: F = X F X only.
 extern "C" int gtf_diis_step_dev(gtf_purif_dev_t *p, const double *D_dev, double *F_dev, int iter)
 {
     const int n = p->n;
     const size_t nn = (size_t)n * n;
     cudaStream_t st = p->st;
-    double *cur_F = F_dev;
-    if (iter > 1) {
-        int cur_idx;
-        if (p->len_diis < PUR_MAX_DIIS) {
-            cur_idx = p->len_diis;
-            p->len_diis++;
-        } else {
-            cur_idx = p->bmax_id;
-        }
-        double *cur = p->vecs + nn * cur_idx;
-        cur_F = p->Fvecs + nn * cur_idx;
-        if (gemm_abt(p, F_dev, D_dev, p->W)) return GTF_ERR_CUDA;
-        if (gemm_abt(p, p->W, p->S, p->W2)) return GTF_ERR_CUDA;
-        dim3 g((n + 127) / 128, n);
-        k_antisym<<<g, 128, 0, st>>>(p->W2, cur, n);
-        if (gemm_abt(p, p->X, cur, p->W)) return GTF_ERR_CUDA;
-        if (gemm_abt(p, p->W, p->X, cur)) return GTF_ERR_CUDA;
-        k_dots<<<RED_BLOCKS, RED_THREADS, 0, st>>>(cur, p->vecs, nn, p->len_diis, p->part);
-        CKP(cudaGetLastError());
-        gtf_note_launches(2);
-        double *hpart = p->h_part;   // per object: engines may run on several host threads
-        CKP(cudaMemcpyAsync(hpart, p->part, sizeof(double) * RED_BLOCKS * PUR_MAX_DIIS, cudaMemcpyDeviceToHost, st));
-        CKP(cudaStreamSynchronize(st));
-        for (int i = 0; i < p->len_diis; i++) {
-            double v = 0.0;
-            for (int bk = 0; bk < RED_BLOCKS; bk++) v += hpart[bk * PUR_MAX_DIIS + i];
-            p->b[cur_idx * PUR_LDB + i] = v;
-        }
-        p->bmax = -DBL_MAX;
-        for (int i = 0; i < p->len_diis; i++) {
-            p->b[i * PUR_LDB + cur_idx] = p->b[cur_idx * PUR_LDB + i];
-            if (p->bmax < p->b[i * PUR_LDB + i]) {
-                p->bmax = p->b[i * PUR_LDB + i];
-                p->bmax_id = i;
-            }
-        }
+    if (iter <= 1) {
+        // F = X F X
+        if (gemm_abt(p, p->X, F_dev, p->W)) return GTF_ERR_CUDA;
+        if (gemm_abt(p, p->W, p->X, F_dev)) return GTF_ERR_CUDA;
+        return GTF_OK;
     }
-    // F = X F X
+    k_diis_slot<<<1, 1, 0, st>>>(p->ds);
+    // error vector e = X (F D S - S D F) X (pscf/purif.c:540-566)
+    if (gemm_abt(p, F_dev, D_dev, p->W)) return GTF_ERR_CUDA;
+    if (gemm_abt(p, p->W, p->S, p->W2)) return GTF_ERR_CUDA;
+    dim3 g((n + 127) / 128, n);
+    k_antisym<<<g, 128, 0, st>>>(p->W2, p->E, n);
+    if (gemm_abt(p, p->X, p->E, p->W)) return GTF_ERR_CUDA;
+    if (gemm_abt(p, p->W, p->X, p->E)) return GTF_ERR_CUDA;
+    k_dots<<<RED_BLOCKS, RED_THREADS, 0, st>>>(p->E, p->vecs, nn, p->ds, p->part);
+    k_diis_solve<<<1, 32, 0, st>>>(p->part, p->ds);
+    // this iteration's X F X, then the extrapolation
     if (gemm_abt(p, p->X, F_dev, p->W)) return GTF_ERR_CUDA;
-    if (gemm_abt(p, p->W, p->X, cur_F)) return GTF_ERR_CUDA;
-    if (iter > 1) {
-        double co[PUR_MAX_DIIS + 1];
-        diis_coeffs(p->b, p->len_diis, co);
-        // a singular bordered system (two identical error vectors) gives
-        // non-finite coefficients: keep this iteration's F unextrapolated
-        bool finite = true;
-        for (int i = 0; i < p->len_diis; i++) finite = finite && isfinite(co[i]);
-        if (!finite)
-            for (int i = 0; i < p->len_diis; i++) co[i] = (cur_F == p->Fvecs + nn * i) ? 1.0 : 0.0;
-        Coeffs c;
-        for (int i = 0; i < PUR_MAX_DIIS; i++) c.c[i] = (i < p->len_diis) ? co[i] : 0.0;
-        k_combine<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(F_dev, p->Fvecs, nn, p->len_diis, c);
-        CKP(cudaGetLastError());
-        gtf_note_launches(1);
-    }
+    if (gemm_abt(p, p->W, p->X, p->W2)) return GTF_ERR_CUDA;
+    k_combine<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(F_dev, p->Fvecs, p->W2, nn, p->ds);
+    CKP(cudaGetLastError());
+    gtf_note_launches(5);
     return GTF_OK;
 }
 
