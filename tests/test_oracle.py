@@ -129,6 +129,18 @@ def test_fixtures_pinned_to_reference_build():
         assert float(g["ref_max_dF"]) < 1e-11, case
 
 
+def test_large_fixtures_pinned_to_reference_build():
+    """The benchmark-size fixtures (C54H18, (H2O)64, C96H24) carry the
+    reference build's F for the same density and lists (tests/golden/make_large.py)."""
+    d = os.path.join(GOLDEN, "large")
+    names = sorted(f[:-4] for f in os.listdir(d) if f.endswith(".npz"))
+    assert names == ["c54h18_ccpvdz", "c96h24_ccpvdz", "w64_631g"]
+    for n in names:
+        g = np.load(os.path.join(d, n + ".npz"))
+        assert int(g["ref_pinned"]) == 1, n
+        assert float(g["ref_max_dF"]) < 1e-11, n
+
+
 REF_PROBE = os.path.join(ROOT, "oracle", "_ref", "ref_probe")
 
 
