@@ -626,6 +626,42 @@ def served_measure(count, seed, rate, cut, slots, lanes, incremental, concurrent
     return out
 
 
+def run_served_tau(args):
+    """Served-form screening sweep (--workload served-tau): the largest
+    request below 1000 functions of the served stream (32 requests, seed 7,
+    rate 4/s), solved to |dE| < 1e-6 Ha (30 iterations at most) on the plain
+    FP64 path and in the served form (FP32 quartets below 1e-6, incremental
+    builds, full every 8) with the quartets of the density change dropped
+    below bound x max|dD| < tau for tau = the Schwarz threshold (the
+    default), 1e-9, 1e-8, 1e-7: solve time (set-up excluded, one warm-up
+    solve first) and |E - E_FP64|."""
+    import gtfock_b200 as gb
+    from gtfock_b200 import molecules as mol, workloads
+    items = workloads.served(32, 7, 4.0)
+    t, name, atoms, basis, nbf = max((i for i in items if i[4] < 1000), key=lambda i: i[4])
+    rows = []
+    with tempfile.TemporaryDirectory() as td:
+        xyz = mol.write_xyz(atoms, os.path.join(td, name + ".xyz"), name)
+        gbs = mol.basis_file(basis)
+        for label, prec, tau in [("fp64", 0, None), ("served, tau 1e-10 (default)", 1, 0.0),
+                                 ("served, tau 1e-9", 1, 1e-9), ("served, tau 1e-8", 1, 1e-8),
+                                 ("served, tau 1e-7", 1, 1e-7)]:
+            s = gb.SCFSolver(gbs, xyz, tolscr=TOL)
+            s.set_options(precision=prec, fp32_cutoff=1e-6 if prec else 0.0, etol=1e-6)
+            if tau is not None:
+                s.set_incremental(True, tau, INCR_PERIOD)
+            s.solve(niters=2)
+            t0 = time.perf_counter()
+            e, _ = s.solve(niters=30)
+            dt = time.perf_counter() - t0
+            s.close()
+            rows.append({"form": label, "solve_s": dt, "iterations": len(e), "energy": float(e[-1])})
+    for r in rows:
+        r["dE_vs_fp64"] = abs(r["energy"] - rows[0]["energy"])
+        r["speedup_vs_fp64"] = rows[0]["solve_s"] / r["solve_s"]
+    print(json.dumps({"workload": "%s (%d bf) of the served stream" % (name, nbf), "rows": rows}), flush=True)
+
+
 def run_precision(args):
     """Precision variant: (H2O)64 / 6-31G (832 bf, seed 2024), FP32 ERIs below
     a Schwarz-bound cutoff swept over 1e-4 .. 1e-8, against the FP64 path:
@@ -726,10 +762,12 @@ def main():
                     help="two SCF iterations of (H2O)64 with the split-BF16 purification (ncu case)")
     ap.add_argument("--fp32-cutoff", type=float, default=None,
                     help="with --profile-fock: FP32 for quartets with Schwarz bound below this")
-    ap.add_argument("--workload", choices=["default", "batched", "served", "precision", "c12h26", "batch-scaling"], default="default",
+    ap.add_argument("--workload", choices=["default", "batched", "served", "served-tau", "precision", "c12h26",
+                                           "batch-scaling"], default="default",
                     help="batched / served / precision: the batched, served and precision-sweep workloads; "
                          "c12h26: the 10-iteration C12H26 solve timed beside the reference driver; "
-                         "batch-scaling: large molecules in one batch against builds alone")
+                         "batch-scaling: large molecules in one batch against builds alone; "
+                         "served-tau: screening of the density change swept on one served request")
     ap.add_argument("--count", type=int, default=None, help="molecules (batched) or requests (served)")
     ap.add_argument("--seed", type=int, default=None)
     ap.add_argument("--rate", type=float, default=2.0, help="served: Poisson arrival rate (1/s)")
@@ -756,6 +794,9 @@ def main():
         return
     if args.workload == "precision":
         run_precision(args)
+        return
+    if args.workload == "served-tau":
+        run_served_tau(args)
         return
     if args.workload == "c12h26":
         run_c12h26(args)

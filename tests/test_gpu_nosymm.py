@@ -73,3 +73,23 @@ def test_nosymm_mode_needs_symm0(tmp_path):
     with pytest.raises(gb.GtfError):
         pf.set_nosymm_mode("exact")
     pf.close()
+
+
+@pytest.mark.parametrize("symm", [1, 0])
+def test_two_density_matrices(symm, tmp_path):
+    """max_numdmat = 2 (pfock/pfock.c:1039-1055): one computeFock builds F
+    for both densities, each read back by its index."""
+    case = "h2o_ccpvdz"
+    g = load_golden(case)
+    ns = _ns(case)
+    gbs, xyz = golden_xyz(g, tmp_path)
+    b = gb.BasisSet(gbs, xyz)
+    pf = gb.PFock(b, tolscr=float(g["tol"]), max_numdmat=2, symm=symm)
+    D1, F1 = (ns["D_ns"], ns["F_ns_ref"]) if symm == 0 else (2.0 * g["D"], 2.0 * g["F"])
+    pf.put_density(g["D"], 0)
+    pf.put_density(D1, 1)
+    pf.commit()
+    pf.compute()
+    assert np.abs(pf.get_mat(gb.MAT_F, 0) - g["F"]).max() < F_TOL
+    assert np.abs(pf.get_mat(gb.MAT_F, 1) - F1).max() < 2 * F_TOL
+    pf.close()
