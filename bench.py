@@ -57,6 +57,42 @@ def _dist():
     return rank, world, local
 
 
+class _Ranks:
+    """The ranks of a batched or served workload on several GPUs (one
+    process each, launched by torch.distributed.run): each serves its own
+    share of the molecules or requests, with no exchange on the data path;
+    a gloo group carries the barriers and the gathers of the results.  On
+    one GPU every method is a no-op."""
+
+    def __init__(self):
+        self.rank, self.world, self.local = _dist()
+        self.dist = None
+        if self.world > 1:
+            import datetime
+            import torch.distributed as dist
+            import gtfock_b200 as gb
+            gb.set_device(self.local)
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=1800))
+            self.dist = dist
+
+    def barrier(self):
+        if self.dist:
+            self.dist.barrier()
+
+    def gather(self, obj):
+        """Every rank's obj, in rank order (a one-element list on one GPU)."""
+        if not self.dist:
+            return [obj]
+        parts = [None] * self.world
+        self.dist.all_gather_object(parts, obj)
+        return parts
+
+    def close(self):
+        if self.dist:
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons every 200 ms while running."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -483,32 +519,42 @@ def run_batch_scaling(args):
 
 def run_batched(args):
     """Batched workload (--workload batched): see batched_measure."""
+    rk = _Ranks()
     out = batched_measure(args.count, args.seed, args.fp32_cutoff if args.fp32_cutoff is not None else 1e-6,
-                          args.autotune, args.seq_sample)
-    print(json.dumps(out), flush=True)
+                          args.autotune, args.seq_sample, rk)
+    if rk.rank == 0:
+        print(json.dumps(out), flush=True)
+    rk.close()
 
 
-def batched_measure(count, seed, cut, autotune, seq_sample):
+def batched_measure(count, seed, cut, autotune, seq_sample, rk=None):
     """Batched workload: `count` seeded molecules (water clusters of 2-24 and
     alkanes C2-C16, STO-3G or 6-31G), 15 SCF iterations each.  Solves/s of the
     batched engine in FP64, in mixed precision, and in mixed precision with
     incremental Fock builds, against the plain FP64 GPU path solving the same
     molecules one after another (set-up excluded in all; it is reported
-    separately)."""
+    separately).  On several GPUs (rk) each rank batches its share of the
+    molecules (serve.split_jobs) and solves/s is all molecules over the
+    slowest rank's time; the ranks start each variant together."""
     import numpy as np
     import gtfock_b200 as gb
-    from gtfock_b200 import molecules as mol, workloads
+    from gtfock_b200 import molecules as mol, serve, workloads
+    rk = rk or _Ranks()
     items = workloads.batched(count, seed)
+    owner = serve.split_jobs([i[3] for i in items], rk.world)
+    mine = [k for k in range(len(items)) if owner[k] == rk.rank]
     niter = 15
     out = {"metric": "SCF solves/s, batched (%d molecules, 15 iterations)" % count, "unit": "solves/s",
            "workload": "seeded water clusters 2-24 / alkanes C2-C16, STO-3G or 6-31G, %d-%d bf" %
-           (min(i[3] for i in items), max(i[3] for i in items)), "seed": seed, "fp32_cutoff": cut}
+           (min(i[3] for i in items), max(i[3] for i in items)), "seed": seed, "fp32_cutoff": cut,
+           "n_gpus": rk.world}
     with tempfile.TemporaryDirectory() as td:
-        files = [(mol.basis_file(b), mol.write_xyz(a, os.path.join(td, n + ".xyz"), n)) for n, a, b, _ in items]
+        files = [(mol.basis_file(items[k][2]), mol.write_xyz(items[k][1], os.path.join(td, items[k][0] + ".xyz"),
+                                                              items[k][0])) for k in mine]
         res = {}
         for tag, prec, incr in (("batched_fp64", 0, False), ("batched_mixed", 1, False),
                                 ("batched_mixed_incremental", 1, True)):
-            b = gb.Batch(len(files))
+            b = gb.Batch(max(1, len(files)))
             if incr:
                 b.set_incremental(True, 0.0, INCR_PERIOD)
             t0 = time.perf_counter()
@@ -517,27 +563,38 @@ def batched_measure(count, seed, cut, autotune, seq_sample):
             t1 = time.perf_counter()
             setup_s = t1 - t0
             tune_s = None
-            if autotune:
+            if autotune and files:
                 b.autotune(2)
                 tune_s = time.perf_counter() - t1
-                t1 = time.perf_counter()
+            rk.barrier()
+            t1 = time.perf_counter()
             l0 = gb.launch_count()
-            b.run()
+            if files:
+                b.run()
             t2 = time.perf_counter()
             info = b.info()
-            res[tag] = [b.result(s)[0] for s in slots]
-            out[tag] = {"solves_per_s": len(files) / (t2 - t1), "solve_s": t2 - t1, "setup_s": setup_s,
-                        "autotune_s": tune_s,
-                        "ms_fock": info["ms_fock"], "ms_energy": info["ms_energy"], "ms_diis": info["ms_diis"],
-                        "ms_purification": info["ms_purification"],
-                        "purification_steps": info["purification_steps"], "steps": info["steps"],
-                        "launches": gb.launch_count() - l0}
+            mine_e = {k: [float(x) for x in b.result(s)[0]] for k, s in zip(mine, slots)}
+            stats = {"n": len(files), "solve_s": t2 - t1, "setup_s": setup_s, "autotune_s": tune_s,
+                     "ms_fock": info["ms_fock"], "ms_energy": info["ms_energy"], "ms_diis": info["ms_diis"],
+                     "ms_purification": info["ms_purification"],
+                     "purification_steps": info["purification_steps"], "steps": info["steps"],
+                     "launches": gb.launch_count() - l0}
             b.close()
-        # the plain FP64 GPU path, one molecule after another
-        nseq = min(len(files), seq_sample)
+            parts = rk.gather((mine_e, stats))
+            res[tag] = {}
+            for e, _ in parts:
+                res[tag].update({int(k): v for k, v in e.items()})
+            solve_s = max(p[1]["solve_s"] for p in parts)
+            out[tag] = dict(parts[0][1], solves_per_s=len(items) / solve_s, solve_s=solve_s)
+            out[tag].pop("n")
+            if rk.world > 1:
+                out[tag]["per_rank"] = [p[1] for p in parts]
+        # the plain FP64 GPU path, one molecule after another (each rank its
+        # share's first molecules)
+        nseq = min(len(files), -(-seq_sample // rk.world))
         tsolve = tset = 0.0
-        eseq = []
-        for g, x in files[:nseq]:
+        eseq_mine = {}
+        for k, (g, x) in zip(mine[:nseq], files[:nseq]):
             t0 = time.perf_counter()
             s = gb.SCFSolver(g, x, tolscr=TOL)
             s.set_options(precision=0, etol=0.0)
@@ -547,9 +604,19 @@ def batched_measure(count, seed, cut, autotune, seq_sample):
             s.close()
             tset += t1 - t0
             tsolve += t2 - t1
-            eseq.append(e)
-        out["sequential_fp64"] = {"solves_per_s": nseq / tsolve, "molecules_timed": nseq,
-                                  "setup_s_per_molecule": tset / nseq}
+            eseq_mine[k] = [float(v) for v in e]
+        parts = rk.gather((eseq_mine, nseq, tsolve, tset))
+        eseq_d = {}
+        for e, _, _, _ in parts:
+            eseq_d.update(e)
+        nseq = sum(p[1] for p in parts)
+        out["sequential_fp64"] = {"solves_per_s": nseq / max(p[2] for p in parts), "molecules_timed": nseq,
+                                  "setup_s_per_molecule": sum(p[3] for p in parts) / nseq}
+        # molecules in the order of the global list, where the one-job path ran
+        order = sorted(eseq_d)
+        eseq = [np.array(eseq_d[k]) for k in order]
+        res = {tag: [np.array(v[k]) for k in order] for tag, v in res.items()}
+        nseq = len(order)
         # energies are compared on the molecules whose FP64 one-job run has
         # converged after the 15 iterations (|E_15 - E_14| < 1e-6 Ha); from the
         # core-Hamiltonian guess some clusters and chains do not, and their
@@ -574,32 +641,48 @@ def batched_measure(count, seed, cut, autotune, seq_sample):
 
 def run_served(args):
     """Served workload (--workload served): see served_measure."""
+    rk = _Ranks()
     out = served_measure(args.count, args.seed, args.rate, args.fp32_cutoff if args.fp32_cutoff is not None
-                         else 1e-6, args.slots, args.lanes, not args.no_incremental, not args.turns)
-    print(json.dumps(out), flush=True)
+                         else 1e-6, args.slots, args.lanes, not args.no_incremental, not args.turns, rk=rk)
+    if rk.rank == 0:
+        print(json.dumps(out), flush=True)
+    rk.close()
 
 
-def served_measure(count, seed, rate, cut, slots, lanes, incremental, concurrent=True, with_sequential=True):
+def served_measure(count, seed, rate, cut, slots, lanes, incremental, concurrent=True, with_sequential=True,
+                   rk=None):
     """Served workload: a seeded Poisson stream of SCF requests, sizes
     log-uniform over 20-1500 bf (water clusters in 6-31G, alkanes C4-C40 in
     cc-pVDZ), each iterated until |dE| < 1e-6 Ha (max 30 iterations).  The
     continuous-batching server (mixed precision, incremental Fock builds,
     HBM-footprint admission) against the same stream on the plain FP64 GPU
-    path, one job at a time."""
+    path, one job at a time.  On several GPUs (rk) each rank serves the
+    requests serve.route gives it, from a common start, and the statistics
+    cover the requests of all ranks; the FP64 comparison runs the same shares
+    one job at a time per rank."""
     import gtfock_b200  # noqa: F401
     from gtfock_b200 import serve, workloads
+    rk = rk or _Ranks()
     items = workloads.served(count, seed, rate)
-    reqs = [serve.Request(n, a, b, t, nb) for t, n, a, b, nb in items]
+    reqs_all = [serve.Request(n, a, b, t, nb) for t, n, a, b, nb in items]
+    owner = serve.route(reqs_all, rk.world)
+    reqs = [r for r, k in zip(reqs_all, owner) if k == rk.rank]
     srv = serve.SCFServer(slots=slots, precision=1, fp32_cutoff=cut, max_iters=30, etol=1e-6, tolscr=TOL,
                           lanes=((400, None), (None, None)) if lanes == 2 else ((None, None),),
-                          incremental=incremental, incr_period=INCR_PERIOD, concurrent=concurrent)
+                          incremental=incremental, incr_period=INCR_PERIOD, concurrent=concurrent,
+                          device=rk.local if rk.world > 1 else None)
+    rk.barrier()
     done = serve.run_stream(reqs, srv)
     budget = srv.admission.budget
     srv.close()
+    if rk.world > 1:
+        done = serve.gather_finished(done)
     if not with_sequential:
         return {"served_mixed": serve.latency_stats(done), "energies": {r.name: float(r.energies[-1]) for r in done},
                 "iterations": {r.name: len(r.energies) for r in done}}
     seq = serve.run_sequential(reqs, max_iters=30, etol=1e-6, tolscr=TOL)
+    if rk.world > 1:
+        seq = serve.gather_finished(seq)
     by = {r.name: r for r in seq}
     # compared where both runs converged (|dE| < 1e-6 Ha before 30 iterations)
     conv = [r for r in done if len(r.energies) < 30 and len(by[r.name].energies) < 30]
@@ -612,7 +695,7 @@ def served_measure(count, seed, rate, cut, slots, lanes, incremental, concurrent
            "served_form": "continuous batching%s, FP32 quartets below %g%s" % (
                ", size lanes stepped concurrently on their own streams" if concurrent else "",
                cut, ", incremental Fock builds (full every %d)" % INCR_PERIOD if incremental else ""),
-           "fp32_cutoff": cut, "slots_per_lane": slots, "lanes": lanes,
+           "fp32_cutoff": cut, "slots_per_lane": slots, "lanes": lanes, "n_gpus": rk.world,
            "hbm_budget_gb": budget / 1e9,
            "served_mixed": serve.latency_stats(done), "sequential_fp64": serve.latency_stats(seq),
            "max_dE_served_vs_fp64": dE, "converged_requests": len(conv),

@@ -137,6 +137,8 @@ def load():
     _sig(L, "gtf_batch_job_device_bytes", [_vp, _i], ctypes.c_size_t)
     _sig(L, "gtf_batch_job_stats", [_vp, _i, _dp, _i])
     _sig(L, "gtf_device_memory", [ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)])
+    _sig(L, "gtf_set_device", [_i])
+    _sig(L, "gtf_get_device", [_ip])
     _sig(L, "gtf_debug_fail_alloc", [_i], None)
     _sig(L, "gtf_debug_live_allocs", [], ctypes.c_longlong)
     _sig(L, "gtf_pfock_compute_noalloc", [_vp, _vp, _vp])
@@ -155,6 +157,20 @@ def device_info():
     cc = ctypes.c_int()
     L.gtf_device_info(ctypes.byref(n), ctypes.byref(cc))
     return n.value, cc.value
+
+
+def set_device(dev):
+    """Device of the calling thread for the library's later calls (one
+    process per GPU; a new thread starts on device 0 and selects again)."""
+    if load().gtf_set_device(int(dev)) != 0:
+        raise GtfError("gtf_set_device(%d) failed" % dev)
+
+
+def get_device():
+    d = ctypes.c_int()
+    if load().gtf_get_device(ctypes.byref(d)) != 0:
+        raise GtfError("gtf_get_device failed")
+    return d.value
 
 
 def device_memory():

@@ -92,6 +92,24 @@ extern "C" void gtf_note_launches(int n) { g_launches += (unsigned long long)n; 
 
 extern "C" unsigned long long gtf_launch_count(void) { return g_launches.load(); }
 
+// Device of the calling host thread for this library's later calls on it
+// (cudaSetDevice): one process per GPU selects its own; a thread it starts
+// selects again, since a new thread begins on device 0.
+extern "C" int gtf_set_device(int dev)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || dev < 0 || dev >= n) {
+        cudaGetLastError();
+        return GTF_ERR_INVALID;
+    }
+    return cudaSetDevice(dev) == cudaSuccess ? GTF_OK : GTF_ERR_CUDA;
+}
+
+extern "C" int gtf_get_device(int *dev)
+{
+    return cudaGetDevice(dev) == cudaSuccess ? GTF_OK : GTF_ERR_CUDA;
+}
+
 extern "C" int gtf_device_memory(size_t *free_bytes, size_t *total_bytes)
 {
     size_t fr = 0, to = 0;

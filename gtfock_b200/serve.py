@@ -18,6 +18,12 @@ comparison.
 Admission is by HBM footprint (Admission): the estimated bytes of a waiting
 request must fit the budget left by the jobs on the device, each counted at
 its measured size, and the device's free memory at that moment.
+
+Several GPUs serve one stream with one process (and one server) each and no
+exchange between them: route() assigns every request to a rank from the
+stream alone, so each process keeps its own share; split_jobs() does the
+same for a fixed set of molecules; gather_finished() brings the finished
+requests to every rank for the statistics.
 """
 import os
 import tempfile
@@ -26,7 +32,7 @@ import time
 
 import numpy as np
 
-from . import BasisSet, Batch, SCFSolver, device_memory
+from . import BasisSet, Batch, SCFSolver, device_memory, set_device
 from . import molecules as mol
 
 
@@ -112,7 +118,12 @@ class SCFServer:
     def __init__(self, slots=64, mem_budget=None, precision=1, fp32_cutoff=1e-6, max_iters=30,
                  etol=1e-6, tolscr=1e-10, lanes=((400, None), (None, None)), share=0.5,
                  incremental=False, incr_tau=0.0, incr_period=8, reserve=2 << 30, free_fn=None,
-                 concurrent=False):
+                 concurrent=False, device=None):
+        # device: the GPU of this server (one process per GPU); the batches
+        # are created on it, and the lane threads select it when they start
+        self.device = device
+        if device is not None:
+            set_device(device)
         self.admission = Admission(mem_budget, reserve, free_fn)
         self._mu = threading.Lock()   # admission state
         # concurrent: run_stream steps every lane from a thread of its own,
@@ -294,6 +305,8 @@ def _run_stream_concurrent(requests, server):
 
     def lane_loop(ln):
         try:
+            if server.device is not None:
+                set_device(server.device)   # a new thread starts on device 0
             while not stop.is_set():
                 if ln.live:
                     done = server.step_lane(ln, now)
@@ -367,3 +380,70 @@ def latency_stats(done):
     span = max(r.finished for r in done) - min(r.arrival for r in done)
     return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "mean_s": float(lat.mean()), "solves_per_s": len(done) / span, "makespan_s": span}
+
+
+def est_seconds(nbf):
+    """Rough service time of one request on one B200, in seconds: set-up plus
+    20-30 SCF iterations whose Fock builds grow about as nbf^3 over 20-1500
+    functions (1430 functions: about 5 s)."""
+    return 0.05 + 1.7e-9 * float(nbf) ** 3
+
+
+def route(requests, nranks):
+    """Rank (0 .. nranks-1) of each request when `nranks` GPUs serve one
+    stream, one process each: in arrival order, a request goes to the rank
+    whose estimated backlog clears first (list scheduling on est_seconds;
+    among ranks already idle, the one idle longest, then the lower rank).
+    The assignment depends on the stream alone, so every process computes
+    the same one and keeps its own share."""
+    if nranks < 1:
+        raise ValueError("nranks must be >= 1")
+    out = [0] * len(requests)
+    if nranks == 1:
+        return out
+    free = [0.0] * nranks
+    order = sorted(range(len(requests)), key=lambda i: (requests[i].arrival, requests[i].name))
+    for i in order:
+        r = requests[i]
+        if r.nbf is None:
+            raise ValueError("route needs the basis size of request %s" % r.name)
+        k = min(range(nranks), key=lambda j: (max(free[j], r.arrival), free[j], j))
+        free[k] = max(free[k], r.arrival) + est_seconds(r.nbf)
+        out[i] = k
+    return out
+
+
+def split_jobs(nbfs, nranks):
+    """Rank of each molecule of a fixed batch over `nranks` GPUs: the
+    costliest first, each to the least-loaded rank (est_seconds; ties to the
+    lower rank)."""
+    if nranks < 1:
+        raise ValueError("nranks must be >= 1")
+    load = [0.0] * nranks
+    out = [0] * len(nbfs)
+    for i in sorted(range(len(nbfs)), key=lambda i: (-nbfs[i], i)):
+        k = min(range(nranks), key=lambda j: (load[j], j))
+        load[k] += est_seconds(nbfs[i])
+        out[i] = k
+    return out
+
+
+def gather_finished(done, group=None):
+    """The finished requests of every rank, on every rank, as Request
+    objects without geometry (name, basis size, arrival, admission and
+    completion times, energies), through torch.distributed's object
+    all-gather on `group` (the default group when None).  Each rank's times
+    are seconds from its own start of the stream; the ranks start together
+    after a barrier."""
+    import torch.distributed as dist
+    mine = [(r.name, r.nbf, r.arrival, r.admitted, r.finished,
+             [float(e) for e in (r.energies if r.energies is not None else [])]) for r in done]
+    parts = [None] * dist.get_world_size(group)
+    dist.all_gather_object(parts, mine, group=group)
+    out = []
+    for part in parts:
+        for name, nbf, arrival, admitted, finished, energies in part:
+            q = Request(name, None, None, arrival, nbf)
+            q.admitted, q.finished, q.energies = admitted, finished, np.array(energies)
+            out.append(q)
+    return out

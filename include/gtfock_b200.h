@@ -244,6 +244,14 @@ int gtf_batch_set_incremental(gtf_batch_t *b, int on, double tau, int period);
 int gtf_batch_autotune(gtf_batch_t *b, int reps);
 void gtf_batch_destroy(gtf_batch_t *b);
 
+/* Device of the calling host thread for the library's later calls on it
+ * (cudaSetDevice; engines, batches and solvers stay on the device they were
+ * created on).  One process per GPU selects its own device; a host thread
+ * it starts selects again.  0 on success, negative for a device that does
+ * not exist. */
+int gtf_set_device(int dev);
+int gtf_get_device(int *dev);
+
 /* Free and total bytes of the current device (cudaMemGetInfo); 0 on success. */
 int gtf_device_memory(size_t *free_bytes, size_t *total_bytes);
 
