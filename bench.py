@@ -42,6 +42,9 @@ TOL = 1e-10
 NITER = 10
 MIXED_CUTOFF = 1e-6
 INCR_PERIOD = 8          # incremental builds: a full build every 8 builds
+# served form: quartets of the density change dropped below bound x max|dD| <
+# 1e-9 (profiles/served_form_tau_sweep_w74.md: no measurable error added)
+SERVED_TAU = 1e-9
 SERVED_COUNT = 32        # requests of the served stream in the default run
 # DRAM bytes (read + write) of all k_fock launches of one C54H18 build, from one
 # ncu capture (profiles/fock_c54h18_dram_traffic.md); the kernels are FP64 bound
@@ -669,7 +672,8 @@ def served_measure(count, seed, rate, cut, slots, lanes, incremental, concurrent
     reqs = [r for r, k in zip(reqs_all, owner) if k == rk.rank]
     srv = serve.SCFServer(slots=slots, precision=1, fp32_cutoff=cut, max_iters=30, etol=1e-6, tolscr=TOL,
                           lanes=((400, None), (None, None)) if lanes == 2 else ((None, None),),
-                          incremental=incremental, incr_period=INCR_PERIOD, concurrent=concurrent,
+                          incremental=incremental, incr_tau=SERVED_TAU, incr_period=INCR_PERIOD,
+                          concurrent=concurrent,
                           device=rk.local if rk.world > 1 else None)
     rk.barrier()
     done = serve.run_stream(reqs, srv)
@@ -694,7 +698,8 @@ def served_measure(count, seed, rate, cut, slots, lanes, incremental, concurrent
                                                                  min(i[4] for i in items), max(i[4] for i in items)),
            "served_form": "continuous batching%s, FP32 quartets below %g%s" % (
                ", size lanes stepped concurrently on their own streams" if concurrent else "",
-               cut, ", incremental Fock builds (full every %d)" % INCR_PERIOD if incremental else ""),
+               cut, ", incremental Fock builds (full every %d, change screened at %g)" % (INCR_PERIOD, SERVED_TAU)
+               if incremental else ""),
            "fp32_cutoff": cut, "slots_per_lane": slots, "lanes": lanes, "n_gpus": rk.world,
            "hbm_budget_gb": budget / 1e9,
            "served_mixed": serve.latency_stats(done), "sequential_fp64": serve.latency_stats(seq),
