@@ -70,11 +70,16 @@ class _Ranks:
     def __init__(self):
         self.rank, self.world, self.local = _dist()
         self.dist = None
+        self.device = None
         if self.world > 1:
             import datetime
             import torch.distributed as dist
             import gtfock_b200 as gb
-            gb.set_device(self.local)
+            # one rank per GPU; more ranks than GPUs share them in turn (the
+            # ranks never wait on one another's kernels, only on the host)
+            ndev = max(1, gb.device_info()[0])
+            self.device = self.local % ndev
+            gb.set_device(self.device)
             dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=1800))
             self.dist = dist
 
@@ -674,7 +679,7 @@ def served_measure(count, seed, rate, cut, slots, lanes, incremental, concurrent
                           lanes=((400, None), (None, None)) if lanes == 2 else ((None, None),),
                           incremental=incremental, incr_tau=SERVED_TAU, incr_period=INCR_PERIOD,
                           concurrent=concurrent,
-                          device=rk.local if rk.world > 1 else None)
+                          device=rk.device if rk.world > 1 else None)
     rk.barrier()
     done = serve.run_stream(reqs, srv)
     budget = srv.admission.budget
@@ -704,7 +709,7 @@ def served_measure(count, seed, rate, cut, slots, lanes, incremental, concurrent
            "hbm_budget_gb": budget / 1e9,
            "served_mixed": serve.latency_stats(done), "sequential_fp64": serve.latency_stats(seq),
            "max_dE_served_vs_fp64": dE, "converged_requests": len(conv),
-           "converged_within_1e-6": within,
+           "converged_within_1e-6": within, "requests_served": len(done),
            "iterations_served": sum(len(r.energies) for r in done),
            "iterations_fp64": sum(len(r.energies) for r in seq),
            "worst_request": None if worst is None else {
