@@ -1,7 +1,7 @@
 /*
  * fock_oracle.c -- CPU restatement of GTFock's hot path for one process.
  *
- * TEST INFRASTRUCTURE ONLY (the checker; never linked by the product).
+ * TEST INFRASTRUCTURE ONLY (the oracle; never linked by the product).
  * Restates, for nprow = npcol = np2 = 1 and full nbf x nbf matrices:
  *   schwartz_screening   pfock/screening.c:15-180
  *   fock_task + update_F pfock/fock_task.c:29-219

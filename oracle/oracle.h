@@ -1,7 +1,7 @@
 /*
  * oracle.h -- CPU restatement of GTFock's Fock-build and purification path.
  *
- * TEST INFRASTRUCTURE ONLY.  This library is the checker: tests/, the
+ * TEST INFRASTRUCTURE ONLY.  This library is the oracle: tests/, the
  * __graft_entry__ smoke check and bench.py's CPU-baseline leg call it; the
  * product library (gtfock_b200/) never links, loads or calls it.
  *

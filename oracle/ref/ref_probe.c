@@ -1,7 +1,7 @@
 /*
  * ref_probe.c -- drives the reference's own PFock engine (pfock/pfock.c,
  * compiled unchanged from the reference sources by oracle/ref/Makefile) on
- * one process and dumps what the checker compares against:
+ * one process and dumps what the tests compare the oracle against:
  *   <out>.screen : nshells, nnz, maxvalue, shellptr[nshells+1],
  *                  shellid[nnz], shellrid[nnz], shellvalue[nnz]
  *                  (pfock/screening.c:110-175)
