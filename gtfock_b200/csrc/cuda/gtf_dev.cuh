@@ -33,10 +33,12 @@
 // |K_ab K_cd| is below GTF_PRIMQ_EPS (pairs are stored in descending |K|, so
 // the loops stop there).  A primitive integral is at most |K_ab K_cd| /
 // sqrt(p+q) times angular factors of order 10 for s-d shells, so a skipped one
-// is below ~1e-15 Ha; on C54H18 / cc-pVDZ the Fock matrix moves by less than
-// 3e-13 Ha against no primitive screening, at the level of the atomics' rounding.
-#define GTF_PRIM_EPS 1e-17
-#define GTF_PRIMQ_EPS 1e-17
+// is below ~1e-14 Ha.  Against the reference-pinned Fock matrices of C54H18 /
+// cc-pVDZ, (H2O)64 / 6-31G and C96H24 / cc-pVDZ the largest element error is
+// 1.8e-12, 4.1e-13 and 2.0e-12 Ha (1.1e-12, 4.2e-13, 1.4e-12 at 1e-17, where
+// the atomics' rounding dominates), and the builds are 6% faster than at 1e-17.
+#define GTF_PRIM_EPS 1e-15
+#define GTF_PRIMQ_EPS 1e-15
 
 // ---------------------------------------------------------------------------
 // Cartesian component tables (lexicographic: xx, xy, xz, yy, yz, zz)
