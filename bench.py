@@ -48,7 +48,7 @@ SERVED_TAU = 1e-9
 SERVED_COUNT = 32        # requests of the served stream in the default run
 # DRAM bytes (read + write) of all k_fock launches of one C54H18 build, from one
 # ncu capture (profiles/fock_c54h18_dram_traffic.md); the kernels are FP64 bound
-FOCK_BUILD_DRAM_BYTES = 648.9e6 + 85.0e6
+FOCK_BUILD_DRAM_BYTES = 648.2e6 + 84.9e6
 METRIC = "SCF solves/s (C54H18 cc-pVDZ, 10 iterations, FP64)"
 WORKLOAD = "C54H18 graphene flake / cc-pVDZ (846 bf), Schwarz 1e-10, 10 SCF iterations, FP64"
 
