@@ -115,7 +115,7 @@ class SCFServer:
     the large lane takes one step -- so small jobs are not held to the pace of
     a 1000-function molecule, while the large ones keep progressing."""
 
-    def __init__(self, slots=64, mem_budget=None, precision=1, fp32_cutoff=1e-6, max_iters=30,
+    def __init__(self, slots=64, mem_budget=None, precision=1, fp32_cutoff=1e-4, max_iters=30,
                  etol=1e-6, tolscr=1e-10, lanes=((400, None), (None, None)), share=0.5,
                  incremental=False, incr_tau=0.0, incr_period=8, reserve=2 << 30, free_fn=None,
                  concurrent=False, device=None):
