@@ -686,6 +686,7 @@ def served_measure(count, seed, rate, cut, slots, lanes, incremental, concurrent
         return [r for r, k in zip(reqs_all, owner) if k == rk.rank]
 
     runs = []
+    host = []
     for _ in range(max(1, repeats)):
         reqs = share()
         srv = serve.SCFServer(slots=slots, precision=1, fp32_cutoff=cut, max_iters=30, etol=1e-6, tolscr=TOL,
@@ -696,6 +697,7 @@ def served_measure(count, seed, rate, cut, slots, lanes, incremental, concurrent
         rk.barrier()
         done = serve.run_stream(reqs, srv)
         budget = srv.admission.budget
+        host.append(dict(srv.stats))
         srv.close()
         if rk.world > 1:
             done = serve.gather_finished(done)
@@ -729,6 +731,7 @@ def served_measure(count, seed, rate, cut, slots, lanes, incremental, concurrent
            "max_dE_served_vs_fp64": dE, "converged_requests": len(conv),
            "converged_within_1e-6": within, "requests_served": len(done),
            "served_runs": {"solves_per_s": [serve.latency_stats(d)["solves_per_s"] for d in runs],
+                           "host": host,
                            "note": "the stream replayed %d times; statistics of the run of median makespan, "
                                    "max_dE over all runs" % len(runs)},
            "iterations_served": sum(len(r.energies) for r in done),

@@ -26,6 +26,7 @@
 
 #include <vector>
 
+#include "devmem.cuh"
 #include "diis_dev.cuh"
 #include "gtf_cuda.h"
 #include "gtfock_b200.h"
@@ -499,10 +500,12 @@ static size_t job_buffer_bytes(int n) { return sizeof(double) * (size_t)n * n * 
 
 extern "C" size_t gtf_batch_job_bytes(int nbf) { return job_buffer_bytes(nbf); }
 
-static void job_free(BJob &j)
+// The job's buffers are on the batch's stream `st` (devmem.cu's pool); the
+// caller has synchronized `st` or queued nothing on it that uses them.
+static void job_free(BJob &j, cudaStream_t st)
 {
-    if (j.mem) cudaFree(j.mem);
-    if (j.fcopy) cudaFree(j.fcopy);
+    gtf_dfree(j.mem, st);
+    gtf_dfree(j.fcopy, st);
     if (j.pd) gtf_purif_destroy(j.pd);
     if (j.pf) {
         PFock_destroyOvlMat(j.pf);
@@ -520,7 +523,7 @@ extern "C" void gtf_batch_destroy(gtf_batch_t *b)
     if (b->fock_exec) cudaGraphExecDestroy(b->fock_exec);
     if (b->fb) gtf_fock_batch_destroy(b->fb);
     for (auto &j : b->jobs)
-        if (j.used) job_free(j);
+        if (j.used) job_free(j, b->st);
     void *dp[] = {b->d_jobs, b->d_gd, b->d_tp, b->d_energy, b->d_dots, b->d_diis, b->d_scal, b->d_active,
                   b->d_iters, b->d_count, b->d_list};
     for (void *p : dp)
@@ -605,7 +608,7 @@ extern "C" int gtf_batch_add(gtf_batch_t *b, const char *bsfile, const char *xyz
     j.enuc = CInt_getNucEnergy(j.basis);
     if (PFock_create(j.basis, 1, 1, 4, tolscr, 1, 1, &j.pf) != PFOCK_STATUS_SUCCESS) {
         j.pf = nullptr;
-        job_free(j);
+        job_free(j, b->st);
         return -4;
     }
     j.used = 1;
@@ -613,7 +616,7 @@ extern "C" int gtf_batch_add(gtf_batch_t *b, const char *bsfile, const char *xyz
     if ((prec_mode != 0 && gtf_pfock_set_precision(j.pf, prec_mode, fp32_cutoff) != PFOCK_STATUS_SUCCESS) ||
         PFock_createOvlMat(j.pf, j.basis) != PFOCK_STATUS_SUCCESS ||
         PFock_createCoreHMat(j.pf, j.basis) != PFOCK_STATUS_SUCCESS) {
-        job_free(j);
+        job_free(j, b->st);
         return -5;
     }
     const size_t nn = (size_t)j.n * j.n;
@@ -627,12 +630,12 @@ extern "C" int gtf_batch_add(gtf_batch_t *b, const char *bsfile, const char *xyz
             gtf_purif_set_sx_dev(j.pd, d.S, d.X) != GTF_OK ||
             (prec_mode == 1 && gtf_purif_set_mode(j.pd, 1) != GTF_OK)) {
             j.pd = nullptr;
-            job_free(j);
+            job_free(j, b->st);
             return -6;
         }
-    } else if (cudaMalloc(&j.mem, j.bytes) != cudaSuccess) {
+    } else if (gtf_dmalloc((void **)&j.mem, j.bytes, b->st) != cudaSuccess) {
         j.mem = nullptr;
-        job_free(j);
+        job_free(j, b->st);
         return -6;
     }
     d.D = const_cast<double *>(gtf_fock_mat_dev(j.eng, 0, 0));
@@ -640,9 +643,9 @@ extern "C" int gtf_batch_add(gtf_batch_t *b, const char *bsfile, const char *xyz
     d.Fe = d.F;
     if (b->incr) {
         if (gtf_pfock_set_incremental(j.pf, 1, b->incr_tau, b->incr_period) != PFOCK_STATUS_SUCCESS ||
-            cudaMalloc(&j.fcopy, sizeof(double) * nn) != cudaSuccess) {
+            gtf_dmalloc((void **)&j.fcopy, sizeof(double) * nn, b->st) != cudaSuccess) {
             j.fcopy = nullptr;
-            job_free(j);
+            job_free(j, b->st);
             return -6;
         }
         j.bytes += sizeof(double) * nn;
@@ -667,9 +670,13 @@ extern "C" int gtf_batch_add(gtf_batch_t *b, const char *bsfile, const char *xyz
     // initial guess (pscf/scf.c:34-76) into the engine's density buffer
     std::vector<double> D0(nn);
     gtf_initial_density(j.basis, D0.data(), j.n);
-    if (cudaMemcpy(d.D, D0.data(), sizeof(double) * nn, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaDeviceSynchronize() != cudaSuccess) {
-        job_free(j);
+    // the engine's set-up (its stream) and the job's buffers (the batch's
+    // stream) are complete before the batch's launches use them; the other
+    // lanes' work is not waited for
+    if (cudaStreamSynchronize((cudaStream_t)gtf_fock_stream(j.eng)) != cudaSuccess ||
+        cudaMemcpyAsync(d.D, D0.data(), sizeof(double) * nn, cudaMemcpyHostToDevice, b->st) != cudaSuccess ||
+        cudaStreamSynchronize(b->st) != cudaSuccess) {
+        job_free(j, b->st);
         return -7;
     }
     j.iter = 0;
@@ -686,7 +693,7 @@ extern "C" int gtf_batch_remove(gtf_batch_t *b, int slot)
 {
     if (!b || slot < 0 || slot >= b->capacity || !b->jobs[slot].used) return -1;
     cudaStreamSynchronize(b->st);
-    job_free(b->jobs[slot]);
+    job_free(b->jobs[slot], b->st);
     b->dirty = 1;
     return 0;
 }

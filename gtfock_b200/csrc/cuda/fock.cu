@@ -34,6 +34,7 @@
 #include <tuple>
 #include <vector>
 
+#include "devmem.cuh"
 #include "gtf_cuda.h"
 #include "gtf_dev.cuh"
 // the Fock kernels live in fock_kernel.cuh, instantiated across several
@@ -191,7 +192,10 @@ static std::atomic<long long> g_live_allocs{0};   // dev_malloc'd and not yet de
 extern "C" void gtf_debug_fail_alloc(int n) { g_fail_alloc.store(n > 0 ? n : 0); }
 extern "C" long long gtf_debug_live_allocs(void) { return g_live_allocs.load(); }
 
-static cudaError_t dev_malloc(void **p, size_t bytes)
+// Buffers come from the device's stream-ordered pool on the engine's stream
+// (devmem.cu): creating and destroying engines while other engines' kernels
+// run then synchronizes nothing but this engine's own stream.
+static cudaError_t dev_malloc(void **p, size_t bytes, cudaStream_t st)
 {
     int n = g_fail_alloc.load();
     while (n > 0 && !g_fail_alloc.compare_exchange_weak(n, n - 1)) {
@@ -200,28 +204,32 @@ static cudaError_t dev_malloc(void **p, size_t bytes)
         *p = nullptr;
         return cudaErrorMemoryAllocation;
     }
-    const cudaError_t e = cudaMalloc(p, bytes);
+    const cudaError_t e = gtf_dmalloc(p, bytes, st);
     if (e == cudaSuccess) g_live_allocs++;
     return e;
 }
 
-static void dev_free(void *p)
+// ordered on `st` after the buffer's last use there (or after the host has
+// synchronized every stream that used it)
+static void dev_free(void *p, cudaStream_t st)
 {
     if (!p) return;
-    cudaFree(p);
+    gtf_dfree(p, st);
     g_live_allocs--;
 }
 
-// Device temporaries of one set-up call: released when the call returns, on
-// success and on every error path alike.
+// Device temporaries of one set-up call on stream `st` (every use of them is
+// on that stream): released when the call returns, on success and on every
+// error path alike, ordered after their last use.
 struct DevTemps {
     std::vector<void *> p;
-    DevTemps() = default;
+    cudaStream_t st;
+    explicit DevTemps(cudaStream_t s) : st(s) {}
     DevTemps(const DevTemps &) = delete;
     DevTemps &operator=(const DevTemps &) = delete;
     ~DevTemps()
     {
-        for (void *q : p) dev_free(q);
+        for (void *q : p) dev_free(q, st);
     }
     template <typename T>
     int get(T **out, size_t n)
@@ -229,7 +237,7 @@ struct DevTemps {
         *out = nullptr;
         if (n == 0) n = 1;
         void *q = nullptr;
-        cudaError_t e = dev_malloc(&q, n * sizeof(T));
+        cudaError_t e = dev_malloc(&q, n * sizeof(T), st);
         if (e != cudaSuccess) {
             snprintf(g_errbuf, sizeof(g_errbuf), "cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
             return GTF_ERR_ALLOC;
@@ -242,7 +250,7 @@ struct DevTemps {
     {
         for (size_t k = 0; k < p.size(); k++)
             if (p[k] == q) {
-                dev_free(q);
+                dev_free(q, st);
                 p.erase(p.begin() + (long)k);
                 return;
             }
@@ -260,7 +268,7 @@ static int dalloc(gtf_fock_dev *f, T **p, size_t n)
 {
     *p = nullptr;
     if (n == 0) n = 1;
-    cudaError_t e = dev_malloc((void **)p, n * sizeof(T));
+    cudaError_t e = dev_malloc((void **)p, n * sizeof(T), f->stream);
     if (e != cudaSuccess) {
         snprintf(g_errbuf, sizeof(g_errbuf), "cudaMalloc(%zu bytes): %s", n * sizeof(T),
                  cudaGetErrorString(e));
@@ -1432,7 +1440,7 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
 
     // ---- Schwarz values of every shell pair (M >= N), one class at a time ----
     const size_t n2 = (size_t)ns * ns;
-    DevTemps tmps;
+    DevTemps tmps(st);
     DALLOC(f->d_sq, n2);
     unsigned long long *d_gmax;
     TALLOC(tmps, d_gmax, 1);
@@ -1689,35 +1697,43 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
     CK(cudaMemsetAsync(f->d_J, 0, sizeof(double) * nn * max_numdmat, st));
     CK(cudaMemsetAsync(f->d_K, 0, sizeof(double) * nn * max_numdmat, st));
     f->host_stage_bytes = nn * sizeof(double);
-    CK(cudaMallocHost((void **)&f->d_host_stage, f->host_stage_bytes));
+    f->d_host_stage = (double *)gtf_pinned_alloc(f->host_stage_bytes);
+    if (!f->d_host_stage) {
+        snprintf(g_errbuf, sizeof(g_errbuf), "pinned host buffer of %zu bytes", f->host_stage_bytes);
+        return GTF_ERR_ALLOC;
+    }
     CK(cudaStreamSynchronize(st));
     return GTF_OK;
 }
 
+// Every buffer is freed on the engine's stream after the host has waited for
+// it (a batch that used the engine's buffers on its own stream has
+// synchronized that stream before destroying the engine).
 extern "C" void gtf_fock_destroy(gtf_fock_dev_t *f)
 {
     if (!f) return;
     cudaStreamSynchronize(f->stream);
+    cudaStream_t st = f->stream;
     void *ptrs[] = {f->d_sh_L, f->d_sh_nprim, f->d_sh_pstart, f->d_f_start, f->d_fc_start, f->d_sph2shell,
                     f->d_cart2shell, f->d_Z, f->d_sh_xyz, f->d_alpha, f->d_coef, f->d_atom_xyz, f->d_sq,
                     f->d_shellptr, f->d_shellid, f->d_shellrid, f->d_shellvalue, f->d_pairs, f->d_pair_v,
                     f->d_pp, f->d_pp32, f->d_counters, f->d_D, f->d_Dc, f->d_Fj, f->d_Fk, f->d_F, f->d_J, f->d_K,
                     f->d_Ds, f->d_Da, f->d_Dca, f->d_Fka, f->d_ut_static, f->d_ut_dyn, f->d_Dprev, f->d_Dd,
                     f->d_dyn, f->d_Dta, f->d_Dcta, f->d_Fja, f->d_Fscr};
-    for (void *p : ptrs) dev_free(p);   // all from dalloc
+    for (void *p : ptrs) dev_free(p, st);   // all from dalloc
     for (int c = 0; c < NCLSPAIR; c++) {
-        dev_free(f->tasks[c].d_nket);
-        dev_free(f->tasks[c].d_unit_prefix);
-        dev_free(f->tasks[c].d_n64);
-        dev_free(f->tasks[c].d_cum64);
-        dev_free(f->tasks[c].d_cum32);
-        dev_free(f->tasks[c].d_unit_prefix32);
+        dev_free(f->tasks[c].d_nket, st);
+        dev_free(f->tasks[c].d_unit_prefix, st);
+        dev_free(f->tasks[c].d_n64, st);
+        dev_free(f->tasks[c].d_cum64, st);
+        dev_free(f->tasks[c].d_cum32, st);
+        dev_free(f->tasks[c].d_unit_prefix32, st);
     }
-    // the one-electron matrices come from onee.cu's own allocations
+    // the one-electron matrices come from onee.cu's own allocations (the
+    // same pool, on this stream)
     void *onee[] = {f->d_S, f->d_X, f->d_H};
-    for (void *p : onee)
-        if (p) cudaFree(p);
-    if (f->d_host_stage) cudaFreeHost(f->d_host_stage);
+    for (void *p : onee) gtf_dfree(p, st);
+    gtf_pinned_free(f->d_host_stage);
     // a partly created engine has some of these unset: destroying a null
     // handle would leave a stale error for the next cudaGetLastError
     cudaEvent_t evs[] = {f->ev0, f->ev1, f->ev2, f->ev3};
@@ -2368,7 +2384,7 @@ extern "C" int gtf_fock_class_work_screened(gtf_fock_dev_t *f, double *flops, do
     const int nt = (int)f->h_ut.size();
     std::vector<double> cnt(nt > 0 ? nt : 1, 0.0);
     if (nt > 0) {
-        DevTemps tmps;
+        DevTemps tmps(f->stream);
         double *d_out;
         TALLOC(tmps, d_out, nt);
         CK(cudaMemsetAsync(d_out, 0, sizeof(double) * nt, f->stream));
@@ -2455,7 +2471,7 @@ extern "C" void gtf_fock_release_onee(gtf_fock_dev_t *f, int which)
     double **p = which == 0 ? &f->d_S : which == 1 ? &f->d_X : &f->d_H;
     if (*p) {
         cudaStreamSynchronize(f->stream);
-        cudaFree(*p);
+        gtf_dfree(*p, f->stream);
         *p = nullptr;
     }
 }
@@ -2763,22 +2779,20 @@ static long long solo_units_threshold(bool *overridden)
     return GTF_SOLO_UNITS;
 }
 
+// The descriptors live in the device's stream-ordered pool (devmem.cu) and
+// are freed on the batch's stream after the host has waited for it.
 extern "C" void gtf_fock_batch_destroy(gtf_fock_batch_t *b)
 {
     if (!b) return;
     cudaStreamSynchronize(b->st);
-    cudaFree(b->d_xf);
-    cudaFree(b->d_counters);
-    if (b->d_delta) cudaFree(b->d_delta);
-    if (b->d_full) cudaFree(b->d_full);
-    if (b->h_full) cudaFreeHost(b->h_full);
-    if (b->d_ut) cudaFree(b->d_ut);
-    if (b->d_pdesc) cudaFree(b->d_pdesc);
-    if (b->d_ptot) cudaFree(b->d_ptot);
+    cudaStream_t st = b->st;
+    void *ptrs[] = {b->d_xf, b->d_counters, b->d_delta, b->d_full, b->d_ut, b->d_pdesc, b->d_ptot};
+    for (void *p : ptrs) gtf_dfree(p, st);
+    gtf_pinned_free(b->h_full);
     for (int c = 0; c < NCLSPAIR; c++)
         for (int p = 0; p < 2; p++) {
-            cudaFree(b->d_desc[c][p]);
-            cudaFree(b->d_prefix[c][p]);
+            gtf_dfree(b->d_desc[c][p], st);
+            gtf_dfree(b->d_prefix[c][p], st);
         }
     delete b;
 }
@@ -2868,8 +2882,8 @@ extern "C" int gtf_fock_batch_create(gtf_fock_dev_t *const *engines, int M, void
         if (f->nbf > b->maxn) b->maxn = f->nbf;
         if (f->nbf_cart > b->maxnc) b->maxnc = f->nbf_cart;
     }
-    CKB_(cudaMalloc(&b->d_xf, sizeof(XformDesc) * M));
-    CKB_(cudaMemcpy(b->d_xf, xf.data(), sizeof(XformDesc) * M, cudaMemcpyHostToDevice));
+    CKB_(gtf_dmalloc((void **)&b->d_xf, sizeof(XformDesc) * M, b->st));
+    CKB_(cudaMemcpyAsync(b->d_xf, xf.data(), sizeof(XformDesc) * M, cudaMemcpyHostToDevice, b->st));
     int nblocks = 2 * NCLSPAIR;
     bool solo_env = false;
     const long long solo_min = solo_units_threshold(&solo_env);
@@ -2915,10 +2929,10 @@ extern "C" int gtf_fock_batch_create(gtf_fock_dev_t *const *engines, int M, void
             b->total[c][p] = pre.back();
             if (d.empty()) continue;
             b->one[c][p] = d[0];
-            CKB_(cudaMalloc(&b->d_desc[c][p], sizeof(FockLaunch) * d.size()));
-            CKB_(cudaMalloc(&b->d_prefix[c][p], sizeof(long long) * pre.size()));
-            CKB_(cudaMemcpy(b->d_desc[c][p], d.data(), sizeof(FockLaunch) * d.size(), cudaMemcpyHostToDevice));
-            CKB_(cudaMemcpy(b->d_prefix[c][p], pre.data(), sizeof(long long) * pre.size(), cudaMemcpyHostToDevice));
+            CKB_(gtf_dmalloc((void **)&b->d_desc[c][p], sizeof(FockLaunch) * d.size(), b->st));
+            CKB_(gtf_dmalloc((void **)&b->d_prefix[c][p], sizeof(long long) * pre.size(), b->st));
+            CKB_(cudaMemcpyAsync(b->d_desc[c][p], d.data(), sizeof(FockLaunch) * d.size(), cudaMemcpyHostToDevice, b->st));
+            CKB_(cudaMemcpyAsync(b->d_prefix[c][p], pre.data(), sizeof(long long) * pre.size(), cudaMemcpyHostToDevice, b->st));
             if (b->dyn) {
                 PrefixDesc q;
                 q.tot = nullptr;
@@ -2959,35 +2973,36 @@ extern "C" int gtf_fock_batch_create(gtf_fock_dev_t *const *engines, int M, void
         b->ut_n = (int)ut.size();
         b->ut_nidx = nidx;
         b->ut_nbras = nbras;
-        CKB_(cudaMalloc(&b->d_delta, sizeof(DeltaDesc) * M));
-        CKB_(cudaMemcpy(b->d_delta, dd.data(), sizeof(DeltaDesc) * M, cudaMemcpyHostToDevice));
-        CKB_(cudaMalloc(&b->d_full, sizeof(int) * M));
-        CKB_(cudaMallocHost(&b->h_full, sizeof(int) * M));
+        CKB_(gtf_dmalloc((void **)&b->d_delta, sizeof(DeltaDesc) * M, b->st));
+        CKB_(cudaMemcpyAsync(b->d_delta, dd.data(), sizeof(DeltaDesc) * M, cudaMemcpyHostToDevice, b->st));
+        CKB_(gtf_dmalloc((void **)&b->d_full, sizeof(int) * M, b->st));
+        b->h_full = (int *)gtf_pinned_alloc(sizeof(int) * M);
+        CKB_(b->h_full ? cudaSuccess : cudaErrorMemoryAllocation);
         for (int m = 0; m < M; m++) b->h_full[m] = 1;
-        CKB_(cudaMemcpy(b->d_full, b->h_full, sizeof(int) * M, cudaMemcpyHostToDevice));
+        CKB_(cudaMemcpyAsync(b->d_full, b->h_full, sizeof(int) * M, cudaMemcpyHostToDevice, b->st));
         if (!ut.empty()) {
-            CKB_(cudaMalloc(&b->d_ut, sizeof(UnitTask) * ut.size()));
-            CKB_(cudaMemcpy(b->d_ut, ut.data(), sizeof(UnitTask) * ut.size(), cudaMemcpyHostToDevice));
+            CKB_(gtf_dmalloc((void **)&b->d_ut, sizeof(UnitTask) * ut.size(), b->st));
+            CKB_(cudaMemcpyAsync(b->d_ut, ut.data(), sizeof(UnitTask) * ut.size(), cudaMemcpyHostToDevice, b->st));
         }
         size_t ntot = 0;
         for (auto &v : ptot) ntot += v.size();
         b->npdesc = (int)pdesc.size();
         if (ntot > 0) {
-            CKB_(cudaMalloc(&b->d_ptot, sizeof(const long long *) * ntot));
+            CKB_(gtf_dmalloc((void **)&b->d_ptot, sizeof(const long long *) * ntot, b->st));
             std::vector<const long long *> flat;
             for (size_t k = 0; k < ptot.size(); k++) {
                 pdesc[k].tot = b->d_ptot + flat.size();
                 flat.insert(flat.end(), ptot[k].begin(), ptot[k].end());
             }
-            CKB_(cudaMemcpy(b->d_ptot, flat.data(), sizeof(const long long *) * ntot, cudaMemcpyHostToDevice));
+            CKB_(cudaMemcpyAsync(b->d_ptot, flat.data(), sizeof(const long long *) * ntot, cudaMemcpyHostToDevice, b->st));
         }
         if (b->npdesc > 0) {
-            CKB_(cudaMalloc(&b->d_pdesc, sizeof(PrefixDesc) * pdesc.size()));
-            CKB_(cudaMemcpy(b->d_pdesc, pdesc.data(), sizeof(PrefixDesc) * pdesc.size(), cudaMemcpyHostToDevice));
+            CKB_(gtf_dmalloc((void **)&b->d_pdesc, sizeof(PrefixDesc) * pdesc.size(), b->st));
+            CKB_(cudaMemcpyAsync(b->d_pdesc, pdesc.data(), sizeof(PrefixDesc) * pdesc.size(), cudaMemcpyHostToDevice, b->st));
         }
     }
     b->ncounter_blocks = nblocks;
-    CKB_(cudaMalloc(&b->d_counters, sizeof(unsigned long long) * (size_t)nblocks * GTF_MAX_SLICES));
+    CKB_(gtf_dmalloc((void **)&b->d_counters, sizeof(unsigned long long) * (size_t)nblocks * GTF_MAX_SLICES, b->st));
     *out = b;
     return GTF_OK;
 }

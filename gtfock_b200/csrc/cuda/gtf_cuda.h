@@ -133,7 +133,7 @@ size_t gtf_fock_device_bytes(gtf_fock_dev_t *f);
 
 /* ---- split BF16 products on the tensor cores (purif_bf16.cu) ---- */
 typedef struct gtf_bf16x3 gtf_bf16x3_t;
-int gtf_bf16x3_create(int n, gtf_bf16x3_t **out);
+int gtf_bf16x3_create(int n, void *stream, gtf_bf16x3_t **out);
 void gtf_bf16x3_destroy(gtf_bf16x3_t *g);
 int gtf_bf16x3_abt(gtf_bf16x3_t *g, const double *A, const double *B, double *C, void *stream);
 

@@ -11,6 +11,7 @@
 #include <cusolverDn.h>
 #include <stdio.h>
 
+#include "devmem.cuh"
 #include "gtf_cuda.h"
 #include "gtf_dev.cuh"
 
@@ -213,12 +214,14 @@ extern "C" int gtf_onee_compute(gtf_fock_dev_t *f, int want_sx, int want_h, doub
     cudaStream_t st = (cudaStream_t)gtf_fock_stream(f);
     const size_t nn = (size_t)nbf * nbf;
     double *dS = nullptr, *dH = nullptr;
+    // S, H and X live in the device's stream-ordered pool on the engine's
+    // stream, which frees them (devmem.cu); so do the eigensolver's buffers
     if (want_sx) {
-        if (!*S) CKC(cudaMalloc((void **)S, sizeof(double) * nn));
+        if (!*S) CKC(gtf_dmalloc((void **)S, sizeof(double) * nn, st));
         dS = *S;
     }
     if (want_h) {
-        if (!*H) CKC(cudaMalloc((void **)H, sizeof(double) * nn));
+        if (!*H) CKC(gtf_dmalloc((void **)H, sizeof(double) * nn, st));
         dH = *H;
     }
     const long long npair = (long long)ns * ns;
@@ -227,25 +230,21 @@ extern "C" int gtf_onee_compute(gtf_fock_dev_t *f, int want_sx, int want_h, doub
                                                             nullptr, nullptr);
     CKC(cudaGetLastError());
     if (want_sx) {
-        if (!*X) CKC(cudaMalloc((void **)X, sizeof(double) * nn));
-        cusolverDnHandle_t sh;
-        cublasHandle_t bh;
-        if (cusolverDnCreate(&sh) != CUSOLVER_STATUS_SUCCESS) return GTF_ERR_CUDA;
-        if (cublasCreate(&bh) != CUBLAS_STATUS_SUCCESS) {
-            cusolverDnDestroy(sh);
-            return GTF_ERR_CUDA;
-        }
-        cusolverDnSetStream(sh, st);
-        cublasSetStream(bh, st);
+        if (!*X) CKC(gtf_dmalloc((void **)X, sizeof(double) * nn, st));
+        SolverLease sl(st);
+        BlasLease bl(st);
+        if (!sl.h || !bl.h) return GTF_ERR_CUDA;
+        cusolverDnHandle_t sh = sl.h;
+        cublasHandle_t bh = bl.h;
         double *V, *w, *Y, *work;
         int *info, lwork = 0;
-        CKC(cudaMalloc((void **)&V, sizeof(double) * nn));
-        CKC(cudaMalloc((void **)&Y, sizeof(double) * nn));
-        CKC(cudaMalloc((void **)&w, sizeof(double) * nbf));
-        CKC(cudaMalloc((void **)&info, sizeof(int)));
+        CKC(gtf_dmalloc((void **)&V, sizeof(double) * nn, st));
+        CKC(gtf_dmalloc((void **)&Y, sizeof(double) * nn, st));
+        CKC(gtf_dmalloc((void **)&w, sizeof(double) * nbf, st));
+        CKC(gtf_dmalloc((void **)&info, sizeof(int), st));
         CKC(cudaMemcpyAsync(V, dS, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
         cusolverDnDsyevd_bufferSize(sh, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nbf, V, nbf, w, &lwork);
-        CKC(cudaMalloc((void **)&work, sizeof(double) * (lwork > 0 ? lwork : 1)));
+        CKC(gtf_dmalloc((void **)&work, sizeof(double) * (lwork > 0 ? lwork : 1), st));
         cusolverStatus_t ss =
             cusolverDnDsyevd(sh, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nbf, V, nbf, w, work, lwork, info);
         int hinfo = 0;
@@ -263,13 +262,11 @@ extern "C" int gtf_onee_compute(gtf_fock_dev_t *f, int want_sx, int want_h, doub
             cublasDgemm(bh, CUBLAS_OP_N, CUBLAS_OP_T, nbf, nbf, nbf, &one, Y, nbf, V, nbf, &zero, *X, nbf);
             CKC(cudaStreamSynchronize(st));
         }
-        cudaFree(V);
-        cudaFree(Y);
-        cudaFree(w);
-        cudaFree(info);
-        cudaFree(work);
-        cublasDestroy(bh);
-        cusolverDnDestroy(sh);
+        gtf_dfree(V, st);
+        gtf_dfree(Y, st);
+        gtf_dfree(w, st);
+        gtf_dfree(info, st);
+        gtf_dfree(work, st);
         if (ret) return ret;
     }
     CKC(cudaStreamSynchronize(st));
@@ -288,7 +285,7 @@ extern "C" int gtf_onee_full(gtf_fock_dev_t *f, double *S_host, double *T_host, 
     cudaStream_t st = (cudaStream_t)gtf_fock_stream(f);
     const size_t nn = (size_t)nbf * nbf;
     double *buf;
-    CKC(cudaMalloc((void **)&buf, sizeof(double) * nn * 3));
+    CKC(gtf_dmalloc((void **)&buf, sizeof(double) * nn * 3, st));
     const long long npair = (long long)ns * ns;
     k_onee<<<(unsigned)((npair + 127) / 128), 128, 0, st>>>(sh_L, sh_nprim, sh_pstart, f_start, sh_xyz, alpha,
                                                             coef, Z, atom_xyz, ns, natoms, nbf, pure, buf, nullptr,
@@ -298,6 +295,6 @@ extern "C" int gtf_onee_full(gtf_fock_dev_t *f, double *S_host, double *T_host, 
     if (T_host) CKC(cudaMemcpyAsync(T_host, buf + nn, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
     if (V_host) CKC(cudaMemcpyAsync(V_host, buf + 2 * nn, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
     CKC(cudaStreamSynchronize(st));
-    cudaFree(buf);
+    gtf_dfree(buf, st);
     return GTF_OK;
 }

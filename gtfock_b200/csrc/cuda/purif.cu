@@ -15,6 +15,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include "devmem.cuh"
 #include "diis_dev.cuh"
 #include "gtf_cuda.h"
 
@@ -44,7 +45,8 @@ extern "C" void gtf_note_launches(int n);
 struct gtf_purif_dev {
     int n, nocc;
     cudaStream_t st;
-    cublasHandle_t blas;
+    int own_st;               // the stream was created here
+    cublasHandle_t blas;      // leased for the duration of one call (BlasLease)
     double *S, *X, *D, *D2, *D3, *F, *W, *W2;
     double *vecs, *Fvecs;
     double *part;     // [RED_BLOCKS * 16] block partials
@@ -339,18 +341,23 @@ extern "C" int gtf_purif_create(int nbf, int nocc, void *stream, gtf_purif_dev_t
     p->n = nbf;
     p->nocc = nocc;
     p->st = (cudaStream_t)stream;
-    if (!p->st) CKP(cudaStreamCreateWithFlags(&p->st, cudaStreamNonBlocking));
-    CKB(cublasCreate(&p->blas));
-    CKB(cublasSetStream(p->blas, p->st));
+    if (!p->st) {
+        CKP(cudaStreamCreateWithFlags(&p->st, cudaStreamNonBlocking));
+        p->own_st = 1;
+    }
+    // device buffers from the stream-ordered pool on the object's stream,
+    // pinned host scalars from the pinned pool (devmem.cu): creating and
+    // destroying this object synchronizes nothing else
     const size_t nn = (size_t)nbf * nbf;
     double **bufs[] = {&p->S, &p->X, &p->D, &p->D2, &p->D3, &p->F, &p->W, &p->W2, &p->E};
-    for (double **b : bufs) CKP(cudaMalloc((void **)b, sizeof(double) * nn));
-    CKP(cudaMalloc((void **)&p->vecs, sizeof(double) * nn * PUR_MAX_DIIS));
-    CKP(cudaMalloc((void **)&p->Fvecs, sizeof(double) * nn * PUR_MAX_DIIS));
-    CKP(cudaMalloc((void **)&p->part, sizeof(double) * RED_BLOCKS * 16));
-    CKP(cudaMalloc((void **)&p->scal, sizeof(double) * 16));
-    CKP(cudaMallocHost((void **)&p->h_scal, sizeof(double) * 16));
-    CKP(cudaMalloc((void **)&p->ds, sizeof(DiisState)));
+    for (double **b : bufs) CKP(gtf_dmalloc((void **)b, sizeof(double) * nn, p->st));
+    CKP(gtf_dmalloc((void **)&p->vecs, sizeof(double) * nn * PUR_MAX_DIIS, p->st));
+    CKP(gtf_dmalloc((void **)&p->Fvecs, sizeof(double) * nn * PUR_MAX_DIIS, p->st));
+    CKP(gtf_dmalloc((void **)&p->part, sizeof(double) * RED_BLOCKS * 16, p->st));
+    CKP(gtf_dmalloc((void **)&p->scal, sizeof(double) * 16, p->st));
+    p->h_scal = (double *)gtf_pinned_alloc(sizeof(double) * 16);
+    if (!p->h_scal) return GTF_ERR_ALLOC;
+    CKP(gtf_dmalloc((void **)&p->ds, sizeof(DiisState), p->st));
     CKP(cudaEventCreate(&p->e0));
     CKP(cudaEventCreate(&p->e1));
     k_diis_reset<<<1, 128, 0, p->st>>>(p->ds);
@@ -363,7 +370,7 @@ extern "C" int gtf_purif_set_mode(gtf_purif_dev_t *p, int mode)
 {
     if (mode != 0 && mode != 1) return GTF_ERR_INVALID;
     if (mode == 1 && !p->bx) {
-        const int r = gtf_bf16x3_create(p->n, &p->bx);
+        const int r = gtf_bf16x3_create(p->n, p->st, &p->bx);
         if (r != GTF_OK) return r;
     }
     p->mode = mode;
@@ -382,13 +389,12 @@ extern "C" void gtf_purif_destroy(gtf_purif_dev_t *p)
     cudaStreamSynchronize(p->st);
     if (p->bx) gtf_bf16x3_destroy(p->bx);
     double *bufs[] = {p->S, p->X, p->D, p->D2, p->D3, p->F, p->W, p->W2, p->E, p->vecs, p->Fvecs, p->part, p->scal};
-    for (double *b : bufs)
-        if (b) cudaFree(b);
-    if (p->ds) cudaFree(p->ds);
-    if (p->h_scal) cudaFreeHost(p->h_scal);
-    cublasDestroy(p->blas);
-    cudaEventDestroy(p->e0);
-    cudaEventDestroy(p->e1);
+    for (double *b : bufs) gtf_dfree(b, p->st);
+    gtf_dfree(p->ds, p->st);
+    gtf_pinned_free(p->h_scal);
+    if (p->e0) cudaEventDestroy(p->e0);
+    if (p->e1) cudaEventDestroy(p->e1);
+    if (p->own_st) cudaStreamDestroy(p->st);
     delete p;
 }
 
@@ -420,6 +426,9 @@ extern "C" int gtf_purif_set_sx_dev(gtf_purif_dev_t *p, const double *S_dev, con
 
 extern "C" int gtf_purif_run_dev(gtf_purif_dev_t *p, const double *F_dev, double *D_dev, int *iters)
 {
+    BlasLease lease(p->st);
+    if (!lease.h) return GTF_ERR_CUDA;
+    p->blas = lease.h;
     const int n = p->n;
     const size_t nn = (size_t)n * n;
     const unsigned ge = (unsigned)((nn + 255) / 256);
@@ -516,6 +525,9 @@ extern "C" int gtf_purif_run(gtf_purif_dev_t *p, const double *F_host, double *D
 // no host synchronisation.  iter <= 1: F = X F X only.
 extern "C" int gtf_diis_step_dev(gtf_purif_dev_t *p, const double *D_dev, double *F_dev, int iter)
 {
+    BlasLease lease(p->st);
+    if (!lease.h) return GTF_ERR_CUDA;
+    p->blas = lease.h;
     const int n = p->n;
     const size_t nn = (size_t)n * n;
     cudaStream_t st = p->st;

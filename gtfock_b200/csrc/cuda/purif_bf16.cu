@@ -28,6 +28,7 @@
 
 #include <type_traits>
 
+#include "devmem.cuh"
 #include "gtf_cuda.h"
 
 extern "C" void gtf_note_launches(int n);
@@ -88,20 +89,24 @@ struct gtf_bf16x3 {
     float *C;
     void *ws;
     size_t ws_bytes;
+    cudaStream_t st;   // the buffers' stream (stream-ordered pool, devmem.cu)
 };
 
 // The B operand has np rows (rows n..np-1 zero) so that the output's
 // contiguous dimension N = np meets the epilogue's 16-byte alignment.
-extern "C" int gtf_bf16x3_create(int n, gtf_bf16x3_t **out)
+// Buffers on `stream` (the purification object's); the products must run on
+// the same stream, and the caller synchronizes it before destroying.
+extern "C" int gtf_bf16x3_create(int n, void *stream, gtf_bf16x3_t **out)
 {
     *out = nullptr;
     gtf_bf16x3 *g = new gtf_bf16x3();
     g->n = n;
     g->np = (n + 7) / 8 * 8;
+    g->st = (cudaStream_t)stream;
     const size_t ab = sizeof(__nv_bfloat16) * (size_t)g->np * 3 * g->np;
-    if (cudaMalloc(&g->A, ab) != cudaSuccess || cudaMalloc(&g->B, ab) != cudaSuccess ||
-        cudaMalloc(&g->C, sizeof(float) * 3 * (size_t)n * g->np) != cudaSuccess ||
-        cudaMemset(g->B, 0, ab) != cudaSuccess) {
+    if (gtf_dmalloc((void **)&g->A, ab, g->st) != cudaSuccess || gtf_dmalloc((void **)&g->B, ab, g->st) != cudaSuccess ||
+        gtf_dmalloc((void **)&g->C, sizeof(float) * 3 * (size_t)n * g->np, g->st) != cudaSuccess ||
+        cudaMemsetAsync(g->B, 0, ab, g->st) != cudaSuccess) {
         gtf_bf16x3_destroy(g);
         return GTF_ERR_ALLOC;
     }
@@ -114,10 +119,10 @@ extern "C" int gtf_bf16x3_create(int n, gtf_bf16x3_t **out)
 extern "C" void gtf_bf16x3_destroy(gtf_bf16x3_t *g)
 {
     if (!g) return;
-    cudaFree(g->A);
-    cudaFree(g->B);
-    cudaFree(g->C);
-    cudaFree(g->ws);
+    gtf_dfree(g->A, g->st);
+    gtf_dfree(g->B, g->st);
+    gtf_dfree(g->C, g->st);
+    gtf_dfree(g->ws, g->st);
     delete g;
 }
 
@@ -151,9 +156,9 @@ extern "C" int gtf_bf16x3_abt(gtf_bf16x3_t *g, const double *A, const double *B,
     if (gemm.can_implement(args) != cutlass::Status::kSuccess) return GTF_ERR_INVALID;
     const size_t need = Gemm::get_workspace_size(args);
     if (need > g->ws_bytes) {
-        cudaFree(g->ws);
+        gtf_dfree(g->ws, st);   // ordered after the previous products on st
         g->ws = nullptr;
-        if (cudaMalloc(&g->ws, need) != cudaSuccess) return GTF_ERR_ALLOC;
+        if (gtf_dmalloc(&g->ws, need, st) != cudaSuccess) return GTF_ERR_ALLOC;
         g->ws_bytes = need;
     }
     if (gemm.initialize(args, g->ws, st) != cutlass::Status::kSuccess) return GTF_ERR_CUDA;

@@ -140,6 +140,10 @@ class SCFServer:
                        etol=etol)
         self.credit = 0.0
         self.tmp = tempfile.mkdtemp(prefix="gtf_serve_")
+        # host-side time accounting: job set-up (Batch.add), removal, and
+        # the steps of each lane, in seconds
+        self.stats = {"adds": 0, "add_s": 0.0, "removes": 0, "remove_s": 0.0,
+                      "steps": [0] * len(self.lanes), "step_s": [0.0] * len(self.lanes)}
 
     @property
     def mem_used(self):
@@ -181,7 +185,10 @@ class SCFServer:
     def admit(self, r, now):
         ln = self._lane(r)
         with ln.lock:
+            t0 = time.perf_counter()
             r.slot = ln.batch.add(mol.basis_file(r.basis), self._xyz(r), **self.kw)
+            self.stats["add_s"] += time.perf_counter() - t0
+            self.stats["adds"] += 1
             r.admitted = now
             ln.live[r.slot] = r
             nbytes = ln.batch.job_device_bytes(r.slot)
@@ -235,14 +242,21 @@ class SCFServer:
         with ln.lock:
             if not ln.live:
                 return done
+            k = self.lanes.index(ln)
+            t0 = time.perf_counter()
             ln.batch.step()
+            self.stats["step_s"][k] += time.perf_counter() - t0
+            self.stats["steps"][k] += 1
             for s in list(ln.live):
                 e, fin = ln.batch.result(s)
                 if fin:
                     r = ln.live.pop(s)
                     r.energies = e
                     r.finished = now_fn()
+                    t1 = time.perf_counter()
                     ln.batch.remove(s)
+                    self.stats["remove_s"] += time.perf_counter() - t1
+                    self.stats["removes"] += 1
                     with self._mu:
                         self.admission.release(id(r))
                     done.append(r)
