@@ -107,6 +107,9 @@ def load():
     _sig(L, "gtf_launch_count", [], ctypes.c_ulonglong)
     _sig(L, "gtf_batch_create", [_i], _vp)
     _sig(L, "gtf_batch_add", [_vp, _cp, _cp, _d, _i, _d, _i, _d])
+    _sig(L, "gtf_batch_prepare", [_vp, _cp, _cp, _d, _i, _d, ctypes.POINTER(_vp)])
+    _sig(L, "gtf_batch_attach", [_vp, _vp, _i, _d])
+    _sig(L, "gtf_batch_job_free", [_vp], None)
     _sig(L, "gtf_batch_step", [_vp])
     _sig(L, "gtf_batch_run", [_vp])
     _sig(L, "gtf_batch_result", [_vp, _i, _dp, _ip, _ip])
@@ -561,6 +564,31 @@ class Batch:
             raise GtfError("gtf_batch_add failed (%d)" % slot)
         self.max_iters[slot] = max_iters
         return slot
+
+    def prepare(self, gbs, xyz, tolscr=1e-10, precision=0, fp32_cutoff=0.0):
+        """The part of add() that touches no state of the batch (basis,
+        engine, S, H_core, X): may run while another thread steps the batch.
+        Returns a job handle for attach()."""
+        job = _vp()
+        r = load().gtf_batch_prepare(self.h, gbs.encode(), xyz.encode(), tolscr, precision, fp32_cutoff,
+                                     ctypes.byref(job))
+        if r != 0:
+            raise GtfError("gtf_batch_prepare failed (%d)" % r)
+        return job
+
+    def attach(self, job, max_iters=30, etol=1e-11):
+        """Put a prepared job in a free slot (not while the batch steps);
+        consumes the job.  Returns the slot."""
+        slot = load().gtf_batch_attach(self.h, job, max_iters, etol)
+        if slot < 0:
+            raise GtfError("gtf_batch_attach failed (%d)" % slot)
+        self.max_iters[slot] = max_iters
+        return slot
+
+    @staticmethod
+    def release(job):
+        """Release a prepared job that will not be attached."""
+        load().gtf_batch_job_free(job)
 
     def step(self):
         r = load().gtf_batch_step(self.h)

@@ -24,6 +24,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <utility>
 #include <vector>
 
 #include "devmem.cuh"
@@ -582,20 +583,19 @@ extern "C" gtf_batch_t *gtf_batch_create(int capacity)
     return b;
 }
 
-// Set-up of one SCF job (pscf/scf.c:298-314, init_oedmat pscf/scf.c:131-185)
-// in a free slot; returns the slot or a negative error.
-extern "C" int gtf_batch_add(gtf_batch_t *b, const char *bsfile, const char *xyzfile, double tolscr, int prec_mode,
-                             double fp32_cutoff, int max_iters, double etol)
+// A job set up but not yet in a batch (gtf_batch_prepare / gtf_batch_attach).
+struct gtf_batch_job {
+    BJob j;
+    int prec_mode;
+};
+
+// The part of a job's set-up that touches no batch: basis, engine (screening,
+// pair data, task lists, precision, incremental builds), S, H_core and X, all
+// on the engine's own stream, which is synchronized at the end.  Returns 0 or
+// gtf_batch_add's error codes -3 .. -5.
+static int job_prepare(BJob &j, const char *bsfile, const char *xyzfile, double tolscr, int prec_mode,
+                       double fp32_cutoff, int incr, double incr_tau, int incr_period)
 {
-    if (!b || !bsfile || !xyzfile || max_iters <= 0 || !(etol >= 0.0)) return -1;
-    int slot = -1;
-    for (int s = 0; s < b->capacity; s++)
-        if (!b->jobs[s].used) {
-            slot = s;
-            break;
-        }
-    if (slot < 0) return -2;
-    BJob &j = b->jobs[slot];
     j = BJob();
     if (CInt_createBasisSet(&j.basis) != CINT_STATUS_SUCCESS ||
         CInt_loadBasisSet(j.basis, (char *)bsfile, (char *)xyzfile) != CINT_STATUS_SUCCESS) {
@@ -608,17 +608,28 @@ extern "C" int gtf_batch_add(gtf_batch_t *b, const char *bsfile, const char *xyz
     j.enuc = CInt_getNucEnergy(j.basis);
     if (PFock_create(j.basis, 1, 1, 4, tolscr, 1, 1, &j.pf) != PFOCK_STATUS_SUCCESS) {
         j.pf = nullptr;
-        job_free(j, b->st);
+        job_free(j, nullptr);
         return -4;
     }
     j.used = 1;
     j.eng = gtf_pfock_device(j.pf);
     if ((prec_mode != 0 && gtf_pfock_set_precision(j.pf, prec_mode, fp32_cutoff) != PFOCK_STATUS_SUCCESS) ||
         PFock_createOvlMat(j.pf, j.basis) != PFOCK_STATUS_SUCCESS ||
-        PFock_createCoreHMat(j.pf, j.basis) != PFOCK_STATUS_SUCCESS) {
-        job_free(j, b->st);
+        PFock_createCoreHMat(j.pf, j.basis) != PFOCK_STATUS_SUCCESS ||
+        (incr && gtf_pfock_set_incremental(j.pf, 1, incr_tau, incr_period) != PFOCK_STATUS_SUCCESS) ||
+        cudaStreamSynchronize((cudaStream_t)gtf_fock_stream(j.eng)) != cudaSuccess) {
+        job_free(j, nullptr);
         return -5;
     }
+    return 0;
+}
+
+// The job's batch buffers (on the batch's stream), its device descriptor and
+// initial density, in `slot`; -6 / -7 on failure (the job is released).
+static int job_attach(gtf_batch *b, int slot, BJob &&src, int prec_mode, int max_iters, double etol)
+{
+    BJob &j = b->jobs[slot];
+    j = std::move(src);
     const size_t nn = (size_t)j.n * j.n;
     j.bytes = job_buffer_bytes(j.n);
     JobDev &d = j.dv;
@@ -642,8 +653,7 @@ extern "C" int gtf_batch_add(gtf_batch_t *b, const char *bsfile, const char *xyz
     d.F = const_cast<double *>(gtf_fock_mat_dev(j.eng, 1, 0));
     d.Fe = d.F;
     if (b->incr) {
-        if (gtf_pfock_set_incremental(j.pf, 1, b->incr_tau, b->incr_period) != PFOCK_STATUS_SUCCESS ||
-            gtf_dmalloc((void **)&j.fcopy, sizeof(double) * nn, b->st) != cudaSuccess) {
+        if (gtf_dmalloc((void **)&j.fcopy, sizeof(double) * nn, b->st) != cudaSuccess) {
             j.fcopy = nullptr;
             job_free(j, b->st);
             return -6;
@@ -667,14 +677,13 @@ extern "C" int gtf_batch_add(gtf_batch_t *b, const char *bsfile, const char *xyz
     d.diis = 0;
     d.ds = b->d_diis + slot;
     k_j_diis_reset<<<1, 128, 0, b->st>>>(d.ds);
-    // initial guess (pscf/scf.c:34-76) into the engine's density buffer
+    // initial guess (pscf/scf.c:34-76) into the engine's density buffer; the
+    // engine's set-up is complete (job_prepare), and the job's buffers on the
+    // batch's stream are before the batch's launches use them; the other
+    // lanes' work is not waited for
     std::vector<double> D0(nn);
     gtf_initial_density(j.basis, D0.data(), j.n);
-    // the engine's set-up (its stream) and the job's buffers (the batch's
-    // stream) are complete before the batch's launches use them; the other
-    // lanes' work is not waited for
-    if (cudaStreamSynchronize((cudaStream_t)gtf_fock_stream(j.eng)) != cudaSuccess ||
-        cudaMemcpyAsync(d.D, D0.data(), sizeof(double) * nn, cudaMemcpyHostToDevice, b->st) != cudaSuccess ||
+    if (cudaMemcpyAsync(d.D, D0.data(), sizeof(double) * nn, cudaMemcpyHostToDevice, b->st) != cudaSuccess ||
         cudaStreamSynchronize(b->st) != cudaSuccess) {
         job_free(j, b->st);
         return -7;
@@ -687,6 +696,73 @@ extern "C" int gtf_batch_add(gtf_batch_t *b, const char *bsfile, const char *xyz
     j.failed = 0;
     b->dirty = 1;
     return slot;
+}
+
+static int free_slot(const gtf_batch *b)
+{
+    for (int s = 0; s < b->capacity; s++)
+        if (!b->jobs[s].used) return s;
+    return -1;
+}
+
+// Set-up of one SCF job (pscf/scf.c:298-314, init_oedmat pscf/scf.c:131-185)
+// in a free slot; returns the slot or a negative error.
+extern "C" int gtf_batch_add(gtf_batch_t *b, const char *bsfile, const char *xyzfile, double tolscr, int prec_mode,
+                             double fp32_cutoff, int max_iters, double etol)
+{
+    if (!b || !bsfile || !xyzfile || max_iters <= 0 || !(etol >= 0.0)) return -1;
+    const int slot = free_slot(b);
+    if (slot < 0) return -2;
+    BJob j;
+    const int r = job_prepare(j, bsfile, xyzfile, tolscr, prec_mode, fp32_cutoff, b->incr, b->incr_tau,
+                              b->incr_period);
+    if (r) return r;
+    return job_attach(b, slot, std::move(j), prec_mode, max_iters, etol);
+}
+
+// gtf_batch_add in two parts, so that a server can set a job up while the
+// batch it will join is stepping on another thread: gtf_batch_prepare touches
+// no state of the batch but its (fixed) incremental setting; gtf_batch_attach
+// takes a free slot and must not overlap a step of the batch.
+extern "C" int gtf_batch_prepare(gtf_batch_t *b, const char *bsfile, const char *xyzfile, double tolscr,
+                                 int prec_mode, double fp32_cutoff, gtf_batch_job_t **out)
+{
+    if (!out) return -1;
+    *out = nullptr;
+    if (!b || !bsfile || !xyzfile) return -1;
+    gtf_batch_job *job = new gtf_batch_job();
+    job->prec_mode = prec_mode;
+    const int r = job_prepare(job->j, bsfile, xyzfile, tolscr, prec_mode, fp32_cutoff, b->incr, b->incr_tau,
+                              b->incr_period);
+    if (r) {
+        delete job;
+        return r;
+    }
+    *out = job;
+    return 0;
+}
+
+extern "C" int gtf_batch_attach(gtf_batch_t *b, gtf_batch_job_t *job, int max_iters, double etol)
+{
+    if (!b || !job || max_iters <= 0 || !(etol >= 0.0)) {
+        gtf_batch_job_free(job);
+        return -1;
+    }
+    const int slot = free_slot(b);
+    if (slot < 0) {
+        gtf_batch_job_free(job);
+        return -2;
+    }
+    const int r = job_attach(b, slot, std::move(job->j), job->prec_mode, max_iters, etol);
+    delete job;
+    return r;
+}
+
+extern "C" void gtf_batch_job_free(gtf_batch_job_t *job)
+{
+    if (!job) return;
+    job_free(job->j, nullptr);
+    delete job;
 }
 
 extern "C" int gtf_batch_remove(gtf_batch_t *b, int slot)

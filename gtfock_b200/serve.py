@@ -142,7 +142,7 @@ class SCFServer:
         self.tmp = tempfile.mkdtemp(prefix="gtf_serve_")
         # host-side time accounting: job set-up (Batch.add), removal, and
         # the steps of each lane, in seconds
-        self.stats = {"adds": 0, "add_s": 0.0, "removes": 0, "remove_s": 0.0,
+        self.stats = {"adds": 0, "add_s": 0.0, "prepare_s": 0.0, "attach_s": 0.0, "removes": 0, "remove_s": 0.0,
                       "steps": [0] * len(self.lanes), "step_s": [0.0] * len(self.lanes)}
 
     @property
@@ -184,9 +184,18 @@ class SCFServer:
 
     def admit(self, r, now):
         ln = self._lane(r)
+        kw = self.kw
+        # the set-up runs while the lane keeps stepping; only the attach
+        # (batch buffers, slot) waits for the lane between two steps
+        t0 = time.perf_counter()
+        job = ln.batch.prepare(mol.basis_file(r.basis), self._xyz(r), tolscr=kw["tolscr"],
+                               precision=kw["precision"], fp32_cutoff=kw["fp32_cutoff"])
+        t1 = time.perf_counter()
         with ln.lock:
-            t0 = time.perf_counter()
-            r.slot = ln.batch.add(mol.basis_file(r.basis), self._xyz(r), **self.kw)
+            t2 = time.perf_counter()
+            r.slot = ln.batch.attach(job, max_iters=kw["max_iters"], etol=kw["etol"])
+            self.stats["prepare_s"] += t1 - t0
+            self.stats["attach_s"] += time.perf_counter() - t2
             self.stats["add_s"] += time.perf_counter() - t0
             self.stats["adds"] += 1
             r.admitted = now

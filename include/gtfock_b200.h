@@ -216,6 +216,20 @@ typedef struct gtf_batch gtf_batch_t;
 gtf_batch_t *gtf_batch_create(int capacity);
 int gtf_batch_add(gtf_batch_t *b, const char *bsfile, const char *xyzfile, double tolscr, int prec_mode,
                   double fp32_cutoff, int max_iters, double etol);
+/* gtf_batch_add in two parts, for a server that sets a job up on one host
+ * thread while the batch steps on another: gtf_batch_prepare does the whole
+ * set-up that touches no state of the batch (basis, engine, S, H_core, X, on
+ * the engine's own stream; it reads only the batch's incremental setting,
+ * fixed before the first job) and may overlap a gtf_batch_step of `b`;
+ * gtf_batch_attach puts the job in a free slot (its batch buffers and initial
+ * density) and must not overlap a step.  attach consumes the job, on success
+ * and on error alike; gtf_batch_job_free releases one never attached.
+ * Return codes as gtf_batch_add's (prepare: 0 on success). */
+typedef struct gtf_batch_job gtf_batch_job_t;
+int gtf_batch_prepare(gtf_batch_t *b, const char *bsfile, const char *xyzfile, double tolscr, int prec_mode,
+                      double fp32_cutoff, gtf_batch_job_t **job);
+int gtf_batch_attach(gtf_batch_t *b, gtf_batch_job_t *job, int max_iters, double etol);
+void gtf_batch_job_free(gtf_batch_job_t *job);
 int gtf_batch_step(gtf_batch_t *b);
 int gtf_batch_run(gtf_batch_t *b);
 int gtf_batch_result(gtf_batch_t *b, int slot, double *energies, int *niters, int *done);
@@ -237,7 +251,8 @@ int gtf_batch_job_stats(gtf_batch_t *b, int slot, double *out, int n);
  * batched jobs, [5] batch steps.  Writes min(n, 6) values, returns that count. */
 int gtf_batch_stats(gtf_batch_t *b, double *out, int n);
 /* Incremental Fock builds (gtf_pfock_set_incremental) for every job of the
- * batch; set before the first gtf_batch_add (-2 otherwise).  0 on success. */
+ * batch; set before the first gtf_batch_add or gtf_batch_prepare (-2 after a
+ * job has joined).  0 on success. */
 int gtf_batch_set_incremental(gtf_batch_t *b, int on, double tau, int period);
 /* Tunes the batch's launch shapes for its current jobs (see
  * gtf_pfock_autotune); call between steps. */

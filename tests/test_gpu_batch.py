@@ -145,3 +145,38 @@ def test_solo_launches_in_a_batch(tmp_path, monkeypatch):
         assert done and n >= 1
         assert abs(e[n - 1] - ref[n - 1]) < 1e-9, (c, e[n - 1], ref[n - 1])
     b.close()
+
+
+def test_prepare_attach_while_stepping(tmp_path):
+    """gtf_batch_prepare on one thread while the batch steps on another, then
+    gtf_batch_attach between steps: the attached jobs give the oracle's
+    energies (as gtf_batch_add's do); a prepared job that is released
+    instead leaves nothing behind."""
+    import threading
+    b = gb.Batch(3)
+    g0, gbs0, xyz0 = _inputs("c4h10_ccpvdz", tmp_path)
+    s0 = b.add(gbs0, xyz0, tolscr=float(g0["tol"]), max_iters=len(g0["energies"]))
+    jobs = {}
+
+    def prep():
+        for c in ["h2o_ccpvdz", "ch4_ccpvdz"]:
+            g, gbs, xyz = _inputs(c, tmp_path)
+            jobs[c] = (b.prepare(gbs, xyz, tolscr=float(g["tol"])), g)
+        g, gbs, xyz = _inputs("h2o_631g", tmp_path)
+        jobs["released"] = (b.prepare(gbs, xyz, tolscr=float(g["tol"])), g)
+
+    th = threading.Thread(target=prep)
+    th.start()
+    while th.is_alive():
+        b.step()
+    th.join()
+    gb.Batch.release(jobs.pop("released")[0])
+    slots = {c: (b.attach(job, max_iters=len(g["energies"])), g) for c, (job, g) in jobs.items()}
+    b.run()
+    for c, (s, g) in list(slots.items()) + [("c4h10_ccpvdz", (s0, g0))]:
+        e, done = b.result(s)
+        ref = g["energies"]
+        assert done
+        n = min(len(e), len(ref))
+        assert abs(e[n - 1] - ref[n - 1]) < 1e-9, (c, e[n - 1], ref[n - 1])
+    b.close()
