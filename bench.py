@@ -460,8 +460,9 @@ def run_c12h26(args):
 def c12h26_measure(warmup, steps):
     """10-iteration SCF of C12H26 / cc-pVDZ (298 bf), the CPU-runnable
     configuration the reference's own driver is timed on (--impl reference):
-    resident solves (mean of `steps` after `warmup`) and the median of three
-    end-to-end runs from the host files through the C API."""
+    resident solves (mean of `steps` after `warmup`) and the median of five
+    end-to-end runs from the host files through the C API (after a garbage
+    collection of the Python heap, so that none falls inside them)."""
     import gtfock_b200 as gb
     from gtfock_b200 import molecules as mol
     with tempfile.TemporaryDirectory() as td:
@@ -476,8 +477,10 @@ def c12h26_measure(warmup, steps):
             e, tm = s.solve(niters=NITER)
         dt = (time.perf_counter() - t0) / steps
         s.close()
+        import gc
+        gc.collect()
         e2e = []
-        for _ in range(3):
+        for _ in range(5):
             t0 = time.perf_counter()
             e2, _ = gb.scf_run(gbs, xyz, TOL, NITER, device_resident=False)
             e2e.append(time.perf_counter() - t0)
@@ -591,6 +594,7 @@ def batched_measure(count, seed, cut, autotune, seq_sample, rk=None):
                      "purification_steps": info["purification_steps"], "steps": info["steps"],
                      "launches": gb.launch_count() - l0}
             b.close()
+            gb.device_trim(0)   # untimed: the jobs' cached device memory back to the driver
             parts = rk.gather((mine_e, stats))
             res[tag] = {}
             for e, _ in parts:

@@ -141,6 +141,7 @@ def load():
     _sig(L, "gtf_batch_job_stats", [_vp, _i, _dp, _i])
     _sig(L, "gtf_device_memory", [ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)])
     _sig(L, "gtf_set_device", [_i])
+    _sig(L, "gtf_device_trim", [ctypes.c_size_t])
     _sig(L, "gtf_get_device", [_ip])
     _sig(L, "gtf_debug_fail_alloc", [_i], None)
     _sig(L, "gtf_debug_live_allocs", [], ctypes.c_longlong)
@@ -167,6 +168,13 @@ def set_device(dev):
     process per GPU; a new thread starts on device 0 and selects again)."""
     if load().gtf_set_device(int(dev)) != 0:
         raise GtfError("gtf_set_device(%d) failed" % dev)
+
+
+def device_trim(keep=0):
+    """Return the library's cached pool blocks on the current device to the
+    driver, down to `keep` bytes (waits for the device)."""
+    if load().gtf_device_trim(int(keep)) != 0:
+        raise GtfError("gtf_device_trim failed")
 
 
 def get_device():

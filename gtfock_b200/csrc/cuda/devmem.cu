@@ -29,8 +29,13 @@ namespace {
 constexpr int kMaxDev = 64;
 std::once_flag g_pool_once[kMaxDev];
 
-// keep up to 2 GiB of freed blocks in the pool between synchronizations, so
-// that the next molecule's buffers are carved from memory already mapped
+// Keep up to 16 GiB of freed blocks in the pool between synchronizations,
+// so that the next molecule's buffers are carved from memory already mapped:
+// returning many GiB to the driver at a synchronization takes a large
+// fraction of a second, which a served stream would otherwise pay at random
+// points.  gtf_device_memory counts these cached blocks as free, and
+// gtf_device_trim returns them at a quiet moment.
+constexpr uint64_t kPoolKeep = 16ull << 30;
 void configure_pool(int dev)
 {
     cudaMemPool_t pool;
@@ -38,10 +43,42 @@ void configure_pool(int dev)
         cudaGetLastError();
         return;
     }
-    uint64_t thr = 2ull << 30;
+    uint64_t thr = kPoolKeep;
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
 }
 }  // namespace
+
+// bytes the current device's pool holds without an allocation in them
+extern "C" size_t gtf_pool_cached_bytes(void)
+{
+    int dev = 0;
+    cudaMemPool_t pool;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    uint64_t reserved = 0, used = 0;
+    if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) != cudaSuccess ||
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return reserved > used ? (size_t)(reserved - used) : 0;
+}
+
+// return the current device's cached pool blocks to the driver, down to
+// `keep` bytes (waits for the frees in flight on every stream)
+extern "C" int gtf_device_trim(size_t keep)
+{
+    int dev = 0;
+    cudaMemPool_t pool;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return GTF_ERR_CUDA;
+    }
+    if (cudaDeviceSynchronize() != cudaSuccess) return GTF_ERR_CUDA;
+    return cudaMemPoolTrimTo(pool, keep) == cudaSuccess ? GTF_OK : GTF_ERR_CUDA;
+}
 
 extern "C" cudaError_t gtf_dmalloc(void **p, size_t bytes, cudaStream_t st)
 {

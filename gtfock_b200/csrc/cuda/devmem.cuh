@@ -12,6 +12,8 @@ cudaError_t gtf_dmalloc(void **p, size_t bytes, cudaStream_t st);
 // free ordered on `st`: every use of p must be ordered before it on `st`,
 // or have completed (host-synchronized) before the call
 void gtf_dfree(void *p, cudaStream_t st);
+// unallocated bytes cached in the current device's pool
+size_t gtf_pool_cached_bytes(void);
 // pinned host block (never returned to the driver; reused by later calls)
 void *gtf_pinned_alloc(size_t bytes);
 void gtf_pinned_free(void *p);

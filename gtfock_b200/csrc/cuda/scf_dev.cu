@@ -110,6 +110,10 @@ extern "C" int gtf_get_device(int *dev)
     return cudaGetDevice(dev) == cudaSuccess ? GTF_OK : GTF_ERR_CUDA;
 }
 
+extern "C" size_t gtf_pool_cached_bytes(void);
+
+// free bytes include the blocks cached in the library's memory pool, which
+// its next allocations reuse
 extern "C" int gtf_device_memory(size_t *free_bytes, size_t *total_bytes)
 {
     size_t fr = 0, to = 0;
@@ -117,6 +121,8 @@ extern "C" int gtf_device_memory(size_t *free_bytes, size_t *total_bytes)
         cudaGetLastError();
         return GTF_ERR_CUDA;
     }
+    fr += gtf_pool_cached_bytes();
+    if (fr > to) fr = to;
     if (free_bytes) *free_bytes = fr;
     if (total_bytes) *total_bytes = to;
     return GTF_OK;

@@ -32,7 +32,7 @@ import time
 
 import numpy as np
 
-from . import BasisSet, Batch, SCFSolver, device_memory, set_device
+from . import BasisSet, Batch, SCFSolver, device_memory, device_trim, set_device
 from . import molecules as mol
 
 
@@ -274,6 +274,7 @@ class SCFServer:
     def close(self):
         for ln in self.lanes:
             ln.batch.close()
+        device_trim(0)   # the jobs' cached device memory back to the driver
 
 
 def run_stream(requests, server):

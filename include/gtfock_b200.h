@@ -267,8 +267,15 @@ void gtf_batch_destroy(gtf_batch_t *b);
 int gtf_set_device(int dev);
 int gtf_get_device(int *dev);
 
-/* Free and total bytes of the current device (cudaMemGetInfo); 0 on success. */
+/* Free and total bytes of the current device (cudaMemGetInfo, plus the
+ * blocks cached in the library's memory pool, which its next allocations
+ * reuse); 0 on success. */
 int gtf_device_memory(size_t *free_bytes, size_t *total_bytes);
+/* The library takes device buffers from the device's stream-ordered memory
+ * pool and keeps up to 16 GiB of freed blocks cached; gtf_device_trim waits
+ * for the device and returns the cached blocks to the driver down to `keep`
+ * bytes (a server calls it when it stops).  0 on success. */
+int gtf_device_trim(size_t keep);
 
 /* Test hook: the n-th device allocation of an engine's set-up from now on
  * fails as an out-of-memory cudaMalloc would (n <= 0 disarms), so that the
