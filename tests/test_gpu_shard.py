@@ -1,8 +1,9 @@
 """Sharded Fock builds on the GPU: the parts of n shards built by the CUDA
 kernels sum to the whole F (FP64 and mixed precision), the shards' work is
-balanced by the weighted split, and the NCCL path of
-ShardedFock (device F all-reduced in place) gives the whole F on a one-rank
-group (the only group a one-GPU run can form)."""
+balanced by the weighted split, the NCCL path of ShardedFock (device F
+all-reduced in place) gives the whole F on a one-rank group (the only NCCL
+group a one-GPU run can form), and two processes sharing the GPU, each
+building its shard and summing over gloo, both hold the whole F."""
 import os
 import socket
 
@@ -102,3 +103,54 @@ def test_sharded_fock_nccl_one_rank(tmp_path):
         sf.close()
     finally:
         dist.destroy_process_group()
+
+
+def _shard_rank(rank, world, port, gbs, xyz, tol, D_path, out):
+    import torch
+    import torch.distributed as dist
+    import gtfock_b200 as gb_
+    from gtfock_b200.shard import ShardedFock
+    dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank, world_size=world)
+    try:
+        b = gb_.BasisSet(gbs, xyz)
+        D = np.load(D_path)
+        sf = ShardedFock(b, tolscr=tol)
+        Fh = sf.compute_fock(D)                               # host F, gloo all-reduce
+        Fd = sf.compute_fock_dev(torch.from_numpy(D).cuda())  # device F, gloo all-reduce
+        torch.cuda.synchronize()
+        np.save(out + ".h%d.npy" % rank, Fh)
+        np.save(out + ".d%d.npy" % rank, Fd.cpu().numpy())
+        np.save(out + ".w%d.npy" % rank, np.array([sf.pf.shard_work()]))
+        sf.close()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_fock_two_processes(tmp_path):
+    """Two processes, each building one shard of every class launch with the
+    library's split and summing F over a gloo group: both hold the pinned
+    C4H10 / cc-pVDZ F.  With one GPU both processes share it (they wait on
+    one another only on the host); a node with a GPU per rank runs the same
+    code with NCCL for the device F."""
+    import multiprocessing as mp
+    g = load_golden("c4h10_ccpvdz")
+    gbs, xyz = golden_xyz(g, tmp_path)
+    D_path = str(tmp_path / "D.npy")
+    np.save(D_path, g["D"])
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    out = str(tmp_path / "sf")
+    ctx = mp.get_context("spawn")
+    procs = [ctx.Process(target=_shard_rank, args=(r, 2, port, gbs, xyz, float(g["tol"]), D_path, out))
+             for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(300)
+        assert p.exitcode == 0
+    for r in range(2):
+        assert np.abs(np.load(out + ".h%d.npy" % r) - g["F"]).max() < 1e-10
+        assert np.abs(np.load(out + ".d%d.npy" % r) - g["F"]).max() < 1e-10
+    w0, w1 = (float(np.load(out + ".w%d.npy" % r)[0]) for r in range(2))
+    assert abs(w0 - w1) <= 0.1 * (w0 + w1)
