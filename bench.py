@@ -812,6 +812,9 @@ def run_precision(args):
             msc = pf.timing()["ms_eri"]
             nq32, nq = pf.precision_stats()
             s.set_options(precision=1, fp32_cutoff=cut, etol=1e-10)
+            # FP64 purification products: these rows isolate the ERI precision
+            # (mixed precision would otherwise select the split-BF16 products)
+            s.set_purification(0)
             t0 = time.perf_counter()
             e, _ = s.solve(niters=60)
             tc = time.perf_counter() - t0
