@@ -101,4 +101,9 @@ class ShardedFock:
         return allreduce_fock(F, self.group)
 
     def close(self):
+        # the engine frees F on its own stream: work of other streams (the
+        # all-reduce) that uses the view must be complete
+        import torch
+        if torch.cuda.is_available():
+            torch.cuda.synchronize()
         self.pf.close()

@@ -127,7 +127,9 @@ PFockStatus_t gtf_pfock_precision_stats(PFock_t pfock, double *nquart_fp32, doub
  * dev_D on its own stream, which is not ordered after the caller's streams:
  * the kernels or copies that write dev_D must have completed before the call
  * (synchronize the stream that produced it).  The call returns once F is
- * complete. */
+ * complete.  *dev_F is freed with the engine on the engine's own stream:
+ * work of other streams that still reads or writes it must have completed
+ * before PFock_destroy. */
 PFockStatus_t gtf_pfock_compute_dev(PFock_t pfock, const double *dev_D,
                                     const double **dev_F);
 
