@@ -44,6 +44,8 @@ MIXED_CUTOFF = 1e-6
 # served and batched forms: FP32 quartets below a Schwarz bound of 1e-4
 # (profiles/precision_sweep_w64.md: |dE| 6.8e-10 Ha at 1e-4 on (H2O)64)
 SERVED_CUTOFF = 1e-4
+# size lanes of the server: (largest basis of the lane, slots); None = no limit
+LANES = {1: ((None, None),), 2: ((400, None), (None, None)), 3: ((400, None), (800, None), (None, None))}
 INCR_PERIOD = 8          # incremental builds: a full build every 8 builds
 # served form: quartets of the density change dropped below bound x max|dD| <
 # 1e-9 (profiles/served_form_tau_sweep_w74.md: no measurable error added)
@@ -694,7 +696,7 @@ def served_measure(count, seed, rate, cut, slots, lanes, incremental, concurrent
     for _ in range(max(1, repeats)):
         reqs = share()
         srv = serve.SCFServer(slots=slots, precision=1, fp32_cutoff=cut, max_iters=30, etol=1e-6, tolscr=TOL,
-                              lanes=((400, None), (None, None)) if lanes == 2 else ((None, None),),
+                              lanes=LANES[lanes],
                               incremental=incremental, incr_tau=SERVED_TAU, incr_period=INCR_PERIOD,
                               concurrent=concurrent,
                               device=rk.device if rk.world > 1 else None)
@@ -896,7 +898,7 @@ def main():
     ap.add_argument("--seed", type=int, default=None)
     ap.add_argument("--rate", type=float, default=2.0, help="served: Poisson arrival rate (1/s)")
     ap.add_argument("--slots", type=int, default=64, help="served: resident jobs per lane at most")
-    ap.add_argument("--lanes", type=int, default=2, choices=[1, 2],
+    ap.add_argument("--lanes", type=int, default=2, choices=[1, 2, 3],
                     help="served: size lanes (2: up to 400 functions, and the rest)")
     ap.add_argument("--seq-sample", type=int, default=256, help="batched: molecules timed on the one-job path")
     ap.add_argument("--no-incremental", action="store_true", help="served: plain (not incremental) Fock builds")
