@@ -2476,6 +2476,9 @@ extern "C" void gtf_fock_release_onee(gtf_fock_dev_t *f, int which)
     }
 }
 
+// angular momentum of each shell, host copy (onee.cu groups shell pairs by class)
+extern "C" const int *gtf_fock_shell_L_host(gtf_fock_dev_t *f) { return f->h_sh_L.data(); }
+
 // basis arrays for onee.cu
 extern "C" void gtf_fock_basis_dev(gtf_fock_dev_t *f, const int **sh_L, const int **sh_nprim,
                                    const int **sh_pstart, const int **f_start, const int **fc_start,

@@ -158,6 +158,10 @@ void gtf_purif_reset(gtf_purif_dev_t *p);
 int gtf_purif_stats(gtf_purif_dev_t *p, double *ms_gemm, double *ms_total, double *errnorm,
                     double *idem_err, double *tr_err);
 
+/* page-locked host blocks from a process-wide free list (devmem.cu) */
+void *gtf_pinned_alloc(size_t bytes);
+void gtf_pinned_free(void *p);
+
 /* bookkeeping (scf_dev.cu) */
 void gtf_note_launches(int n);
 unsigned long long gtf_launch_count(void);

@@ -11,6 +11,8 @@
 #include <cusolverDn.h>
 #include <stdio.h>
 
+#include <vector>
+
 #include "devmem.cuh"
 #include "gtf_cuda.h"
 #include "gtf_dev.cuh"
@@ -21,6 +23,7 @@ extern "C" void gtf_fock_basis_dev(gtf_fock_dev_t *f, const int **sh_L, const in
                                    const int **Z, const double **atom_xyz, int *nshells, int *natoms, int *nbf,
                                    int *pure);
 extern "C" void *gtf_fock_stream(gtf_fock_dev_t *f);
+extern "C" const int *gtf_fock_shell_L_host(gtf_fock_dev_t *f);
 
 __constant__ double c_gh_x[4] = {-1.6506801238857845559, -0.52464762327529031788, 0.52464762327529031788,
                                  1.6506801238857845559};
@@ -33,156 +36,220 @@ __constant__ double c_sph_d1[5][6] = {
     {0.0, 0.0, 1.7320508075688772, 0.0, 0.0, 0.0},
     {0.8660254037844386, 0.0, 0.0, -0.8660254037844386, 0.0, 0.0}};
 
-__device__ __forceinline__ int cx_of(int L, int c) { return cart_x(L, c); }
-__device__ __forceinline__ int cy_of(int L, int c) { return cart_y(L, c); }
-__device__ __forceinline__ int cz_of(int L, int c) { return cart_z(L, c); }
+// One warp per unordered shell pair {A, B}, oriented so that L(A) >= L(B).
+// The lanes share out the pair's primitive pairs for S and T, and its
+// (primitive pair, nucleus) terms for V; the warp sums are taken by shuffles
+// in a fixed order, so the matrices are the same from run to run.  The block
+// of (A, B) is written together with its transpose, so S and H come out
+// exactly symmetric.  One launch per angular class pair keeps every
+// per-pair array in registers.
+struct OneePair {
+    int a, b;
+};
 
 template <int N>
-__device__ void nuclear_rys(double T, double (&u)[3], double (&w)[3])
+__device__ __forceinline__ void warp_sum(double (&v)[N])
 {
-    double uu[N], ww[N];
-    rys_roots<N>(T, uu, ww, RysTab<double>::ptr(N));
 #pragma unroll
-    for (int i = 0; i < N; i++) {
-        u[i] = uu[i];
-        w[i] = ww[i];
+    for (int k = 0; k < N; k++)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+}
+
+// spherical (pure d) or Cartesian block of c1 (+ c2 when given) at rows
+// fa.., columns fb.., and at the mirrored place
+template <int LA, int LB>
+__device__ __forceinline__ void onee_put(const double (&c1)[ncart(LA) * ncart(LB)], const double *c2, int pure,
+                                         int fa, int fb, int nbf, bool mirror, double *__restrict__ M)
+{
+    constexpr int NA = ncart(LA), NB = ncart(LB);
+    const int sa = (pure && LA == 2) ? 5 : NA, sb = (pure && LB == 2) ? 5 : NB;
+    for (int m = 0; m < sa; m++) {
+        for (int n = 0; n < sb; n++) {
+            double v1 = 0.0, v2 = 0.0;
+#pragma unroll
+            for (int ia = 0; ia < NA; ia++) {
+                const double tm = (pure && LA == 2) ? c_sph_d1[m][ia] : (m == ia ? 1.0 : 0.0);
+#pragma unroll
+                for (int ib = 0; ib < NB; ib++) {
+                    const double tn = (pure && LB == 2) ? c_sph_d1[n][ib] : (n == ib ? 1.0 : 0.0);
+                    v1 += tm * tn * c1[ia + NA * ib];
+                    if (c2) v2 += tm * tn * c2[ia + NA * ib];
+                }
+            }
+            const double v = c2 ? v1 + v2 : v1;
+            M[(size_t)(fa + m) * nbf + fb + n] = v;
+            if (mirror) M[(size_t)(fb + n) * nbf + fa + m] = v;
+        }
     }
 }
 
-__global__ void __launch_bounds__(128) k_onee(const int *__restrict__ sh_L, const int *__restrict__ sh_nprim,
-                                              const int *__restrict__ sh_pstart, const int *__restrict__ f_start,
-                                              const double *__restrict__ sh_xyz, const double *__restrict__ alpha,
-                                              const double *__restrict__ coef, const int *__restrict__ Z,
-                                              const double *__restrict__ atom_xyz, int ns, int natoms, int nbf,
-                                              int pure, double *__restrict__ S, double *__restrict__ H,
-                                              double *__restrict__ Tout, double *__restrict__ Vout)
+template <int LA, int LB, bool WANT_V>
+__global__ void __launch_bounds__(128)
+    k_onee(const OneePair *__restrict__ pairs, int npairs, const int *__restrict__ sh_nprim,
+           const int *__restrict__ sh_pstart, const int *__restrict__ f_start, const double *__restrict__ sh_xyz,
+           const double *__restrict__ alpha, const double *__restrict__ coef, const int *__restrict__ Z,
+           const double *__restrict__ atom_xyz, int natoms, int nbf, int pure, double *__restrict__ S,
+           double *__restrict__ H, double *__restrict__ Tout, double *__restrict__ Vout)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)ns * ns) return;
-    const int A = (int)(t / ns), B = (int)(t % ns);
-    const int LA = sh_L[A], LB = sh_L[B];
-    const int na = ncart(LA), nb = ncart(LB);
-    const double Ax = sh_xyz[3 * A], Ay = sh_xyz[3 * A + 1], Az = sh_xyz[3 * A + 2];
-    const double Bx = sh_xyz[3 * B], By = sh_xyz[3 * B + 1], Bz = sh_xyz[3 * B + 2];
-    const double R2 = (Ax - Bx) * (Ax - Bx) + (Ay - By) * (Ay - By) + (Az - Bz) * (Az - Bz);
-    double Sc[36], Tc[36], Vc[36];
-    for (int k = 0; k < 36; k++) {
+    constexpr int NA = ncart(LA), NB = ncart(LB), NR = (LA + LB) / 2 + 1;
+    __shared__ double s_t[4][NA * NB];  // the warp's T block, kept across the V loop
+    const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    if (w >= npairs) return;  // the same for every lane of the warp
+    const int A = pairs[w].a, B = pairs[w].b;
+    const double Ac[3] = {sh_xyz[3 * A], sh_xyz[3 * A + 1], sh_xyz[3 * A + 2]};
+    const double Bc[3] = {sh_xyz[3 * B], sh_xyz[3 * B + 1], sh_xyz[3 * B + 2]};
+    const double AB[3] = {Ac[0] - Bc[0], Ac[1] - Bc[1], Ac[2] - Bc[2]};
+    const double R2 = AB[0] * AB[0] + AB[1] * AB[1] + AB[2] * AB[2];
+    const int npa = sh_nprim[A], npb = sh_nprim[B], pa0 = sh_pstart[A], pb0 = sh_pstart[B];
+    const int npp = npa * npb;
+    const int fa = f_start[A], fb = f_start[B];
+    const bool mirror = A != B;
+
+    // S and T: lanes over primitive pairs
+    double Sc[NA * NB], Tc[NA * NB];
+#pragma unroll
+    for (int k = 0; k < NA * NB; k++) {
         Sc[k] = 0.0;
         Tc[k] = 0.0;
-        Vc[k] = 0.0;
     }
-    const int nroot = (LA + LB) / 2 + 1;
-    for (int i = 0; i < sh_nprim[A]; i++) {
-        for (int j = 0; j < sh_nprim[B]; j++) {
-            const double a = alpha[sh_pstart[A] + i], b = alpha[sh_pstart[B] + j];
-            const double p = a + b, ip = 1.0 / p;
-            const double K = coef[sh_pstart[A] + i] * coef[sh_pstart[B] + j] * exp(-a * b * ip * R2);
-            const double P[3] = {(a * Ax + b * Bx) * ip, (a * Ay + b * By) * ip, (a * Az + b * Bz) * ip};
-            const double PA[3] = {P[0] - Ax, P[1] - Ay, P[2] - Az};
-            const double PB[3] = {P[0] - Bx, P[1] - By, P[2] - Bz};
-            // 1-D overlap factors s[d][ia][jb], ia <= 2, jb <= 4 (Gauss-Hermite, exact)
-            double s[3][3][5];
-            const double rsp = rsqrt(p);
-            for (int d = 0; d < 3; d++) {
-                for (int ia = 0; ia <= LA; ia++)
-                    for (int jb = 0; jb <= LB + 2; jb++) s[d][ia][jb] = 0.0;
-                for (int k = 0; k < 4; k++) {
-                    const double x = c_gh_x[k] * rsp;
-                    const double xa = x + PA[d], xb = x + PB[d];
-                    double pa = 1.0;
-                    for (int ia = 0; ia <= LA; ia++) {
-                        double pb = 1.0;
-                        for (int jb = 0; jb <= LB + 2; jb++) {
-                            s[d][ia][jb] += c_gh_w[k] * pa * pb;
-                            pb *= xb;
-                        }
-                        pa *= xa;
+    for (int q = lane; q < npp; q += 32) {
+        const int i = q / npb, j = q - i * npb;
+        const double a = alpha[pa0 + i], b = alpha[pb0 + j];
+        const double p = a + b, ip = 1.0 / p;
+        const double K = coef[pa0 + i] * coef[pb0 + j] * exp(-a * b * ip * R2);
+        // 1-D overlap factors s[d][ia][jb] (4-point Gauss-Hermite, exact to degree 7)
+        double s[3][LA + 1][LB + 3];
+        const double rsp = rsqrt(p);
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const double P = (a * Ac[d] + b * Bc[d]) * ip;
+            const double PA = P - Ac[d], PB = P - Bc[d];
+#pragma unroll
+            for (int ia = 0; ia <= LA; ia++)
+#pragma unroll
+                for (int jb = 0; jb <= LB + 2; jb++) s[d][ia][jb] = 0.0;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const double x = c_gh_x[k] * rsp;
+                const double xa = x + PA, xb = x + PB;
+                double pa = 1.0;
+#pragma unroll
+                for (int ia = 0; ia <= LA; ia++) {
+                    double pb = 1.0;
+#pragma unroll
+                    for (int jb = 0; jb <= LB + 2; jb++) {
+                        s[d][ia][jb] += c_gh_w[k] * pa * pb;
+                        pb *= xb;
                     }
-                }
-                for (int ia = 0; ia <= LA; ia++)
-                    for (int jb = 0; jb <= LB + 2; jb++) s[d][ia][jb] *= rsp;
-            }
-            // nuclear attraction: Rys quadrature per nucleus
-            double V[36];
-            for (int k = 0; k < na * nb; k++) V[k] = 0.0;
-            for (int c = 0; c < natoms; c++) {
-                const double PC[3] = {P[0] - atom_xyz[3 * c], P[1] - atom_xyz[3 * c + 1], P[2] - atom_xyz[3 * c + 2]};
-                const double T = p * (PC[0] * PC[0] + PC[1] * PC[1] + PC[2] * PC[2]);
-                double u[3], w[3];
-                if (nroot == 1) nuclear_rys<1>(T, u, w);
-                else if (nroot == 2) nuclear_rys<2>(T, u, w);
-                else nuclear_rys<3>(T, u, w);
-                const double pref = -(double)Z[c] * 2.0 * M_PI * ip * K;
-                for (int r = 0; r < nroot; r++) {
-                    const double Bv = (1.0 - u[r]) * 0.5 * ip;
-                    double I1[3][3][3];  // [dim][ia][jb]
-                    for (int d = 0; d < 3; d++) {
-                        const double C = PA[d] - u[r] * PC[d];
-                        const double AB = (d == 0 ? Ax - Bx : d == 1 ? Ay - By : Az - Bz);
-                        double g[5];
-                        g[0] = 1.0;
-                        if (LA + LB >= 1) g[1] = C;
-                        for (int e = 1; e < LA + LB; e++) g[e + 1] = C * g[e] + e * Bv * g[e - 1];
-                        // transfer to (ia, jb): t(a, b+1) = t(a+1, b) + AB t(a, b)
-                        double tt[5][3];
-                        for (int e = 0; e <= LA + LB; e++) tt[e][0] = g[e];
-                        for (int jb = 0; jb < LB; jb++)
-                            for (int e = 0; e <= LA + LB - jb - 1; e++) tt[e][jb + 1] = tt[e + 1][jb] + AB * tt[e][jb];
-                        for (int ia = 0; ia <= LA; ia++)
-                            for (int jb = 0; jb <= LB; jb++) I1[d][ia][jb] = tt[ia][jb];
-                    }
-                    const double wr = w[r] * pref;
-                    for (int ib = 0; ib < nb; ib++)
-                        for (int ia = 0; ia < na; ia++)
-                            V[ia + na * ib] += wr * I1[0][cx_of(LA, ia)][cx_of(LB, ib)] *
-                                               I1[1][cy_of(LA, ia)][cy_of(LB, ib)] *
-                                               I1[2][cz_of(LA, ia)][cz_of(LB, ib)];
+                    pa *= xa;
                 }
             }
-            for (int ib = 0; ib < nb; ib++) {
-                const int bx = cx_of(LB, ib), by = cy_of(LB, ib), bz = cz_of(LB, ib);
-                for (int ia = 0; ia < na; ia++) {
-                    const int ax = cx_of(LA, ia), ay = cy_of(LA, ia), az = cz_of(LA, ia);
-                    const int ex[3] = {ax, ay, az}, eb[3] = {bx, by, bz};
-                    const double sv = s[0][ax][bx] * s[1][ay][by] * s[2][az][bz];
-                    double tv = 0.0;
-                    for (int d = 0; d < 3; d++) {
-                        const int ii = ex[d], jj = eb[d];
-                        double v = -2.0 * b * (2 * jj + 1) * s[d][ii][jj] + 4.0 * b * b * s[d][ii][jj + 2];
-                        if (jj >= 2) v += jj * (jj - 1) * s[d][ii][jj - 2];
-                        double o = 1.0;
-                        for (int e = 0; e < 3; e++)
-                            if (e != d) o *= s[e][ex[e]][eb[e]];
-                        tv += -0.5 * v * o;
-                    }
-                    Sc[ia + na * ib] += K * sv;
-                    Tc[ia + na * ib] += K * tv;
-                    Vc[ia + na * ib] += V[ia + na * ib];
+#pragma unroll
+            for (int ia = 0; ia <= LA; ia++)
+#pragma unroll
+                for (int jb = 0; jb <= LB + 2; jb++) s[d][ia][jb] *= rsp;
+        }
+#pragma unroll
+        for (int ib = 0; ib < NB; ib++) {
+#pragma unroll
+            for (int ia = 0; ia < NA; ia++) {
+                const int ex[3] = {cart_x(LA, ia), cart_y(LA, ia), cart_z(LA, ia)};
+                const int eb[3] = {cart_x(LB, ib), cart_y(LB, ib), cart_z(LB, ib)};
+                const double sv = s[0][ex[0]][eb[0]] * s[1][ex[1]][eb[1]] * s[2][ex[2]][eb[2]];
+                double tv = 0.0;
+#pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    const int ii = ex[d], jj = eb[d];
+                    double v = -2.0 * b * (2 * jj + 1) * s[d][ii][jj] + 4.0 * b * b * s[d][ii][jj + 2];
+                    if (jj >= 2) v += jj * (jj - 1) * s[d][ii][jj >= 2 ? jj - 2 : 0];
+                    double o = 1.0;
+#pragma unroll
+                    for (int e = 0; e < 3; e++)
+                        if (e != d) o *= s[e][ex[e]][eb[e]];
+                    tv += -0.5 * v * o;
                 }
+                Sc[ia + NA * ib] += K * sv;
+                Tc[ia + NA * ib] += K * tv;
             }
         }
     }
-    const int sa = (pure && LA == 2) ? 5 : na, sb = (pure && LB == 2) ? 5 : nb;
-    const int fa = f_start[A], fb = f_start[B];
-    for (int m = 0; m < sa; m++) {
-        for (int n = 0; n < sb; n++) {
-            double vs = 0.0, vt = 0.0, vv = 0.0;
-            for (int ia = 0; ia < na; ia++) {
-                const double tm = (pure && LA == 2) ? c_sph_d1[m][ia] : (m == ia ? 1.0 : 0.0);
-                if (tm == 0.0) continue;
-                for (int ib = 0; ib < nb; ib++) {
-                    const double tn = (pure && LB == 2) ? c_sph_d1[n][ib] : (n == ib ? 1.0 : 0.0);
-                    if (tn == 0.0) continue;
-                    vs += tm * tn * Sc[ia + na * ib];
-                    vt += tm * tn * Tc[ia + na * ib];
-                    vv += tm * tn * Vc[ia + na * ib];
-                }
+    warp_sum(Sc);
+    warp_sum(Tc);
+    if (lane == 0) {
+        if (S) onee_put<LA, LB>(Sc, nullptr, pure, fa, fb, nbf, mirror, S);
+        if (Tout) onee_put<LA, LB>(Tc, nullptr, pure, fa, fb, nbf, mirror, Tout);
+#pragma unroll
+        for (int k = 0; k < NA * NB; k++) s_t[wib][k] = Tc[k];
+    }
+    if constexpr (WANT_V) {
+        // V: lanes over (primitive pair, nucleus), Rys quadrature of 1/|r - C|
+        double Vc[NA * NB];
+#pragma unroll
+        for (int k = 0; k < NA * NB; k++) Vc[k] = 0.0;
+        const int nq = npp * natoms;
+        for (int q = lane; q < nq; q += 32) {
+            const int pp = q / natoms, c = q - pp * natoms;
+            const int i = pp / npb, j = pp - i * npb;
+            const double a = alpha[pa0 + i], b = alpha[pb0 + j];
+            const double p = a + b, ip = 1.0 / p;
+            const double K = coef[pa0 + i] * coef[pb0 + j] * exp(-a * b * ip * R2);
+            double PA[3], PC[3];
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                const double P = (a * Ac[d] + b * Bc[d]) * ip;
+                PA[d] = P - Ac[d];
+                PC[d] = P - atom_xyz[3 * c + d];
             }
-            const size_t o = (size_t)(fa + m) * nbf + fb + n;
-            if (S) S[o] = vs;
-            if (H) H[o] = vt + vv;
-            if (Tout) Tout[o] = vt;
-            if (Vout) Vout[o] = vv;
+            const double T = p * (PC[0] * PC[0] + PC[1] * PC[1] + PC[2] * PC[2]);
+            double u[NR], wt[NR];
+            rys_roots<NR>(T, u, wt, RysTab<double>::ptr(NR));
+            const double pref = -(double)Z[c] * 2.0 * M_PI * ip * K;
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                const double Bv = (1.0 - u[r]) * 0.5 * ip;
+                double I1[3][LA + 1][LB + 1];  // [dim][ia][jb]
+#pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    const double C = PA[d] - u[r] * PC[d];
+                    double g[LA + LB + 1];
+                    g[0] = 1.0;
+                    if (LA + LB >= 1) g[LA + LB >= 1 ? 1 : 0] = C;
+#pragma unroll
+                    for (int e = 1; e < LA + LB; e++) g[e + 1] = C * g[e] + e * Bv * g[e - 1];
+                    // transfer to (ia, jb): t(a, b+1) = t(a+1, b) + AB t(a, b)
+                    double tt[LA + LB + 1][LB + 1];
+#pragma unroll
+                    for (int e = 0; e <= LA + LB; e++) tt[e][0] = g[e];
+#pragma unroll
+                    for (int jb = 0; jb < LB; jb++)
+#pragma unroll
+                        for (int e = 0; e <= LA + LB - jb - 1; e++) tt[e][jb + 1] = tt[e + 1][jb] + AB[d] * tt[e][jb];
+#pragma unroll
+                    for (int ia = 0; ia <= LA; ia++)
+#pragma unroll
+                        for (int jb = 0; jb <= LB; jb++) I1[d][ia][jb] = tt[ia][jb];
+                }
+                const double wr = wt[r] * pref;
+#pragma unroll
+                for (int ib = 0; ib < NB; ib++)
+#pragma unroll
+                    for (int ia = 0; ia < NA; ia++)
+                        Vc[ia + NA * ib] += wr * I1[0][cart_x(LA, ia)][cart_x(LB, ib)] *
+                                            I1[1][cart_y(LA, ia)][cart_y(LB, ib)] *
+                                            I1[2][cart_z(LA, ia)][cart_z(LB, ib)];
+            }
+        }
+        warp_sum(Vc);
+        if (lane == 0) {
+            if (Vout) onee_put<LA, LB>(Vc, nullptr, pure, fa, fb, nbf, mirror, Vout);
+            if (H) {
+                double Tk[NA * NB];
+#pragma unroll
+                for (int k = 0; k < NA * NB; k++) Tk[k] = s_t[wib][k];
+                onee_put<LA, LB>(Tk, Vc, pure, fa, fb, nbf, mirror, H);
+            }
         }
     }
 }
@@ -204,6 +271,84 @@ __global__ void k_scale_cols(double *Y, const double *V, const double *w, int n)
         }                                                                               \
     } while (0)
 
+// class index of an oriented pair L(A) >= L(B): ss, ps, pp, ds, dp, dd
+static int onee_class(int la, int lb) { return la * (la + 1) / 2 + lb; }
+
+template <bool WANT_V>
+static void onee_launch_class(int cls, unsigned grid, cudaStream_t st, const OneePair *pairs, int n,
+                              const int *sh_nprim, const int *sh_pstart, const int *f_start,
+                              const double *sh_xyz, const double *alpha, const double *coef, const int *Z,
+                              const double *atom_xyz, int natoms, int nbf, int pure, double *S, double *H,
+                              double *T, double *V)
+{
+#define GTF_ONEE(LA, LB)                                                                                  \
+    k_onee<LA, LB, WANT_V><<<grid, 128, 0, st>>>(pairs, n, sh_nprim, sh_pstart, f_start, sh_xyz, alpha, \
+                                                 coef, Z, atom_xyz, natoms, nbf, pure, S, H, T, V)
+    switch (cls) {
+    case 0: GTF_ONEE(0, 0); break;
+    case 1: GTF_ONEE(1, 0); break;
+    case 2: GTF_ONEE(1, 1); break;
+    case 3: GTF_ONEE(2, 0); break;
+    case 4: GTF_ONEE(2, 1); break;
+    default: GTF_ONEE(2, 2); break;
+    }
+#undef GTF_ONEE
+}
+
+// S, H = T + V, T and V of the whole basis into the given device arrays (any
+// may be null; V is evaluated only when H or V is asked for).  One warp per
+// unordered shell pair, one launch per angular class pair, ordered on st.
+static int onee_matrices(gtf_fock_dev_t *f, cudaStream_t st, double *S, double *H, double *T, double *V)
+{
+    const int *sh_L, *sh_nprim, *sh_pstart, *f_start, *fc_start, *Z;
+    const double *sh_xyz, *alpha, *coef, *atom_xyz;
+    int ns, natoms, nbf, pure;
+    gtf_fock_basis_dev(f, &sh_L, &sh_nprim, &sh_pstart, &f_start, &fc_start, &sh_xyz, &alpha, &coef, &Z, &atom_xyz,
+                       &ns, &natoms, &nbf, &pure);
+    const int *hL = gtf_fock_shell_L_host(f);
+    // the unordered pairs grouped by class, each oriented L(a) >= L(b)
+    int count[6] = {0, 0, 0, 0, 0, 0};
+    for (int A = 0; A < ns; A++) {
+        if (hL[A] < 0 || hL[A] > 2) return GTF_ERR_INVALID;
+        for (int B = 0; B <= A; B++) count[onee_class(hL[A] > hL[B] ? hL[A] : hL[B], hL[A] > hL[B] ? hL[B] : hL[A])]++;
+    }
+    int start[7] = {0};
+    for (int c = 0; c < 6; c++) start[c + 1] = start[c] + count[c];
+    std::vector<OneePair> h(start[6]);
+    int fill[6];
+    for (int c = 0; c < 6; c++) fill[c] = start[c];
+    for (int A = 0; A < ns; A++)
+        for (int B = 0; B <= A; B++) {
+            const bool swap = hL[B] > hL[A];
+            const OneePair pr = swap ? OneePair{B, A} : OneePair{A, B};
+            h[fill[onee_class(hL[pr.a], hL[pr.b])]++] = pr;
+        }
+    OneePair *d = nullptr;
+    CKC(gtf_dmalloc((void **)&d, sizeof(OneePair) * h.size(), st));
+    CKC(cudaMemcpyAsync(d, h.data(), sizeof(OneePair) * h.size(), cudaMemcpyHostToDevice, st));
+    const bool want_v = H || V;
+    for (int c = 0; c < 6; c++) {
+        if (!count[c]) continue;
+        const unsigned grid = (unsigned)((count[c] + 3) / 4);  // 4 warps per block
+        if (want_v)
+            onee_launch_class<true>(c, grid, st, d + start[c], count[c], sh_nprim, sh_pstart, f_start, sh_xyz,
+                                    alpha, coef, Z, atom_xyz, natoms, nbf, pure, S, H, T, V);
+        else
+            onee_launch_class<false>(c, grid, st, d + start[c], count[c], sh_nprim, sh_pstart, f_start, sh_xyz,
+                                     alpha, coef, Z, atom_xyz, natoms, nbf, pure, S, H, T, V);
+    }
+    const cudaError_t e = cudaGetLastError();
+    gtf_dfree(d, st);
+    // h is read by the copy above: keep it until the stream has passed it
+    const cudaError_t e2 = cudaStreamSynchronize(st);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        fprintf(stderr, "gtfock_b200 one-electron kernels: %s\n",
+                cudaGetErrorString(e != cudaSuccess ? e : e2));
+        return GTF_ERR_CUDA;
+    }
+    return GTF_OK;
+}
+
 extern "C" int gtf_onee_compute(gtf_fock_dev_t *f, int want_sx, int want_h, double **S, double **X, double **H)
 {
     const int *sh_L, *sh_nprim, *sh_pstart, *f_start, *fc_start, *Z;
@@ -224,11 +369,10 @@ extern "C" int gtf_onee_compute(gtf_fock_dev_t *f, int want_sx, int want_h, doub
         if (!*H) CKC(gtf_dmalloc((void **)H, sizeof(double) * nn, st));
         dH = *H;
     }
-    const long long npair = (long long)ns * ns;
-    k_onee<<<(unsigned)((npair + 127) / 128), 128, 0, st>>>(sh_L, sh_nprim, sh_pstart, f_start, sh_xyz, alpha,
-                                                            coef, Z, atom_xyz, ns, natoms, nbf, pure, dS, dH,
-                                                            nullptr, nullptr);
-    CKC(cudaGetLastError());
+    {
+        const int e = onee_matrices(f, st, dS, dH, nullptr, nullptr);
+        if (e != GTF_OK) return e;
+    }
     if (want_sx) {
         if (!*X) CKC(gtf_dmalloc((void **)X, sizeof(double) * nn, st));
         SolverLease sl(st);
@@ -286,11 +430,13 @@ extern "C" int gtf_onee_full(gtf_fock_dev_t *f, double *S_host, double *T_host, 
     const size_t nn = (size_t)nbf * nbf;
     double *buf;
     CKC(gtf_dmalloc((void **)&buf, sizeof(double) * nn * 3, st));
-    const long long npair = (long long)ns * ns;
-    k_onee<<<(unsigned)((npair + 127) / 128), 128, 0, st>>>(sh_L, sh_nprim, sh_pstart, f_start, sh_xyz, alpha,
-                                                            coef, Z, atom_xyz, ns, natoms, nbf, pure, buf, nullptr,
-                                                            buf + nn, buf + 2 * nn);
-    CKC(cudaGetLastError());
+    {
+        const int e = onee_matrices(f, st, buf, nullptr, buf + nn, buf + 2 * nn);
+        if (e != GTF_OK) {
+            gtf_dfree(buf, st);
+            return e;
+        }
+    }
     if (S_host) CKC(cudaMemcpyAsync(S_host, buf, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
     if (T_host) CKC(cudaMemcpyAsync(T_host, buf + nn, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
     if (V_host) CKC(cudaMemcpyAsync(V_host, buf + 2 * nn, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));

@@ -47,11 +47,24 @@ purif_t *create_purif(BasisSet_t basis, int nprow_purif, int npcol_purif, int np
     p->meshsize = n * n;
     p->bmax_id = -1;
     const size_t bytes = sizeof(double) * (size_t)n * n;
-    p->H_block = (double *)calloc(1, bytes);
-    p->X_block = (double *)calloc(1, bytes);
-    p->S_block = (double *)calloc(1, bytes);
-    p->F_block = (double *)calloc(1, bytes);
-    p->D_block = (double *)calloc(1, bytes);
+    /* page-locked, so that every copy of a block to or from the device is a
+     * direct DMA; plain heap memory if the pinned blocks cannot be had */
+    double **blk[5] = {&p->H_block, &p->X_block, &p->S_block, &p->F_block, &p->D_block};
+    p->host_pinned = 1;
+    for (int k = 0; k < 5; k++) {
+        *blk[k] = (double *)gtf_pinned_alloc(bytes);
+        if (*blk[k] == NULL) {
+            p->host_pinned = 0;
+            break;
+        }
+        memset(*blk[k], 0, bytes);
+    }
+    if (!p->host_pinned) {
+        for (int k = 0; k < 5; k++) {
+            gtf_pinned_free(*blk[k]);
+            *blk[k] = (double *)calloc(1, bytes);
+        }
+    }
     if (!p->H_block || !p->X_block || !p->S_block || !p->F_block || !p->D_block) {
         destroy_purif(p);
         return NULL;
@@ -72,11 +85,13 @@ void destroy_purif(purif_t *p)
 {
     if (p == NULL) return;
     if (p->dev) gtf_purif_destroy((gtf_purif_dev_t *)p->dev);
-    free(p->H_block);
-    free(p->X_block);
-    free(p->S_block);
-    free(p->F_block);
-    free(p->D_block);
+    double *blk[5] = {p->H_block, p->X_block, p->S_block, p->F_block, p->D_block};
+    for (int k = 0; k < 5; k++) {
+        if (p->host_pinned)
+            gtf_pinned_free(blk[k]);
+        else
+            free(blk[k]);
+    }
     free(p);
 }
 

@@ -54,6 +54,7 @@ typedef struct _purif_t
     void *dev;
     int sx_uploaded;
     int last_iters;
+    int host_pinned;   /* the five blocks are page-locked (copied by DMA) */
 } purif_t;
 
 #ifdef __cplusplus
