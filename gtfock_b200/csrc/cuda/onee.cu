@@ -57,15 +57,18 @@ __device__ __forceinline__ void warp_sum(double (&v)[N])
 }
 
 // spherical (pure d) or Cartesian block of c1 (+ c2 when given) at rows
-// fa.., columns fb.., and at the mirrored place
+// fa.., columns fb.., and at the mirrored place.  A diagonal block (fa == fb)
+// is evaluated on and above its diagonal and mirrored, since the two
+// triangles of c1 agree only to rounding (contracted multiply-adds).
 template <int LA, int LB>
 __device__ __forceinline__ void onee_put(const double (&c1)[ncart(LA) * ncart(LB)], const double *c2, int pure,
-                                         int fa, int fb, int nbf, bool mirror, double *__restrict__ M)
+                                         int fa, int fb, int nbf, double *__restrict__ M)
 {
     constexpr int NA = ncart(LA), NB = ncart(LB);
     const int sa = (pure && LA == 2) ? 5 : NA, sb = (pure && LB == 2) ? 5 : NB;
+    const bool diag = fa == fb;
     for (int m = 0; m < sa; m++) {
-        for (int n = 0; n < sb; n++) {
+        for (int n = diag ? m : 0; n < sb; n++) {
             double v1 = 0.0, v2 = 0.0;
 #pragma unroll
             for (int ia = 0; ia < NA; ia++) {
@@ -79,7 +82,7 @@ __device__ __forceinline__ void onee_put(const double (&c1)[ncart(LA) * ncart(LB
             }
             const double v = c2 ? v1 + v2 : v1;
             M[(size_t)(fa + m) * nbf + fb + n] = v;
-            if (mirror) M[(size_t)(fb + n) * nbf + fa + m] = v;
+            M[(size_t)(fb + n) * nbf + fa + m] = v;
         }
     }
 }
@@ -105,7 +108,6 @@ __global__ void __launch_bounds__(128)
     const int npa = sh_nprim[A], npb = sh_nprim[B], pa0 = sh_pstart[A], pb0 = sh_pstart[B];
     const int npp = npa * npb;
     const int fa = f_start[A], fb = f_start[B];
-    const bool mirror = A != B;
 
     // S and T: lanes over primitive pairs
     double Sc[NA * NB], Tc[NA * NB];
@@ -178,8 +180,8 @@ __global__ void __launch_bounds__(128)
     warp_sum(Sc);
     warp_sum(Tc);
     if (lane == 0) {
-        if (S) onee_put<LA, LB>(Sc, nullptr, pure, fa, fb, nbf, mirror, S);
-        if (Tout) onee_put<LA, LB>(Tc, nullptr, pure, fa, fb, nbf, mirror, Tout);
+        if (S) onee_put<LA, LB>(Sc, nullptr, pure, fa, fb, nbf, S);
+        if (Tout) onee_put<LA, LB>(Tc, nullptr, pure, fa, fb, nbf, Tout);
 #pragma unroll
         for (int k = 0; k < NA * NB; k++) s_t[wib][k] = Tc[k];
     }
@@ -243,12 +245,12 @@ __global__ void __launch_bounds__(128)
         }
         warp_sum(Vc);
         if (lane == 0) {
-            if (Vout) onee_put<LA, LB>(Vc, nullptr, pure, fa, fb, nbf, mirror, Vout);
+            if (Vout) onee_put<LA, LB>(Vc, nullptr, pure, fa, fb, nbf, Vout);
             if (H) {
                 double Tk[NA * NB];
 #pragma unroll
                 for (int k = 0; k < NA * NB; k++) Tk[k] = s_t[wib][k];
-                onee_put<LA, LB>(Tk, Vc, pure, fa, fb, nbf, mirror, H);
+                onee_put<LA, LB>(Tk, Vc, pure, fa, fb, nbf, H);
             }
         }
     }
