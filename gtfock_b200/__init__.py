@@ -315,6 +315,8 @@ class PFock:
         fl = np.zeros(32)
         npq = np.zeros(32)
         n = load().gtf_pfock_class_work(self.h, _dptr(fl), _dptr(npq))
+        if n < 0:
+            raise GtfError("gtf_pfock_class_work failed (%d)" % n)
         return [(float(fl[i]), float(npq[i])) for i in range(n)]
 
     def class_work_screened(self):

