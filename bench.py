@@ -455,6 +455,49 @@ def profile_fock(args):
     print(json.dumps(out), flush=True)
 
 
+def run_setup(args):
+    """Set-up steps of one solve through the C API, in the order pscf/scf.c
+    calls them (basis, PFock_create, createOvlMat, createCoreHMat,
+    create_purif) and their tear-down, for C54H18 / cc-pVDZ and
+    (H2O)16 / 6-31G: the median of `steps` repeats after `warmup`, ms."""
+    import gtfock_b200 as gb
+    from gtfock_b200 import molecules as mol
+    L = gb.load()
+    out = {"workload": "set-up of one solve through the C API", "unit": "ms (median)", "molecules": []}
+    with tempfile.TemporaryDirectory() as td:
+        for name, atoms, bas in (("C54H18 / cc-pVDZ", mol.graphene_flake(2), "cc-pvdz"),
+                                 ("(H2O)16 / 6-31G", mol.water_cluster(16, 7), "6-31g")):
+            xyz = mol.write_xyz(atoms, os.path.join(td, "m.xyz"))
+            rows = {k: [] for k in ("basis", "PFock_create", "createOvlMat", "createCoreHMat", "create_purif",
+                                    "work_model", "destroy")}
+            nbf = 0
+            for k in range(args.warmup + args.steps):
+                t = [time.perf_counter()]
+                b = gb.BasisSet(mol.basis_file(bas), xyz)
+                t.append(time.perf_counter())
+                pf = gb.PFock(b, tolscr=TOL)
+                t.append(time.perf_counter())
+                L.PFock_createOvlMat(pf.h, b.h)
+                t.append(time.perf_counter())
+                L.PFock_createCoreHMat(pf.h, b.h)
+                t.append(time.perf_counter())
+                pr = gb.Purif(b)
+                t.append(time.perf_counter())
+                pf.timing()
+                t.append(time.perf_counter())
+                nbf = b.nbf
+                pr.close()
+                pf.close()
+                b.close()
+                t.append(time.perf_counter())
+                if k >= args.warmup:
+                    for key, a, z in zip(rows, t[:-1], t[1:]):
+                        rows[key].append(1e3 * (z - a))
+            out["molecules"].append({"molecule": name, "nbf": nbf,
+                                     **{k: round(statistics.median(v), 3) for k, v in rows.items()}})
+    print(json.dumps(out), flush=True)
+
+
 def run_c12h26(args):
     print(json.dumps(c12h26_measure(args.warmup, args.steps)), flush=True)
 
@@ -889,11 +932,12 @@ def main():
     ap.add_argument("--fp32-cutoff", type=float, default=None,
                     help="with --profile-fock: FP32 for quartets with Schwarz bound below this")
     ap.add_argument("--workload", choices=["default", "batched", "served", "served-tau", "precision", "c12h26",
-                                           "batch-scaling"], default="default",
+                                           "batch-scaling", "setup"], default="default",
                     help="batched / served / precision: the batched, served and precision-sweep workloads; "
                          "c12h26: the 10-iteration C12H26 solve timed beside the reference driver; "
                          "batch-scaling: large molecules in one batch against builds alone; "
-                         "served-tau: screening of the density change swept on one served request")
+                         "served-tau: screening of the density change swept on one served request; "
+                         "setup: the C-API set-up steps of one solve, timed one by one")
     ap.add_argument("--count", type=int, default=None, help="molecules (batched) or requests (served)")
     ap.add_argument("--seed", type=int, default=None)
     ap.add_argument("--rate", type=float, default=2.0, help="served: Poisson arrival rate (1/s)")
@@ -931,6 +975,9 @@ def main():
         return
     if args.workload == "batch-scaling":
         run_batch_scaling(args)
+        return
+    if args.workload == "setup":
+        run_setup(args)
         return
     if args.profile_purif:
         profile_purification(args)

@@ -219,10 +219,12 @@ class BasisSet:
         self.nocc = L.CInt_getNumOccOrb(self.h)
         self.enuc = L.CInt_getNucEnergy(self.h)
 
-    def __del__(self):
+    def close(self):
         if getattr(self, "h", None) is not None and _lib is not None:
             _lib.CInt_destroyBasisSet(self.h)
             self.h = None
+
+    __del__ = close
 
 
 class PFock:
