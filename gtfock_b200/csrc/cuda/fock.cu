@@ -546,6 +546,59 @@ __global__ void k_screen_prep(BasisDev b, const int2 *__restrict__ mn, const int
     make_pair(b, a, bb, off[t], 0, 0, pairs + t, pp, npp);
 }
 
+// Screening slices: the ket components cd = CD0 .. CD0+N-1 (cd = k + NA*l)
+// of the diagonal quartet (MN|MN) at a time, folded into the sums
+// s[m][n] = sum_{i,j,k,l} T[m][i] T[n][j] T[m][k] T[n][l] (ij|kl), so that no
+// thread holds all NA*NB*NA*NB integrals (1296 for (dd|dd)).
+__host__ __device__ constexpr int screen_slice_n(int LA, int LB)
+{
+    // whole quartets up to 81 integrals; else slices of at most 54
+    return ncart(LA) * ncart(LB) * ncart(LA) * ncart(LB) <= 81 ? ncart(LA) * ncart(LB)
+           : ncart(LA) * ncart(LB) * 3 <= 54                   ? 3
+                                                               : 1;
+}
+
+template <int LA, int LB, int CD0, int N>
+__device__ __forceinline__ void screen_slices(const PairRec &pr, const PPStored &src, int pure,
+                                              double (&s)[ncart(LA) * ncart(LB)])
+{
+    constexpr int NA = ncart(LA), NB = ncart(LB), NR = LA + LB + 1;
+    if constexpr (CD0 < NA * NB) {
+        double acc[NA * NB * N];
+#pragma unroll
+        for (int k = 0; k < NA * NB * N; k++) acc[k] = 0.0;
+        eri_accumulate_cd<LA, LB, LA, LB, CD0, N, false>(src, pr, src, pr, acc, RysTab<double>::ptr(NR));
+        const int sa = nsph_of(LA, pure), sb = nsph_of(LB, pure);
+#pragma unroll
+        for (int m = 0; m < NA; m++) {
+#pragma unroll
+            for (int n = 0; n < NB; n++) {
+                if (m >= sa || n >= sb) continue;
+                double v = 0.0;
+#pragma unroll
+                for (int t = 0; t < N; t++) {
+                    const int k = (CD0 + t) % NA, l = (CD0 + t) / NA;
+                    const double tk = sph_coef(LA, pure, m, k), tl = sph_coef(LB, pure, n, l);
+                    if (tk == 0.0 || tl == 0.0) continue;
+#pragma unroll
+                    for (int i = 0; i < NA; i++) {
+                        const double ti = sph_coef(LA, pure, m, i);
+                        if (ti == 0.0) continue;
+#pragma unroll
+                        for (int j = 0; j < NB; j++) {
+                            const double tj = sph_coef(LB, pure, n, j);
+                            if (tj == 0.0) continue;
+                            v += ti * tj * tk * tl * acc[i + NA * (j + NB * t)];
+                        }
+                    }
+                }
+                s[m * NB + n] += v;
+            }
+        }
+        screen_slices<LA, LB, CD0 + N, N>(pr, src, pure, s);
+    }
+}
+
 // max |(mn|mn)| over the diagonal of (MN|MN) in the basis's own functions
 // (pfock/screening.c:59-90), for the pairs of one class
 template <int LA, int LB>
@@ -558,36 +611,17 @@ __global__ void __launch_bounds__(64) k_screen(const PairRec *__restrict__ pairs
     if (t >= n) return;
     const PairRec pr = pairs[t];
     PPStored src{pp};
-    double acc[NA * NB * NA * NB];
+    double s[NA * NB];
 #pragma unroll
-    for (int k = 0; k < NA * NB * NA * NB; k++) acc[k] = 0.0;
-    eri_accumulate<LA, LB, LA, LB>(src, pr, src, pr, acc);
-    const int sa = (pure && LA == 2) ? 5 : NA;
-    const int sb = (pure && LB == 2) ? 5 : NB;
+    for (int k = 0; k < NA * NB; k++) s[k] = 0.0;
+    screen_slices<LA, LB, 0, screen_slice_n(LA, LB)>(pr, src, pure, s);
+    const int sa = nsph_of(LA, pure), sb = nsph_of(LB, pure);
     double mx = 0.0;
-    for (int m = 0; m < sa; m++) {
-        for (int n2 = 0; n2 < sb; n2++) {
-            double s = 0.0;
-            for (int i = 0; i < NA; i++) {
-                const double ti = sph_coef(LA, pure, m, i);
-                if (ti == 0.0) continue;
-                for (int k = 0; k < NA; k++) {
-                    const double tk = sph_coef(LA, pure, m, k);
-                    if (tk == 0.0) continue;
-                    for (int j = 0; j < NB; j++) {
-                        const double tj = sph_coef(LB, pure, n2, j);
-                        if (tj == 0.0) continue;
-                        for (int l = 0; l < NB; l++) {
-                            const double tl = sph_coef(LB, pure, n2, l);
-                            if (tl == 0.0) continue;
-                            s += ti * tj * tk * tl * acc[i + NA * (j + NB * (k + NA * l))];
-                        }
-                    }
-                }
-            }
-            if (fabs(s) > mx) mx = fabs(s);
-        }
-    }
+#pragma unroll
+    for (int m = 0; m < NA; m++)
+#pragma unroll
+        for (int n2 = 0; n2 < NB; n2++)
+            if (m < sa && n2 < sb && fabs(s[m * NB + n2]) > mx) mx = fabs(s[m * NB + n2]);
     const int M = mn[t].x, N = mn[t].y;
     sq[(size_t)M * ns + N] = mx;
     sq[(size_t)N * ns + M] = mx;
